@@ -1,0 +1,296 @@
+"""Initial models (the reference's GET_MODEL hooks) and named workloads.
+
+Each builder returns ``(spec, prim, eps)``:
+
+* ``spec`` -- a dict that :func:`cumc3d_b200.capi.make_config` turns into a
+  ``cumc_config`` (grid, flags, solver options, model descriptor);
+* ``prim`` -- float64 array of shape (nz+6, ny+6, nx+6, 8), the Fortran
+  ``prim(1:8,-2:nx+3,-2:ny+3,-2:nz+3)`` in memory order;
+* ``eps``  -- float64 array of shape (nz+6, ny+6, nx+6).
+
+Cells the reference's GET_MODEL leaves unset hold NaN in ``eps`` (its
+``epsilon`` array is never zeroed, solver/mhd/initial.f90:239-240 only zeroes
+``prim`` and ``cons``), so any read of an undefined value becomes visible.
+"""
+import math
+
+import numpy as np
+
+from .capi import IBX, IBY, IBZ, IRHO, ITAU, IVX, IVY, IVZ
+
+
+def faces(start, end, n):
+    """Uniform face coordinates for indices -3..n+3 (solver/mhd/getgrid.f90:26-34)."""
+    d = (end - start) / float(n)
+    j = np.arange(-3, n + 4, dtype=np.float64)
+    return start + j * d
+
+
+def centers(xf):
+    """Cell centres for indices -2..n+3 (solver/mhd/getgrid.f90:55-63)."""
+    return (xf[1:] + xf[:-1]) / 2.0
+
+
+def _alloc(nx, ny, nz):
+    prim = np.zeros((nz + 6, ny + 6, nx + 6, 8), dtype=np.float64)
+    eps = np.full((nz + 6, ny + 6, nx + 6), np.nan, dtype=np.float64)
+    return prim, eps
+
+
+def _base_spec(nx, ny, nz, n_dim, bflag, xr, yr, zr, **kw):
+    spec = dict(nx=nx, ny=ny, nz=nz, n_dim=n_dim, coordinate_flag=kw.pop("coordinate_flag", 0),
+                boundary_flag=list(bflag),
+                xF=faces(xr[0], xr[1], nx), yF=faces(yr[0], yr[1], ny), zF=faces(zr[0], zr[1], nz))
+    spec.update(kw)
+    return spec
+
+
+# ---------------------------------------------------------------------------
+# 1D Brio-Wu shock tube: model/riemann/src/riemann1d.f90:229-250 (test 10)
+# ---------------------------------------------------------------------------
+def brio_wu(nx=800, recon="ppm", riemann="hlld", cfl=0.8, precision="fp64"):
+    spec = _base_spec(nx, 1, 1, 1, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), (0.0, 1.0),
+                      cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      model=dict(gamma=2.0, floor="eps"), t_end=0.1,
+                      name="brio_wu_%d" % nx)
+    prim, eps = _alloc(nx, 1, 1)
+    g = 2.0
+    x = centers(spec["xF"])  # index -2..nx+3 -> position j+2
+    for j in range(0, nx + 1):
+        left = x[j + 2] <= 0.5
+        prim[:, :, j + 2, IRHO] = 1.0 if left else 0.125
+        prim[:, :, j + 2, ITAU] = 1.0 if left else 0.1
+        prim[:, :, j + 2, IBY] = 1.0 if left else -1.0
+        prim[:, :, j + 2, IBX] = 0.75
+        eps[:, :, j + 2] = prim[:, :, j + 2, ITAU] / prim[:, :, j + 2, IRHO] / (g - 1.0)
+    return spec, prim, eps
+
+
+# ---------------------------------------------------------------------------
+# 1D Riemann problem with arbitrary left/right states (the batched workload)
+# ---------------------------------------------------------------------------
+def riemann_1d(nx, left, right, bx, gamma=5.0 / 3.0, recon="ppm", riemann="hlld", cfl=0.8,
+               precision="fp64", t_end=0.1):
+    """left/right: dicts with rho, p, vx, vy, vz, by, bz.  Bx shared by both sides."""
+    spec = _base_spec(nx, 1, 1, 1, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), (0.0, 1.0),
+                      cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      model=dict(gamma=gamma, floor="eps"), t_end=t_end, name="riemann1d_%d" % nx)
+    prim, eps = _alloc(nx, 1, 1)
+    x = centers(spec["xF"])
+    for j in range(0, nx + 1):
+        s = left if x[j + 2] <= 0.5 else right
+        prim[:, :, j + 2, IRHO] = s["rho"]
+        prim[:, :, j + 2, ITAU] = s["p"]
+        prim[:, :, j + 2, IVX] = s["vx"]
+        prim[:, :, j + 2, IVY] = s["vy"]
+        prim[:, :, j + 2, IVZ] = s["vz"]
+        prim[:, :, j + 2, IBY] = s["by"]
+        prim[:, :, j + 2, IBZ] = s["bz"]
+        prim[:, :, j + 2, IBX] = bx
+        eps[:, :, j + 2] = s["p"] / s["rho"] / (gamma - 1.0)
+    return spec, prim, eps
+
+
+def batch_problems(n_problems=512, seed=20261203, nmin=128, nmax=4096):
+    """Seeded parameters of the batched workload (one 1D Riemann problem each)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n_problems):
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        sides = []
+        for _s in range(2):
+            sides.append(dict(
+                rho=float(math.exp(rng.uniform(math.log(0.1), math.log(10.0)))),
+                p=float(math.exp(rng.uniform(math.log(0.01), math.log(10.0)))),
+                vx=float(rng.uniform(-1, 1)), vy=float(rng.uniform(-1, 1)), vz=float(rng.uniform(-1, 1)),
+                by=float(rng.uniform(-2, 2)), bz=float(rng.uniform(-2, 2))))
+        bx = float(rng.uniform(-1, 1))
+        out.append(dict(n=n, left=sides[0], right=sides[1], bx=bx))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# 3D MHD blast: the 3D analogue of model/riemann/src/riemann2d.f90:522-544
+# ---------------------------------------------------------------------------
+def blast_3d(n=256, recon="weno", riemann="hlld", cfl=0.4, precision="fp64", nx=None, ny=None, nz=None,
+             radius=0.1):
+    nx = nx or n
+    ny = ny or n
+    nz = nz or n
+    spec = _base_spec(nx, ny, nz, 3, (0, 0, 0, 0, 0, 0), (-0.5, 0.5), (-0.5, 0.5), (-0.5, 0.5),
+                      cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      model=dict(gamma=5.0 / 3.0, floor="eps"), steps=200,
+                      name="blast3d_%dx%dx%d" % (nx, ny, nz))
+    g = 5.0 / 3.0
+    x = centers(spec["xF"])
+    y = centers(spec["yF"])
+    z = centers(spec["zF"])
+    r = np.sqrt(z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2)
+    prim = np.zeros((nz + 6, ny + 6, nx + 6, 8), dtype=np.float64)
+    prim[..., IRHO] = 1.0
+    prim[..., ITAU] = np.where(r <= radius, 10.0, 0.1)
+    b0 = 1.0 / math.sqrt(2.0)
+    prim[..., IBX] = b0
+    prim[..., IBY] = b0
+    eps = prim[..., ITAU] / prim[..., IRHO] / (g - 1.0)
+    return spec, prim, np.ascontiguousarray(eps)
+
+
+# ---------------------------------------------------------------------------
+# 3D circularly polarised Alfven wave along (1,1,1)/sqrt(3)
+# ---------------------------------------------------------------------------
+def alfven_3d(n=256, recon="ppm", riemann="hlld", cfl=0.4, precision="fp64", amp=0.1,
+              fix_periodic_normal_faces=1):
+    """Face B from an edge-centred vector potential, so div B = 0 to roundoff.
+
+    Wave vector k = 2*pi*(1,1,1) on the unit periodic box (wavelength 1/sqrt3).
+    B = B_par e1 + amp (cos(phase) e2 + sin(phase) e3), v = -amp/sqrt(rho) (...)
+    with e1 = (1,1,1)/sqrt3 the propagation direction.
+    """
+    spec = _base_spec(n, n, n, 3, (0, 0, 0, 0, 0, 0), (0.0, 1.0), (0.0, 1.0), (0.0, 1.0),
+                      cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      fix_periodic_normal_faces=fix_periodic_normal_faces,
+                      model=dict(gamma=5.0 / 3.0, floor="eps"), name="alfven3d_%d" % n)
+    g = 5.0 / 3.0
+    rho0, p0, bpar = 1.0, 0.1, 1.0
+    kk = 2.0 * math.pi
+    e1 = np.array([1.0, 1.0, 1.0]) / math.sqrt(3.0)
+    e2 = np.array([1.0, -1.0, 0.0]) / math.sqrt(2.0)
+    e3 = np.cross(e1, e2)
+    xF, yF, zF = spec["xF"], spec["yF"], spec["zF"]
+    xc, yc, zc = centers(xF), centers(yF), centers(zF)
+    kvec = kk * np.array([1.0, 1.0, 1.0])
+    kmag = np.linalg.norm(kvec)
+
+    # vector potential A = B_par/2 (e1 x r) + amp/|k| (sin(phase) e2 + cos(phase) e3) gives
+    # curl A = B_par e1 + amp (cos(phase) e2 + sin(phase) e3) (uniform part via the first term)
+    def A(px, py, pz):
+        phase = kvec[0] * px + kvec[1] * py + kvec[2] * pz
+        r = np.stack(np.broadcast_arrays(px, py, pz), axis=-1)
+        uni = 0.5 * bpar * np.cross(e1, r)
+        wav = (amp / kmag) * (np.sin(phase)[..., None] * e2 + np.cos(phase)[..., None] * e3)
+        return uni + wav
+
+    prim = np.zeros((n + 6, n + 6, n + 6, 8), dtype=np.float64)
+    Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+    phase = kvec[0] * X + kvec[1] * Y + kvec[2] * Z
+    bperp = amp * (np.cos(phase)[..., None] * e2 + np.sin(phase)[..., None] * e3)
+    vperp = -bperp / math.sqrt(rho0)
+    prim[..., IRHO] = rho0
+    prim[..., ITAU] = p0
+    prim[..., IVX] = vperp[..., 0]
+    prim[..., IVY] = vperp[..., 1]
+    prim[..., IVZ] = vperp[..., 2]
+    # face B = (1/area) * circulation of A around the face (edge midpoints, Stokes)
+    # x-face at (xF[j], y-center, z-center): Bx = (Az(y+)-Az(y-))/dy - (Ay(z+)-Ay(z-))/dz
+    dy = yF[1:] - yF[:-1]
+    dz = zF[1:] - zF[:-1]
+    dx = xF[1:] - xF[:-1]
+    ZC, YC, XF = np.meshgrid(zc, yc, xF[1:], indexing="ij")
+    Ap = A(XF, YC + 0.5 * dy[None, :, None], ZC)
+    Am = A(XF, YC - 0.5 * dy[None, :, None], ZC)
+    Bp = A(XF, YC, ZC + 0.5 * dz[:, None, None])
+    Bm = A(XF, YC, ZC - 0.5 * dz[:, None, None])
+    prim[..., IBX] = (Ap[..., 2] - Am[..., 2]) / dy[None, :, None] - (Bp[..., 1] - Bm[..., 1]) / dz[:, None, None]
+    ZC, YF_, XC = np.meshgrid(zc, yF[1:], xc, indexing="ij")
+    Ap = A(XC, YF_, ZC + 0.5 * dz[:, None, None])
+    Am = A(XC, YF_, ZC - 0.5 * dz[:, None, None])
+    Bp = A(XC + 0.5 * dx[None, None, :], YF_, ZC)
+    Bm = A(XC - 0.5 * dx[None, None, :], YF_, ZC)
+    prim[..., IBY] = (Ap[..., 0] - Am[..., 0]) / dz[:, None, None] - (Bp[..., 2] - Bm[..., 2]) / dx[None, None, :]
+    ZF_, YC, XC = np.meshgrid(zF[1:], yc, xc, indexing="ij")
+    Ap = A(XC + 0.5 * dx[None, None, :], YC, ZF_)
+    Am = A(XC - 0.5 * dx[None, None, :], YC, ZF_)
+    Bp = A(XC, YC + 0.5 * dy[None, :, None], ZF_)
+    Bm = A(XC, YC - 0.5 * dy[None, :, None], ZF_)
+    prim[..., IBZ] = (Ap[..., 1] - Am[..., 1]) / dx[None, None, :] - (Bp[..., 0] - Bm[..., 0]) / dy[None, :, None]
+    eps = prim[..., ITAU] / prim[..., IRHO] / (g - 1.0)
+    vA = bpar / math.sqrt(rho0)
+    spec["t_end"] = (1.0 / math.sqrt(3.0)) / vA  # one wave period
+    return spec, prim, np.ascontiguousarray(eps)
+
+
+# ---------------------------------------------------------------------------
+# magnetised torus in cylindrical coordinates (model/torus-cyn/src/model.f90)
+# ---------------------------------------------------------------------------
+def torus_cyl(nr=192, nphi=128, nz=192, r_range=(2.0, 42.0), z_range=(-20.0, 20.0), recon="weno",
+              riemann="hlld", cfl=0.4, precision="fp64", learned=0, seed=20261203, s_in=6.0, s_max=10.0,
+              rho_atm=1e-6, p_atm=1e-8, rho_cut=0.2, beta_min=100.0, noise=0.01, r_sh=0.0):
+    """Constant-angular-momentum (q=2) polytrope, n=1.5, around GM=1.
+
+    Follows GET_MODEL of model/torus-cyn/src/model.f90:6-315 with r_sh=0
+    (Newtonian), A_phi proportional to max(rho - rho_cut, 0), the field scaled
+    to the minimum plasma beta, and seeded pressure noise.
+    """
+    g = 5.0 / 3.0
+    q = 2.0
+    spec = _base_spec(nr, nphi, nz, 3, (1, 1, 0, 0, 1, 1), r_range, (0.0, 2.0 * math.pi), z_range,
+                      coordinate_flag=1, cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      learned=learned, steps=2000, name="torus_cyl_%dx%dx%d" % (nr, nphi, nz))
+    xF, yF, zF = spec["xF"], spec["yF"], spec["zF"]
+    x, z = centers(xF), centers(zF)
+    dx = xF[1:] - xF[:-1]
+    dz = zF[1:] - zF[:-1]
+
+    def phi_g(r, zz):
+        return -1.0 / (np.sqrt(r * r + zz * zz) - r_sh)
+
+    lkep2 = s_max ** (2.0 * q - 1.0) / (s_max - r_sh) ** 2
+    c_const = phi_g(s_in, 0.0) - lkep2 * s_in ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q)
+    h_max = -phi_g(s_max, 0.0) + lkep2 * s_max ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q) + c_const
+    k_poly = h_max * (g - 1.0) / g
+    R2, Z2 = np.meshgrid(x, z, indexing="xy")  # shape (nz+6, nr+6)
+    enth = -phi_g(R2, Z2) + lkep2 * R2 ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q) + c_const
+    enth = np.maximum(enth, 0.0)
+    rho_t = (enth * (g - 1.0) / g / k_poly) ** (1.0 / (g - 1.0))
+    inside = (rho_t > rho_atm) & (R2 >= s_in)
+    rho2 = np.where(inside, rho_t, rho_atm)
+    p2 = np.where(inside, k_poly * rho_t ** g, p_atm)
+    vphi2 = np.where(inside, np.sqrt(lkep2) * R2 ** (-q) * R2, 0.0)
+    prim = np.zeros((nz + 6, nphi + 6, nr + 6, 8), dtype=np.float64)
+    prim[..., IRHO] = rho2[:, None, :]
+    prim[..., ITAU] = p2[:, None, :]
+    prim[..., IVY] = vphi2[:, None, :]
+    # vector potential at cell centres, corners, then face B (model.f90:117-226)
+    a_phi = np.maximum(rho2 - rho_cut, 0.0)
+
+    def face_b(a_ph):
+        a_c = np.zeros_like(a_ph)
+        a_c[:-1, :-1] = 0.25 * (a_ph[:-1, :-1] + a_ph[:-1, 1:] + a_ph[1:, :-1] + a_ph[1:, 1:])
+        bx = np.zeros_like(a_ph)
+        bz = np.zeros_like(a_ph)
+        bx[1:, :] = -(a_c[1:, :] - a_c[:-1, :]) / dz[1:, None]
+        bz[:, 1:] = (xF[None, 2:] * a_c[:, 1:] - xF[None, 1:-1] * a_c[:, :-1]) / (x[None, 1:] * dx[None, 1:])
+        return bx, bz
+
+    bx, bz = face_b(a_phi)
+    bxc = np.zeros_like(bx)
+    bxc[:, 1:] = (xF[None, 2:] * bx[:, 1:] + xF[None, 1:-1] * bx[:, :-1]) / (xF[None, 2:] + xF[None, 1:-1])
+    bzc = np.zeros_like(bz)
+    bzc[1:, :] = 0.5 * (bz[1:, :] + bz[:-1, :])
+    b2 = bxc ** 2 + bzc ** 2
+    sel = (b2 > 0) & inside
+    beta = np.min(2.0 * p2[sel] / b2[sel]) if np.any(sel) else 1.0
+    b0 = math.sqrt(beta / beta_min)
+    bx, bz = face_b(a_phi * b0)
+    prim[..., IBX] = bx[:, None, :]
+    prim[..., IBZ] = bz[:, None, :]
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pert = 1.0 + noise * (rng.random(prim.shape[:3]) - 0.5) / 0.5
+    prim[..., ITAU] = np.where(inside[:, None, :], prim[..., ITAU] * pert, prim[..., ITAU])
+    eps = prim[..., ITAU] / prim[..., IRHO] / (g - 1.0)
+    eps_floor = p_atm / rho_atm / (g - 1.0)
+    spec["model"] = dict(gamma=g, floor="torus", rho_floor=rho_atm, eps_floor=eps_floor, p_floor=p_atm,
+                         source="pm_cyl", r_sh=r_sh, bc="torus_cyl")
+    return spec, prim, np.ascontiguousarray(eps)
+
+
+# ---------------------------------------------------------------------------
+# named workloads
+# ---------------------------------------------------------------------------
+WORKLOADS = {
+    "brio_wu": brio_wu,
+    "blast3d": blast_3d,
+    "alfven3d": alfven_3d,
+    "torus_cyl": torus_cyl,
+}

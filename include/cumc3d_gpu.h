@@ -1,0 +1,172 @@
+/*
+ * cumc3d_gpu.h -- C-ABI of the B200 (sm_100a) finite-volume MHD stage engine.
+ *
+ * This is the drop-in boundary for the per-timestep update of CUMC3D
+ * (leon-astrophy/cumc3d, solver/mhd).  The reference's Fortran main loop
+ *
+ *     CALL initial_update                      (solver/mhd/initial.f90:86-116)
+ *     DO while (global_time < total_time)      (solver/mhd/main.f90:98-139)
+ *        CALL finddt                           (solver/mhd/rungekutta.f90:221-332)
+ *        IF (global_time + dt > total_time) dt = total_time - global_time
+ *        CALL rungekutta(n_step)               (solver/mhd/rungekutta.f90:12-208)
+ *     END DO
+ *
+ * becomes a sequence of calls on one opaque handle.  Every entry point is a
+ * plain C function taking plain pointers and sizes; nothing here depends on
+ * PyTorch or on CUDA headers.  All calls return 0 on success and a non-zero
+ * CUMC_E* code on failure; cumc_last_error() gives the message.  A handle
+ * owns its device buffers and one CUDA stream, and must not be shared between
+ * host threads.  There is no CPU fallback: when no CUDA device is present
+ * cumc_create fails with CUMC_ECUDA.
+ *
+ * Array layout exchanged with the host is the reference's Fortran layout:
+ *   prim(imin:imax, -2:nx+3, -2:ny+3, -2:nz+3)   column-major, imax = 8
+ *   epsilon(-2:nx+3, -2:ny+3, -2:nz+3)
+ * i.e. a flat double array with the variable index fastest, then x, y, z.
+ * Variable order is (rho, vx, vy, vz, p, Bx_face, By_face, Bz_face) as set up
+ * by SETUP_EQNS (solver/mhd/setup.f90:39-90).
+ */
+#ifndef CUMC3D_GPU_H
+#define CUMC3D_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- status codes ---------------- */
+#define CUMC_OK          0
+#define CUMC_EINVAL      1   /* bad argument or unsupported configuration      */
+#define CUMC_ECUDA       2   /* CUDA runtime error / no device                 */
+#define CUMC_ENOMEM      3   /* device allocation failed                       */
+#define CUMC_ESTATE      4   /* non-finite or non-positive state found (guard) */
+#define CUMC_ENOTREADY   5   /* call order violated (e.g. step before state)   */
+
+/* ---------------- option enums ---------------- */
+/* reconstruction, solver/mhd/parameter.h:102-115 */
+#define CUMC_RECON_TVD_MM 0
+#define CUMC_RECON_TVD_VL 1
+#define CUMC_RECON_TVD_MC 2
+#define CUMC_RECON_PPM    3
+#define CUMC_RECON_WENO   4
+/* Riemann solver, solver/mhd/parameter.h:90-100 */
+#define CUMC_RS_LF   0
+#define CUMC_RS_HLL  1
+#define CUMC_RS_HLLC 2
+#define CUMC_RS_HLLD 3
+/* arithmetic form */
+#define CUMC_FP64 0   /* plain: FP64 end to end                                  */
+#define CUMC_FP32 1   /* FP32 reconstruction + Riemann flux, FP64 elsewhere      */
+/* per-stage floors (CUSTOM_CHECKRHO + FINDPRESSURE of the model) */
+#define CUMC_FLOOR_NONE  0
+#define CUMC_FLOOR_EPS   1   /* model/riemann/src/custom.f90:260-284          */
+#define CUMC_FLOOR_TORUS 2   /* model/torus-cyn/src/custom.f90:240-275,
+                                model/torus-cyn/src/findpressure.f90:7-37    */
+/* model source terms (CUSTOM_SOURCE) */
+#define CUMC_SRC_NONE     0
+#define CUMC_SRC_CONST_GY 1  /* model/riemann/src/custom.f90:289-316          */
+#define CUMC_SRC_PM_CYL   2  /* model/torus-cyn/src/custom.f90:280-320        */
+#define CUMC_SRC_PM_SPH   3  /* model/torus-sph/src/custom.f90 (radial form)  */
+/* model boundary hooks (CUSTOM_BOUNDARY_X/Y/Z) */
+#define CUMC_BC_NONE      0
+#define CUMC_BC_TORUS_CYL 1  /* model/torus-cyn/src/custom.f90:146-208        */
+#define CUMC_BC_TORUS_SPH 2  /* model/torus-sph/src/custom.f90 (x clamp only) */
+
+/* Model descriptor: replaces the per-stage device hooks each reference model
+ * links in (EOS, floors, sources, custom boundaries; SURVEY layer L6). */
+typedef struct cumc_model {
+    double gamma;        /* ggas: ideal-gas adiabatic index                       */
+    int    floor_kind;   /* CUMC_FLOOR_*                                          */
+    double rho_floor;    /* torus floor: rho_floor, eps_floor, p_floor            */
+    double eps_floor;
+    double p_floor;
+    int    source_kind;  /* CUMC_SRC_*                                            */
+    double g_const;      /* constant gravity magnitude for CUMC_SRC_CONST_GY (0.1) */
+    double r_sh;         /* pseudo-Newtonian radius for point-mass gravity        */
+    int    bc_kind;      /* CUMC_BC_*                                             */
+} cumc_model;
+
+/* Solver configuration: the compile-time PARAMETERs of solver/mhd/parameter.h
+ * moved to run time, plus the face coordinates CUSTOM_GRID/GETGRID produce. */
+typedef struct cumc_config {
+    int nx, ny, nz;              /* interior zones (ny = nz = 1 for 1D)           */
+    int n_dim;                   /* 1, 2 or 3                                     */
+    int coordinate_flag;         /* 0 Cartesian, 1 cylindrical, 2 spherical       */
+    int boundary_flag[6];        /* xin xout yin yout zin zout: 0 periodic,
+                                    1 outflow, 2 reflect, 3 axis, 4 equator       */
+    const double *xF;            /* face coordinates, indices -3..nx+3 (nx+7)     */
+    const double *yF;            /* indices -3..ny+3 (ny+7)                       */
+    const double *zF;            /* indices -3..nz+3 (nz+7)                       */
+    double cfl;                  /* Courant number                                */
+    int recon;                   /* CUMC_RECON_*                                  */
+    int riemann;                 /* CUMC_RS_*                                     */
+    int precision;               /* CUMC_FP64 / CUMC_FP32                         */
+    int learned;                 /* 1: learned smooth-face flag in WENO (FP32 form)*/
+    int fixpole;                 /* -DFIXPOLE: axis EMF average (spherical only)  */
+    int fix_periodic_normal_faces; /* 0 = reference behaviour (see DESIGN)        */
+    cumc_model model;
+} cumc_config;
+
+typedef struct cumc_handle cumc_handle;
+
+/* ---------------- lifecycle ----------------
+ * cumc_create replaces BUILD_HYDRO/BUILD_MHD/BUILD_RIEMANN/GETGRID/{TVD,PPM,WENO}_WEIGHT
+ * and POPULATE_DEVICE (solver/mhd/initial.f90:7-78, setup.f90:340-395,
+ * getgrid.f90:13-168, openacc.f90:5-24).  Boundary-flag combinations the
+ * reference rejects with STOP (setup.f90:111-325) return CUMC_EINVAL. */
+int cumc_create(const cumc_config *cfg, cumc_handle **out);
+/* replaces CLEAR_DEVICE (solver/mhd/openacc.f90:30-47) */
+int cumc_destroy(cumc_handle *h);
+
+/* Upload/download the primitive state in the Fortran layout described above.
+ * set_state is what GET_MODEL leaves behind (solver/mhd/initial.f90:68-74);
+ * get_state is the !$ACC UPDATE HOST(prim, epsilon) of dataio.f90:25-27. */
+int cumc_set_state(cumc_handle *h, const double *prim, const double *eps);
+int cumc_get_state(cumc_handle *h, double *prim, double *eps);
+
+/* Download one internal array in Fortran layout (diagnostics and tests).
+ * which: 0 cons(8,...), 1 bcell(3,...), 2 cs(...), 3 u_old(8,...) */
+#define CUMC_ARR_CONS  0
+#define CUMC_ARR_BCELL 1
+#define CUMC_ARR_CS    2
+int cumc_get_array(cumc_handle *h, int which, double *out, size_t n_doubles);
+
+/* INITIAL_UPDATE: CUSTOM_CHECKRHO -> FROMRVETOU -> BOUNDARY -> UPDATE(0)
+ * (solver/mhd/initial.f90:86-116). */
+int cumc_initial_update(cumc_handle *h);
+
+/* FINDDT (solver/mhd/rungekutta.f90:221-332): CFL step, min-reduced on the
+ * device.  Copies dt back to the host. */
+int cumc_finddt(cumc_handle *h, double *dt);
+
+/* RUNGEKUTTA (solver/mhd/rungekutta.f90:12-208) with the given dt. */
+int cumc_rk3_step(cumc_handle *h, double dt);
+
+/* The main loop of solver/mhd/main.f90:98-139 on the device: repeat
+ * FINDDT, clamp to t_end, RUNGEKUTTA, t += dt, until t >= t_end or
+ * max_steps steps were taken.  dt never leaves the device; steps are
+ * replayed from a captured CUDA graph.  *t_inout is the simulation time
+ * before and after; *steps_out the number of steps taken. */
+int cumc_evolve(cumc_handle *h, double t_end, int max_steps,
+                double *t_inout, int *steps_out);
+
+/* FIND_DIVB (solver/mhd/mhd_module.f90:110-201): max |div B| over the
+ * interior from the face fields. */
+int cumc_max_divb(cumc_handle *h, double *max_divb);
+
+/* Synchronise the handle's stream (for timing). */
+int cumc_sync(cumc_handle *h);
+
+/* Number of kernel launches the handle issued since creation. */
+int64_t cumc_launch_count(cumc_handle *h);
+
+/* Message of the last failed call on this handle (or of the last failed
+ * cumc_create when h is NULL). */
+const char *cumc_last_error(cumc_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUMC3D_GPU_H */

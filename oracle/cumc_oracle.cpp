@@ -1,0 +1,1413 @@
+/*
+ * cumc_oracle.cpp -- CPU restatement of CUMC3D's per-timestep MHD update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle for the B200
+ * engine in cumc3d_b200/csrc.  It is built into oracle/_build/liboracle*.so
+ * and is loaded only by tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * reference legs of bench.py.  The product never links or calls it.
+ *
+ * PARITY UNPINNED: the reference (Fortran 90 + OpenACC, leon-astrophy/cumc3d)
+ * cannot be compiled in this environment (no Fortran compiler, no HDF5) and
+ * ships no tests, golden vectors or fixtures for this path.  This restatement
+ * therefore follows the Fortran routine by routine, loop by loop, in the same
+ * floating-point operation order (Fortran left-to-right evaluation, x**2 as
+ * x*x), and is checked by invariants instead of reference outputs
+ * (tests/test_oracle_invariants.py).
+ *
+ * Layout mirrors the reference: prim(imin:imax,-2:nx+3,-2:ny+3,-2:nz+3) with
+ * the variable index fastest.  All arrays start as NaN so that any read of a
+ * value the reference leaves undefined shows up in the checked outputs.
+ *
+ * The scalar type is a template parameter: `double` for parity and timing,
+ * `CReal` (a counting double) for exact operation counts per zone-update.
+ *
+ * Reference files cited below are paths inside leon-astrophy/cumc3d.
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdio>
+#include <limits>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "../include/cumc3d_gpu.h"
+
+namespace orc {
+
+/* ------------------------------------------------------------------ */
+/* scalar types                                                        */
+/* ------------------------------------------------------------------ */
+struct OpCounts { uint64_t add = 0, mul = 0, div = 0, sqrt = 0, cmp = 0; };
+static OpCounts g_ops;
+
+struct CReal {
+    double v;
+    CReal() : v(0.0) {}
+    CReal(double x) : v(x) {}
+    explicit operator double() const { return v; }
+};
+inline CReal operator+(CReal a, CReal b) { g_ops.add++; return CReal(a.v + b.v); }
+inline CReal operator-(CReal a, CReal b) { g_ops.add++; return CReal(a.v - b.v); }
+inline CReal operator*(CReal a, CReal b) { g_ops.mul++; return CReal(a.v * b.v); }
+inline CReal operator/(CReal a, CReal b) { g_ops.div++; return CReal(a.v / b.v); }
+inline CReal operator-(CReal a) { return CReal(-a.v); }
+inline bool operator<(CReal a, CReal b) { g_ops.cmp++; return a.v < b.v; }
+inline bool operator>(CReal a, CReal b) { g_ops.cmp++; return a.v > b.v; }
+inline bool operator<=(CReal a, CReal b) { g_ops.cmp++; return a.v <= b.v; }
+inline bool operator>=(CReal a, CReal b) { g_ops.cmp++; return a.v >= b.v; }
+inline bool operator==(CReal a, CReal b) { g_ops.cmp++; return a.v == b.v; }
+
+inline double dv(double x) { return x; }
+inline double dv(CReal x) { return x.v; }
+
+inline double sqrt_(double x) { return std::sqrt(x); }
+inline CReal sqrt_(CReal x) { g_ops.sqrt++; return CReal(std::sqrt(x.v)); }
+inline double abs_(double x) { return std::fabs(x); }
+inline CReal abs_(CReal x) { return CReal(std::fabs(x.v)); }
+/* Fortran SIGN(1.0D0, x): magnitude 1 with the sign bit of x */
+inline double sign1_(double x) { return std::copysign(1.0, x); }
+inline CReal sign1_(CReal x) { return CReal(std::copysign(1.0, x.v)); }
+template <class R> inline R min_(R a, R b) { return (b < a) ? b : a; }
+template <class R> inline R max_(R a, R b) { return (b > a) ? b : a; }
+template <class R> inline R min3_(R a, R b, R c) { return min_(min_(a, b), c); }
+template <class R> inline R max3_(R a, R b, R c) { return max_(max_(a, b), c); }
+
+/* variable indices, solver/mhd/setup.f90:39-96 (no custom equations) */
+enum { irho = 1, ivx = 2, ivy = 3, ivz = 4, itau = 5, ibx = 6, iby = 7, ibz = 8 };
+enum { imin = 1, imax = 8, iex = 9, iey = 10, iez = 11 };
+/* face EMF indices, solver/mhd/mhd_module.f90:19-24 */
+enum { iyx = 1, izx = 2, ixy = 3, izy = 4, ixz = 5, iyz = 6 };
+enum { x_dir = 1, y_dir = 2, z_dir = 3 };
+
+static const double kNaN = std::numeric_limits<double>::quiet_NaN();
+static const double small_num = 2.2250738585072014e-308; /* TINY(1.0D0) */
+
+/* SSP-RK3 coefficients, solver/mhd/definition.f90:127-132 */
+static const double rk20 = 3.0 / 4.0, rk21 = 1.0 / 4.0, rk22 = 1.0 / 4.0;
+static const double rk30 = 1.0 / 3.0, rk31 = 2.0 / 3.0, rk32 = 2.0 / 3.0;
+
+/* WENO-Z constants, solver/mhd/weno_module.f90:16-25 */
+static const double smallpara = 1.0e-40;
+static const double g_weno_1 = 1.0 / 10.0, g_weno_2 = 6.0 / 10.0, g_weno_3 = 3.0 / 10.0;
+static const double r_weno_1 = 13.0 / 12.0, r_weno_2 = 1.0 / 4.0;
+
+/* ------------------------------------------------------------------ */
+/* the simulation                                                      */
+/* ------------------------------------------------------------------ */
+template <class R>
+struct Sim {
+    cumc_config cfg;
+    int nx, ny, nz, n_dim, coord;
+    int NX, NY, NZ; /* padded extents n+6 */
+    double ggas, cfl;
+    std::string err;
+
+    /* grid (1D), index offset 3 for the -3..n+3 face arrays, 2 for cells */
+    std::vector<double> xF_, yF_, zF_;
+    std::vector<double> x_, y_, z_, dx_, dy_, dz_, xbar_, dx_cb_, sine_, sinf_, dsine_, dcose_;
+    std::vector<double> wx_, wy_, wz_; /* (-2:n+3, 14) */
+    int bfac_xin[12], bfac_xout[12], bfac_yin[12], bfac_yout[12], bfac_zin[12], bfac_zout[12];
+
+    /* state */
+    std::vector<R> prim, cons, u_old, l_rk, sc, flux;  /* 8 vars */
+    std::vector<R> primL, primR, uL, uR, fluxL, fluxR;  /* 8 vars */
+    std::vector<R> eps, cs, dpdrho, dpdeps, epsL, epsR, csL, csR;
+    std::vector<R> bcell, ecell;  /* 3 vars */
+    std::vector<R> eface;         /* 6 vars */
+    std::vector<R> efx, efy, efz;
+
+    /* ---- indexing ---- */
+    inline size_t c3(int j, int k, int l) const {
+        return (size_t)(j + 2) + (size_t)NX * ((size_t)(k + 2) + (size_t)NY * (size_t)(l + 2));
+    }
+    inline R &P(int i, int j, int k, int l) { return prim[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &U(int i, int j, int k, int l) { return cons[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &UO(int i, int j, int k, int l) { return u_old[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &LR(int i, int j, int k, int l) { return l_rk[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &SC(int i, int j, int k, int l) { return sc[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &FL(int i, int j, int k, int l) { return flux[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &PL(int i, int j, int k, int l) { return primL[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &PR(int i, int j, int k, int l) { return primR[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &UL(int i, int j, int k, int l) { return uL[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &URr(int i, int j, int k, int l) { return uR[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &FXL(int i, int j, int k, int l) { return fluxL[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &FXR(int i, int j, int k, int l) { return fluxR[(size_t)(i - 1) + 8 * c3(j, k, l)]; }
+    inline R &E(int j, int k, int l) { return eps[c3(j, k, l)]; }
+    inline R &CS(int j, int k, int l) { return cs[c3(j, k, l)]; }
+    inline R &BC(int i, int j, int k, int l) { return bcell[(size_t)(i - ibx) + 3 * c3(j, k, l)]; }
+    inline R &EC(int i, int j, int k, int l) { return ecell[(size_t)(i - iex) + 3 * c3(j, k, l)]; }
+    inline R &EF(int i, int j, int k, int l) { return eface[(size_t)(i - 1) + 6 * c3(j, k, l)]; }
+    inline R &EX(int j, int k, int l) { return efx[c3(j, k, l)]; }
+    inline R &EY(int j, int k, int l) { return efy[c3(j, k, l)]; }
+    inline R &EZ(int j, int k, int l) { return efz[c3(j, k, l)]; }
+
+    double &xF(int j) { return xF_[j + 3]; }
+    double &yF(int j) { return yF_[j + 3]; }
+    double &zF(int j) { return zF_[j + 3]; }
+    double &x(int j) { return x_[j + 2]; }
+    double &y(int j) { return y_[j + 2]; }
+    double &z(int j) { return z_[j + 2]; }
+    double &dx(int j) { return dx_[j + 2]; }
+    double &dy(int j) { return dy_[j + 2]; }
+    double &dz(int j) { return dz_[j + 2]; }
+    double &xbar(int j) { return xbar_[j + 2]; }
+    double &dx_cb(int j) { return dx_cb_[j + 2]; }
+    double &sine(int j) { return sine_[j + 2]; }
+    double &sinf(int j) { return sinf_[j + 3]; }
+    double &dsine(int j) { return dsine_[j + 2]; }
+    double &dcose(int j) { return dcose_[j + 2]; }
+    double *wx(int j) { return &wx_[(size_t)(j + 2) * 14]; }
+    double *wy(int j) { return &wy_[(size_t)(j + 2) * 14]; }
+    double *wz(int j) { return &wz_[(size_t)(j + 2) * 14]; }
+
+    /* ================================================================ */
+    /* setup                                                            */
+    /* ================================================================ */
+    int init(const cumc_config *c) {
+        cfg = *c;
+        nx = c->nx; ny = c->ny; nz = c->nz; n_dim = c->n_dim; coord = c->coordinate_flag;
+        if (nx < 1 || ny < 1 || nz < 1 || n_dim < 1 || n_dim > 3 || coord < 0 || coord > 2) {
+            err = "bad grid extents or flags"; return CUMC_EINVAL;
+        }
+        if ((n_dim < 2 && ny != 1) || (n_dim < 3 && nz != 1)) { err = "degenerate directions need n=1"; return CUMC_EINVAL; }
+        for (int d = 0; d < 3; ++d) {
+            int a = c->boundary_flag[2 * d], b = c->boundary_flag[2 * d + 1];
+            if ((a == 0) != (b == 0)) { err = "periodic boundary flags must come in pairs"; return CUMC_EINVAL; }
+        }
+        NX = nx + 6; NY = ny + 6; NZ = nz + 6;
+        ggas = c->model.gamma;
+        cfl = c->cfl;
+        int rc = setup_eqns();
+        if (rc) return rc;
+        get_grid();
+        build_weights();
+        size_t n3 = (size_t)NX * NY * NZ;
+        auto nanv = [&](std::vector<R> &v, size_t n) { v.assign(n, R(kNaN)); };
+        nanv(prim, 8 * n3); nanv(cons, 8 * n3); nanv(u_old, 8 * n3); nanv(l_rk, 8 * n3);
+        nanv(sc, 8 * n3); nanv(flux, 8 * n3);
+        nanv(primL, 8 * n3); nanv(primR, 8 * n3); nanv(uL, 8 * n3); nanv(uR, 8 * n3);
+        nanv(fluxL, 8 * n3); nanv(fluxR, 8 * n3);
+        nanv(eps, n3); nanv(cs, n3); nanv(dpdrho, n3); nanv(dpdeps, n3);
+        nanv(epsL, n3); nanv(epsR, n3); nanv(csL, n3); nanv(csR, n3);
+        nanv(bcell, 3 * n3); nanv(ecell, 3 * n3); nanv(eface, 6 * n3);
+        nanv(efx, n3); nanv(efy, n3); nanv(efz, n3);
+        return CUMC_OK;
+    }
+
+    /* SETUP_EQNS parity factors, solver/mhd/setup.f90:99-325 */
+    int setup_eqns() {
+        for (int i = 0; i < 12; ++i)
+            bfac_xin[i] = bfac_xout[i] = bfac_yin[i] = bfac_yout[i] = bfac_zin[i] = bfac_zout[i] = 1;
+        const int *bf = cfg.boundary_flag;
+        if (bf[0] == 2) { bfac_xin[ivx] = -1; bfac_xin[ibx] = -1; }
+        else if (bf[0] == 3) { bfac_xin[ivx] = -1; bfac_xin[ibx] = -1; bfac_xin[ivz] = -1; bfac_xin[ibz] = -1; }
+        else if (bf[0] == 4) { err = "Equatorial symmetry is not allowed for the x-boundary"; return CUMC_EINVAL; }
+        if (bf[1] == 2) { bfac_xout[ivx] = -1; bfac_xout[ibx] = -1; }
+        else if (bf[1] == 3) { bfac_xout[ivx] = -1; bfac_xout[ibx] = -1; bfac_xout[ivz] = -1; bfac_xout[ibz] = -1; }
+        else if (bf[1] == 4) { err = "Equatorial symmetry is not allowed for the x-boundary"; return CUMC_EINVAL; }
+        if (bf[2] == 2) { bfac_yin[ivy] = -1; bfac_yin[iby] = -1; }
+        else if (bf[2] == 3) { bfac_yin[ivy] = -1; bfac_yin[iby] = -1; bfac_yin[ivz] = -1; bfac_yin[ibz] = -1; }
+        else if (bf[2] == 4) { bfac_yin[ivy] = -1; bfac_yin[ibx] = -1; bfac_yin[ibz] = -1; }
+        if (bf[3] == 2) { bfac_yout[ivy] = -1; bfac_yout[iby] = -1; }
+        else if (bf[3] == 3) { bfac_yout[ivy] = -1; bfac_yout[iby] = -1; bfac_yout[ivz] = -1; bfac_yout[ibz] = -1; }
+        else if (bf[3] == 4) { bfac_yout[ivy] = -1; bfac_yout[ibx] = -1; bfac_yout[ibz] = -1; }
+        if (bf[4] == 2) { bfac_zin[ivz] = -1; bfac_zin[ibz] = -1; }
+        else if (bf[4] == 3) { err = "Axial symmetry is not allowed for the z-boundary"; return CUMC_EINVAL; }
+        else if (bf[4] == 4) { bfac_zin[ivz] = -1; bfac_zin[ibx] = -1; bfac_zin[iby] = -1; }
+        if (bf[5] == 2) { bfac_zout[ivz] = -1; bfac_zout[ibz] = -1; }
+        else if (bf[5] == 3) { err = "Axial symmetry is not allowed for the z-boundary"; return CUMC_EINVAL; }
+        else if (bf[5] == 4) { bfac_zout[ivz] = -1; bfac_zout[ibx] = -1; bfac_zout[iby] = -1; }
+        int *all[6] = {bfac_xin, bfac_xout, bfac_yin, bfac_yout, bfac_zin, bfac_zout};
+        for (int s = 0; s < 6; ++s) {
+            int *b = all[s];
+            if (b[ivz] * b[iby] * b[ivy] * b[ibz] < 0) { err = "Error in boundary flags for vz and by"; return CUMC_EINVAL; }
+            b[iex] = b[ivz] * b[iby];
+            if (b[ivx] * b[ibz] * b[ivz] * b[ibx] < 0) { err = "Error in boundary flags for vx and bz"; return CUMC_EINVAL; }
+            b[iey] = b[ivx] * b[ibz];
+            if (b[ivy] * b[ibx] * b[ivx] * b[iby] < 0) { err = "Error in boundary flags for vy and bx"; return CUMC_EINVAL; }
+            b[iez] = b[ivy] * b[ibx];
+        }
+        return CUMC_OK;
+    }
+
+    /* GetGrid, solver/mhd/getgrid.f90:13-98 (face coordinates come from the
+     * caller, the CUSTOM_GRID hook; volumes are not used on the stage path) */
+    void get_grid() {
+        xF_.assign(nx + 7, 0.0); yF_.assign(ny + 7, 0.0); zF_.assign(nz + 7, 0.0);
+        for (int j = -3; j <= nx + 3; ++j) xF(j) = cfg.xF[j + 3];
+        for (int j = -3; j <= ny + 3; ++j) yF(j) = cfg.yF[j + 3];
+        for (int j = -3; j <= nz + 3; ++j) zF(j) = cfg.zF[j + 3];
+        x_.assign(NX, kNaN); y_.assign(NY, kNaN); z_.assign(NZ, kNaN);
+        dx_.assign(NX, kNaN); dy_.assign(NY, kNaN); dz_.assign(NZ, kNaN);
+        xbar_.assign(NX, kNaN); dx_cb_.assign(NX, kNaN);
+        sine_.assign(NY, kNaN); sinf_.assign(NY + 1, kNaN); dsine_.assign(NY, kNaN); dcose_.assign(NY, kNaN);
+        for (int j = -2; j <= nx + 3; ++j) dx(j) = xF(j) - xF(j - 1);
+        for (int j = -2; j <= ny + 3; ++j) dy(j) = yF(j) - yF(j - 1);
+        for (int j = -2; j <= nz + 3; ++j) dz(j) = zF(j) - zF(j - 1);
+        for (int j = -2; j <= nx + 3; ++j) x(j) = (xF(j) + xF(j - 1)) / 2.0;
+        for (int j = -2; j <= ny + 3; ++j) y(j) = (yF(j) + yF(j - 1)) / 2.0;
+        for (int j = -2; j <= nz + 3; ++j) z(j) = (zF(j) + zF(j - 1)) / 2.0;
+        for (int j = -1; j <= nx + 3; ++j) {
+            dx_cb(j) = xF(j) * xF(j) * xF(j) - xF(j - 1) * xF(j - 1) * xF(j - 1);
+            xbar(j) = (dx_cb(j) / 3.0) / (x(j) * dx(j));
+        }
+        for (int k = -1; k <= ny + 3; ++k) {
+            dcose(k) = -(std::cos(yF(k)) - std::cos(yF(k - 1)));
+            dsine(k) = (std::sin(yF(k)) - std::sin(yF(k - 1)));
+        }
+        for (int k = -2; k <= ny + 3; ++k) sine(k) = std::sin(y(k));
+        for (int k = -3; k <= ny + 3; ++k) sinf(k) = std::sin(yF(k));
+        if (cfg.fixpole && coord == 2) {
+            yF(0) = 0.0; yF(ny) = 4.0 * std::atan(1.0);
+            sinf(0) = 0.0; sinf(ny) = 0.0;
+        }
+    }
+
+    /* TVD_WEIGHT tvd_module.f90:25-55; PPM_WEIGHT/PPM_INTERPOLANT
+     * ppmc_module.f90:17-145; WENO_WEIGHT/WENO_INTERPOLANT weno_module.f90:35-149 */
+    static void ppm_interpolant(double dm2, double dm1, double dc, double dp1, double dp2, double *w) {
+        double a1R = dc / (dc + dp1);
+        double a1L = dm1 / (dm1 + dc);
+        double aR = 2.0 * dp1 * dc / (dp1 + dc);
+        double aL = 2.0 * dc * dm1 / (dc + dm1);
+        double deltaXR = dm1 + dc + dp1 + dp2;
+        double deltaXL = dm2 + dm1 + dc + dp1;
+        double z1R = (dm1 + dc) / (2.0 * dc + dp1);
+        double z1L = (dm2 + dm1) / (2.0 * dm1 + dc);
+        double zR = (dp2 + dp1) / (2.0 * dp1 + dc);
+        double zL = (dp1 + dc) / (2.0 * dc + dm1);
+        double cc1 = dc / (dm1 + dc + dp1);
+        double cp1 = dp1 / (dc + dp1 + dp2);
+        double cm1 = dm1 / (dm2 + dm1 + dc);
+        double cc2 = (2.0 * dm1 + dc) / (dp1 + dc);
+        double cp2 = (2.0 * dc + dp1) / (dp2 + dp1);
+        double cm2 = (2.0 * dm2 + dm1) / (dc + dm1);
+        double cc3 = (dc + 2.0 * dp1) / (dm1 + dc);
+        double cp3 = (dp1 + 2.0 * dp2) / (dc + dp1);
+        double cm3 = (dm1 + 2.0 * dc) / (dm2 + dm1);
+        w[0] = a1L;
+        w[1] = aL * (z1L - zL) / deltaXL;
+        w[2] = (-dm1 * z1L) / deltaXL;
+        w[3] = dc * zL / deltaXL;
+        w[4] = a1R;
+        w[5] = aR * (z1R - zR) / deltaXR;
+        w[6] = (-dc * z1R) / deltaXR;
+        w[7] = dp1 * zR / deltaXR;
+        w[8] = cm1 * cm2;
+        w[9] = cm1 * cm3;
+        w[10] = cc1 * cc2;
+        w[11] = cc1 * cc3;
+        w[12] = cp1 * cp2;
+        w[13] = cp1 * cp3;
+    }
+    static void weno_interpolant(double dm2, double dm1, double dc, double dp1, double dp2, double *w) {
+        double alpha12 = dp2 / (dp1 + dp2);
+        double alpha01 = dp1 / (dc + dp1);
+        double alpha10 = dc / (dm1 + dc);
+        double alpha21 = dm1 / (dm2 + dm1);
+        w[0] = (1.0 - alpha01);
+        w[1] = alpha01;
+        w[2] = (1.0 - alpha12);
+        w[3] = alpha12;
+        w[4] = (1.0 - alpha10);
+        w[5] = alpha10;
+        w[6] = (1.0 - alpha21);
+        w[7] = alpha21;
+        w[8] = (1.0 - alpha21);
+        w[9] = alpha12;
+    }
+    void build_weights() {
+        wx_.assign((size_t)NX * 14, kNaN); wy_.assign((size_t)NY * 14, kNaN); wz_.assign((size_t)NZ * 14, kNaN);
+        int rc = cfg.recon;
+        auto fill = [&](int n, double *(Sim::*w)(int), double &(Sim::*d)(int)) {
+            if (rc == CUMC_RECON_WENO || rc == CUMC_RECON_PPM) {
+                for (int j = 0; j <= n + 1; ++j) {
+                    double dm2 = (this->*d)(j - 2), dm1 = (this->*d)(j - 1), dc = (this->*d)(j),
+                           dp1 = (this->*d)(j + 1), dp2 = (this->*d)(j + 2);
+                    if (rc == CUMC_RECON_WENO) weno_interpolant(dm2, dm1, dc, dp1, dp2, (this->*w)(j));
+                    else ppm_interpolant(dm2, dm1, dc, dp1, dp2, (this->*w)(j));
+                }
+            } else {
+                for (int j = -1; j <= n + 2; ++j) {
+                    (this->*w)(j)[0] = ((this->*d)(j) + (this->*d)(j + 1)) / (this->*d)(j);
+                    (this->*w)(j)[1] = ((this->*d)(j) + (this->*d)(j - 1)) / (this->*d)(j);
+                }
+            }
+        };
+        fill(nx, &Sim::wx, &Sim::dx);
+        fill(ny, &Sim::wy, &Sim::dy);
+        fill(nz, &Sim::wz, &Sim::dz);
+    }
+
+    /* ================================================================ */
+    /* model hooks                                                      */
+    /* ================================================================ */
+    /* EOSEPSILON_NM model/riemann/src/getepsilon.f90:4-16 */
+    inline R eos_eps(R rho, R p) { return p / rho / (ggas - 1.0); }
+    /* EOSSOUNDSPEED model/riemann/src/soundspeed.f90:4-21 */
+    inline R eos_cs(R p, R rho, R e) {
+        R dpdden = e * (ggas - 1.0);
+        R dpdint = rho * (ggas - 1.0);
+        return sqrt_(dpdden + dpdint * p / (rho * rho));
+    }
+
+    /* CUSTOM_CHECKRHO */
+    void custom_checkrho() {
+        const cumc_model &m = cfg.model;
+        if (m.floor_kind == CUMC_FLOOR_EPS) {
+            /* model/riemann/src/custom.f90:260-284 */
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j) E(j, k, l) = max_(E(j, k, l), R(0.0));
+        } else if (m.floor_kind == CUMC_FLOOR_TORUS) {
+            /* model/torus-cyn/src/custom.f90:240-275, uniform floor arrays */
+            const double rho_floor = m.rho_floor, eps_floor = m.eps_floor;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j) {
+                        R diff = P(irho, j, k, l) - rho_floor;
+                        R factor = max_(sign1_(diff), R(0.0));
+                        P(irho, j, k, l) = factor * P(irho, j, k, l) + (1.0 - factor) * rho_floor;
+                        for (int i = ivx; i <= ivz; ++i) P(i, j, k, l) = factor * P(i, j, k, l);
+                        E(j, k, l) = factor * E(j, k, l) + (1.0 - factor) * eps_floor;
+                        if (E(j, k, l) < 0.0) E(j, k, l) = eps_floor;
+                    }
+        }
+    }
+
+    /* FINDPRESSURE: model/riemann/src/findpressure.f90:76-99 and
+     * model/torus-cyn/src/findpressure.f90:7-37 (the floor branch) */
+    void findpressure() {
+        const cumc_model &m = cfg.model;
+        const bool torus = (m.floor_kind == CUMC_FLOOR_TORUS);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = -2; l <= nz + 3; ++l)
+            for (int k = -2; k <= ny + 3; ++k)
+                for (int j = -2; j <= nx + 3; ++j) {
+                    size_t c = c3(j, k, l);
+                    if (!torus || P(irho, j, k, l) > m.rho_floor) {
+                        P(itau, j, k, l) = P(irho, j, k, l) * eps[c] * (ggas - 1.0);
+                        dpdrho[c] = eps[c] * (ggas - 1.0);
+                        dpdeps[c] = P(irho, j, k, l) * (ggas - 1.0);
+                    } else {
+                        P(itau, j, k, l) = R(m.p_floor);
+                        dpdrho[c] = R(m.eps_floor * (ggas - 1.0));
+                        dpdeps[c] = R(m.rho_floor * (ggas - 1.0));
+                    }
+                    cs[c] = sqrt_(dpdrho[c] + dpdeps[c] * P(itau, j, k, l) / (P(irho, j, k, l) * P(irho, j, k, l)));
+                }
+    }
+
+    /* CUSTOM_SOURCE */
+    void custom_source() {
+        const cumc_model &m = cfg.model;
+        if (m.source_kind == CUMC_SRC_CONST_GY) {
+            /* model/riemann/src/custom.f90:299-312 */
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j)
+                        SC(ivy, j, k, l) = SC(ivy, j, k, l) - m.g_const * P(irho, j, k, l);
+        } else if (m.source_kind == CUMC_SRC_PM_CYL) {
+            /* model/torus-cyn/src/custom.f90:298-314 */
+            const double r_sh = m.r_sh;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j) {
+                        R diff = P(irho, j, k, l) - m.rho_floor;
+                        R factor = max_(sign1_(diff), R(0.0));
+                        R radius = sqrt_(R(x(j) * x(j) + z(l) * z(l)));
+                        R dphidr = R(x(j)) / radius / ((radius - r_sh) * (radius - r_sh));
+                        R dphidz = R(z(l)) / radius / ((radius - r_sh) * (radius - r_sh));
+                        SC(ivx, j, k, l) = SC(ivx, j, k, l) + (-(factor * P(irho, j, k, l) * dphidr));
+                        SC(ivz, j, k, l) = SC(ivz, j, k, l) + (-(factor * P(irho, j, k, l) * dphidz));
+                        SC(itau, j, k, l) = SC(itau, j, k, l) +
+                            (-(factor * P(irho, j, k, l) * (P(ivx, j, k, l) * dphidr + P(ivz, j, k, l) * dphidz)));
+                    }
+        } else if (m.source_kind == CUMC_SRC_PM_SPH) {
+            /* model/torus-sph/src/custom.f90 CUSTOM_SOURCE (radial form) */
+            const double r_sh = m.r_sh;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j) {
+                        R diff = P(irho, j, k, l) - m.rho_floor;
+                        R factor = max_(sign1_(diff), R(0.0));
+                        R dphidr = R(1.0) / R((x(j) - r_sh) * (x(j) - r_sh));
+                        SC(ivx, j, k, l) = SC(ivx, j, k, l) + (-(factor * P(irho, j, k, l) * dphidr));
+                        SC(itau, j, k, l) = SC(itau, j, k, l) + (-(factor * P(irho, j, k, l) * P(ivx, j, k, l) * dphidr));
+                    }
+        }
+    }
+
+    /* CUSTOM_BOUNDARY_X/Y/Z */
+    void custom_boundary() {
+        const int kind = cfg.model.bc_kind;
+        if (kind == CUMC_BC_TORUS_CYL || kind == CUMC_BC_TORUS_SPH) {
+            /* model/torus-cyn/src/custom.f90:146-170 */
+            for (int l = -2; l <= nz + 3; ++l)
+                for (int k = -2; k <= ny + 3; ++k)
+                    for (int j = 1; j <= 3; ++j) {
+                        P(ivx, 1 - j, k, l) = min_(P(ivx, 1 - j, k, l), R(0.0));
+                        P(ivx, nx + j, k, l) = max_(P(ivx, nx + j, k, l), R(0.0));
+                    }
+        }
+        if (kind == CUMC_BC_TORUS_CYL) {
+            /* model/torus-cyn/src/custom.f90:184-208 */
+            for (int l = 1; l <= 3; ++l)
+                for (int k = -2; k <= ny + 3; ++k)
+                    for (int j = -2; j <= nx + 3; ++j) {
+                        P(ivz, j, k, 1 - l) = min_(P(ivz, j, k, 1 - l), R(0.0));
+                        P(ivz, j, k, nz + l) = max_(P(ivz, j, k, nz + l), R(0.0));
+                    }
+        }
+    }
+
+    /* ================================================================ */
+    /* conversions, solver/mhd/fromrvetou.f90                           */
+    /* ================================================================ */
+    template <class F>
+    void face_to_cell_b(F &&face) {
+        /* fromrvetou.f90:48-90 (from prim) and 153-195 (from cons) */
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    if (coord == 0) {
+                        BC(ibx, j, k, l) = 0.5 * (face(ibx, j, k, l) + face(ibx, j - 1, k, l));
+                        BC(iby, j, k, l) = 0.5 * (face(iby, j, k, l) + face(iby, j, k - 1, l));
+                        BC(ibz, j, k, l) = 0.5 * (face(ibz, j, k, l) + face(ibz, j, k, l - 1));
+                    } else if (coord == 1) {
+                        BC(ibx, j, k, l) = (xF(j) * face(ibx, j, k, l) + xF(j - 1) * face(ibx, j - 1, k, l)) / (xF(j) + xF(j - 1));
+                        BC(iby, j, k, l) = 0.5 * (face(iby, j, k, l) + face(iby, j, k - 1, l));
+                        BC(ibz, j, k, l) = 0.5 * (face(ibz, j, k, l) + face(ibz, j, k, l - 1));
+                    } else {
+                        BC(ibx, j, k, l) = 1.5 * dx(j) / dx_cb(j) *
+                            ((xF(j) * xF(j)) * face(ibx, j, k, l) + (xF(j - 1) * xF(j - 1)) * face(ibx, j - 1, k, l));
+                        BC(iby, j, k, l) = 0.5 * dy(k) / dcose(k) *
+                            (sinf(k) * face(iby, j, k, l) + sinf(k - 1) * face(iby, j, k - 1, l));
+                        BC(ibz, j, k, l) = 0.5 * (face(ibz, j, k, l) + face(ibz, j, k, l - 1));
+                    }
+                }
+    }
+
+    /* FROMRVETOU fromrvetou.f90:21-121 */
+    void fromrvetou() {
+        face_to_cell_b([&](int i, int j, int k, int l) -> R { return P(i, j, k, l); });
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 0; l <= nz; ++l)
+            for (int k = 0; k <= ny; ++k)
+                for (int j = 0; j <= nx; ++j) {
+                    R vsquare = P(ivx, j, k, l) * P(ivx, j, k, l) + P(ivy, j, k, l) * P(ivy, j, k, l) + P(ivz, j, k, l) * P(ivz, j, k, l);
+                    R bsquare = BC(ibx, j, k, l) * BC(ibx, j, k, l) + BC(iby, j, k, l) * BC(iby, j, k, l) + BC(ibz, j, k, l) * BC(ibz, j, k, l);
+                    U(irho, j, k, l) = P(irho, j, k, l);
+                    for (int i = ivx; i <= ivz; ++i) U(i, j, k, l) = P(i, j, k, l) * P(irho, j, k, l);
+                    U(itau, j, k, l) = P(irho, j, k, l) * (E(j, k, l) + 0.5 * vsquare) + 0.5 * bsquare;
+                    for (int i = ibx; i <= ibz; ++i) U(i, j, k, l) = P(i, j, k, l);
+                }
+    }
+
+    /* FROMUTORVE fromrvetou.f90:126-227 */
+    void fromutorve() {
+        face_to_cell_b([&](int i, int j, int k, int l) -> R { return U(i, j, k, l); });
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    P(irho, j, k, l) = U(irho, j, k, l);
+                    for (int i = ivx; i <= ivz; ++i) P(i, j, k, l) = U(i, j, k, l) / U(irho, j, k, l);
+                    for (int i = ibx; i <= ibz; ++i) P(i, j, k, l) = U(i, j, k, l);
+                    R bsquare = BC(ibx, j, k, l) * BC(ibx, j, k, l) + BC(iby, j, k, l) * BC(iby, j, k, l) + BC(ibz, j, k, l) * BC(ibz, j, k, l);
+                    R vsquare = P(ivx, j, k, l) * P(ivx, j, k, l) + P(ivy, j, k, l) * P(ivy, j, k, l) + P(ivz, j, k, l) * P(ivz, j, k, l);
+                    E(j, k, l) = (U(itau, j, k, l) - 0.5 * bsquare) / U(irho, j, k, l) - 0.5 * vsquare;
+                }
+    }
+
+    /* ================================================================ */
+    /* ghost fill, solver/mhd/boundary.f90                              */
+    /* ================================================================ */
+    /* One array (or one component list) filled x then y then z exactly as
+     * BOUNDARYP_NM (397-770) and BOUNDARY1D_NM (29-389) do. */
+    template <class A>
+    void fill_x(A &&a, int sin_, int sout_) {
+        const int *bf = cfg.boundary_flag;
+        for (int l = -2; l <= nz + 3; ++l)
+            for (int k = -2; k <= ny + 3; ++k)
+                for (int j = 1; j <= 3; ++j) {
+                    if (bf[0] == 0) a(1 - j, k, l) = R(a(nx + 1 - j, k, l));
+                    else if (bf[0] == 1) a(1 - j, k, l) = R(a(1, k, l));
+                    else a(1 - j, k, l) = R(double(sin_)) * a(j, k, l);
+                }
+        for (int l = -2; l <= nz + 3; ++l)
+            for (int k = -2; k <= ny + 3; ++k)
+                for (int j = 1; j <= 3; ++j) {
+                    if (bf[1] == 0) a(nx + j, k, l) = R(a(j, k, l));
+                    else if (bf[1] == 1) a(nx + j, k, l) = R(a(nx, k, l));
+                    else a(nx + j, k, l) = R(double(sout_)) * a(nx + 1 - j, k, l);
+                }
+    }
+    /* y_out_flag lets BOUNDARY1D_NM reproduce its y-outer test of
+     * boundary_flag(3) for the periodic case (boundary.f90:243) */
+    template <class A>
+    void fill_y(A &&a, int sin_, int sout_, bool eps_quirk) {
+        const int *bf = cfg.boundary_flag;
+        for (int l = -2; l <= nz + 3; ++l)
+            for (int k = 1; k <= 3; ++k)
+                for (int j = -2; j <= nx + 3; ++j) {
+                    if (bf[2] == 0) a(j, 1 - k, l) = R(a(j, ny + 1 - k, l));
+                    else if (bf[2] == 1) a(j, 1 - k, l) = R(a(j, 1, l));
+                    else a(j, 1 - k, l) = R(double(sin_)) * a(j, k, l);
+                }
+        int mode = eps_quirk ? (bf[2] == 0 ? 0 : (bf[3] == 1 ? 1 : (bf[3] >= 2 ? 2 : -1))) : bf[3];
+        for (int l = -2; l <= nz + 3; ++l)
+            for (int k = 1; k <= 3; ++k)
+                for (int j = -2; j <= nx + 3; ++j) {
+                    if (mode == 0) a(j, ny + k, l) = R(a(j, k, l));
+                    else if (mode == 1) a(j, ny + k, l) = R(a(j, ny, l));
+                    else if (mode >= 2) a(j, ny + k, l) = R(double(sout_)) * a(j, ny + 1 - k, l);
+                }
+    }
+    template <class A>
+    void fill_z(A &&a, int sin_, int sout_) {
+        const int *bf = cfg.boundary_flag;
+        for (int l = 1; l <= 3; ++l)
+            for (int k = -2; k <= ny + 3; ++k)
+                for (int j = -2; j <= nx + 3; ++j) {
+                    if (bf[4] == 0) a(j, k, 1 - l) = R(a(j, k, nz + 1 - l));
+                    else if (bf[4] == 1) a(j, k, 1 - l) = R(a(j, k, 1));
+                    else a(j, k, 1 - l) = R(double(sin_)) * a(j, k, l);
+                }
+        for (int l = 1; l <= 3; ++l)
+            for (int k = -2; k <= ny + 3; ++k)
+                for (int j = -2; j <= nx + 3; ++j) {
+                    if (bf[5] == 0) a(j, k, nz + l) = R(a(j, k, l));
+                    else if (bf[5] == 1) a(j, k, nz + l) = R(a(j, k, nz));
+                    else a(j, k, nz + l) = R(double(sout_)) * a(j, k, nz + 1 - l);
+                }
+    }
+
+    /* BOUNDARYP_NM boundary.f90:397-770 + custom hooks, then
+     * BOUNDARY1D_NM(epsilon, even...) boundary.f90:5-13 */
+    void boundary() {
+        auto pv = [&](int i) { return [this, i](int j, int k, int l) -> R & { return P(i, j, k, l); }; };
+        auto bv = [&](int i) { return [this, i](int j, int k, int l) -> R & { return BC(i, j, k, l); }; };
+        /* x pass: hydro 1..5, bcell, prim(iby), prim(ibz) */
+        for (int i = imin; i <= itau; ++i) fill_x(pv(i), bfac_xin[i], bfac_xout[i]);
+        for (int i = ibx; i <= ibz; ++i) fill_x(bv(i), bfac_xin[i], bfac_xout[i]);
+        fill_x(pv(iby), bfac_xin[iby], bfac_xout[iby]);
+        fill_x(pv(ibz), bfac_xin[ibz], bfac_xout[ibz]);
+        /* option: a periodic direction also carries its normal face field, so
+         * face 0 is face n (the reference leaves face 0 at its initial value) */
+        const int *bf = cfg.boundary_flag;
+        const bool fixn = cfg.fix_periodic_normal_faces != 0;
+        if (fixn && bf[0] == 0) fill_x(pv(ibx), 1, 1);
+        /* y pass: hydro, bcell, prim(ibx), prim(ibz) */
+        for (int i = imin; i <= itau; ++i) fill_y(pv(i), bfac_yin[i], bfac_yout[i], false);
+        for (int i = ibx; i <= ibz; ++i) fill_y(bv(i), bfac_yin[i], bfac_yout[i], false);
+        fill_y(pv(ibx), bfac_yin[ibx], bfac_yout[ibx], false);
+        fill_y(pv(ibz), bfac_yin[ibz], bfac_yout[ibz], false);
+        if (fixn && bf[2] == 0) fill_y(pv(iby), 1, 1, false);
+        /* z pass: hydro, bcell, prim(ibx), prim(iby) */
+        for (int i = imin; i <= itau; ++i) fill_z(pv(i), bfac_zin[i], bfac_zout[i]);
+        for (int i = ibx; i <= ibz; ++i) fill_z(bv(i), bfac_zin[i], bfac_zout[i]);
+        fill_z(pv(ibx), bfac_zin[ibx], bfac_zout[ibx]);
+        fill_z(pv(iby), bfac_zin[iby], bfac_zout[iby]);
+        if (fixn && bf[4] == 0) fill_z(pv(ibz), 1, 1);
+        custom_boundary();
+        /* epsilon: all-even parity */
+        auto ev = [this](int j, int k, int l) -> R & { return E(j, k, l); };
+        fill_x(ev, 1, 1);
+        fill_y(ev, 1, 1, true);
+        fill_z(ev, 1, 1);
+    }
+
+    /* UPDATE update.f90:12-33: FINDPRESSURE (+ empty CUSTOM_UPDATE) */
+    void update() { findpressure(); }
+
+    /* ================================================================ */
+    /* reconstruction                                                   */
+    /* ================================================================ */
+    /* PPMC ppmc_module.f90:359-464 */
+    static void ppmc(const double *wgt, R vm2, R vm1, R vc, R vp1, R vp2, R &vm_out, R &vp_out) {
+        const double a0m = wgt[0], a1m = wgt[1], a2m = wgt[2], a3m = wgt[3];
+        const double a0p = wgt[4], a1p = wgt[5], a2p = wgt[6], a3p = wgt[7];
+        const double b0m = wgt[8], b1m = wgt[9], b0c = wgt[10], b1c = wgt[11], b0p = wgt[12], b1p = wgt[13];
+        R deltap1 = b0p * (vp2 - vp1) + b1p * (vp1 - vc);
+        R deltac = b0c * (vp1 - vc) + b1c * (vc - vm1);
+        R deltam1 = b0m * (vc - vm1) + b1m * (vm1 - vm2);
+        R dmc, dmp1, dmm1, condition;
+        condition = (vp1 - vc) * (vc - vm1);
+        if (condition > 0.0) dmc = min3_(abs_(deltac), 2.0 * abs_(vc - vm1), 2.0 * abs_(vc - vp1)) * sign1_(deltac);
+        else dmc = R(0.0);
+        condition = (vp2 - vp1) * (vp1 - vc);
+        if (condition > 0.0) dmp1 = min3_(abs_(deltap1), 2.0 * abs_(vp1 - vc), 2.0 * abs_(vp1 - vp2)) * sign1_(deltap1);
+        else dmp1 = R(0.0);
+        condition = (vc - vm1) * (vm1 - vm2);
+        if (condition > 0.0) dmm1 = min3_(abs_(deltam1), 2.0 * abs_(vm1 - vm2), 2.0 * abs_(vm1 - vc)) * sign1_(deltam1);
+        else dmm1 = R(0.0);
+        vp_out = vc + a0p * (vp1 - vc) + a1p * (vp1 - vc) + a2p * dmp1 + a3p * dmc;
+        vm_out = vm1 + a0m * (vc - vm1) + a1m * (vc - vm1) + a2m * dmc + a3m * dmm1;
+        R vl = vm_out, vr = vp_out;
+        if ((vr - vc) * (vc - vl) <= 0.0) {
+            vp_out = vc;
+            vm_out = vc;
+        } else {
+            condition = (vr - vl) * (vl - 3.0 * vc + 2.0 * vr);
+            if (condition < 0.0) vm_out = 3.0 * vc - 2.0 * vr;
+            condition = (vp_out - vm_out) * (3.0 * vc - 2.0 * vl - vr);
+            if (condition < 0.0) vp_out = 3.0 * vc - 2.0 * vl;
+        }
+    }
+
+    /* WENO (WENO-Z) weno_module.f90:315-408 */
+    static void weno(const double *wgt, R vm2, R vm1, R vc, R vp1, R vp2, R &vm_out, R &vp_out) {
+        R U01 = wgt[0] * vc + wgt[1] * vp1;
+        R U12 = wgt[2] * vp1 + wgt[3] * vp2;
+        R U10 = wgt[4] * vm1 + wgt[5] * vc;
+        R U21 = wgt[6] * vm2 + wgt[7] * vm1;
+        R U00 = vm1 + wgt[8] * (vm1 - vm2);
+        R U11 = vp1 + wgt[9] * (vp1 - vp2);
+        R P1 = (6.0 * vc - 1.0 * U10 - 2.0 * U00) / 3.0;
+        R P2 = (-1.0 * U10 + 2.0 * vc + 2.0 * U01) / 3.0;
+        R P3 = (2.0 * U01 + 2.0 * vp1 - 1.0 * U12) / 3.0;
+        R t1 = 2.0 * U10 - 2.0 * U00, t2 = 4.0 * vc - 2.0 * U10 - 2.0 * U00;
+        R B1 = r_weno_1 * (t1 * t1) + r_weno_2 * (t2 * t2);
+        R t3 = 2.0 * U10 - 4.0 * vc + 2.0 * U01, t4 = -2.0 * U10 + 2.0 * U01;
+        R B2 = r_weno_1 * (t3 * t3) + r_weno_2 * (t4 * t4);
+        R t5 = 2.0 * U01 - 4.0 * vp1 + 2.0 * U12, t6 = -6.0 * U01 + 8.0 * vp1 - 2.0 * U12;
+        R B3 = r_weno_1 * (t5 * t5) + r_weno_2 * (t6 * t6);
+        R tau5 = abs_(B1 - B3);
+        R q1 = tau5 / (smallpara + B1), q2 = tau5 / (smallpara + B2), q3 = tau5 / (smallpara + B3);
+        R w1 = g_weno_1 * (1.0 + q1 * q1);
+        R w2 = g_weno_2 * (1.0 + q2 * q2);
+        R w3 = g_weno_3 * (1.0 + q3 * q3);
+        vp_out = (w1 * P1 + w2 * P2 + w3 * P3) / (w1 + w2 + w3);
+        P1 = (6.0 * vc - 1.0 * U01 - 2.0 * U11) / 3.0;
+        P2 = (-1.0 * U01 + 2.0 * vc + 2.0 * U10) / 3.0;
+        P3 = (2.0 * U10 + 2.0 * vm1 - 1.0 * U21) / 3.0;
+        t1 = 2.0 * U01 - 2.0 * U11; t2 = 4.0 * vc - 2.0 * U01 - 2.0 * U11;
+        B1 = r_weno_1 * (t1 * t1) + r_weno_2 * (t2 * t2);
+        t3 = 2.0 * U01 - 4.0 * vc + 2.0 * U10; t4 = 2.0 * U01 - 2.0 * U10;
+        B2 = r_weno_1 * (t3 * t3) + r_weno_2 * (t4 * t4);
+        t5 = 2.0 * U10 - 4.0 * vm1 + 2.0 * U21; t6 = 8.0 * vm1 - 6.0 * U10 - 2.0 * U21;
+        B3 = r_weno_1 * (t5 * t5) + r_weno_2 * (t6 * t6);
+        tau5 = abs_(B1 - B3);
+        q1 = tau5 / (smallpara + B1); q2 = tau5 / (smallpara + B2); q3 = tau5 / (smallpara + B3);
+        w1 = g_weno_1 * (1.0 + q1 * q1);
+        w2 = g_weno_2 * (1.0 + q2 * q2);
+        w3 = g_weno_3 * (1.0 + q3 * q3);
+        vm_out = (w1 * P1 + w2 * P2 + w3 * P3) / (w1 + w2 + w3);
+    }
+
+    /* TVD tvd_module.f90:279-344 */
+    static void tvd(int lim, const double *wgt, R vm, R vc, R vp, R &vm_out, R &vp_out) {
+        const double cf = wgt[0], cb = wgt[1];
+        R dqf = 2.0 * (vp - vc) / cf;
+        R dqb = 2.0 * (vc - vm) / cb;
+        R slope;
+        if (lim == CUMC_RECON_TVD_MM) {
+            slope = 0.5 * (sign1_(dqf) + sign1_(dqb)) * min_(abs_(dqf), abs_(dqb));
+        } else if (lim == CUMC_RECON_TVD_VL) {
+            R dq2 = dqf * dqb;
+            if (dq2 <= 0.0) slope = R(0.0);
+            else slope = (dq2 * (cf * dqb + cb * dqf) / (dqb * dqb + dqf * dqf + dq2 * (cf + cb - 2.0)));
+        } else {
+            if (dqf == 0.0) slope = R(0.0);
+            else {
+                R v_tvd = dqb / dqf;
+                slope = max_(R(0.0), min3_(0.5 * (1.0 + v_tvd), R(cf), cb * v_tvd));
+                slope = dqf * slope;
+            }
+        }
+        vp_out = vc + 0.5 * slope;
+        vm_out = vc - 0.5 * slope;
+    }
+
+    /* one cell's 5-point (or 3-point) reconstruction along a direction */
+    inline void recon1(const double *w, R (&v)[5], R &vm_out, R &vp_out) {
+        int rc = cfg.recon;
+        if (rc == CUMC_RECON_PPM) ppmc(w, v[0], v[1], v[2], v[3], v[4], vm_out, vp_out);
+        else if (rc == CUMC_RECON_WENO) weno(w, v[0], v[1], v[2], v[3], v[4], vm_out, vp_out);
+        else tvd(rc, w, v[1], v[2], v[3], vm_out, vp_out);
+    }
+
+    /* {TVD,PPMC,WENO}_recon{x,y,z}: tvd_module.f90:62-274,
+     * ppmc_module.f90:151-352, weno_module.f90:154-308 */
+    void recon(int dir) {
+        int jl = 1, jh = nx, kl = 1, kh = ny, ll = 1, lh = nz;
+        int dj = 0, dk = 0, dl = 0;
+        int ibn, ibt1, ibt2;
+        if (dir == x_dir) { jl = 0; jh = nx + 1; dj = 1; ibn = ibx; ibt1 = iby; ibt2 = ibz; }
+        else if (dir == y_dir) { kl = 0; kh = ny + 1; dk = 1; ibn = iby; ibt1 = ibx; ibt2 = ibz; }
+        else { ll = 0; lh = nz + 1; dl = 1; ibn = ibz; ibt1 = ibx; ibt2 = iby; }
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = ll; l <= lh; ++l)
+            for (int k = kl; k <= kh; ++k)
+                for (int j = jl; j <= jh; ++j) {
+                    const double *w = (dir == x_dir) ? wx(j) : (dir == y_dir) ? wy(k) : wz(l);
+                    int jm = j - dj, km = k - dk, lm = l - dl;
+                    R v[5];
+                    for (int i = imin; i <= itau; ++i) {
+                        for (int s = -2; s <= 2; ++s) v[s + 2] = P(i, j + s * dj, k + s * dk, l + s * dl);
+                        recon1(w, v, PR(i, jm, km, lm), PL(i, j, k, l));
+                    }
+                    epsR[c3(jm, km, lm)] = eos_eps(PR(irho, jm, km, lm), PR(itau, jm, km, lm));
+                    epsL[c3(j, k, l)] = eos_eps(PL(irho, j, k, l), PL(itau, j, k, l));
+                    csR[c3(jm, km, lm)] = eos_cs(PR(itau, jm, km, lm), PR(irho, jm, km, lm), epsR[c3(jm, km, lm)]);
+                    csL[c3(j, k, l)] = eos_cs(PL(itau, j, k, l), PL(irho, j, k, l), epsL[c3(j, k, l)]);
+                    for (int i : {ibt1, ibt2}) {
+                        for (int s = -2; s <= 2; ++s) v[s + 2] = BC(i, j + s * dj, k + s * dk, l + s * dl);
+                        recon1(w, v, PR(i, jm, km, lm), PL(i, j, k, l));
+                    }
+                    PR(ibn, jm, km, lm) = P(ibn, jm, km, lm);
+                    PL(ibn, j, k, l) = P(ibn, j, k, l);
+                }
+    }
+
+    /* ================================================================ */
+    /* BUILDSTATES spatial.f90:272-403 (over the faces the solver reads) */
+    /* ================================================================ */
+    void dir_indices(int dir, int &ivn, int &ivt1, int &ivt2, int &ibn, int &ibt1, int &ibt2) {
+        if (dir == x_dir) { ivn = ivx; ivt1 = ivy; ivt2 = ivz; ibn = ibx; ibt1 = iby; ibt2 = ibz; }
+        else if (dir == y_dir) { ivn = ivy; ivt1 = ivz; ivt2 = ivx; ibn = iby; ibt1 = ibz; ibt2 = ibx; }
+        else { ivn = ivz; ivt1 = ivx; ivt2 = ivy; ibn = ibz; ibt1 = ibx; ibt2 = iby; }
+    }
+    void face_range(int dir, int &jl, int &kl, int &ll) {
+        jl = (dir == x_dir) ? 0 : 1; kl = (dir == y_dir) ? 0 : 1; ll = (dir == z_dir) ? 0 : 1;
+    }
+
+    void buildstates(int dir) {
+        int ivn, ivt1, ivt2, ibn, ibt1, ibt2, jl, kl, ll;
+        dir_indices(dir, ivn, ivt1, ivt2, ibn, ibt1, ibt2);
+        face_range(dir, jl, kl, ll);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = ll; l <= nz; ++l)
+            for (int k = kl; k <= ny; ++k)
+                for (int j = jl; j <= nx; ++j) {
+                    for (int side = 0; side < 2; ++side) {
+                        auto Pf = [&](int i) -> R & { return side == 0 ? PL(i, j, k, l) : PR(i, j, k, l); };
+                        auto Uf = [&](int i) -> R & { return side == 0 ? UL(i, j, k, l) : URr(i, j, k, l); };
+                        auto Ff = [&](int i) -> R & { return side == 0 ? FXL(i, j, k, l) : FXR(i, j, k, l); };
+                        R ef = side == 0 ? epsL[c3(j, k, l)] : epsR[c3(j, k, l)];
+                        R b2 = Pf(ibx) * Pf(ibx) + Pf(iby) * Pf(iby) + Pf(ibz) * Pf(ibz);
+                        R v2 = Pf(ivx) * Pf(ivx) + Pf(ivy) * Pf(ivy) + Pf(ivz) * Pf(ivz);
+                        R vb = Pf(ibx) * Pf(ivx) + Pf(iby) * Pf(ivy) + Pf(ibz) * Pf(ivz);
+                        for (int i = imin; i <= itau; ++i) Uf(i) = Pf(i) * Pf(irho);
+                        Uf(irho) = Pf(irho);
+                        for (int i = ibx; i <= ibz; ++i) Uf(i) = Pf(i);
+                        Uf(itau) = Pf(irho) * (0.5 * v2 + ef) + 0.5 * b2;
+                        for (int i = imin; i <= itau; ++i) Ff(i) = Uf(i) * Pf(ivn);
+                        Ff(ivn) = Ff(ivn) + Pf(itau) + 0.5 * (b2) - Pf(ibn) * Pf(ibn);
+                        Ff(ivt1) = Ff(ivt1) - Pf(ibn) * Pf(ibt1);
+                        Ff(ivt2) = Ff(ivt2) - Pf(ibn) * Pf(ibt2);
+                        Ff(itau) = Ff(itau) + (Pf(itau) + 0.5 * (b2)) * Pf(ivn) - Pf(ibn) * vb;
+                        Ff(ibn) = R(0.0);
+                        Ff(ibt1) = (Pf(ivn) * Pf(ibt1) - Pf(ivt1) * Pf(ibn));
+                        Ff(ibt2) = (Pf(ivn) * Pf(ibt2) - Pf(ivt2) * Pf(ibn));
+                    }
+                }
+    }
+
+    /* ================================================================ */
+    /* Riemann solvers, rsolver_module.f90                              */
+    /* ================================================================ */
+    static R signalspeed(R cs_, R bn, R bt1, R bt2, R rho) { /* 32-48 */
+        R a2 = cs_ * cs_;
+        R a4 = a2 * a2;
+        R b2n = (bn * bn / rho);
+        R b2t1 = (bt1 * bt1 / rho);
+        R b2t2 = (bt2 * bt2 / rho);
+        R b2 = b2n + b2t1 + b2t2;
+        R b4 = b2 * b2;
+        return sqrt_(0.5 * (a2 + b2 + sqrt_(max_((a4 + b4 + 2.0 * b2 * a2) - 4.0 * a2 * b2n, R(0.0)))));
+    }
+    static R hll_state(R ul, R ur, R fl, R fr, R sl, R sr) { return (sr * ur - sl * ul - (fr - fl)) / (sr - sl); } /* 54-59 */
+    static R hll_flux(R yl, R yr, R xl, R xr, R sl, R sr) { return (sr * yl - sl * yr + sl * sr * (xr - xl)) / (sr - sl); } /* 61-66 */
+    static R roe(R xl, R xr, R rhol, R rhor) { return (sqrt_(rhol) * xl + sqrt_(rhor) * xr) / (sqrt_(rhol) + sqrt_(rhor)); } /* 68-73 */
+    static R sstar_hllc(R pl, R pr, R rhol, R rhor, R vl, R vr, R sl, R sr, R bl, R br) { /* 86-93 */
+        return (rhor * vr * (sr - vr) - rhol * vl * (sl - vl) + pl - pr + br * br - bl * bl) / (rhor * (sr - vr) - rhol * (sl - vl));
+    }
+
+    void riemann(int dir) {
+        int ivn, ivt1, ivt2, ibn, ibt1, ibt2, jl, kl, ll;
+        dir_indices(dir, ivn, ivt1, ivt2, ibn, ibt1, ibt2);
+        face_range(dir, jl, kl, ll);
+        const int rs = cfg.riemann;
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = ll; l <= nz; ++l)
+            for (int k = kl; k <= ny; ++k)
+                for (int j = jl; j <= nx; ++j) {
+                    size_t c = c3(j, k, l);
+                    R *pl = &primL[8 * c - 1], *pr = &primR[8 * c - 1]; /* 1-based */
+                    R *ul = &uL[8 * c - 1], *ur = &uR[8 * c - 1];
+                    R *fl = &fluxL[8 * c - 1], *fr = &fluxR[8 * c - 1];
+                    R *fo = &flux[8 * c - 1];
+                    R cfsL = signalspeed(csL[c], pl[ibn], pl[ibt1], pl[ibt2], pl[irho]);
+                    R cfsR = signalspeed(csR[c], pr[ibn], pr[ibt1], pr[ibt2], pr[irho]);
+                    if (rs == CUMC_RS_LF) { /* LFNM 133-222 */
+                        R sL = abs_(pl[ivn]) + cfsL, sR = abs_(pr[ivn]) + cfsR;
+                        R splus = max_(sL, sR);
+                        for (int i = imin; i <= imax; ++i) fo[i] = 0.5 * (fl[i] + fr[i] - splus * (ur[i] - ul[i]));
+                        continue;
+                    }
+                    R ubar = roe(pl[ivn], pr[ivn], pl[irho], pr[irho]);
+                    R cbar = roe(cfsL, cfsR, pl[irho], pr[irho]);
+                    R sL = min_(pl[ivn] - cfsL, ubar - cbar);
+                    R sR = max_(pr[ivn] + cfsR, ubar + cbar);
+                    if (rs == CUMC_RS_HLL) { /* HLLNM 227-326 */
+                        if (sL >= 0.0) { for (int i = imin; i <= imax; ++i) fo[i] = fl[i]; }
+                        else if (sL <= 0.0 && sR >= 0.0) { for (int i = imin; i <= imax; ++i) fo[i] = hll_flux(fl[i], fr[i], ul[i], ur[i], sL, sR); }
+                        else if (sR <= 0.0) { for (int i = imin; i <= imax; ++i) fo[i] = fr[i]; }
+                        continue;
+                    }
+                    if (sL >= 0.0) { for (int i = imin; i <= imax; ++i) fo[i] = fl[i]; continue; }
+                    if (sR <= 0.0) { for (int i = imin; i <= imax; ++i) fo[i] = fr[i]; continue; }
+                    R b2L = pl[ibx] * pl[ibx] + pl[iby] * pl[iby] + pl[ibz] * pl[ibz];
+                    R b2R = pr[ibx] * pr[ibx] + pr[iby] * pr[iby] + pr[ibz] * pr[ibz];
+                    R pLt = pl[itau] + 0.5 * b2L;
+                    R pRt = pr[itau] + 0.5 * b2R;
+                    if (rs == CUMC_RS_HLLC) hllc_star(pl, pr, ul, ur, fl, fr, fo, sL, sR, pLt, pRt, ivn, ivt1, ivt2, ibn, ibt1, ibt2);
+                    else hlld_star(pl, pr, ul, ur, fl, fr, fo, sL, sR, pLt, pRt, ivn, ivt1, ivt2, ibn, ibt1, ibt2);
+                }
+    }
+
+    /* HLLCNM star region, rsolver_module.f90:423-498 */
+    static void hllc_star(R *pl, R *pr, R *ul, R *ur, R *fl, R *fr, R *fo, R sL, R sR, R pLt, R pRt,
+                          int ivn, int ivt1, int ivt2, int ibn, int ibt1, int ibt2) {
+        R u_hll[9], p_hll[9], us[9];
+        R sstar = sstar_hllc(pLt, pRt, pl[irho], pr[irho], pl[ivn], pr[ivn], sL, sR, pl[ibn], pr[ibn]);
+        u_hll[ibn] = pl[ibn];
+        u_hll[ibt1] = hll_state(pl[ibt1], pr[ibt1], fl[ibt1], fr[ibt1], sL, sR);
+        u_hll[ibt2] = hll_state(pl[ibt2], pr[ibt2], fl[ibt2], fr[ibt2], sL, sR);
+        u_hll[irho] = hll_state(pl[irho], pr[irho], fl[irho], fr[irho], sL, sR);
+        u_hll[ivt1] = hll_state(ul[ivt1], ur[ivt1], fl[ivt1], fr[ivt1], sL, sR);
+        u_hll[ivt2] = hll_state(ul[ivt2], ur[ivt2], fl[ivt2], fr[ivt2], sL, sR);
+        p_hll[ivn] = sstar;
+        p_hll[ivt1] = u_hll[ivt1] / u_hll[irho];
+        p_hll[ivt2] = u_hll[ivt2] / u_hll[irho];
+        const bool left = (sstar >= 0.0);
+        R *pS = left ? pl : pr, *uS = left ? ul : ur, *fS = left ? fl : fr;
+        R s = left ? sL : sR, pSt = left ? pLt : pRt;
+        us[irho] = uS[irho] * (s - pS[ivn]) / (s - sstar);
+        R vb = pS[ibx] * pS[ivx] + pS[iby] * pS[ivy] + pS[ibz] * pS[ivz];
+        R vbhll = u_hll[ibx] * p_hll[ivx] + u_hll[iby] * p_hll[ivy] + u_hll[ibz] * p_hll[ivz];
+        R ps = pS[irho] * (s - pS[ivn]) * (sstar - pS[ivn]) + pSt;
+        us[ibn] = u_hll[ibn];
+        us[ibt1] = u_hll[ibt1];
+        us[ibt2] = u_hll[ibt2];
+        us[ivn] = us[irho] * sstar;
+        us[ivt1] = (uS[ivt1] * (s - pS[ivn]) - (us[ibn] * us[ibt1] - pS[ibn] * pS[ibt1])) / (s - sstar);
+        us[ivt2] = (uS[ivt2] * (s - pS[ivn]) - (us[ibn] * us[ibt2] - pS[ibn] * pS[ibt2])) / (s - sstar);
+        us[itau] = (uS[itau] * (s - pS[ivn]) + (ps * sstar - pSt * pS[ivn]) - ((vbhll * us[ibn] - vb * pS[ibn]))) / (s - sstar);
+        for (int i = imin; i <= imax; ++i) fo[i] = fS[i] + s * (us[i] - uS[i]);
+    }
+
+    /* HLLDNM star / double-star regions, rsolver_module.f90:613-750.
+     * The reference never assigns the normal component of the double-star
+     * states (usstarL/usstarR(ibn)); those PRIVATE arrays then hold undefined
+     * values.  Here they take the HLLD value B_n (Miyoshi & Kusano 2005:
+     * B_x is constant across the fan), i.e. usstar(ibn) = ustar(ibn). */
+    static void hlld_star(R *pl, R *pr, R *ul, R *ur, R *fl, R *fr, R *fo, R sL, R sR, R pLt, R pRt,
+                          int ivn, int ivt1, int ivt2, int ibn, int ibt1, int ibt2) {
+        R usL[9], usR[9], pstL[9], pstR[9], ussL[9], ussR[9], pssL[9], pssR[9];
+        R sM = sstar_hllc(pLt, pRt, pl[irho], pr[irho], pl[ivn], pr[ivn], sL, sR, pl[ibn], pr[ibn]);
+        for (int i = irho; i <= itau; ++i) usL[i] = ul[i] * (sL - pl[ivn]) / (sL - sM);
+        for (int i = irho; i <= itau; ++i) usR[i] = ur[i] * (sR - pr[ivn]) / (sR - sM);
+        R sstarL = sM - abs_(pl[ibn]) / sqrt_(usL[irho]);
+        R sstarR = sM + abs_(pr[ibn]) / sqrt_(usR[irho]);
+        if (((sstarL - sL) < 1.0e-4 * (sM - sL)) || ((sstarR - sR) > -1.0e-4 * (sR - sM))) {
+            usL[ibn] = pl[ibn];
+            usL[ibt1] = hll_state(pl[ibt1], pr[ibt1], fl[ibt1], fr[ibt1], sL, sR);
+            usL[ibt2] = hll_state(pl[ibt2], pr[ibt2], fl[ibt2], fr[ibt2], sL, sR);
+            usR[ibn] = pr[ibn];
+            usR[ibt1] = usL[ibt1];
+            usR[ibt2] = usL[ibt2];
+            sstarL = sM;
+            sstarR = sM;
+        } else {
+            R fac_1 = (pl[irho] * (sL - pl[ivn]) * (sL - sM) - pl[ibn] * pl[ibn]);
+            usL[ibn] = pl[ibn];
+            usL[ibt1] = (pl[ibt1] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
+            usL[ibt2] = (pl[ibt2] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
+            fac_1 = (pr[irho] * (sR - pr[ivn]) * (sR - sM) - pr[ibn] * pr[ibn]);
+            usR[ibn] = pr[ibn];
+            usR[ibt1] = (pr[ibt1] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
+            usR[ibt2] = (pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
+        }
+        usL[ivn] = usL[irho] * sM;
+        usL[ivt1] = usL[ivt1] - (usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1]) / (sL - sM);
+        usL[ivt2] = usL[ivt2] - (usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2]) / (sL - sM);
+        usR[ivn] = usR[irho] * sM;
+        usR[ivt1] = usR[ivt1] - (usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1]) / (sR - sM);
+        usR[ivt2] = usR[ivt2] - (usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2]) / (sR - sM);
+        pstL[ivn] = sM;
+        pstL[ivt1] = usL[ivt1] / usL[irho];
+        pstL[ivt2] = usL[ivt2] / usL[irho];
+        pstR[ivn] = sM;
+        pstR[ivt1] = usR[ivt1] / usR[irho];
+        pstR[ivt2] = usR[ivt2] / usR[irho];
+        R pLs = pl[irho] * (sL - pl[ivn]) * (sM - pl[ivn]) + pLt;
+        R pRs = pr[irho] * (sR - pr[ivn]) * (sM - pr[ivn]) + pRt;
+        R bdotu = pl[ibx] * pl[ivx] + pl[iby] * pl[ivy] + pl[ibz] * pl[ivz];
+        R bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
+        usL[itau] = usL[itau] + ((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn]) / (sL - sM);
+        bdotu = pr[ibx] * pr[ivx] + pr[iby] * pr[ivy] + pr[ibz] * pr[ivz];
+        bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
+        usR[itau] = usR[itau] + ((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn]) / (sR - sM);
+        if (sstarL >= 0.0) {
+            for (int i = imin; i <= imax; ++i) fo[i] = fl[i] + sL * (usL[i] - ul[i]);
+        } else if (sstarR <= 0.0) {
+            for (int i = imin; i <= imax; ++i) fo[i] = fr[i] + sR * (usR[i] - ur[i]);
+        } else {
+            ussL[irho] = usL[irho];
+            ussR[irho] = usR[irho];
+            R fac_1 = 1.0 / (sqrt_(usL[irho]) + sqrt_(usR[irho]));
+            R fac_2 = sign1_(pl[ibn]);
+            pssL[ivn] = sM;
+            pssL[ivt1] = fac_1 * (sqrt_(usL[irho]) * pstL[ivt1] + sqrt_(usR[irho]) * pstR[ivt1] + (usR[ibt1] - usL[ibt1]) * fac_2);
+            pssL[ivt2] = fac_1 * (sqrt_(usL[irho]) * pstL[ivt2] + sqrt_(usR[irho]) * pstR[ivt2] + (usR[ibt2] - usL[ibt2]) * fac_2);
+            ussL[ibt1] = fac_1 * (sqrt_(usL[irho]) * usR[ibt1] + sqrt_(usR[irho]) * usL[ibt1] + sqrt_(usL[irho] * usR[irho]) * (pstR[ivt1] - pstL[ivt1]) * fac_2);
+            ussL[ibt2] = fac_1 * (sqrt_(usL[irho]) * usR[ibt2] + sqrt_(usR[irho]) * usL[ibt2] + sqrt_(usL[irho] * usR[irho]) * (pstR[ivt2] - pstL[ivt2]) * fac_2);
+            ussL[ibn] = usL[ibn];
+            ussL[ivn] = ussL[irho] * pssL[ivn];
+            ussL[ivt1] = ussL[irho] * pssL[ivt1];
+            ussL[ivt2] = ussL[irho] * pssL[ivt2];
+            bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
+            R bdotuss = ussL[ibx] * pssL[ivx] + ussL[iby] * pssL[ivy] + ussL[ibz] * pssL[ivz];
+            ussL[itau] = usL[itau] - sqrt_(usL[irho]) * (bdotus - bdotuss) * fac_2;
+            pssR[ivn] = sM;
+            pssR[ivt1] = pssL[ivt1];
+            pssR[ivt2] = pssL[ivt2];
+            ussR[ibt1] = ussL[ibt1];
+            ussR[ibt2] = ussL[ibt2];
+            ussR[ibn] = usR[ibn];
+            ussR[ivn] = ussR[irho] * pssR[ivn];
+            ussR[ivt1] = ussR[irho] * pssR[ivt1];
+            ussR[ivt2] = ussR[irho] * pssR[ivt2];
+            bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
+            bdotuss = ussR[ibx] * pssR[ivx] + ussR[iby] * pssR[ivy] + ussR[ibz] * pssR[ivz];
+            ussR[itau] = usR[itau] + sqrt_(usR[irho]) * (bdotus - bdotuss) * fac_2;
+            if (sM >= 0.0) {
+                for (int i = imin; i <= imax; ++i) fo[i] = fl[i] + sL * (usL[i] - ul[i]) + sstarL * (ussL[i] - usL[i]);
+            } else {
+                for (int i = imin; i <= imax; ++i) fo[i] = fr[i] + sR * (usR[i] - ur[i]) + sstarR * (ussR[i] - usR[i]);
+            }
+        }
+    }
+
+    /* ================================================================ */
+    /* SPATIAL pieces                                                   */
+    /* ================================================================ */
+    /* GET_SOURCE spatial.f90:167-267 */
+    void get_source() {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    for (int i = imin; i <= imax; ++i) SC(i, j, k, l) = R(0.0);
+                    if (coord == 0) continue;
+                    R bx = BC(ibx, j, k, l), by = BC(iby, j, k, l), bz = BC(ibz, j, k, l);
+                    R rho = P(irho, j, k, l), vx = P(ivx, j, k, l), vy = P(ivy, j, k, l), vz = P(ivz, j, k, l), p = P(itau, j, k, l);
+                    R bsquare = bx * bx + by * by + bz * bz;
+                    if (coord == 1) {
+                        SC(ivx, j, k, l) = SC(ivx, j, k, l) + (p + rho * vy * vy + 0.5 * bsquare - by * by) / (x(j));
+                        SC(ivy, j, k, l) = SC(ivy, j, k, l) - (rho * vx * vy - bx * by) / (x(j));
+                    } else {
+                        R G = R(3.0 * x(j) * dx(j) / dx_cb(j));
+                        R tf = R(dsine(k) / dcose(k));
+                        SC(ivx, j, k, l) = SC(ivx, j, k, l) + (2.0 * p + bx * bx + rho * (vy * vy + vz * vz)) * G;
+                        SC(ivy, j, k, l) = SC(ivy, j, k, l) + (p + rho * vz * vz + 0.5 * bsquare - bz * bz) * G * tf
+                                           - (rho * vx * vy - bx * by) * G;
+                        SC(ivz, j, k, l) = SC(ivz, j, k, l) - (rho * vx * vz - bx * bz) * G
+                                           - (rho * vy * vz - by * bz) * G * tf;
+                    }
+                }
+    }
+
+    /* FLUX_DIFF spatial.f90:408-592 */
+    void flux_diff(int dir) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j)
+                    for (int i = imin; i <= itau; ++i) {
+                        R dflux;
+                        if (dir == x_dir) {
+                            if (coord == 0) dflux = (FL(i, j, k, l) - FL(i, j - 1, k, l)) / (dx(j));
+                            else if (coord == 1) dflux = (xF(j) * FL(i, j, k, l) - xF(j - 1) * FL(i, j - 1, k, l)) / (x(j) * dx(j));
+                            else dflux = (xF(j) * xF(j) * FL(i, j, k, l) - xF(j - 1) * xF(j - 1) * FL(i, j - 1, k, l)) / (dx_cb(j) / 3.0);
+                            LR(i, j, k, l) = -dflux;
+                        } else if (dir == y_dir) {
+                            if (coord == 0) dflux = (FL(i, j, k, l) - FL(i, j, k - 1, l)) / (dy(k));
+                            else if (coord == 1) dflux = (FL(i, j, k, l) - FL(i, j, k - 1, l)) / (x(j) * dy(k));
+                            else dflux = (sinf(k) * FL(i, j, k, l) - sinf(k - 1) * FL(i, j, k - 1, l)) / (xbar(j) * dcose(k));
+                            LR(i, j, k, l) = LR(i, j, k, l) - dflux;
+                        } else {
+                            if (coord == 0 || coord == 1) dflux = (FL(i, j, k, l) - FL(i, j, k, l - 1)) / dz(l);
+                            else dflux = (FL(i, j, k, l) - FL(i, j, k, l - 1)) * dy(k) / (xbar(j) * dz(l) * dcose(k));
+                            LR(i, j, k, l) = LR(i, j, k, l) - dflux;
+                        }
+                    }
+    }
+
+    /* MHD_FLUX mhd_module.f90:206-280 */
+    void mhd_flux(int dir) {
+        int jl, kl, ll;
+        face_range(dir, jl, kl, ll);
+        for (int l = ll; l <= nz; ++l)
+            for (int k = kl; k <= ny; ++k)
+                for (int j = jl; j <= nx; ++j) {
+                    if (dir == x_dir) { EF(iyx, j, k, l) = FL(ibz, j, k, l); EF(izx, j, k, l) = -FL(iby, j, k, l); }
+                    else if (dir == y_dir) { EF(ixy, j, k, l) = -FL(ibz, j, k, l); EF(izy, j, k, l) = FL(ibx, j, k, l); }
+                    else { EF(ixz, j, k, l) = FL(iby, j, k, l); EF(iyz, j, k, l) = -FL(ibx, j, k, l); }
+                }
+    }
+
+    /* BOUNDARY_EFIELD mhd_module.f90:478-840 */
+    void boundary_efield() {
+        auto ecv = [&](int i) { return [this, i](int j, int k, int l) -> R & { return EC(i, j, k, l); }; };
+        auto efv = [&](int i) { return [this, i](int j, int k, int l) -> R & { return EF(i, j, k, l); }; };
+        for (int i = iex; i <= iez; ++i) fill_x(ecv(i), bfac_xin[i], bfac_xout[i]);
+        fill_x(efv(ixz), bfac_xin[iex], bfac_xout[iex]);
+        fill_x(efv(ixy), bfac_xin[iex], bfac_xout[iex]);
+        fill_x(efv(iyz), bfac_xin[iey], bfac_xout[iey]);
+        fill_x(efv(izy), bfac_xin[iez], bfac_xout[iez]);
+        for (int i = iex; i <= iez; ++i) fill_y(ecv(i), bfac_yin[i], bfac_yout[i], false);
+        fill_y(efv(ixz), bfac_yin[iex], bfac_yout[iex], false);
+        fill_y(efv(iyx), bfac_yin[iey], bfac_yout[iey], false);
+        fill_y(efv(iyz), bfac_yin[iey], bfac_yout[iey], false);
+        fill_y(efv(izx), bfac_yin[iez], bfac_yout[iez], false);
+        for (int i = iex; i <= iez; ++i) fill_z(ecv(i), bfac_zin[i], bfac_zout[i]);
+        fill_z(efv(ixy), bfac_zin[iex], bfac_zout[iex]);
+        fill_z(efv(iyx), bfac_zin[iey], bfac_zout[iey]);
+        fill_z(efv(izx), bfac_zin[iez], bfac_zout[iez]);
+        fill_z(efv(izy), bfac_zin[iez], bfac_zout[iez]);
+    }
+
+    /* flux_ct mhd_module.f90:285-473 */
+    void flux_ct() {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    EC(iex, j, k, l) = P(ivz, j, k, l) * BC(iby, j, k, l) - P(ivy, j, k, l) * BC(ibz, j, k, l);
+                    EC(iey, j, k, l) = P(ivx, j, k, l) * BC(ibz, j, k, l) - P(ivz, j, k, l) * BC(ibx, j, k, l);
+                    EC(iez, j, k, l) = P(ivy, j, k, l) * BC(ibx, j, k, l) - P(ivx, j, k, l) * BC(iby, j, k, l);
+                }
+        if (n_dim == 1) {
+            for (int j = 1; j <= nx; ++j) {
+                EF(ixy, j, 1, 1) = EC(iex, j, 1, 1);
+                EF(izy, j, 1, 1) = EC(iez, j, 1, 1);
+                EF(ixy, j, 0, 1) = EC(iex, j, 1, 1);
+                EF(izy, j, 0, 1) = EC(iez, j, 1, 1);
+                EF(ixz, j, 1, 1) = EC(iex, j, 1, 1);
+                EF(iyz, j, 1, 1) = EC(iey, j, 1, 1);
+                EF(ixz, j, 1, 0) = EC(iex, j, 1, 1);
+                EF(iyz, j, 1, 0) = EC(iey, j, 1, 1);
+            }
+        } else if (n_dim == 2) {
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    EF(ixz, j, k, 1) = EC(iex, j, k, 1);
+                    EF(iyz, j, k, 1) = EC(iey, j, k, 1);
+                    EF(ixz, j, k, 0) = EC(iex, j, k, 1);
+                    EF(iyz, j, k, 0) = EC(iey, j, k, 1);
+                }
+        }
+        boundary_efield();
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 0; l <= nz; ++l)
+            for (int k = 0; k <= ny; ++k)
+                for (int j = 0; j <= nx; ++j) {
+                    EX(j, k, l) = 0.50 * (EF(ixy, j, k, l) + EF(ixy, j, k, l + 1) + EF(ixz, j, k, l) + EF(ixz, j, k + 1, l))
+                                  - 0.25 * (EC(iex, j, k, l) + EC(iex, j, k, l + 1) + EC(iex, j, k + 1, l) + EC(iex, j, k + 1, l + 1));
+                    EY(j, k, l) = 0.50 * (EF(iyx, j, k, l) + EF(iyx, j, k, l + 1) + EF(iyz, j, k, l) + EF(iyz, j + 1, k, l))
+                                  - 0.25 * (EC(iey, j, k, l) + EC(iey, j, k, l + 1) + EC(iey, j + 1, k, l) + EC(iey, j + 1, k, l + 1));
+                    EZ(j, k, l) = 0.50 * (EF(izx, j, k, l) + EF(izx, j, k + 1, l) + EF(izy, j, k, l) + EF(izy, j + 1, k, l))
+                                  - 0.25 * (EC(iez, j, k, l) + EC(iez, j, k + 1, l) + EC(iez, j + 1, k, l) + EC(iez, j + 1, k + 1, l));
+                }
+        if (cfg.fixpole && coord == 2) {
+            /* mhd_module.f90:437-461: REAL (single precision) accumulators */
+            for (int j = 1; j <= nx; ++j) {
+                float sum1 = 0.0f, sum2 = 0.0f;
+                for (int l = 1; l <= nz; ++l) {
+                    sum1 = (float)((double)sum1 + dv(EX(j, 0, l)));
+                    sum2 = (float)((double)sum2 + dv(EX(j, ny, l)));
+                }
+                for (int l = -2; l <= nz + 3; ++l) {
+                    EX(j, 0, l) = R((double)sum1 / (double)nz);
+                    EX(j, ny, l) = R((double)sum2 / (double)nz);
+                }
+            }
+        }
+    }
+
+    /* l_operator spatial.f90:597-713 */
+    void l_operator() {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j)
+                    for (int i = imin; i <= itau; ++i) LR(i, j, k, l) = LR(i, j, k, l) + SC(i, j, k, l);
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 0; l <= nz; ++l)
+            for (int k = 0; k <= ny; ++k)
+                for (int j = 0; j <= nx; ++j) {
+                    if (coord == 0) {
+                        LR(ibx, j, k, l) = -((EZ(j, k, l) - EZ(j, k - 1, l)) / (dy(k)) - (EY(j, k, l) - EY(j, k, l - 1)) / (dz(l)));
+                        LR(iby, j, k, l) = -((EX(j, k, l) - EX(j, k, l - 1)) / (dz(l)) - (EZ(j, k, l) - EZ(j - 1, k, l)) / (dx(j)));
+                        LR(ibz, j, k, l) = -((EY(j, k, l) - EY(j - 1, k, l)) / (dx(j)) - (EX(j, k, l) - EX(j, k - 1, l)) / (dy(k)));
+                    } else if (coord == 1) {
+                        LR(ibx, j, k, l) = -(EZ(j, k, l) - EZ(j, k - 1, l)) / (xF(j) * dy(k)) + (EY(j, k, l) - EY(j, k, l - 1)) / (dz(l));
+                        LR(iby, j, k, l) = -(EX(j, k, l) - EX(j, k, l - 1)) / (dz(l)) + (EZ(j, k, l) - EZ(j - 1, k, l)) / (dx(j));
+                        LR(ibz, j, k, l) = -(xF(j) * EY(j, k, l) - xF(j - 1) * EY(j - 1, k, l)) / (x(j) * dx(j)) + (EX(j, k, l) - EX(j, k - 1, l)) / (x(j) * dy(k));
+                    } else {
+                        LR(ibx, j, k, l) = (-(sinf(k) * EZ(j, k, l) - sinf(k - 1) * EZ(j, k - 1, l)) + (EY(j, k, l) - EY(j, k, l - 1)) * (dy(k) / dz(l))) / (xF(j) * dcose(k) + small_num);
+                        LR(iby, j, k, l) = (-(EX(j, k, l) - EX(j, k, l - 1)) / (xbar(j) * sinf(k) * dz(l) + small_num) + (xF(j) * EZ(j, k, l) - xF(j - 1) * EZ(j - 1, k, l)) / (x(j) * dx(j)));
+                        LR(ibz, j, k, l) = (-(xF(j) * EY(j, k, l) - xF(j - 1) * EY(j - 1, k, l)) / (x(j) * dx(j)) + (EX(j, k, l) - EX(j, k - 1, l)) / (xbar(j) * dy(k)));
+                    }
+                }
+    }
+
+    /* SPATIAL spatial.f90:11-162 */
+    void spatial() {
+        get_source();
+        custom_source();
+        for (int dir = 1; dir <= n_dim; ++dir) {
+            recon(dir);
+            buildstates(dir);
+            riemann(dir);
+            flux_diff(dir);
+            mhd_flux(dir);
+        }
+        flux_ct();
+        l_operator();
+    }
+
+    /* ================================================================ */
+    /* time integration, rungekutta.f90                                 */
+    /* ================================================================ */
+    void rk_combine(int stage, double dt) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 0; l <= nz; ++l)
+            for (int k = 0; k <= ny; ++k)
+                for (int j = 0; j <= nx; ++j)
+                    for (int i = imin; i <= imax; ++i) {
+                        /* the reference's l_rk is undefined for hydro at index 0
+                         * (spatial.f90:440-449 fills 1..n); zero it here */
+                        bool ghost0 = (j == 0 || k == 0 || l == 0);
+                        R lr = (ghost0 && i < ibx) ? R(0.0) : LR(i, j, k, l);
+                        if (stage == 1) U(i, j, k, l) = UO(i, j, k, l) + dt * lr;
+                        else if (stage == 2) U(i, j, k, l) = rk20 * UO(i, j, k, l) + rk21 * U(i, j, k, l) + rk22 * dt * lr;
+                        else U(i, j, k, l) = rk30 * UO(i, j, k, l) + rk31 * U(i, j, k, l) + rk32 * dt * lr;
+                    }
+    }
+
+    /* RUNGEKUTTA rungekutta.f90:12-208 */
+    void rungekutta(double dt) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int l = 0; l <= nz; ++l)
+            for (int k = 0; k <= ny; ++k)
+                for (int j = 0; j <= nx; ++j)
+                    for (int i = imin; i <= imax; ++i) UO(i, j, k, l) = U(i, j, k, l);
+        for (int stage = 1; stage <= 3; ++stage) {
+            spatial();
+            rk_combine(stage, dt);
+            fromutorve();
+            custom_checkrho();
+            if (stage == 3) custom_checkrho(); /* OPERATOR_SPLIT is empty */
+            fromrvetou();
+            boundary();
+            update();
+        }
+    }
+
+    /* INITIAL_UPDATE initial.f90:86-116 */
+    void initial_update() {
+        custom_checkrho();
+        fromrvetou();
+        boundary();
+        update();
+    }
+
+    /* FINDDT rungekutta.f90:221-332 */
+    double finddt() {
+        double dt_out2 = 1.0e5;
+#pragma omp parallel for collapse(2) schedule(static) reduction(min : dt_out2)
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    R rho = P(irho, j, k, l);
+                    R a2 = CS(j, k, l) * CS(j, k, l);
+                    R a4 = a2 * a2;
+                    R b2x = (BC(ibx, j, k, l) * BC(ibx, j, k, l) / rho);
+                    R b2y = (BC(iby, j, k, l) * BC(iby, j, k, l) / rho);
+                    R b2z = (BC(ibz, j, k, l) * BC(ibz, j, k, l) / rho);
+                    R b2 = b2x + b2y + b2z;
+                    R b4 = b2 * b2;
+                    R cfx = sqrt_(0.5 * (a2 + b2 + sqrt_((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2x)));
+                    R cfy = sqrt_(0.5 * (a2 + b2 + sqrt_((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2y)));
+                    R cfz = sqrt_(0.5 * (a2 + b2 + sqrt_((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2z)));
+                    R lambda1 = abs_(P(ivx, j, k, l)) + cfx;
+                    R lambda2 = abs_(P(ivy, j, k, l)) + cfy;
+                    R lambda3 = abs_(P(ivz, j, k, l)) + cfz;
+                    R lambda = max3_(lambda1, lambda2, lambda3);
+                    R dtt = R(dx(j));
+                    if (coord == 0) {
+                        if (n_dim > 1) dtt = min_(dtt, R(dy(k)));
+                        if (n_dim > 2) dtt = min_(dtt, R(dz(l)));
+                    } else if (coord == 1) {
+                        if (n_dim > 1 && ny > 1) dtt = min_(dtt, R(x(j) * dy(k)));
+                        if (n_dim > 2) dtt = min_(dtt, R(dz(l)));
+                    } else {
+                        if (n_dim > 1) dtt = min_(dtt, R(x(j) * dy(k)));
+                        if (n_dim > 2) dtt = min_(dtt, R(x(j) * sine(k) * dz(l)));
+                    }
+                    dtt = dtt * cfl / lambda;
+                    double d = dv(dtt);
+                    if (d < dt_out2) dt_out2 = d;
+                }
+        return std::min(1.0e5, dt_out2);
+    }
+
+    /* FIND_DIVB mhd_module.f90:110-201 */
+    double find_divb() {
+        double m = 0.0;
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    double d;
+                    double bx = dv(P(ibx, j, k, l)), bxm = dv(P(ibx, j - 1, k, l));
+                    double by = dv(P(iby, j, k, l)), bym = dv(P(iby, j, k - 1, l));
+                    double bz = dv(P(ibz, j, k, l)), bzm = dv(P(ibz, j, k, l - 1));
+                    if (coord == 0)
+                        d = (bx - bxm) / (dx(j)) + (by - bym) / (dy(k)) + (bz - bzm) / (dz(l));
+                    else if (coord == 1)
+                        d = (xF(j) * bx - xF(j - 1) * bxm) / (x(j) * dx(j)) + (by - bym) / (x(j) * dy(k)) + (bz - bzm) / (dz(l));
+                    else
+                        d = (xF(j) * xF(j) * bx - xF(j - 1) * xF(j - 1) * bxm) / (dx_cb(j) / 3.0)
+                            + (sinf(k) * by - sinf(k - 1) * bym) * (x(j) * dx(j)) / (dx_cb(j) * dcose(k) / 3.0)
+                            + (bz - bzm) * (x(j) * dx(j) * dy(k)) / (dx_cb(j) * dcose(k) * dz(l) / 3.0);
+                    m = std::max(m, std::fabs(d));
+                }
+        return m;
+    }
+};
+
+/* ------------------------------------------------------------------ */
+/* C API (used by tests, smoke and the bench baselines only)           */
+/* ------------------------------------------------------------------ */
+struct Handle {
+    int counting;
+    Sim<double> *d = nullptr;
+    Sim<CReal> *c = nullptr;
+    std::string err;
+};
+
+static std::string g_err;
+
+} // namespace orc
+
+using namespace orc;
+
+template <class R>
+static void set_state_t(Sim<R> *s, const double *prim, const double *eps) {
+    size_t n3 = (size_t)s->NX * s->NY * s->NZ;
+    for (size_t i = 0; i < 8 * n3; ++i) s->prim[i] = R(prim[i]);
+    for (size_t i = 0; i < n3; ++i) s->eps[i] = R(eps[i]);
+}
+template <class R>
+static void get_state_t(Sim<R> *s, double *prim, double *eps) {
+    size_t n3 = (size_t)s->NX * s->NY * s->NZ;
+    for (size_t i = 0; i < 8 * n3; ++i) prim[i] = dv(s->prim[i]);
+    for (size_t i = 0; i < n3; ++i) eps[i] = dv(s->eps[i]);
+}
+
+extern "C" {
+
+void *orc_create(const cumc_config *cfg, int counting) {
+    Handle *h = new Handle();
+    h->counting = counting;
+    int rc;
+    if (counting) { h->c = new Sim<CReal>(); rc = h->c->init(cfg); if (rc) g_err = h->c->err; }
+    else { h->d = new Sim<double>(); rc = h->d->init(cfg); if (rc) g_err = h->d->err; }
+    if (rc) { delete h->c; delete h->d; delete h; return nullptr; }
+    return h;
+}
+const char *orc_last_error(void) { return g_err.c_str(); }
+
+void orc_destroy(void *p) {
+    Handle *h = (Handle *)p;
+    if (!h) return;
+    delete h->c; delete h->d; delete h;
+}
+
+void orc_set_state(void *p, const double *prim, const double *eps) {
+    Handle *h = (Handle *)p;
+    if (h->counting) set_state_t(h->c, prim, eps); else set_state_t(h->d, prim, eps);
+}
+void orc_get_state(void *p, double *prim, double *eps) {
+    Handle *h = (Handle *)p;
+    if (h->counting) get_state_t(h->c, prim, eps); else get_state_t(h->d, prim, eps);
+}
+/* which: 0 cons, 1 bcell, 2 cs */
+void orc_get_array(void *p, int which, double *out) {
+    Handle *h = (Handle *)p;
+    auto grab = [&](auto *s) {
+        size_t n3 = (size_t)s->NX * s->NY * s->NZ;
+        if (which == 0) for (size_t i = 0; i < 8 * n3; ++i) out[i] = dv(s->cons[i]);
+        else if (which == 1) for (size_t i = 0; i < 3 * n3; ++i) out[i] = dv(s->bcell[i]);
+        else if (which == 2) for (size_t i = 0; i < n3; ++i) out[i] = dv(s->cs[i]);
+    };
+    if (h->counting) grab(h->c); else grab(h->d);
+}
+void orc_initial_update(void *p) {
+    Handle *h = (Handle *)p;
+    if (h->counting) h->c->initial_update(); else h->d->initial_update();
+}
+double orc_finddt(void *p) {
+    Handle *h = (Handle *)p;
+    return h->counting ? h->c->finddt() : h->d->finddt();
+}
+void orc_rk3_step(void *p, double dt) {
+    Handle *h = (Handle *)p;
+    if (h->counting) h->c->rungekutta(dt); else h->d->rungekutta(dt);
+}
+/* main.f90:98-139 loop; returns the number of steps */
+int orc_evolve(void *p, double t_end, int max_steps, double *t_inout) {
+    Handle *h = (Handle *)p;
+    double t = *t_inout;
+    int n = 0;
+    while (t < t_end && n < max_steps) {
+        double dt = orc_finddt(p);
+        if (t + dt > t_end) dt = t_end - t;
+        orc_rk3_step(h, dt);
+        t = t + dt;
+        ++n;
+    }
+    *t_inout = t;
+    return n;
+}
+double orc_max_divb(void *p) {
+    Handle *h = (Handle *)p;
+    return h->counting ? h->c->find_divb() : h->d->find_divb();
+}
+void orc_reset_counts(void) { g_ops = OpCounts(); }
+void orc_get_counts(uint64_t *out5) {
+    out5[0] = g_ops.add; out5[1] = g_ops.mul; out5[2] = g_ops.div; out5[3] = g_ops.sqrt; out5[4] = g_ops.cmp;
+}
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+} /* extern "C" */

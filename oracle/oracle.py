@@ -1,0 +1,135 @@
+"""ctypes front end of the CPU oracle (oracle/cumc_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline / reference legs of bench.py, never by the product package.
+
+PARITY UNPINNED: the reference is Fortran and cannot be built here (no
+Fortran compiler); it ships no golden vectors.  The oracle is a line-by-line
+restatement checked by invariants (tests/test_oracle_invariants.py).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(BUILD, "liboracle.so")
+SRC = os.path.join(HERE, "cumc_oracle.cpp")
+
+# one recipe for parity and timing: no FP contraction (bitwise order is kept),
+# OpenMP loops as in the reference's CPU build, generic x86-64 code.
+CXXFLAGS = ["-std=c++17", "-O3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared"]
+
+
+def build(force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+            os.path.getmtime(SRC), os.path.getmtime(os.path.join(HERE, "..", "include", "cumc3d_gpu.h"))):
+        subprocess.check_call(["g++"] + CXXFLAGS + ["-o", LIB, SRC])
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_void_p, C.c_int]
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_get_array.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_initial_update.argtypes = [C.c_void_p]
+        L.orc_finddt.argtypes = [C.c_void_p]
+        L.orc_finddt.restype = C.c_double
+        L.orc_rk3_step.argtypes = [C.c_void_p, C.c_double]
+        L.orc_evolve.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_double)]
+        L.orc_evolve.restype = C.c_int
+        L.orc_max_divb.argtypes = [C.c_void_p]
+        L.orc_max_divb.restype = C.c_double
+        L.orc_get_counts.argtypes = [C.POINTER(C.c_uint64)]
+        L.orc_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """Mirror of the engine's host API, running the CPU restatement."""
+
+    def __init__(self, spec, counting=False):
+        from cumc3d_b200.capi import make_config  # structures only
+        self.spec = spec
+        self._cfg, self._keep = make_config(spec)
+        L = lib()
+        self.h = L.orc_create(C.byref(self._cfg), 1 if counting else 0)
+        if not self.h:
+            raise ValueError("oracle create failed: %s" % L.orc_last_error().decode())
+        self.shape = (spec["nz"] + 6, spec["ny"] + 6, spec["nx"] + 6)
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, prim, eps):
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        assert prim.shape == self.shape + (8,) and eps.shape == self.shape
+        lib().orc_set_state(self.h, prim.ctypes.data, eps.ctypes.data)
+
+    def get_state(self):
+        prim = np.empty(self.shape + (8,))
+        eps = np.empty(self.shape)
+        lib().orc_get_state(self.h, prim.ctypes.data, eps.ctypes.data)
+        return prim, eps
+
+    def get_array(self, which):
+        ncomp = {0: 8, 1: 3, 2: 1}[which]
+        out = np.empty(self.shape + ((ncomp,) if ncomp > 1 else ()))
+        lib().orc_get_array(self.h, which, out.ctypes.data)
+        return out
+
+    def initial_update(self):
+        lib().orc_initial_update(self.h)
+
+    def finddt(self):
+        return lib().orc_finddt(self.h)
+
+    def rk3_step(self, dt):
+        lib().orc_rk3_step(self.h, dt)
+
+    def evolve(self, t_end, max_steps, t=0.0):
+        tt = C.c_double(t)
+        n = lib().orc_evolve(self.h, t_end, max_steps, C.byref(tt))
+        return tt.value, n
+
+    def max_divb(self):
+        return lib().orc_max_divb(self.h)
+
+
+def reset_counts():
+    lib().orc_reset_counts()
+
+
+def get_counts():
+    out = (C.c_uint64 * 5)()
+    lib().orc_get_counts(out)
+    return dict(add=out[0], mul=out[1], div=out[2], sqrt=out[3], cmp=out[4])
+
+
+def num_threads():
+    return lib().orc_num_threads()
