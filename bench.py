@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MHD stage engine (one JSON line on stdout, rank 0).
+
+Workload (the metric's headline configuration): 3D Cartesian MHD blast on
+256^3 zones over [-0.5,0.5]^3, periodic, gamma = 5/3, WENO-Z reconstruction,
+HLLD flux, constrained transport, SSP-RK3, CFL 0.4.  A step is one full RK3
+step (FINDDT + 3 stages) over all 256^3 zones; the workload is 200 steps.
+
+  value   zone-updates/s, device-timed with CUDA events on the engine's stream,
+          state resident in HBM (7 GB, far larger than the 126 MB L2);
+  e2e     the same metric through the C-ABI with host buffers: pinned-host
+          upload of the Fortran-layout state, INITIAL_UPDATE, the K steps and
+          the download of the result, all inside the wall-clock window;
+  roofline the dominant kernel's algorithmic HBM bytes per launch over its
+          CUDA-event duration, against the measured copy bandwidth;
+  cpu_baseline  the CPU oracle (a restatement of the reference's Fortran,
+          OpenMP on all host cores) on a bounded slab of the same workload.
+
+`--impl reference` times that CPU oracle alone (the reference itself is
+Fortran and cannot be built on this image).  For N > 1 each rank runs an
+independent replica (weak scaling); time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic HBM bytes of the fused face-flux kernel per zone (per launch):
+# read 5 primitives + 2 transverse cell fields + 1 face field, write 5 hydro
+# fluxes + 2 face EMFs, all FP64
+FLUX_BYTES_PER_ZONE = (8 + 7) * 8
+# whole RK3 step: 8 FP64 state words read+written per stage, u_old re-read in
+# stages 2 and 3: (64+64) + 3*64 + 3*64
+STEP_BYTES_PER_ZONE = 512
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+def cpu_oracle_rate(n, nz_slab, steps, workload):
+    """Wall-clock zone-updates/s of the CPU oracle on a slab of the workload."""
+    from cumc3d_b200 import models
+    from oracle import oracle as O
+    spec, prim, eps = workload(n, nz=nz_slab)
+    o = O.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = o.finddt()
+        o.rk3_step(dt)
+    el = time.perf_counter() - t0
+    zones = spec["nx"] * spec["ny"] * spec["nz"]
+    o.close()
+    return zones * steps / el, O.num_threads(), el
+
+
+def reference_arm(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from cumc3d_b200 import models
+    from oracle import oracle as O
+    O.build()
+    n = 48
+    spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
+    o = O.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    for _ in range(args.warmup):
+        o.rk3_step(o.finddt())
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.rk3_step(o.finddt())
+    el = time.perf_counter() - t0
+    zones = n ** 3
+    value = zones * args.steps / el
+    sample = "blast3d at %d^3 (same domain, same scheme), %d timed steps after %d warm-up" % (n, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "blast3d_256^3_weno_hlld_ct_rk3_cfl0.4 (reference arm: CPU oracle on a %d^3 sample)" % n,
+                   "recon": args.recon, "riemann": args.riemann},
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--recon", default="weno")
+    ap.add_argument("--riemann", default="hlld")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=2)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    world, rank, local, dist = dist_setup(args.gpus)
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import engine, models
+    torch.cuda.set_device(local)
+    engine.load_library()
+
+    n = args.n
+    spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)
+    zones = spec["nx"] * spec["ny"] * spec["nz"]
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.evolve(1e30, args.warmup)
+    s.sync()
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = s.launch_count()
+    e0.record(stream)
+    _, nsteps = s.evolve(1e30, args.steps)
+    e1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = s.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * zones * nsteps / (ms * 1e-3)
+
+    # per-kernel-class timing (CUDA events on the engine stream, eager launches)
+    prof = s.profile_step(args.profile_steps)
+    per_stage = {k: v for k, v in prof.items() if k != "dt"}
+    dominant = max(per_stage, key=per_stage.get)
+    launches_of = args.profile_steps * 3
+    avg_ms = prof[dominant] / launches_of
+    peak_gbs, peak_kind = load_peaks()
+    if dominant.startswith("flux"):
+        bytes_launch = FLUX_BYTES_PER_ZONE * zones
+        kname = "k_flux<%s,%s,%s>" % (dominant[-1], args.recon, args.riemann)
+    else:
+        bytes_launch = None
+        kname = dominant
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tdat = json.load(f)
+        key = "%s/%s/%s/%s" % (dominant, args.recon, args.riemann, args.precision)
+        if key in tdat:
+            traffic = tdat[key]["bytes_per_zone"] * zones
+    achieved = (bytes_launch / (avg_ms * 1e-3) / 1e9) if bytes_launch else None
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peak_kind,
+                "avg_launch_ms": avg_ms, "class_ms_per_step": {k: v / args.profile_steps for k, v in prof.items()}}
+    step_gbs = STEP_BYTES_PER_ZONE * value / world / 1e9
+    try:
+        fp64_peak = engine.fp64_peak_tflops()
+    except Exception:
+        fp64_peak = None
+
+    # end to end through the C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        hp = torch.from_numpy(prim).pin_memory()
+        he = torch.from_numpy(eps).pin_memory()
+        out_p = torch.empty_like(hp).pin_memory()
+        out_e = torch.empty_like(he).pin_memory()
+        s2 = engine.Solver(spec)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2.set_state_ptr(hp.data_ptr(), he.data_ptr())
+        s2.initial_update()
+        _, n2 = s2.evolve(1e30, args.steps)
+        s2.get_state_ptr(out_p.data_ptr(), out_e.data_ptr())
+        s2.sync()
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        s2.close()
+        nbytes_in = hp.numel() * 8 + he.numel() * 8
+        e2e = {"value": world * zones * n2 / el, "unit": "zone-updates/s",
+               "h2d_bytes_per_step": nbytes_in / max(n2, 1), "d2h_bytes_per_step": nbytes_in / max(n2, 1),
+               "wall_s": el, "steps": n2,
+               "note": "state upload and result download once per run of %d steps, amortised per step" % n2}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            nz_slab = 64
+            rate, cores, el = cpu_oracle_rate(n, nz_slab, 2, lambda nn, nz: models.blast_3d(
+                nn, nz=nz, recon=args.recon, riemann=args.riemann))
+            cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port",
+                   "sample": "CPU oracle, %dx%dx%d periodic slab of the blast, 2 RK3 steps (%.1f s)" % (
+                       n, n, nz_slab, el)}
+        except Exception as ex:  # the baseline must not hide the GPU number
+            cpu = {"value": None, "unit": "zone-updates/s", "cores": None, "kind": "port", "sample": "failed: %s" % ex}
+
+    s.close()
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+            "steps": nsteps, "warmup": args.warmup, "ms_per_step": ms / nsteps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": "blast3d_%d^3_%s_%s_ct_rk3_cfl0.4" % (n, args.recon, args.riemann),
+                       "grid": [n, n, n], "recon": args.recon, "riemann": args.riemann,
+                       "precision": args.precision, "boundary": "periodic", "steps_in_workload": 200,
+                       "l2": "state 7 GB resident in HBM, >> 126 MB L2 (no flush needed)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": roofline,
+            "step_hbm": {"bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved_gbs": step_gbs,
+                         "frac": step_gbs / peak_gbs},
+            "fp64_peak_tflops_measured": fp64_peak,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

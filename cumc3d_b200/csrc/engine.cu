@@ -1,0 +1,1352 @@
+// engine.cu -- stage kernels, ghost fills, time loop and the C-ABI of the
+// B200 MHD stage engine (declared in include/cumc3d_gpu.h).
+//
+// One RK stage of the reference (solver/mhd/rungekutta.f90:61-100) is issued
+// as the kernel sequence
+//
+//   k_flux x/y/z        recon + EOS + BUILDSTATES + Riemann + MHD_FLUX      (flux_kernel.cuh)
+//   k_ecell             cell EMF + the 1D/2D face-EMF fill                  (mhd_module.f90:310-356)
+//   k_ebnd x/y/z        BOUNDARY_EFIELD                                     (mhd_module.f90:478-840)
+//   k_edge              edge EMFs (GS05 arithmetic average)                 (mhd_module.f90:364-432)
+//   k_fixpole           FIXPOLE axis average (spherical only)               (mhd_module.f90:437-461)
+//   k_rk                FLUX_DIFF + GET_SOURCE + CUSTOM_SOURCE + l_operator
+//                       + the Shu-Osher stage combination                   (spatial.f90:167-713,
+//                                                                            rungekutta.f90:61-167)
+//   k_recover           FROMUTORVE + CUSTOM_CHECKRHO + FROMRVETOU
+//                       + FINDPRESSURE on the interior                       (fromrvetou.f90, update.f90)
+//   k_cons0             FROMRVETOU on the index-0 ghost layer (face fields)
+//   k_bnd x/y/z         BOUNDARY (prim, bcell, epsilon, p, c_s)              (boundary.f90:5-770)
+//   k_custom_bc         CUSTOM_BOUNDARY_X/Z of the torus models
+//
+// FINDDT is a deterministic min-reduction (exact, order independent) whose
+// result stays on the device; a whole step is captured once as a CUDA graph
+// and replayed by cumc_evolve.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cumc3d_gpu.h"
+#include "engine.cuh"
+#include "mhd_device.cuh"
+
+namespace cumc {
+
+static const double rk20 = 3.0 / 4.0, rk21 = 1.0 / 4.0, rk22 = 1.0 / 4.0;
+static const double rk30 = 1.0 / 3.0, rk31 = 2.0 / 3.0, rk32 = 2.0 / 3.0;
+static const double small_num = 2.2250738585072014e-308;  // TINY(1.0D0)
+
+// grid-metric accessors (offsets +2 for cell arrays, +3 for face arrays)
+#define XC(j) d.x[(j) + 2]
+#define DX(j) d.dx[(j) + 2]
+#define XF(j) d.xF[(j) + 3]
+#define XBAR(j) d.xbar[(j) + 2]
+#define DXCB(j) d.dx_cb[(j) + 2]
+#define DY(k) d.dy[(k) + 2]
+#define SINE(k) d.sine[(k) + 2]
+#define SINF(k) d.sinf[(k) + 3]
+#define DCOSE(k) d.dcose[(k) + 2]
+#define DSINE(k) d.dsine[(k) + 2]
+#define ZC(l) d.z[(l) + 2]
+#define DZ(l) d.dz[(l) + 2]
+
+__device__ __forceinline__ void set_error(const Dev &d, int code, int cell, int stage) {
+    if (atomicCAS(&d.S->err_code, 0, code) == 0) {
+        d.S->err_cell = cell;
+        d.S->err_stage = stage;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// cell EMFs + the 1D/2D face-EMF assignment, mhd_module.f90:310-356
+// ---------------------------------------------------------------------------
+__global__ void k_ecell(const Dev d) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int l = blockIdx.z + 1;
+    if (j > d.nx || k > d.ny || l > d.nz) return;
+    const int c = cidx(d, j, k, l);
+    const double vx = d.P[1][c], vy = d.P[2][c], vz = d.P[3][c];
+    const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
+    const double ex = vz * by - vy * bz;
+    const double ey = vx * bz - vz * bx;
+    const double ez = vy * bx - vx * by;
+    d.EC[0][c] = ex;
+    d.EC[1][c] = ey;
+    d.EC[2][c] = ez;
+    if (d.n_dim == 1) {
+        const int c0y = cidx(d, j, 0, 1), c0z = cidx(d, j, 1, 0);
+        d.EF[e_xy][c] = ex;
+        d.EF[e_zy][c] = ez;
+        d.EF[e_xy][c0y] = ex;
+        d.EF[e_zy][c0y] = ez;
+        d.EF[e_xz][c] = ex;
+        d.EF[e_yz][c] = ey;
+        d.EF[e_xz][c0z] = ex;
+        d.EF[e_yz][c0z] = ey;
+    } else if (d.n_dim == 2) {
+        const int c0z = cidx(d, j, k, 0);
+        d.EF[e_xz][c] = ex;
+        d.EF[e_yz][c] = ey;
+        d.EF[e_xz][c0z] = ex;
+        d.EF[e_yz][c0z] = ey;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ghost fills.  Each pass covers one axis for every cell of the other two
+// padded axes, exactly like the reference's sequential x -> y -> z loops.
+// ---------------------------------------------------------------------------
+// source index of ghost layer g (1..3) on one side of an axis with n cells
+__device__ __forceinline__ int ghost_src(int flag, bool inner, int g, int n) {
+    if (flag == 0) {  // periodic: modular map (equals the reference's sequential copy)
+        int dst = inner ? 1 - g : n + g;
+        return ((dst - 1) % n + n) % n + 1;
+    }
+    if (flag == 1) return inner ? 1 : n;  // outflow
+    return inner ? g : n + 1 - g;         // reflect/axis/equator (parity applied by caller)
+}
+
+struct FillList {
+    double *a[16];
+    signed char par[16];  // parity factor, 0 = plain copy
+    int n;
+};
+
+__device__ __forceinline__ void fill_one(const FillList &fl, int dst, int src, bool parity) {
+#pragma unroll 4
+    for (int m = 0; m < fl.n; ++m) {
+        double v = fl.a[m][src];
+        if (parity) v = (double)fl.par[m] * v;
+        fl.a[m][dst] = v;
+    }
+}
+
+// AXIS: 0 x, 1 y, 2 z.  Thread grid: (other0 padded) x (other1 padded) x 3 layers.
+template <int AXIS>
+__global__ void k_fill(const Dev d, const FillList in_list, const FillList out_list, int eps_out_mode) {
+    if (d.S->done) return;
+    int o0 = blockIdx.x * blockDim.x + threadIdx.x;  // fastest remaining axis, padded index
+    int o1 = blockIdx.y;
+    int g = blockIdx.z + 1;
+    int n, flag_in, flag_out, dstride;
+    int j, k, l;
+    if (AXIS == 0) {
+        if (o0 >= d.NY) return;
+        k = o0 - 2; l = o1 - 2; j = 0;
+        n = d.nx; flag_in = d.bf[0]; flag_out = d.bf[1]; dstride = 1;
+    } else if (AXIS == 1) {
+        if (o0 >= d.NX) return;
+        j = o0 - 2; l = o1 - 2; k = 0;
+        n = d.ny; flag_in = d.bf[2]; flag_out = d.bf[3]; dstride = d.NX;
+    } else {
+        if (o0 >= d.NX) return;
+        j = o0 - 2; k = o1 - 2; l = 0;
+        n = d.nz; flag_in = d.bf[4]; flag_out = d.bf[5]; dstride = d.NX * d.NY;
+    }
+    const int base = cidx(d, j, k, l);  // index of position 0 along AXIS
+    // inner side
+    {
+        int s = ghost_src(flag_in, true, g, n);
+        fill_one(in_list, base + (1 - g) * dstride, base + s * dstride, flag_in >= 2);
+    }
+    // outer side
+    {
+        int s = ghost_src(flag_out, false, g, n);
+        fill_one(out_list, base + (n + g) * dstride, base + s * dstride, flag_out >= 2);
+    }
+    // epsilon with the BOUNDARY1D_NM y-outer rule (boundary.f90:243-282)
+    if (AXIS == 1 && eps_out_mode >= 0) {
+        int s = ghost_src(eps_out_mode, false, g, n);
+        double v = d.EPS[base + s * dstride];
+        d.EPS[base + (n + g) * dstride] = v;  // epsilon is even on every side
+    }
+}
+
+// CUSTOM_BOUNDARY_X/Z: torus velocity clamps (model/torus-cyn/src/custom.f90:146-208)
+__global__ void k_custom_bc(const Dev d) {
+    if (d.S->done) return;
+    const int o0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int o1 = blockIdx.y;
+    const int g = blockIdx.z + 1;
+    if (o0 < d.NY && o1 < d.NZ) {  // x ghosts: (k = o0-2, l = o1-2)
+        const int k = o0 - 2, l = o1 - 2;
+        const int ci = cidx(d, 1 - g, k, l), co = cidx(d, d.nx + g, k, l);
+        d.P[1][ci] = dmin(d.P[1][ci], 0.0);
+        d.P[1][co] = dmax(d.P[1][co], 0.0);
+    }
+    if (d.bc_kind == 1 && o0 < d.NX && o1 < d.NY) {  // z ghosts: (j = o0-2, k = o1-2)
+        const int j = o0 - 2, k = o1 - 2;
+        const int ci = cidx(d, j, k, 1 - g), co = cidx(d, j, k, d.nz + g);
+        d.P[3][ci] = dmin(d.P[3][ci], 0.0);
+        d.P[3][co] = dmax(d.P[3][co], 0.0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// edge EMFs, mhd_module.f90:364-432
+// ---------------------------------------------------------------------------
+__global__ void k_edge(const Dev d) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z;
+    if (j > d.nx || k > d.ny || l > d.nz) return;
+    const int c = cidx(d, j, k, l);
+    const int sy = d.NX, sz = d.NX * d.NY;
+    {
+        const double *fxy = d.EF[e_xy], *fxz = d.EF[e_xz], *ex = d.EC[0];
+        d.EX[c] = 0.50 * (fxy[c] + fxy[c + sz] + fxz[c] + fxz[c + sy])
+                  - 0.25 * (ex[c] + ex[c + sz] + ex[c + sy] + ex[c + sy + sz]);
+    }
+    {
+        const double *fyx = d.EF[e_yx], *fyz = d.EF[e_yz], *ey = d.EC[1];
+        d.EY[c] = 0.50 * (fyx[c] + fyx[c + sz] + fyz[c] + fyz[c + 1])
+                  - 0.25 * (ey[c] + ey[c + sz] + ey[c + 1] + ey[c + 1 + sz]);
+    }
+    {
+        const double *fzx = d.EF[e_zx], *fzy = d.EF[e_zy], *ez = d.EC[2];
+        d.EZ[c] = 0.50 * (fzx[c] + fzx[c + sy] + fzy[c] + fzy[c + 1])
+                  - 0.25 * (ez[c] + ez[c + sy] + ez[c + 1] + ez[c + 1 + sy]);
+    }
+}
+
+// FIXPOLE, mhd_module.f90:437-461 (single-precision accumulators, sequential order)
+__global__ void k_fixpole(const Dev d) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (j > d.nx) return;
+    float sum1 = 0.0f, sum2 = 0.0f;
+    for (int l = 1; l <= d.nz; ++l) {
+        sum1 = (float)((double)sum1 + d.EX[cidx(d, j, 0, l)]);
+        sum2 = (float)((double)sum2 + d.EX[cidx(d, j, d.ny, l)]);
+    }
+    const double a = (double)sum1 / (double)d.nz, b = (double)sum2 / (double)d.nz;
+    for (int l = -2; l <= d.nz + 3; ++l) {
+        d.EX[cidx(d, j, 0, l)] = a;
+        d.EX[cidx(d, j, d.ny, l)] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// du/dt and the Shu-Osher combination over j,k,l = 0..n
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_rk(const Dev d, int stage) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z;
+    if (j > d.nx || k > d.ny || l > d.nz) return;
+    const int c = cidx(d, j, k, l);
+    const int sy = d.NX, sz = d.NX * d.NY;
+    const double dt = d.S->dt;
+    double lr[8];
+    const bool interior = (j >= 1 && k >= 1 && l >= 1);
+    if (interior) {
+        // FLUX_DIFF, spatial.f90:436-583
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            double dflux, L;
+            const double *F = d.FX[i];
+            if (d.coord == 0) dflux = (F[c] - F[c - 1]) / (DX(j));
+            else if (d.coord == 1) dflux = (XF(j) * F[c] - XF(j - 1) * F[c - 1]) / (XC(j) * DX(j));
+            else dflux = (XF(j) * XF(j) * F[c] - XF(j - 1) * XF(j - 1) * F[c - 1]) / (DXCB(j) / 3.0);
+            L = -dflux;
+            if (d.n_dim > 1) {
+                F = d.FY[i];
+                if (d.coord == 0) dflux = (F[c] - F[c - sy]) / (DY(k));
+                else if (d.coord == 1) dflux = (F[c] - F[c - sy]) / (XC(j) * DY(k));
+                else dflux = (SINF(k) * F[c] - SINF(k - 1) * F[c - sy]) / (XBAR(j) * DCOSE(k));
+                L = L - dflux;
+            }
+            if (d.n_dim > 2) {
+                F = d.FZ[i];
+                if (d.coord != 2) dflux = (F[c] - F[c - sz]) / DZ(l);
+                else dflux = (F[c] - F[c - sz]) * DY(k) / (XBAR(j) * DZ(l) * DCOSE(k));
+                L = L - dflux;
+            }
+            lr[i] = L;
+        }
+        // GET_SOURCE (spatial.f90:191-256) + CUSTOM_SOURCE
+        double sc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        const double rho = d.P[0][c], vx = d.P[1][c], vy = d.P[2][c], vz = d.P[3][c], p = d.P[4][c];
+        if (d.coord != 0) {
+            const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
+            const double bsquare = bx * bx + by * by + bz * bz;
+            if (d.coord == 1) {
+                sc[1] = sc[1] + (p + rho * vy * vy + 0.5 * bsquare - by * by) / (XC(j));
+                sc[2] = sc[2] - (rho * vx * vy - bx * by) / (XC(j));
+            } else {
+                const double G = 3.0 * XC(j) * DX(j) / DXCB(j);
+                const double tf = DSINE(k) / DCOSE(k);
+                sc[1] = sc[1] + (2.0 * p + bx * bx + rho * (vy * vy + vz * vz)) * G;
+                sc[2] = sc[2] + (p + rho * vz * vz + 0.5 * bsquare - bz * bz) * G * tf - (rho * vx * vy - bx * by) * G;
+                sc[3] = sc[3] - (rho * vx * vz - bx * bz) * G - (rho * vy * vz - by * bz) * G * tf;
+            }
+        }
+        if (d.source_kind == 1) {  // model/riemann/src/custom.f90:299-312
+            sc[2] = sc[2] - d.g_const * rho;
+        } else if (d.source_kind == 2) {  // model/torus-cyn/src/custom.f90:298-314
+            const double diff = rho - d.rho_floor;
+            const double factor = dmax(sign1(diff), 0.0);
+            const double xj = XC(j), zl = ZC(l);
+            const double radius = sqrt(xj * xj + zl * zl);
+            const double dphidr = xj / radius / ((radius - d.r_sh) * (radius - d.r_sh));
+            const double dphidz = zl / radius / ((radius - d.r_sh) * (radius - d.r_sh));
+            sc[1] = sc[1] + (-(factor * rho * dphidr));
+            sc[3] = sc[3] + (-(factor * rho * dphidz));
+            sc[4] = sc[4] + (-(factor * rho * (vx * dphidr + vz * dphidz)));
+        } else if (d.source_kind == 3) {  // model/torus-sph/src/custom.f90 (radial)
+            const double diff = rho - d.rho_floor;
+            const double factor = dmax(sign1(diff), 0.0);
+            const double dphidr = 1.0 / ((XC(j) - d.r_sh) * (XC(j) - d.r_sh));
+            sc[1] = sc[1] + (-(factor * rho * dphidr));
+            sc[4] = sc[4] + (-(factor * rho * vx * dphidr));
+        }
+#pragma unroll
+        for (int i = 0; i < 5; ++i) lr[i] = lr[i] + sc[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) lr[i] = 0.0;  // undefined in the reference, never read back
+    }
+    // l_operator face-B induction, spatial.f90:639-702
+    {
+        const double *EX = d.EX, *EY = d.EY, *EZ = d.EZ;
+        if (d.coord == 0) {
+            lr[5] = -((EZ[c] - EZ[c - sy]) / (DY(k)) - (EY[c] - EY[c - sz]) / (DZ(l)));
+            lr[6] = -((EX[c] - EX[c - sz]) / (DZ(l)) - (EZ[c] - EZ[c - 1]) / (DX(j)));
+            lr[7] = -((EY[c] - EY[c - 1]) / (DX(j)) - (EX[c] - EX[c - sy]) / (DY(k)));
+        } else if (d.coord == 1) {
+            lr[5] = -(EZ[c] - EZ[c - sy]) / (XF(j) * DY(k)) + (EY[c] - EY[c - sz]) / (DZ(l));
+            lr[6] = -(EX[c] - EX[c - sz]) / (DZ(l)) + (EZ[c] - EZ[c - 1]) / (DX(j));
+            lr[7] = -(XF(j) * EY[c] - XF(j - 1) * EY[c - 1]) / (XC(j) * DX(j)) + (EX[c] - EX[c - sy]) / (XC(j) * DY(k));
+        } else {
+            lr[5] = (-(SINF(k) * EZ[c] - SINF(k - 1) * EZ[c - sy]) + (EY[c] - EY[c - sz]) * (DY(k) / DZ(l))) / (XF(j) * DCOSE(k) + small_num);
+            lr[6] = (-(EX[c] - EX[c - sz]) / (XBAR(j) * SINF(k) * DZ(l) + small_num) + (XF(j) * EZ[c] - XF(j - 1) * EZ[c - 1]) / (XC(j) * DX(j)));
+            lr[7] = (-(XF(j) * EY[c] - XF(j - 1) * EY[c - 1]) / (XC(j) * DX(j)) + (EX[c] - EX[c - sy]) / (XBAR(j) * DY(k)));
+        }
+    }
+    // rungekutta.f90:61-167
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const double u = d.U[i][c];
+        double un;
+        if (stage == 1) {
+            d.U0[i][c] = u;
+            un = u + dt * lr[i];
+        } else if (stage == 2) {
+            un = rk20 * d.U0[i][c] + rk21 * u + rk22 * dt * lr[i];
+        } else {
+            un = rk30 * d.U0[i][c] + rk31 * u + rk32 * dt * lr[i];
+        }
+        d.U[i][c] = un;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// recovery on the interior: FROMUTORVE (fromrvetou.f90:126-227), the model
+// floors (CUSTOM_CHECKRHO), FROMRVETOU (21-121) and FINDPRESSURE.
+// INIT = 1 is INITIAL_UPDATE's CHECKRHO -> FROMRVETOU -> FINDPRESSURE.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cell_b(const Dev &d, int j, int k, int l, double fx, double fxm, double fy, double fym,
+                                       double fz, double fzm, double *bc) {
+    if (d.coord == 0) {
+        bc[0] = 0.5 * (fx + fxm);
+        bc[1] = 0.5 * (fy + fym);
+        bc[2] = 0.5 * (fz + fzm);
+    } else if (d.coord == 1) {
+        bc[0] = (XF(j) * fx + XF(j - 1) * fxm) / (XF(j) + XF(j - 1));
+        bc[1] = 0.5 * (fy + fym);
+        bc[2] = 0.5 * (fz + fzm);
+    } else {
+        bc[0] = 1.5 * DX(j) / DXCB(j) * ((XF(j) * XF(j)) * fx + (XF(j - 1) * XF(j - 1)) * fxm);
+        bc[1] = 0.5 * DY(k) / DCOSE(k) * (SINF(k) * fy + SINF(k - 1) * fym);
+        bc[2] = 0.5 * (fz + fzm);
+    }
+}
+
+__device__ __forceinline__ void apply_floor(const Dev &d, double &rho, double &vx, double &vy, double &vz, double &e) {
+    if (d.floor_kind == 1) {  // model/riemann/src/custom.f90:272-278
+        e = dmax(e, 0.0);
+    } else if (d.floor_kind == 2) {  // model/torus-cyn/src/custom.f90:253-269
+        const double diff = rho - d.rho_floor;
+        const double factor = dmax(sign1(diff), 0.0);
+        rho = factor * rho + (1.0 - factor) * d.rho_floor;
+        vx = factor * vx;
+        vy = factor * vy;
+        vz = factor * vz;
+        e = factor * e + (1.0 - factor) * d.eps_floor;
+        if (e < 0.0) e = d.eps_floor;
+    }
+}
+
+template <int INIT>
+__global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int l = blockIdx.z + 1;
+    if (j > d.nx || k > d.ny || l > d.nz) return;
+    const int c = cidx(d, j, k, l);
+    const int sy = d.NX, sz = d.NX * d.NY;
+    double rho, vx, vy, vz, e, bfx, bfy, bfz, bc[3];
+    if (!INIT) {
+        const double *Ux = d.U[5], *Uy = d.U[6], *Uz = d.U[7];
+        bfx = Ux[c]; bfy = Uy[c]; bfz = Uz[c];
+        cell_b(d, j, k, l, bfx, Ux[c - 1], bfy, Uy[c - sy], bfz, Uz[c - sz], bc);
+        const double u0 = d.U[0][c];
+        rho = u0;
+        vx = d.U[1][c] / u0;
+        vy = d.U[2][c] / u0;
+        vz = d.U[3][c] / u0;
+        const double bsquare = bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2];
+        const double vsquare = vx * vx + vy * vy + vz * vz;
+        e = (d.U[4][c] - 0.5 * bsquare) / u0 - 0.5 * vsquare;
+    } else {
+        rho = d.P[0][c]; vx = d.P[1][c]; vy = d.P[2][c]; vz = d.P[3][c];
+        e = d.EPS[c];
+        bfx = d.P[5][c]; bfy = d.P[6][c]; bfz = d.P[7][c];
+    }
+    apply_floor(d, rho, vx, vy, vz, e);
+    if (stage == 3) apply_floor(d, rho, vx, vy, vz, e);  // second CUSTOM_CHECKRHO (rungekutta.f90:175-180)
+    // FROMRVETOU: the lower faces are this stage's new values except on the
+    // index-0 layer, which FROMUTORVE leaves untouched (fromrvetou.f90:201)
+    double fxm, fym, fzm;
+    if (!INIT) {
+        fxm = (j > 1) ? d.U[5][c - 1] : d.P[5][c - 1];
+        fym = (k > 1) ? d.U[6][c - sy] : d.P[6][c - sy];
+        fzm = (l > 1) ? d.U[7][c - sz] : d.P[7][c - sz];
+    } else {
+        fxm = d.P[5][c - 1];
+        fym = d.P[6][c - sy];
+        fzm = d.P[7][c - sz];
+    }
+    cell_b(d, j, k, l, bfx, fxm, bfy, fym, bfz, fzm, bc);
+    const double vsquare = vx * vx + vy * vy + vz * vz;
+    const double bsquare = bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2];
+    d.U[0][c] = rho;
+    d.U[1][c] = vx * rho;
+    d.U[2][c] = vy * rho;
+    d.U[3][c] = vz * rho;
+    d.U[4][c] = rho * (e + 0.5 * vsquare) + 0.5 * bsquare;
+    if (INIT) {
+        d.U[5][c] = bfx;
+        d.U[6][c] = bfy;
+        d.U[7][c] = bfz;
+    }
+    // FINDPRESSURE (model/riemann/src/findpressure.f90:88-97, torus floor branch)
+    const double g1 = d.gamma - 1.0;
+    double p, dpdrho, dpdeps;
+    if (d.floor_kind != 2 || rho > d.rho_floor) {
+        p = rho * e * g1;
+        dpdrho = e * g1;
+        dpdeps = rho * g1;
+    } else {
+        p = d.p_floor;
+        dpdrho = d.eps_floor * g1;
+        dpdeps = d.rho_floor * g1;
+    }
+    const double cs = sqrt(dpdrho + dpdeps * p / (rho * rho));
+    d.P[0][c] = rho;
+    d.P[1][c] = vx;
+    d.P[2][c] = vy;
+    d.P[3][c] = vz;
+    d.P[4][c] = p;
+    if (!INIT) {
+        d.P[5][c] = bfx;
+        d.P[6][c] = bfy;
+        d.P[7][c] = bfz;
+    }
+    d.EPS[c] = e;
+    d.BC[0][c] = bc[0];
+    d.BC[1][c] = bc[1];
+    d.BC[2][c] = bc[2];
+    d.CS[c] = cs;
+    // guard: a state no later stage can recover from
+    if (!(rho > 0.0) || !isfinite(e) || !isfinite(p) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz) || !isfinite(cs))
+        set_error(d, CUMC_ESTATE, c, stage);
+}
+
+// FROMRVETOU on the index-0 layer: cons face fields = prim face fields
+__global__ void k_cons0(const Dev d) {
+    if (d.S->done) return;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    const int plane = blockIdx.z;
+    int j, k, l;
+    if (plane == 0) { if (a > d.ny || b > d.nz) return; j = 0; k = a; l = b; }
+    else if (plane == 1) { if (a > d.nx || b > d.nz) return; j = a; k = 0; l = b; }
+    else { if (a > d.nx || b > d.ny) return; j = a; k = b; l = 0; }
+    const int c = cidx(d, j, k, l);
+    d.U[5][c] = d.P[5][c];
+    d.U[6][c] = d.P[6][c];
+    d.U[7][c] = d.P[7][c];
+}
+
+// ---------------------------------------------------------------------------
+// FINDDT, rungekutta.f90:221-332
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_finddt(const Dev d) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int l = blockIdx.z + 1;
+    double dtt = 1.0e5;
+    if (j <= d.nx && k <= d.ny && l <= d.nz) {
+        const int c = cidx(d, j, k, l);
+        const double rho = d.P[0][c];
+        const double a2 = d.CS[c] * d.CS[c];
+        const double a4 = a2 * a2;
+        const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
+        const double b2x = (bx * bx / rho);
+        const double b2y = (by * by / rho);
+        const double b2z = (bz * bz / rho);
+        const double b2 = b2x + b2y + b2z;
+        const double b4 = b2 * b2;
+        const double cfx = sqrt(0.5 * (a2 + b2 + sqrt((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2x)));
+        const double cfy = sqrt(0.5 * (a2 + b2 + sqrt((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2y)));
+        const double cfz = sqrt(0.5 * (a2 + b2 + sqrt((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2z)));
+        const double lambda1 = fabs(d.P[1][c]) + cfx;
+        const double lambda2 = fabs(d.P[2][c]) + cfy;
+        const double lambda3 = fabs(d.P[3][c]) + cfz;
+        const double lambda = dmax3(lambda1, lambda2, lambda3);
+        double t = DX(j);
+        if (d.coord == 0) {
+            if (d.n_dim > 1) t = dmin(t, DY(k));
+            if (d.n_dim > 2) t = dmin(t, DZ(l));
+        } else if (d.coord == 1) {
+            if (d.n_dim > 1 && d.ny > 1) t = dmin(t, XC(j) * DY(k));
+            if (d.n_dim > 2) t = dmin(t, DZ(l));
+        } else {
+            if (d.n_dim > 1) t = dmin(t, XC(j) * DY(k));
+            if (d.n_dim > 2) t = dmin(t, XC(j) * SINE(k) * DZ(l));
+        }
+        t = t * d.cfl / lambda;
+        if (t < dtt) dtt = t;  // NaN never wins (the oracle's comparison)
+    }
+    // deterministic min: positive doubles order like their bit patterns
+    unsigned long long bits = (unsigned long long)__double_as_longlong(dtt);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
+        bits = o < bits ? o : bits;
+    }
+    __shared__ unsigned long long wmin[32];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    if (lane == 0) wmin[warp] = bits;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+        unsigned long long b = lane < nw ? wmin[lane] : ~0ull;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            unsigned long long o = __shfl_xor_sync(0xffffffffu, b, off);
+            b = o < b ? o : b;
+        }
+        if (lane == 0) atomicMin(&d.S->dt_bits, b);
+    }
+}
+
+// dt = MIN(1.0D5, reduced); clamp to total_time (main.f90:104-106) when asked
+__global__ void k_dt_final(const Dev d, int clamp) {
+    if (d.S->done) return;
+    Scalars *S = d.S;
+    double dt = __longlong_as_double((long long)S->dt_bits);
+    if (!(dt < 1.0e5)) dt = 1.0e5;
+    if (clamp && S->t + dt > S->t_end) dt = S->t_end - S->t;
+    if (!(dt > 0.0) || !isfinite(dt)) {
+        if (S->err_code == 0) { S->err_code = CUMC_ESTATE; S->err_cell = -1; S->err_stage = 0; }
+    }
+    S->dt = dt;
+    S->dt_bits = (unsigned long long)__double_as_longlong(1.0e5);
+}
+
+// end of a step inside cumc_evolve: t += dt, count, stop conditions
+__global__ void k_step_end(const Dev d) {
+    Scalars *S = d.S;
+    if (S->done) return;
+    S->t = S->t + S->dt;
+    S->steps += 1;
+    if (!(S->t < S->t_end) || S->steps >= S->max_steps || S->err_code != 0) S->done = 1;
+}
+
+// FIND_DIVB, mhd_module.f90:110-201 (max |div B| from the face fields)
+__global__ void k_divb(const Dev d, unsigned long long *out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int l = blockIdx.z + 1;
+    double a = 0.0;
+    if (j <= d.nx && k <= d.ny && l <= d.nz) {
+        const int c = cidx(d, j, k, l);
+        const int sy = d.NX, sz = d.NX * d.NY;
+        const double bx = d.P[5][c], bxm = d.P[5][c - 1], by = d.P[6][c], bym = d.P[6][c - sy];
+        const double bz = d.P[7][c], bzm = d.P[7][c - sz];
+        double v;
+        if (d.coord == 0) v = (bx - bxm) / (DX(j)) + (by - bym) / (DY(k)) + (bz - bzm) / (DZ(l));
+        else if (d.coord == 1)
+            v = (XF(j) * bx - XF(j - 1) * bxm) / (XC(j) * DX(j)) + (by - bym) / (XC(j) * DY(k)) + (bz - bzm) / (DZ(l));
+        else
+            v = (XF(j) * XF(j) * bx - XF(j - 1) * XF(j - 1) * bxm) / (DXCB(j) / 3.0)
+                + (SINF(k) * by - SINF(k - 1) * bym) * (XC(j) * DX(j)) / (DXCB(j) * DCOSE(k) / 3.0)
+                + (bz - bzm) * (XC(j) * DX(j) * DY(k)) / (DXCB(j) * DCOSE(k) * DZ(l) / 3.0);
+        a = fabs(v);
+        if (!(a == a)) a = 0.0;
+    }
+    unsigned long long bits = (unsigned long long)__double_as_longlong(a);
+    for (int off = 16; off > 0; off >>= 1) {
+        unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
+        bits = o > bits ? o : bits;
+    }
+    if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0) atomicMax(out, bits);
+}
+
+// Fortran layout prim(8, j, k, l) <-> structure of arrays (8 x N3)
+__global__ void k_aos_to_soa(const Dev d, const double *__restrict__ aos, int nv, double *const *dst) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N3) return;
+    for (int v = 0; v < nv; ++v) dst[v][c] = aos[(size_t)c * nv + v];
+}
+__global__ void k_soa_to_aos(const Dev d, double *__restrict__ aos, int nv, const double *const *src) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.N3) return;
+    for (int v = 0; v < nv; ++v) aos[(size_t)c * nv + v] = src[v][c];
+}
+
+// FP64 pipe probe: independent DFMA chains, 8 per thread, no memory traffic
+__global__ void k_dfma_probe(double *out, int iters) {
+    double a[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = 1.0 + 1e-9 * (threadIdx.x + i);
+    const double b = 0.999999999, c = 1e-12;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a[i] = __fma_rn(a[i], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += a[i];
+    if (s == 123.456) out[0] = s;
+}
+
+}  // namespace cumc
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using namespace cumc;
+
+struct cumc_handle {
+    cumc_config cfg;
+    Dev d;
+    cudaStream_t stream = nullptr;
+    std::vector<void *> allocs;
+    std::string err;
+    bool have_state = false;
+    bool initialised = false;
+    int64_t launches = 0;
+    int kernels_per_step = 0;
+    // flux tiles (autotuned or default): block dims per direction
+    dim3 fblk[3];
+    // captured step graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    Scalars *S_host = nullptr;  // pinned mirror
+    unsigned long long *divb_dev = nullptr;
+    double *stage_aos = nullptr;   // 8*N3 doubles (the u_old block doubles as transpose staging)
+    double **ptr_tab = nullptr;    // device table of 8 array pointers for the transposes
+    int prof_class = -1;           // >= 0 while cumc_profile_step is recording
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    double prof_ms[16];
+};
+
+static std::string g_create_err;
+
+static int fail(cumc_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg; else g_create_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(h, CUMC_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+static double *dalloc(cumc_handle *h, size_t n) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, n * sizeof(double));
+    h->allocs.push_back(p);
+    return (double *)p;
+}
+
+template <class TT>
+static TT *upload(cumc_handle *h, const std::vector<TT> &v) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, v.size() * sizeof(TT)) != cudaSuccess) return nullptr;
+    cudaMemcpy(p, v.data(), v.size() * sizeof(TT), cudaMemcpyHostToDevice);
+    h->allocs.push_back(p);
+    return (TT *)p;
+}
+
+// --- setup-time host computations -------------------------------------------
+// SETUP_EQNS parity factors, solver/mhd/setup.f90:99-325
+static int setup_parity(cumc_handle *h, const int *bf, signed char out[6][12]) {
+    enum { ivx = 2, ivy = 3, ivz = 4, ibx = 6, iby = 7, ibz = 8, iex = 9, iey = 10, iez = 11 };
+    int b[6][12];
+    for (int s = 0; s < 6; ++s)
+        for (int i = 0; i < 12; ++i) b[s][i] = 1;
+    // x sides
+    for (int s = 0; s < 2; ++s) {
+        int f = bf[s];
+        if (f == 2) { b[s][ivx] = -1; b[s][ibx] = -1; }
+        else if (f == 3) { b[s][ivx] = -1; b[s][ibx] = -1; b[s][ivz] = -1; b[s][ibz] = -1; }
+        else if (f == 4) return fail(h, CUMC_EINVAL, "Equatorial symmetry is not allowed for the x-boundary");
+    }
+    for (int s = 2; s < 4; ++s) {
+        int f = bf[s];
+        if (f == 2) { b[s][ivy] = -1; b[s][iby] = -1; }
+        else if (f == 3) { b[s][ivy] = -1; b[s][iby] = -1; b[s][ivz] = -1; b[s][ibz] = -1; }
+        else if (f == 4) { b[s][ivy] = -1; b[s][ibx] = -1; b[s][ibz] = -1; }
+    }
+    for (int s = 4; s < 6; ++s) {
+        int f = bf[s];
+        if (f == 2) { b[s][ivz] = -1; b[s][ibz] = -1; }
+        else if (f == 3) return fail(h, CUMC_EINVAL, "Axial symmetry is not allowed for the z-boundary");
+        else if (f == 4) { b[s][ivz] = -1; b[s][ibx] = -1; b[s][iby] = -1; }
+    }
+    for (int s = 0; s < 6; ++s) {
+        int *x = b[s];
+        if (x[ivz] * x[iby] * x[ivy] * x[ibz] < 0) return fail(h, CUMC_EINVAL, "Error in boundary flags for vz and by");
+        x[iex] = x[ivz] * x[iby];
+        if (x[ivx] * x[ibz] * x[ivz] * x[ibx] < 0) return fail(h, CUMC_EINVAL, "Error in boundary flags for vx and bz");
+        x[iey] = x[ivx] * x[ibz];
+        if (x[ivy] * x[ibx] * x[ivx] * x[iby] < 0) return fail(h, CUMC_EINVAL, "Error in boundary flags for vy and bx");
+        x[iez] = x[ivy] * x[ibx];
+        for (int i = 0; i < 12; ++i) out[s][i] = (signed char)x[i];
+    }
+    return CUMC_OK;
+}
+
+// PPM_INTERPOLANT (ppmc_module.f90:91-145) and WENO_INTERPOLANT (weno_module.f90:117-149)
+static void ppm_w(double dm2, double dm1, double dc, double dp1, double dp2, double *w) {
+    double a1R = dc / (dc + dp1);
+    double a1L = dm1 / (dm1 + dc);
+    double aR = 2.0 * dp1 * dc / (dp1 + dc);
+    double aL = 2.0 * dc * dm1 / (dc + dm1);
+    double deltaXR = dm1 + dc + dp1 + dp2;
+    double deltaXL = dm2 + dm1 + dc + dp1;
+    double z1R = (dm1 + dc) / (2.0 * dc + dp1);
+    double z1L = (dm2 + dm1) / (2.0 * dm1 + dc);
+    double zR = (dp2 + dp1) / (2.0 * dp1 + dc);
+    double zL = (dp1 + dc) / (2.0 * dc + dm1);
+    double cc1 = dc / (dm1 + dc + dp1);
+    double cp1 = dp1 / (dc + dp1 + dp2);
+    double cm1 = dm1 / (dm2 + dm1 + dc);
+    double cc2 = (2.0 * dm1 + dc) / (dp1 + dc);
+    double cp2 = (2.0 * dc + dp1) / (dp2 + dp1);
+    double cm2 = (2.0 * dm2 + dm1) / (dc + dm1);
+    double cc3 = (dc + 2.0 * dp1) / (dm1 + dc);
+    double cp3 = (dp1 + 2.0 * dp2) / (dc + dp1);
+    double cm3 = (dm1 + 2.0 * dc) / (dm2 + dm1);
+    w[0] = a1L; w[1] = aL * (z1L - zL) / deltaXL; w[2] = (-dm1 * z1L) / deltaXL; w[3] = dc * zL / deltaXL;
+    w[4] = a1R; w[5] = aR * (z1R - zR) / deltaXR; w[6] = (-dc * z1R) / deltaXR; w[7] = dp1 * zR / deltaXR;
+    w[8] = cm1 * cm2; w[9] = cm1 * cm3; w[10] = cc1 * cc2; w[11] = cc1 * cc3; w[12] = cp1 * cp2; w[13] = cp1 * cp3;
+}
+static void weno_w(double dm2, double dm1, double dc, double dp1, double dp2, double *w) {
+    double a12 = dp2 / (dp1 + dp2), a01 = dp1 / (dc + dp1), a10 = dc / (dm1 + dc), a21 = dm1 / (dm2 + dm1);
+    w[0] = (1.0 - a01); w[1] = a01; w[2] = (1.0 - a12); w[3] = a12; w[4] = (1.0 - a10);
+    w[5] = a10; w[6] = (1.0 - a21); w[7] = a21; w[8] = (1.0 - a21); w[9] = a12;
+}
+
+static std::vector<double> build_weights(int rec, int n, const std::vector<double> &dd /* offset +2 */) {
+    std::vector<double> w((size_t)(n + 6) * 14, 0.0);
+    auto D = [&](int j) { return dd[j + 2]; };
+    if (rec == 3 || rec == 4) {
+        for (int j = 0; j <= n + 1; ++j) {
+            double *o = &w[(size_t)(j + 2) * 14];
+            if (rec == 4) weno_w(D(j - 2), D(j - 1), D(j), D(j + 1), D(j + 2), o);
+            else ppm_w(D(j - 2), D(j - 1), D(j), D(j + 1), D(j + 2), o);
+        }
+    } else {  // TVD_WEIGHT, tvd_module.f90:42-53
+        for (int j = -1; j <= n + 2; ++j) {
+            w[(size_t)(j + 2) * 14 + 0] = (D(j) + D(j + 1)) / D(j);
+            w[(size_t)(j + 2) * 14 + 1] = (D(j) + D(j - 1)) / D(j);
+        }
+    }
+    return w;
+}
+
+static void grid_dims(const Dev &d, dim3 &g, dim3 &b, int j0, int jn, int k0, int kn, int l0, int ln) {
+    // cells j0..jn, k0..kn, l0..ln -> block (32, 8)
+    int nj = jn - j0 + 1, nk = kn - k0 + 1, nl = ln - l0 + 1;
+    (void)d;
+    b = dim3(nj >= 32 ? 32 : (nj >= 16 ? 16 : (nj >= 8 ? 8 : 4)), 1, 1);
+    int by = 256 / b.x;
+    if (by > nk) by = nk < 1 ? 1 : nk;
+    b.y = by;
+    g = dim3((nj + b.x - 1) / b.x, (nk + b.y - 1) / b.y, nl);
+}
+
+static void default_flux_blocks(cumc_handle *h) {
+    const Dev &d = h->d;
+    // x: TS cells along x per tile, rows of k per block
+    int TSx = d.nx + 2 <= 64 ? 64 : (d.nx + 2 <= 96 ? 96 : 128);
+    if (d.nx >= 256 && d.nx <= 300) TSx = 96;
+    int rows = (d.n_dim > 1) ? 2 : 1;
+    h->fblk[0] = dim3(TSx, rows, 1);
+    h->fblk[1] = dim3(32, 8, 1);
+    h->fblk[2] = dim3(32, 8, 1);
+}
+
+static void launch_flux(cumc_handle *h, int dir) {
+    const Dev &d = h->d;
+    dim3 b = h->fblk[dir];
+    dim3 g;
+    const int TS = (dir == 0) ? (int)b.x : (int)b.y;
+    if (dir == 0) g = dim3((d.nx + 1 + TS - 2) / (TS - 1), (d.ny + b.y - 1) / b.y, d.nz);
+    else if (dir == 1) g = dim3((d.nx + b.x - 1) / b.x, (d.ny + 1 + TS - 2) / (TS - 1), d.nz);
+    else g = dim3((d.nx + b.x - 1) / b.x, (d.nz + 1 + TS - 2) / (TS - 1), d.ny);
+    const bool f32 = h->cfg.precision == CUMC_FP32;
+    const size_t smem = 2 * 7 * (size_t)b.x * b.y * (f32 ? sizeof(float) : sizeof(double));
+    if (f32) launch_flux_fp32(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, h->stream);
+    else launch_flux_fp64(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, h->stream);
+    h->launches++;
+}
+
+static FillList make_list(cumc_handle *h, int axis, int side) {
+    // side: 0 inner, 1 outer.  parity side index: 2*axis + side
+    const Dev &d = h->d;
+    const signed char *bf = d.bfac[2 * axis + side];
+    FillList L;
+    L.n = 0;
+    auto add = [&](double *a, int var) { L.a[L.n] = a; L.par[L.n] = bf[var]; L.n++; };
+    for (int i = 0; i < 5; ++i) add(d.P[i], 1 + i);
+    for (int i = 0; i < 3; ++i) add(d.BC[i], 6 + i);
+    // transverse face fields of this axis (boundary.f90:432-433, 543-544, 654-655)
+    for (int i = 0; i < 3; ++i)
+        if (i != axis) add(d.P[5 + i], 6 + i);
+    if (d.fixn && d.bf[2 * axis] == 0) add(d.P[5 + axis], 6 + axis);
+    add(d.CS, 1);   // FINDPRESSURE output, even (recomputed identically by the reference)
+    if (axis != 1 || side == 0) add(d.EPS, 1);  // epsilon y-outer handled separately
+    return L;
+}
+
+static FillList make_elist(cumc_handle *h, int axis, int side) {
+    const Dev &d = h->d;
+    const signed char *bf = d.bfac[2 * axis + side];
+    enum { iex = 9, iey = 10, iez = 11 };
+    FillList L;
+    L.n = 0;
+    auto add = [&](double *a, int var) { L.a[L.n] = a; L.par[L.n] = bf[var]; L.n++; };
+    for (int i = 0; i < 3; ++i) add(d.EC[i], iex + i);
+    if (axis == 0) { add(d.EF[e_xz], iex); add(d.EF[e_xy], iex); add(d.EF[e_yz], iey); add(d.EF[e_zy], iez); }
+    else if (axis == 1) { add(d.EF[e_xz], iex); add(d.EF[e_yx], iey); add(d.EF[e_yz], iey); add(d.EF[e_zx], iez); }
+    else { add(d.EF[e_xy], iex); add(d.EF[e_yx], iey); add(d.EF[e_zx], iez); add(d.EF[e_zy], iez); }
+    return L;
+}
+
+static void launch_fills(cumc_handle *h, bool emf) {
+    const Dev &d = h->d;
+    for (int axis = 0; axis < 3; ++axis) {
+        FillList in = emf ? make_elist(h, axis, 0) : make_list(h, axis, 0);
+        FillList out = emf ? make_elist(h, axis, 1) : make_list(h, axis, 1);
+        int o0 = (axis == 0) ? d.NY : d.NX;
+        int o1 = (axis == 2) ? d.NY : d.NZ;
+        dim3 b(o0 >= 128 ? 128 : 32), g((o0 + b.x - 1) / b.x, o1, 3);
+        int mode = -1;
+        if (!emf && axis == 1) mode = d.eps_y_out_mode;
+        if (axis == 0) k_fill<0><<<g, b, 0, h->stream>>>(d, in, out, mode);
+        else if (axis == 1) k_fill<1><<<g, b, 0, h->stream>>>(d, in, out, mode);
+        else k_fill<2><<<g, b, 0, h->stream>>>(d, in, out, mode);
+        h->launches++;
+    }
+    if (!emf && d.bc_kind != 0) {
+        int o0 = d.NX > d.NY ? d.NX : d.NY;
+        int o1 = d.NY > d.NZ ? d.NY : d.NZ;
+        dim3 b(32), g((o0 + 31) / 32, o1, 3);
+        k_custom_bc<<<g, b, 0, h->stream>>>(d);
+        h->launches++;
+    }
+}
+
+static void launch_cons0(cumc_handle *h) {
+    const Dev &d = h->d;
+    int m = d.nx + 1;
+    if (d.ny + 1 > m) m = d.ny + 1;
+    int mb = (d.ny + 1 > d.nz + 1) ? d.ny + 1 : d.nz + 1;
+    dim3 b(32), g((m + 31) / 32, mb, 3);
+    k_cons0<<<g, b, 0, h->stream>>>(d);
+    h->launches++;
+}
+
+// kernel classes timed by cumc_profile_step
+enum { PC_FLUX_X = 0, PC_FLUX_Y, PC_FLUX_Z, PC_EMF, PC_RK, PC_RECOVER, PC_BND, PC_DT, PC_N };
+
+static void prof_begin(cumc_handle *h) {
+    if (h->prof_class >= 0) cudaEventRecord(h->ev[0], h->stream);
+}
+static void prof_end(cumc_handle *h, int cls) {
+    if (h->prof_class < 0) return;
+    cudaEventRecord(h->ev[1], h->stream);
+    cudaEventSynchronize(h->ev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+    h->prof_ms[cls] += ms;
+}
+
+// one RK stage (rungekutta.f90:61-100)
+static void enqueue_stage(cumc_handle *h, int stage) {
+    const Dev &d = h->d;
+    for (int dir = 0; dir < d.n_dim; ++dir) {
+        prof_begin(h);
+        launch_flux(h, dir);
+        prof_end(h, PC_FLUX_X + dir);
+    }
+    dim3 g, b;
+    prof_begin(h);
+    grid_dims(d, g, b, 1, d.nx, 1, d.ny, 1, d.nz);
+    k_ecell<<<g, b, 0, h->stream>>>(d);
+    h->launches++;
+    launch_fills(h, true);
+    grid_dims(d, g, b, 0, d.nx, 0, d.ny, 0, d.nz);
+    k_edge<<<g, b, 0, h->stream>>>(d);
+    h->launches++;
+    if (h->cfg.fixpole && d.coord == 2) {
+        k_fixpole<<<(d.nx + 127) / 128, 128, 0, h->stream>>>(d);
+        h->launches++;
+    }
+    prof_end(h, PC_EMF);
+    prof_begin(h);
+    k_rk<<<g, b, 0, h->stream>>>(d, stage);
+    h->launches++;
+    prof_end(h, PC_RK);
+    prof_begin(h);
+    grid_dims(d, g, b, 1, d.nx, 1, d.ny, 1, d.nz);
+    k_recover<0><<<g, b, 0, h->stream>>>(d, stage);
+    h->launches++;
+    launch_cons0(h);
+    prof_end(h, PC_RECOVER);
+    prof_begin(h);
+    launch_fills(h, false);
+    prof_end(h, PC_BND);
+}
+
+static void enqueue_finddt(cumc_handle *h, int clamp) {
+    const Dev &d = h->d;
+    dim3 g, b;
+    prof_begin(h);
+    grid_dims(d, g, b, 1, d.nx, 1, d.ny, 1, d.nz);
+    k_finddt<<<g, b, 0, h->stream>>>(d);
+    k_dt_final<<<1, 1, 0, h->stream>>>(d, clamp);
+    h->launches += 2;
+    prof_end(h, PC_DT);
+}
+
+static void enqueue_step(cumc_handle *h, bool with_dt, bool end) {
+    if (with_dt) enqueue_finddt(h, 1);
+    for (int s = 1; s <= 3; ++s) enqueue_stage(h, s);
+    if (end) {
+        k_step_end<<<1, 1, 0, h->stream>>>(h->d);
+        h->launches++;
+    }
+}
+
+static int check_scalars(cumc_handle *h) {
+    CK(cudaMemcpyAsync(h->S_host, h->d.S, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->S_host->err_code) {
+        char buf[256];
+        int c = h->S_host->err_cell;
+        const Dev &d = h->d;
+        int j = c >= 0 ? c % d.NX - 2 : 0, k = c >= 0 ? (c / d.NX) % d.NY - 2 : 0, l = c >= 0 ? c / (d.NX * d.NY) - 2 : 0;
+        snprintf(buf, sizeof buf, "non-finite or non-positive state at cell (%d,%d,%d), stage %d", j, k, l, h->S_host->err_stage);
+        int code = h->S_host->err_code;
+        // clear so the handle stays usable after the caller repairs the state
+        Scalars z = *h->S_host;
+        z.err_code = 0;
+        z.done = 0;
+        cudaMemcpyAsync(h->d.S, &z, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream);
+        cudaStreamSynchronize(h->stream);
+        return fail(h, code, buf);
+    }
+    return CUMC_OK;
+}
+
+extern "C" {
+
+int cumc_create(const cumc_config *cfg, cumc_handle **out) {
+    cumc_handle *h = nullptr;
+    if (!cfg || !out) return fail(nullptr, CUMC_EINVAL, "null argument");
+    *out = nullptr;
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    if (nx < 1 || ny < 1 || nz < 1 || cfg->n_dim < 1 || cfg->n_dim > 3 || cfg->coordinate_flag < 0 || cfg->coordinate_flag > 2)
+        return fail(nullptr, CUMC_EINVAL, "bad grid extents or flags");
+    if ((cfg->n_dim < 2 && ny != 1) || (cfg->n_dim < 3 && nz != 1))
+        return fail(nullptr, CUMC_EINVAL, "degenerate directions need n = 1");
+    if (cfg->recon < 0 || cfg->recon > 4 || cfg->riemann < 0 || cfg->riemann > 3 || cfg->precision < 0 || cfg->precision > 1)
+        return fail(nullptr, CUMC_EINVAL, "bad recon/riemann/precision option");
+    if (!cfg->xF || !cfg->yF || !cfg->zF) return fail(nullptr, CUMC_EINVAL, "face coordinates missing");
+    const int nn[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        int fi = cfg->boundary_flag[2 * a], fo = cfg->boundary_flag[2 * a + 1];
+        if (fi < 0 || fi > 4 || fo < 0 || fo > 4) return fail(nullptr, CUMC_EINVAL, "boundary flag out of range");
+        if ((fi == 0) != (fo == 0)) return fail(nullptr, CUMC_EINVAL, "periodic boundary flags must come in pairs");
+        if ((fi >= 2 || fo >= 2) && nn[a] < 3) return fail(nullptr, CUMC_EINVAL, "parity boundaries need at least 3 zones");
+    }
+    const long long N3 = (long long)(nx + 6) * (ny + 6) * (nz + 6);
+    if (N3 * 8 >= (1ll << 31)) return fail(nullptr, CUMC_EINVAL, "grid too large for 32-bit cell indexing");
+    if (cfg->model.gamma <= 1.0) return fail(nullptr, CUMC_EINVAL, "gamma must exceed 1");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(nullptr, CUMC_ECUDA, "no CUDA device");
+
+    h = new cumc_handle();
+    h->cfg = *cfg;
+    h->cfg.xF = h->cfg.yF = h->cfg.zF = nullptr;
+    Dev &d = h->d;
+    memset(&d, 0, sizeof(Dev));
+    d.nx = nx; d.ny = ny; d.nz = nz; d.n_dim = cfg->n_dim; d.coord = cfg->coordinate_flag;
+    d.NX = nx + 6; d.NY = ny + 6; d.NZ = nz + 6; d.N3 = (int)N3;
+    for (int i = 0; i < 6; ++i) d.bf[i] = cfg->boundary_flag[i];
+    // epsilon y-outer rule of BOUNDARY1D_NM (boundary.f90:243-282)
+    d.eps_y_out_mode = d.bf[2] == 0 ? 0 : (d.bf[3] == 1 ? 1 : (d.bf[3] >= 2 ? 2 : -1));
+    d.fixn = cfg->fix_periodic_normal_faces ? 1 : 0;
+    d.gamma = cfg->model.gamma; d.cfl = cfg->cfl;
+    d.floor_kind = cfg->model.floor_kind; d.source_kind = cfg->model.source_kind; d.bc_kind = cfg->model.bc_kind;
+    d.rho_floor = cfg->model.rho_floor; d.eps_floor = cfg->model.eps_floor; d.p_floor = cfg->model.p_floor;
+    d.g_const = cfg->model.g_const; d.r_sh = cfg->model.r_sh;
+    int rc = setup_parity(h, d.bf, d.bfac);
+    if (rc) { g_create_err = h->err; delete h; return rc; }
+
+    // grid metrics, getgrid.f90:43-98
+    std::vector<double> xF(cfg->xF, cfg->xF + nx + 7), yF(cfg->yF, cfg->yF + ny + 7), zF(cfg->zF, cfg->zF + nz + 7);
+    auto F = [](std::vector<double> &v, int j) -> double & { return v[j + 3]; };
+    std::vector<double> x(nx + 6), dx(nx + 6), xbar(nx + 6, 0.0), dx_cb(nx + 6, 0.0);
+    std::vector<double> y(ny + 6), dy(ny + 6), sine(ny + 6), sinf(ny + 7), dsine(ny + 6, 0.0), dcose(ny + 6, 0.0);
+    std::vector<double> z(nz + 6), dz(nz + 6);
+    for (int j = -2; j <= nx + 3; ++j) dx[j + 2] = F(xF, j) - F(xF, j - 1);
+    for (int j = -2; j <= ny + 3; ++j) dy[j + 2] = F(yF, j) - F(yF, j - 1);
+    for (int j = -2; j <= nz + 3; ++j) dz[j + 2] = F(zF, j) - F(zF, j - 1);
+    for (int j = -2; j <= nx + 3; ++j) x[j + 2] = (F(xF, j) + F(xF, j - 1)) / 2.0;
+    for (int j = -2; j <= ny + 3; ++j) y[j + 2] = (F(yF, j) + F(yF, j - 1)) / 2.0;
+    for (int j = -2; j <= nz + 3; ++j) z[j + 2] = (F(zF, j) + F(zF, j - 1)) / 2.0;
+    for (int j = -1; j <= nx + 3; ++j) {
+        dx_cb[j + 2] = F(xF, j) * F(xF, j) * F(xF, j) - F(xF, j - 1) * F(xF, j - 1) * F(xF, j - 1);
+        xbar[j + 2] = (dx_cb[j + 2] / 3.0) / (x[j + 2] * dx[j + 2]);
+    }
+    for (int k = -1; k <= ny + 3; ++k) {
+        dcose[k + 2] = -(std::cos(F(yF, k)) - std::cos(F(yF, k - 1)));
+        dsine[k + 2] = (std::sin(F(yF, k)) - std::sin(F(yF, k - 1)));
+    }
+    for (int k = -2; k <= ny + 3; ++k) sine[k + 2] = std::sin(y[k + 2]);
+    for (int k = -3; k <= ny + 3; ++k) sinf[k + 3] = std::sin(F(yF, k));
+    if (cfg->fixpole && d.coord == 2) {
+        F(yF, 0) = 0.0; F(yF, ny) = 4.0 * std::atan(1.0);
+        sinf[3] = 0.0; sinf[ny + 3] = 0.0;
+    }
+    std::vector<double> wx = build_weights(cfg->recon, nx, dx), wy = build_weights(cfg->recon, ny, dy),
+                        wz = build_weights(cfg->recon, nz, dz);
+    std::vector<float> wxf(wx.begin(), wx.end()), wyf(wy.begin(), wy.end()), wzf(wz.begin(), wz.end());
+
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        g_create_err = "cudaStreamCreate failed";
+        delete h;
+        return CUMC_ECUDA;
+    }
+    bool ok = true;
+    auto A = [&](double *&p, size_t n) { p = dalloc(h, n); ok = ok && p; };
+    for (int i = 0; i < 8; ++i) { A(d.P[i], N3); A(d.U[i], N3); }
+    {
+        double *blk = dalloc(h, (size_t)8 * N3);
+        ok = ok && blk;
+        for (int i = 0; i < 8; ++i) d.U0[i] = blk ? blk + (size_t)i * N3 : nullptr;
+        h->stage_aos = blk;
+    }
+    {
+        void *t = nullptr;
+        ok = ok && cudaMalloc(&t, 8 * sizeof(double *)) == cudaSuccess;
+        if (t) h->allocs.push_back(t);
+        h->ptr_tab = (double **)t;
+    }
+    ok = ok && cudaEventCreate(&h->ev[0]) == cudaSuccess && cudaEventCreate(&h->ev[1]) == cudaSuccess;
+    A(d.EPS, N3); A(d.CS, N3);
+    for (int i = 0; i < 3; ++i) { A(d.BC[i], N3); A(d.EC[i], N3); }
+    for (int i = 0; i < 5; ++i) {
+        A(d.FX[i], N3);
+        if (d.n_dim > 1) A(d.FY[i], N3); else d.FY[i] = d.FX[i];
+        if (d.n_dim > 2) A(d.FZ[i], N3); else d.FZ[i] = d.FX[i];
+    }
+    for (int i = 0; i < 6; ++i) A(d.EF[i], N3);
+    A(d.EX, N3); A(d.EY, N3); A(d.EZ, N3);
+    d.x = upload(h, x); d.dx = upload(h, dx); d.xF = upload(h, xF); d.xbar = upload(h, xbar); d.dx_cb = upload(h, dx_cb);
+    d.y = upload(h, y); d.dy = upload(h, dy); d.yF = upload(h, yF); d.sine = upload(h, sine); d.sinf = upload(h, sinf);
+    d.dcose = upload(h, dcose); d.dsine = upload(h, dsine);
+    d.z = upload(h, z); d.dz = upload(h, dz); d.zF = upload(h, zF);
+    d.wx = upload(h, wx); d.wy = upload(h, wy); d.wz = upload(h, wz);
+    d.wxf = upload(h, wxf); d.wyf = upload(h, wyf); d.wzf = upload(h, wzf);
+    void *sp = nullptr;
+    ok = ok && cudaMalloc(&sp, sizeof(Scalars)) == cudaSuccess;
+    if (sp) h->allocs.push_back(sp);
+    d.S = (Scalars *)sp;
+    void *dv = nullptr;
+    ok = ok && cudaMalloc(&dv, sizeof(unsigned long long)) == cudaSuccess;
+    if (dv) h->allocs.push_back(dv);
+    h->divb_dev = (unsigned long long *)dv;
+    ok = ok && cudaMallocHost((void **)&h->S_host, sizeof(Scalars)) == cudaSuccess;
+    if (!ok) {
+        g_create_err = "device allocation failed";
+        cumc_destroy(h);
+        return CUMC_ENOMEM;
+    }
+    Scalars s0;
+    memset(&s0, 0, sizeof s0);
+    s0.dt_bits = (unsigned long long)0x40F86A0000000000ull;  // bits of 1.0e5
+    s0.t_end = 1e300;
+    s0.max_steps = 0x7fffffff;
+    cudaMemcpy(d.S, &s0, sizeof s0, cudaMemcpyHostToDevice);
+    // flux kernels need more than 48 KB of dynamic shared memory only for large tiles
+    default_flux_blocks(h);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        g_create_err = "device setup failed";
+        cumc_destroy(h);
+        return CUMC_ECUDA;
+    }
+    *out = h;
+    return CUMC_OK;
+}
+
+int cumc_destroy(cumc_handle *h) {
+    if (!h) return CUMC_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    for (void *p : h->allocs) cudaFree(p);
+    for (int i = 0; i < 2; ++i)
+        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    if (h->S_host) cudaFreeHost(h->S_host);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CUMC_OK;
+}
+
+const char *cumc_last_error(cumc_handle *h) { return h ? h->err.c_str() : g_create_err.c_str(); }
+
+int cumc_set_state(cumc_handle *h, const double *prim, const double *eps) {
+    if (!h || !prim || !eps) return fail(h, CUMC_EINVAL, "null argument");
+    const Dev &d = h->d;
+    const size_t n3 = (size_t)d.N3;
+    // one copy of the Fortran-layout buffer, transposed on the device
+    CK(cudaMemcpyAsync(h->stage_aos, prim, 8 * n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->ptr_tab, d.P, 8 * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+    k_aos_to_soa<<<(d.N3 + 255) / 256, 256, 0, h->stream>>>(d, h->stage_aos, 8, h->ptr_tab);
+    h->launches++;
+    CK(cudaMemcpyAsync(d.EPS, eps, n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    for (int v = 0; v < 8; ++v) {
+        CK(cudaMemsetAsync(d.U[v], 0, n3 * sizeof(double), h->stream));
+        CK(cudaMemsetAsync(d.U0[v], 0, n3 * sizeof(double), h->stream));
+    }
+    for (int i = 0; i < 3; ++i) CK(cudaMemsetAsync(d.BC[i], 0, n3 * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(d.CS, 0, n3 * sizeof(double), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->have_state = true;
+    h->initialised = false;
+    return CUMC_OK;
+}
+
+static int download_aos(cumc_handle *h, double *const *src_host, int nv, double *out) {
+    const Dev &d = h->d;
+    const size_t n3 = (size_t)d.N3;
+    CK(cudaMemcpyAsync(h->ptr_tab, src_host, nv * sizeof(double *), cudaMemcpyHostToDevice, h->stream));
+    // the u_old block is free between steps; it only holds stage-1 backups
+    k_soa_to_aos<<<(d.N3 + 255) / 256, 256, 0, h->stream>>>(d, h->stage_aos, nv, h->ptr_tab);
+    h->launches++;
+    CK(cudaMemcpyAsync(out, h->stage_aos, nv * n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CUMC_OK;
+}
+
+int cumc_get_state(cumc_handle *h, double *prim, double *eps) {
+    if (!h || !prim || !eps) return fail(h, CUMC_EINVAL, "null argument");
+    const Dev &d = h->d;
+    const size_t n3 = (size_t)d.N3;
+    int rc = download_aos(h, d.P, 8, prim);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(eps, d.EPS, n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CUMC_OK;
+}
+
+int cumc_get_array(cumc_handle *h, int which, double *out, size_t n_doubles) {
+    if (!h || !out) return fail(h, CUMC_EINVAL, "null argument");
+    const Dev &d = h->d;
+    const size_t n3 = (size_t)d.N3;
+    int nc = which == CUMC_ARR_CONS ? 8 : which == CUMC_ARR_BCELL ? 3 : which == CUMC_ARR_CS ? 1 : 0;
+    if (!nc) return fail(h, CUMC_EINVAL, "unknown array");
+    if (n_doubles < n3 * nc) return fail(h, CUMC_EINVAL, "output buffer too small");
+    double *src[8];
+    for (int v = 0; v < nc; ++v) src[v] = which == CUMC_ARR_CONS ? d.U[v] : which == CUMC_ARR_BCELL ? d.BC[v] : d.CS;
+    return download_aos(h, src, nc, out);
+}
+
+int cumc_initial_update(cumc_handle *h) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->have_state) return fail(h, CUMC_ENOTREADY, "set_state first");
+    const Dev &d = h->d;
+    dim3 g, b;
+    grid_dims(d, g, b, 1, d.nx, 1, d.ny, 1, d.nz);
+    k_recover<1><<<g, b, 0, h->stream>>>(d, 0);
+    h->launches++;
+    launch_cons0(h);
+    launch_fills(h, false);
+    CK(cudaGetLastError());
+    int rc = check_scalars(h);
+    if (rc) return rc;
+    h->initialised = true;
+    return CUMC_OK;
+}
+
+int cumc_finddt(cumc_handle *h, double *dt) {
+    if (!h || !dt) return fail(h, CUMC_EINVAL, "null argument");
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    enqueue_finddt(h, 0);
+    CK(cudaGetLastError());
+    int rc = check_scalars(h);
+    if (rc) return rc;
+    *dt = h->S_host->dt;
+    return CUMC_OK;
+}
+
+int cumc_rk3_step(cumc_handle *h, double dt) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, CUMC_EINVAL, "dt must be positive and finite");
+    CK(cudaMemcpyAsync(&h->d.S->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    enqueue_step(h, false, false);
+    CK(cudaGetLastError());
+    return check_scalars(h);
+}
+
+int cumc_evolve(cumc_handle *h, double t_end, int max_steps, double *t_inout, int *steps_out) {
+    if (!h || !t_inout) return fail(h, CUMC_EINVAL, "null argument");
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    if (steps_out) *steps_out = 0;
+    if (max_steps <= 0 || !(*t_inout < t_end)) return CUMC_OK;
+    // device-side loop state
+    Scalars s;
+    CK(cudaMemcpyAsync(h->S_host, h->d.S, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    s = *h->S_host;
+    s.t = *t_inout;
+    s.t_end = t_end;
+    s.steps = 0;
+    s.max_steps = max_steps;
+    s.done = 0;
+    *h->S_host = s;
+    CK(cudaMemcpyAsync(h->d.S, h->S_host, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+    // capture one step the first time
+    if (!h->graph_exec) {
+        int64_t before = h->launches;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(h, true, true);
+        CK(cudaStreamEndCapture(h->stream, &h->graph));
+        CK(cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+        h->kernels_per_step = (int)(h->launches - before);
+        h->launches = before;
+    }
+    // replay in chunks; kernels turn into no-ops once the device sets done
+    int issued = 0;
+    while (true) {
+        int chunk = max_steps - issued;
+        if (chunk > 64) chunk = 64;
+        for (int i = 0; i < chunk; ++i) CK(cudaGraphLaunch(h->graph_exec, h->stream));
+        h->launches += (int64_t)chunk * h->kernels_per_step;
+        issued += chunk;
+        CK(cudaMemcpyAsync(h->S_host, h->d.S, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->S_host->done || issued >= max_steps) break;
+    }
+    *t_inout = h->S_host->t;
+    if (steps_out) *steps_out = h->S_host->steps;
+    int rc = check_scalars(h);
+    // leave the handle usable for single-step calls
+    Scalars z = *h->S_host;
+    z.done = 0;
+    cudaMemcpyAsync(h->d.S, &z, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    return rc;
+}
+
+int cumc_max_divb(cumc_handle *h, double *max_divb) {
+    if (!h || !max_divb) return fail(h, CUMC_EINVAL, "null argument");
+    const Dev &d = h->d;
+    CK(cudaMemsetAsync(h->divb_dev, 0, sizeof(unsigned long long), h->stream));
+    dim3 g, b;
+    grid_dims(d, g, b, 1, d.nx, 1, d.ny, 1, d.nz);
+    k_divb<<<g, b, 0, h->stream>>>(d, h->divb_dev);
+    h->launches++;
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, h->divb_dev, sizeof bits, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double v;
+    memcpy(&v, &bits, sizeof v);
+    *max_divb = v;
+    return CUMC_OK;
+}
+
+int cumc_sync(cumc_handle *h) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    CK(cudaStreamSynchronize(h->stream));
+    return CUMC_OK;
+}
+
+int64_t cumc_launch_count(cumc_handle *h) { return h ? h->launches : 0; }
+
+void *cumc_stream(cumc_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out) {
+    if (!h || !ms_out || n_out < PC_N) return fail(h, CUMC_EINVAL, "need 8 output slots");
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    for (int i = 0; i < PC_N; ++i) h->prof_ms[i] = 0.0;
+    h->prof_class = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        enqueue_finddt(h, 0);
+        for (int st = 1; st <= 3; ++st) enqueue_stage(h, st);
+    }
+    h->prof_class = -1;
+    CK(cudaGetLastError());
+    int rc = check_scalars(h);
+    for (int i = 0; i < PC_N; ++i) ms_out[i] = h->prof_ms[i];
+    return rc;
+}
+
+int cumc_fp64_peak(double *tflops) {
+    if (!tflops) return CUMC_EINVAL;
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CUMC_ECUDA;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    double *out = nullptr;
+    if (cudaMalloc(&out, sizeof(double)) != cudaSuccess) return CUMC_ECUDA;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int iters = 4096, threads = 256, blocks = nsm * 8;
+    k_dfma_probe<<<blocks, threads>>>(out, iters);  // warm-up
+    cudaEventRecord(a);
+    k_dfma_probe<<<blocks, threads>>>(out, iters);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return cudaGetLastError() == cudaSuccess ? CUMC_OK : CUMC_ECUDA;
+}
+
+}  // extern "C"

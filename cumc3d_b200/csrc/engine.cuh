@@ -1,0 +1,69 @@
+// engine.cuh -- device-side layout of one solver instance.
+//
+// State lives in HBM as structure-of-arrays: every variable is its own
+// padded (nx+6)*(ny+6)*(nz+6) double array with x fastest, so a warp reading
+// 32 consecutive cells of one variable issues fully coalesced 256-byte
+// transactions.  Index (j,k,l), j in -2..nx+3, maps to
+// (j+2) + NX*((k+2) + NY*(l+2)), the padded extents of the reference's
+// arrays (solver/mhd/setup.f90:348-375).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cumc {
+
+// device-resident scalars of the time loop (solver/mhd/main.f90:98-116)
+struct Scalars {
+    double dt;                   // step size used by the RK stages
+    double t;                    // global_time
+    double t_end;                // total_time
+    unsigned long long dt_bits;  // FINDDT min-reduction target (bits of a positive double)
+    int steps;                   // steps taken in the current evolve call
+    int max_steps;
+    int done;                    // set when t >= t_end or steps >= max_steps
+    int err_code;                // first guard failure (0 = none)
+    int err_cell;                // padded linear index of that cell
+    int err_stage;
+    int pad[2];
+};
+
+struct Dev {
+    int nx, ny, nz, n_dim, coord;
+    int NX, NY, NZ;
+    int N3;
+    int bf[6];              // boundary_flag
+    int eps_y_out_mode;     // BOUNDARY1D_NM y-outer rule for epsilon (boundary.f90:243)
+    int fixn;               // carry periodic normal faces
+    signed char bfac[6][12];  // parity per side (xin,xout,yin,yout,zin,zout) and variable 1..11
+    double gamma, cfl;
+    int floor_kind, source_kind, bc_kind;
+    double rho_floor, eps_floor, p_floor, g_const, r_sh;
+
+    double *P[8];   // prim
+    double *U[8];   // cons
+    double *U0[8];  // u_old
+    double *EPS, *CS;
+    double *BC[3];  // bcell
+    double *FX[5], *FY[5], *FZ[5];  // hydro face fluxes per direction
+    double *EF[6];  // face EMFs (yx, zx, xy, zy, xz, yz)
+    double *EC[3];  // cell EMFs
+    double *EX, *EY, *EZ;  // edge EMFs
+
+    // grid metrics (getgrid.f90), offsets: cells +2, faces +3
+    const double *x, *dx, *xF, *xbar, *dx_cb;
+    const double *y, *dy, *yF, *sine, *sinf, *dcose, *dsine;
+    const double *z, *dz, *zF;
+    const double *wx, *wy, *wz;  // reconstruction weights, 14 per cell
+    const float *wxf, *wyf, *wzf;
+    Scalars *S;
+};
+
+__device__ __forceinline__ int cidx(const Dev &d, int j, int k, int l) {
+    return (j + 2) + d.NX * ((k + 2) + d.NY * (l + 2));
+}
+
+// host-side launchers of the face-flux kernels (one per precision unit)
+void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
+void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
+
+}  // namespace cumc

@@ -1,0 +1,176 @@
+"""Host-side driver of the B200 engine, over the C-ABI in include/cumc3d_gpu.h.
+
+:class:`Solver` mirrors the reference's time loop (solver/mhd/main.f90:50-139)
+and keeps its routine names: ``initial_update`` (INITIAL_UPDATE), ``finddt``
+(FINDDT), ``rungekutta`` (RUNGEKUTTA), ``find_divb`` (FIND_DIVB).  Every call
+goes through ``libcumc3d_gpu.so``; there is no CPU path.  A missing library or
+a missing CUDA device raises immediately.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import capi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libcumc3d_gpu.so")
+
+# every symbol include/cumc3d_gpu.h declares
+EXPORTS = [
+    "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
+    "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
+    "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak",
+    "cumc_last_error",
+]
+
+PROFILE_CLASSES = ["flux_x", "flux_y", "flux_z", "emf", "rk", "recover", "boundary", "dt"]
+
+_lib = None
+
+
+class CumcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("cumc error %d: %s" % (code, msg))
+        self.code = code
+
+
+def load_library(path=None):
+    """Load the CUDA engine; raises if the shared library is absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError("CUDA engine library missing: %s (run python -m cumc3d_b200.build)" % p)
+    L = C.CDLL(p)
+    L.cumc_create.argtypes = [C.POINTER(capi.CumcConfig), C.POINTER(C.c_void_p)]
+    L.cumc_destroy.argtypes = [C.c_void_p]
+    L.cumc_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.cumc_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.cumc_get_array.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+    L.cumc_initial_update.argtypes = [C.c_void_p]
+    L.cumc_finddt.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.cumc_rk3_step.argtypes = [C.c_void_p, C.c_double]
+    L.cumc_evolve.argtypes = [C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.cumc_max_divb.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.cumc_sync.argtypes = [C.c_void_p]
+    L.cumc_launch_count.argtypes = [C.c_void_p]
+    L.cumc_launch_count.restype = C.c_int64
+    L.cumc_stream.argtypes = [C.c_void_p]
+    L.cumc_stream.restype = C.c_void_p
+    L.cumc_profile_step.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int]
+    L.cumc_fp64_peak.argtypes = [C.POINTER(C.c_double)]
+    L.cumc_last_error.argtypes = [C.c_void_p]
+    L.cumc_last_error.restype = C.c_char_p
+    if path is None:
+        _lib = L
+    return L
+
+
+class Solver:
+    """One simulation on one GPU (a ``cumc_handle``)."""
+
+    def __init__(self, spec):
+        self.spec = spec
+        self._cfg, self._keep = capi.make_config(spec)
+        self.L = load_library()
+        h = C.c_void_p()
+        rc = self.L.cumc_create(C.byref(self._cfg), C.byref(h))
+        if rc != 0:
+            raise CumcError(rc, self.L.cumc_last_error(None).decode())
+        self.h = h
+        self.shape = (spec["nz"] + 6, spec["ny"] + 6, spec["nx"] + 6)
+        self.time = 0.0
+        self.n_step = 0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CumcError(rc, self.L.cumc_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cumc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # GET_MODEL output -> device
+    def set_state(self, prim, eps):
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        if prim.shape != self.shape + (8,) or eps.shape != self.shape:
+            raise ValueError("state must have shape %s / %s" % (self.shape + (8,), self.shape))
+        self._check(self.L.cumc_set_state(self.h, prim.ctypes.data, eps.ctypes.data))
+
+    def get_state(self):
+        prim = np.empty(self.shape + (8,))
+        eps = np.empty(self.shape)
+        self._check(self.L.cumc_get_state(self.h, prim.ctypes.data, eps.ctypes.data))
+        return prim, eps
+
+    def get_array(self, which):
+        nc = {capi.ARR_CONS: 8, capi.ARR_BCELL: 3, capi.ARR_CS: 1}[which]
+        out = np.empty(self.shape + ((nc,) if nc > 1 else ()))
+        self._check(self.L.cumc_get_array(self.h, which, out.ctypes.data, out.size))
+        return out
+
+    def initial_update(self):
+        self._check(self.L.cumc_initial_update(self.h))
+
+    def finddt(self):
+        dt = C.c_double()
+        self._check(self.L.cumc_finddt(self.h, C.byref(dt)))
+        return dt.value
+
+    def rungekutta(self, dt):
+        self._check(self.L.cumc_rk3_step(self.h, dt))
+
+    def evolve(self, t_end, max_steps=2 ** 31 - 1):
+        """main.f90:98-139 on the device; returns (time, steps taken)."""
+        t = C.c_double(self.time)
+        n = C.c_int(0)
+        self._check(self.L.cumc_evolve(self.h, t_end, int(max_steps), C.byref(t), C.byref(n)))
+        self.time = t.value
+        self.n_step += n.value
+        return t.value, n.value
+
+    def find_divb(self):
+        v = C.c_double()
+        self._check(self.L.cumc_max_divb(self.h, C.byref(v)))
+        return v.value
+
+    def sync(self):
+        self._check(self.L.cumc_sync(self.h))
+
+    def launch_count(self):
+        return int(self.L.cumc_launch_count(self.h))
+
+    def stream(self):
+        """The engine's cudaStream_t as an integer handle."""
+        return int(self.L.cumc_stream(self.h) or 0)
+
+    def profile_step(self, nsteps=1):
+        """Per-kernel-class milliseconds summed over nsteps eager steps."""
+        out = (C.c_double * 8)()
+        self._check(self.L.cumc_profile_step(self.h, int(nsteps), out, 8))
+        return dict(zip(PROFILE_CLASSES, list(out)))
+
+    def set_state_ptr(self, prim_ptr, eps_ptr):
+        """set_state from raw host pointers (e.g. pinned buffers)."""
+        self._check(self.L.cumc_set_state(self.h, prim_ptr, eps_ptr))
+
+    def get_state_ptr(self, prim_ptr, eps_ptr):
+        self._check(self.L.cumc_get_state(self.h, prim_ptr, eps_ptr))
+
+
+def fp64_peak_tflops():
+    v = C.c_double()
+    rc = load_library().cumc_fp64_peak(C.byref(v))
+    if rc != 0:
+        raise CumcError(rc, "fp64 peak probe failed")
+    return v.value

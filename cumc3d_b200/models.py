@@ -294,3 +294,38 @@ WORKLOADS = {
     "alfven3d": alfven_3d,
     "torus_cyl": torus_cyl,
 }
+
+
+# ---------------------------------------------------------------------------
+# smooth random state on any geometry (parity tests exercise every code path)
+# ---------------------------------------------------------------------------
+def smooth_state(nx, ny, nz, n_dim, coordinate_flag=0, boundary_flag=(0, 0, 0, 0, 0, 0), x_range=(0.0, 1.0),
+                 y_range=(0.0, 1.0), z_range=(0.0, 1.0), seed=1, recon="weno", riemann="hlld", cfl=0.4,
+                 gamma=5.0 / 3.0, precision="fp64", model=None, **kw):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    spec = _base_spec(nx, ny, nz, n_dim, boundary_flag, x_range, y_range, z_range,
+                      coordinate_flag=coordinate_flag, cfl=cfl, recon=recon, riemann=riemann,
+                      precision=precision, model=model or dict(gamma=gamma, floor="eps"),
+                      name="smooth_%dd_c%d" % (n_dim, coordinate_flag), **kw)
+    xf, yf, zf = spec["xF"], spec["yF"], spec["zF"]
+    X = (centers(xf) - x_range[0]) / (x_range[1] - x_range[0])
+    Y = (centers(yf) - y_range[0]) / (y_range[1] - y_range[0])
+    Z = (centers(zf) - z_range[0]) / (z_range[1] - z_range[0])
+    Zg, Yg, Xg = np.meshgrid(Z, Y, X, indexing="ij")
+
+    def field(a):
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        return a * (np.sin(2 * np.pi * Xg + ph[0]) * np.cos(2 * np.pi * Yg + ph[1]) + 0.5 * np.sin(2 * np.pi * Zg + ph[2]))
+
+    prim = np.zeros((nz + 6, ny + 6, nx + 6, 8))
+    prim[..., IRHO] = 1.0 + field(0.3) + 0.1 * (Xg > 0.5)
+    prim[..., ITAU] = 0.6 + field(0.2) + 0.2 * (Yg > 0.4)
+    prim[..., IVX] = field(0.3)
+    prim[..., IVY] = field(0.3)
+    prim[..., IVZ] = field(0.3)
+    prim[..., IBX] = 0.5 + field(0.2)
+    prim[..., IBY] = -0.3 + field(0.2)
+    prim[..., IBZ] = 0.2 + field(0.2)
+    g = spec["model"]["gamma"]
+    eps = prim[..., ITAU] / prim[..., IRHO] / (g - 1.0)
+    return spec, prim, np.ascontiguousarray(eps)

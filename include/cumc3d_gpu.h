@@ -162,6 +162,22 @@ int cumc_sync(cumc_handle *h);
 /* Number of kernel launches the handle issued since creation. */
 int64_t cumc_launch_count(cumc_handle *h);
 
+/* The handle's CUDA stream (a cudaStream_t), so callers can order their own
+ * work and timing events after the engine's. */
+void *cumc_stream(cumc_handle *h);
+
+/* Diagnostics (no counterpart in the reference, which only has -DDEBUG
+ * system_clock prints, e.g. solver/mhd/rungekutta.f90:22-29): run nsteps
+ * eager steps with CUDA events around each kernel class and return the summed
+ * milliseconds in ms_out[0..7] = flux_x, flux_y, flux_z, emf (cell/face/edge
+ * EMFs and their ghosts), rk (du/dt + stage combination), recover (prim/cons
+ * recovery + floors + EOS), boundary (ghost fill), dt (CFL reduction). */
+int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
+
+/* Measured FP64 fused-multiply-add throughput of the current device in
+ * TFLOP/s (the denominator of the FP64-pipe roofline). */
+int cumc_fp64_peak(double *tflops);
+
 /* Message of the last failed call on this handle (or of the last failed
  * cumc_create when h is NULL). */
 const char *cumc_last_error(cumc_handle *h);
