@@ -113,7 +113,7 @@ def batch_problems(n_problems=512, seed=20261203, nmin=128, nmax=4096):
 # 3D MHD blast: the 3D analogue of model/riemann/src/riemann2d.f90:522-544
 # ---------------------------------------------------------------------------
 def blast_3d(n=256, recon="weno", riemann="hlld", cfl=0.4, precision="fp64", nx=None, ny=None, nz=None,
-             radius=0.1):
+             radius=0.1, p_in=10.0, p_out=0.1):
     nx = nx or n
     ny = ny or n
     nz = nz or n
@@ -128,7 +128,7 @@ def blast_3d(n=256, recon="weno", riemann="hlld", cfl=0.4, precision="fp64", nx=
     r = np.sqrt(z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2)
     prim = np.zeros((nz + 6, ny + 6, nx + 6, 8), dtype=np.float64)
     prim[..., IRHO] = 1.0
-    prim[..., ITAU] = np.where(r <= radius, 10.0, 0.1)
+    prim[..., ITAU] = np.where(r <= radius, p_in, p_out)
     b0 = 1.0 / math.sqrt(2.0)
     prim[..., IBX] = b0
     prim[..., IBY] = b0

@@ -28,7 +28,9 @@ def test_brio_wu_full_run_bitwise(oracle_mod):
 @pytest.mark.parametrize("recon", ["tvdmm", "tvdvl", "tvdmc", "ppm", "weno"])
 @pytest.mark.parametrize("riemann", ["lf", "hll", "hllc", "hlld"])
 def test_blast3d_all_schemes_bitwise(oracle_mod, recon, riemann):
-    spec, prim, eps = models.blast_3d(16, recon=recon, riemann=riemann, radius=0.25)
+    # a 10:1 blast resolved by 8 zones across; the 100:1 blast of the bench
+    # needs more zones before WENO keeps the face pressure positive
+    spec, prim, eps = models.blast_3d(16, recon=recon, riemann=riemann, radius=0.25, p_in=1.0)
     g, o, dg, do = run_pair(spec, prim, eps, 3, oracle_mod)
     assert dg == do
     assert_bitwise(g, o, spec)
@@ -37,7 +39,7 @@ def test_blast3d_all_schemes_bitwise(oracle_mod, recon, riemann):
 
 @pytest.mark.parametrize("fix", [0, 1])
 def test_periodic_normal_faces_option(oracle_mod, fix):
-    spec, prim, eps = models.blast_3d(16, recon="weno", riemann="hlld", radius=0.3)
+    spec, prim, eps = models.blast_3d(16, recon="weno", riemann="hlld", radius=0.3, p_in=1.0)
     spec["fix_periodic_normal_faces"] = fix
     g, o, dg, do = run_pair(spec, prim, eps, 4, oracle_mod)
     assert dg == do
