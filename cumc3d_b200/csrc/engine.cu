@@ -781,13 +781,15 @@ static std::vector<double> build_weights(int rec, int n, const std::vector<doubl
     return w;
 }
 
+// block shape for the cell kernels: x extent a multiple of the warp size so
+// every warp is full (the FINDDT and div B reductions shuffle across all 32
+// lanes), y extent up to 256 threads per block
 static void grid_dims(const Dev &d, dim3 &g, dim3 &b, int j0, int jn, int k0, int kn, int l0, int ln) {
-    // cells j0..jn, k0..kn, l0..ln -> block (32, 8)
-    int nj = jn - j0 + 1, nk = kn - k0 + 1, nl = ln - l0 + 1;
     (void)d;
-    b = dim3(nj >= 32 ? 32 : (nj >= 16 ? 16 : (nj >= 8 ? 8 : 4)), 1, 1);
-    int by = 256 / b.x;
-    if (by > nk) by = nk < 1 ? 1 : nk;
+    int nj = jn - j0 + 1, nk = kn - k0 + 1, nl = ln - l0 + 1;
+    b = dim3(nj >= 64 ? 64 : 32, 1, 1);
+    int by = 1;
+    while (by * 2 <= (int)(256 / b.x) && by < nk) by *= 2;
     b.y = by;
     g = dim3((nj + b.x - 1) / b.x, (nk + b.y - 1) / b.y, nl);
 }
