@@ -63,6 +63,7 @@ class CumcConfig(C.Structure):
         ("learned", C.c_int),
         ("fixpole", C.c_int),
         ("fix_periodic_normal_faces", C.c_int),
+        ("positivity_fallback", C.c_int),
         ("model", CumcModel),
     ]
 
@@ -109,6 +110,7 @@ def make_config(spec):
     cfg.learned = int(spec.get("learned", 0))
     cfg.fixpole = int(spec.get("fixpole", 0))
     cfg.fix_periodic_normal_faces = int(spec.get("fix_periodic_normal_faces", 0))
+    cfg.positivity_fallback = int(spec.get("positivity_fallback", 0))
     cfg.model = model
     return cfg, (xF, yF, zF)
 

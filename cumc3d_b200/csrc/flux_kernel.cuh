@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
         constexpr int NW = (REC == REC_PPM) ? 14 : (REC == REC_WENO) ? 10 : 2;
 #pragma unroll
         for (int m = 0; m < NW; ++m) w[m] = wp[m];
+        bool fallback = false;
 #pragma unroll
         for (int v = 0; v < 7; ++v) {
             const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
@@ -92,6 +93,20 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
             T a3 = (T)__ldg(src + ci + st);
             T vm, vp;
             recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
+            if (v == 4 && d.pos_fallback) {
+                // first-order fallback when an edge density or pressure is not
+                // positive (optional; the reference has no such guard)
+                fallback = !(sVM[0 * nthr + tid] > T(0) && sVP[0 * nthr + tid] > T(0) && vm > T(0) && vp > T(0));
+                if (fallback) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const T cv = (T)__ldg(d.P[u] + ci);
+                        sVM[u * nthr + tid] = cv;
+                        sVP[u * nthr + tid] = cv;
+                    }
+                }
+            }
+            if (fallback) vm = vp = a2;
             sVM[v * nthr + tid] = vm;
             sVP[v * nthr + tid] = vp;
         }

@@ -105,7 +105,14 @@ typedef struct cumc_config {
     int precision;               /* CUMC_FP64 / CUMC_FP32                         */
     int learned;                 /* 1: learned smooth-face flag in WENO (FP32 form)*/
     int fixpole;                 /* -DFIXPOLE: axis EMF average (spherical only)  */
-    int fix_periodic_normal_faces; /* 0 = reference behaviour (see DESIGN)        */
+    int fix_periodic_normal_faces; /* 0 = reference behaviour: a periodic
+                                    direction's face 0 keeps its initial normal
+                                    field (boundary.f90 never fills it);
+                                    1 = face 0 follows face n                     */
+    int positivity_fallback;     /* 0 = reference behaviour; 1 = a cell whose
+                                    reconstructed edge density or pressure is not
+                                    positive falls back to first order (no
+                                    counterpart in the reference)                 */
     cumc_model model;
 } cumc_config;
 

@@ -757,6 +757,14 @@ struct Sim {
                         for (int s = -2; s <= 2; ++s) v[s + 2] = P(i, j + s * dj, k + s * dk, l + s * dl);
                         recon1(w, v, PR(i, jm, km, lm), PL(i, j, k, l));
                     }
+                    /* optional positivity fallback (no counterpart in the reference):
+                     * a cell whose reconstructed edge density or pressure is not
+                     * positive is reconstructed at first order (edge = cell value) */
+                    bool fallback = cfg.positivity_fallback &&
+                        !(PR(irho, jm, km, lm) > 0.0 && PL(irho, j, k, l) > 0.0 &&
+                          PR(itau, jm, km, lm) > 0.0 && PL(itau, j, k, l) > 0.0);
+                    if (fallback)
+                        for (int i = imin; i <= itau; ++i) { PR(i, jm, km, lm) = P(i, j, k, l); PL(i, j, k, l) = P(i, j, k, l); }
                     epsR[c3(jm, km, lm)] = eos_eps(PR(irho, jm, km, lm), PR(itau, jm, km, lm));
                     epsL[c3(j, k, l)] = eos_eps(PL(irho, j, k, l), PL(itau, j, k, l));
                     csR[c3(jm, km, lm)] = eos_cs(PR(itau, jm, km, lm), PR(irho, jm, km, lm), epsR[c3(jm, km, lm)]);
@@ -764,6 +772,7 @@ struct Sim {
                     for (int i : {ibt1, ibt2}) {
                         for (int s = -2; s <= 2; ++s) v[s + 2] = BC(i, j + s * dj, k + s * dk, l + s * dl);
                         recon1(w, v, PR(i, jm, km, lm), PL(i, j, k, l));
+                        if (fallback) { PR(i, jm, km, lm) = BC(i, j, k, l); PL(i, j, k, l) = BC(i, j, k, l); }
                     }
                     PR(ibn, jm, km, lm) = P(ibn, jm, km, lm);
                     PL(ibn, j, k, l) = P(ibn, j, k, l);

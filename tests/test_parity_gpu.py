@@ -82,3 +82,17 @@ def test_spherical_fixpole_bitwise(oracle_mod):
     g, o, dg, do = run_pair(spec, prim, eps, 2, oracle_mod)
     assert dg == do
     assert_bitwise(g, o, spec)
+
+
+def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
+    """The headline blast (p 10 : 0.1, beta 0.2 outside) breaks the reference's
+    WENO-Z + HLLD within a few steps (negative face pressure, see
+    test_oracle_invariants); with the optional first-order fallback both
+    implementations run it, bit for bit."""
+    spec, prim, eps = models.blast_3d(24, recon="weno", riemann="hlld", radius=0.2)
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    g, o, dg, do = run_pair(spec, prim, eps, 8, oracle_mod)
+    assert dg == do
+    assert_bitwise(g, o, spec)
+    assert np.isfinite(interior(g["prim"], spec)).all()
