@@ -1321,6 +1321,22 @@ struct Handle {
 
 static std::string g_err;
 
+/* the operation counters are plain globals: counting runs use one thread */
+struct SerialScope {
+    int saved = 1;
+    bool on;
+    explicit SerialScope(bool c) : on(c) {
+#ifdef _OPENMP
+        if (on) { saved = omp_get_max_threads(); omp_set_num_threads(1); }
+#endif
+    }
+    ~SerialScope() {
+#ifdef _OPENMP
+        if (on) omp_set_num_threads(saved);
+#endif
+    }
+};
+
 } // namespace orc
 
 using namespace orc;
@@ -1377,14 +1393,17 @@ void orc_get_array(void *p, int which, double *out) {
     if (h->counting) grab(h->c); else grab(h->d);
 }
 void orc_initial_update(void *p) {
+    SerialScope serial_(((Handle *)p)->counting != 0);
     Handle *h = (Handle *)p;
     if (h->counting) h->c->initial_update(); else h->d->initial_update();
 }
 double orc_finddt(void *p) {
+    SerialScope serial_(((Handle *)p)->counting != 0);
     Handle *h = (Handle *)p;
     return h->counting ? h->c->finddt() : h->d->finddt();
 }
 void orc_rk3_step(void *p, double dt) {
+    SerialScope serial_(((Handle *)p)->counting != 0);
     Handle *h = (Handle *)p;
     if (h->counting) h->c->rungekutta(dt); else h->d->rungekutta(dt);
 }
