@@ -650,6 +650,7 @@ struct cumc_handle {
     int kernels_per_step = 0;
     // flux tiles (autotuned or default): block dims per direction
     dim3 fblk[3];
+    int flux_mode = 1;  // 0 fused recon+Riemann kernel, 1 split kernels
     // captured step graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -807,6 +808,12 @@ static void default_flux_blocks(cumc_handle *h) {
 
 static void launch_flux(cumc_handle *h, int dir) {
     const Dev &d = h->d;
+    if (h->flux_mode == 1) {
+        if (h->cfg.precision == CUMC_FP32) launch_split_fp32(d, dir, h->cfg.recon, h->cfg.riemann, h->stream);
+        else launch_split_fp64(d, dir, h->cfg.recon, h->cfg.riemann, h->stream);
+        h->launches += 2;
+        return;
+    }
     dim3 b = h->fblk[dir];
     dim3 g;
     const int TS = (dir == 0) ? (int)b.x : (int)b.y;
@@ -1084,6 +1091,13 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
         if (d.n_dim > 2) A(d.FZ[i], N3); else d.FZ[i] = d.FX[i];
     }
     for (int i = 0; i < 6; ++i) A(d.EF[i], N3);
+    for (int i = 0; i < 7; ++i) {
+        double *a = nullptr, *b = nullptr;
+        A(a, N3);
+        A(b, N3);
+        d.QL[i] = a;
+        d.QR[i] = b;
+    }
     A(d.EX, N3); A(d.EY, N3); A(d.EZ, N3);
     d.x = upload(h, x); d.dx = upload(h, dx); d.xF = upload(h, xF); d.xbar = upload(h, xbar); d.dx_cb = upload(h, dx_cb);
     d.y = upload(h, y); d.dy = upload(h, dy); d.yF = upload(h, yF); d.sine = upload(h, sine); d.sinf = upload(h, sinf);

@@ -49,6 +49,7 @@ struct Dev {
     double *EF[6];  // face EMFs (yx, zx, xy, zy, xz, yz)
     double *EC[3];  // cell EMFs
     double *EX, *EY, *EZ;  // edge EMFs
+    void *QL[7], *QR[7];   // face states of the split flux path (double or float)
 
     // grid metrics (getgrid.f90), offsets: cells +2, faces +3
     const double *x, *dx, *xF, *xbar, *dx_cb;
@@ -66,5 +67,7 @@ __device__ __forceinline__ int cidx(const Dev &d, int j, int k, int l) {
 // host-side launchers of the face-flux kernels (one per precision unit)
 void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
 void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
+void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
+void launch_split_fp32(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
 
 }  // namespace cumc

@@ -153,6 +153,161 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// split form: k_recon writes the face states, k_riemann consumes them.  The
+// reconstruction (about 70% of the FP64 work, few registers) then runs at
+// full occupancy instead of at the register-limited occupancy of HLLD.
+// Face states: QL[v][f] = right edge of cell f, QR[v][f] = left edge of cell
+// f+1, v = rho, vx, vy, vz, p, first and second transverse cell field.
+// ---------------------------------------------------------------------------
+template <class T, int DIR, int REC>
+__global__ void __launch_bounds__(256) k_recon(const Dev d) {
+    if (d.S->done) return;
+    int c, j, k, l, ns;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
+    const int e = blockIdx.z;
+    if (DIR == 0) { c = a; j = c; k = b + 1; l = e + 1; ns = d.nx; if (k > d.ny) return; }
+    else if (DIR == 1) { c = b; k = c; j = a + 1; l = e + 1; ns = d.ny; if (j > d.nx) return; }
+    else { c = e; l = c; j = a + 1; k = b + 1; ns = d.nz; if (j > d.nx || k > d.ny) return; }
+    if (c > ns + 1) return;
+    const int st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
+    const int ci = cidx(d, j, k, l);
+    constexpr int tb1 = (DIR == 0) ? 1 : 0;
+    constexpr int tb2 = (DIR == 2) ? 1 : 2;
+    const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
+    T w[14];
+    constexpr int NW = (REC == REC_PPM) ? 14 : (REC == REC_WENO) ? 10 : 2;
+#pragma unroll
+    for (int m = 0; m < NW; ++m) w[m] = wp[m];
+    T *const *QL = reinterpret_cast<T *const *>(d.QL);
+    T *const *QR = reinterpret_cast<T *const *>(d.QR);
+    T vm_rho = T(0), vp_rho = T(0);
+    bool fallback = false;
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+        const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
+        T a0 = T(0), a4 = T(0);
+        if (REC == REC_PPM || REC == REC_WENO) {
+            a0 = (T)__ldg(src + ci - 2 * st);
+            a4 = (T)__ldg(src + ci + 2 * st);
+        }
+        T a1 = (T)__ldg(src + ci - st);
+        T a2 = (T)__ldg(src + ci);
+        T a3 = (T)__ldg(src + ci + st);
+        T vm, vp;
+        recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
+        if (v == 0) { vm_rho = vm; vp_rho = vp; }
+        if (v == 4 && d.pos_fallback) {
+            fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
+            if (fallback) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const T cv = (T)__ldg(d.P[u] + ci);
+                    if (c <= ns) QL[u][ci] = cv;
+                    if (c >= 1) QR[u][ci - st] = cv;
+                }
+            }
+        }
+        if (fallback) vm = vp = a2;
+        if (c <= ns) QL[v][ci] = vp;       // left state of face c
+        if (c >= 1) QR[v][ci - st] = vm;   // right state of face c-1
+    }
+}
+
+template <class T, int DIR, int RS>
+__global__ void __launch_bounds__(128) k_riemann(const Dev d) {
+    if (d.S->done) return;
+    int f, j, k, l, ns;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
+    const int e = blockIdx.z;
+    if (DIR == 0) { f = a; j = f; k = b + 1; l = e + 1; ns = d.nx; if (k > d.ny) return; }
+    else if (DIR == 1) { f = b; k = f; j = a + 1; l = e + 1; ns = d.ny; if (j > d.nx) return; }
+    else { f = e; l = f; j = a + 1; k = b + 1; ns = d.nz; if (j > d.nx || k > d.ny) return; }
+    if (f > ns) return;
+    const int ci = cidx(d, j, k, l);
+    constexpr int tb1 = (DIR == 0) ? 1 : 0;
+    constexpr int tb2 = (DIR == 2) ? 1 : 2;
+    using F = Frame<DIR>;
+    const T *const *QL = reinterpret_cast<const T *const *>(d.QL);
+    const T *const *QR = reinterpret_cast<const T *const *>(d.QR);
+    T pl[9], pr[9];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        pl[1 + v] = QL[v][ci];
+        pr[1 + v] = QR[v][ci];
+    }
+    pl[ibx + tb1] = QL[5][ci];
+    pr[ibx + tb1] = QR[5][ci];
+    pl[ibx + tb2] = QL[6][ci];
+    pr[ibx + tb2] = QR[6][ci];
+    const T bn = (T)d.P[F::ibn - 1][ci];
+    pl[F::ibn] = bn;
+    pr[F::ibn] = bn;
+    const T g = (T)d.gamma;
+    const T epsL = eos_eps(pl[irho], pl[itau], g);
+    const T epsR = eos_eps(pr[irho], pr[itau], g);
+    const T csL = eos_cs(pl[itau], pl[irho], epsL, g);
+    const T csR = eos_cs(pr[itau], pr[irho], epsR, g);
+    T fo[9];
+    riemann_face<T, DIR, RS>(pl, pr, epsL, epsR, csL, csR, fo);
+    double *const *FO = (DIR == 0) ? d.FX : (DIR == 1) ? d.FY : d.FZ;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) FO[v][ci] = (double)fo[1 + v];
+    if (DIR == 0) {
+        d.EF[e_yx][ci] = (double)fo[ibz];
+        d.EF[e_zx][ci] = -(double)fo[iby];
+    } else if (DIR == 1) {
+        d.EF[e_xy][ci] = -(double)fo[ibz];
+        d.EF[e_zy][ci] = (double)fo[ibx];
+    } else {
+        d.EF[e_xz][ci] = (double)fo[iby];
+        d.EF[e_yz][ci] = -(double)fo[ibx];
+    }
+}
+
+// launch geometry of the split kernels: x fastest, whole warps along x
+static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &b) {
+    const int extra = recon ? 2 : 1;  // cells 0..n+1 or faces 0..n along the sweep
+    int nx = d.nx, ny = d.ny, nz = d.nz;
+    if (dir == 0) nx = d.nx + extra;
+    if (dir == 1) ny = d.ny + extra;
+    if (dir == 2) nz = d.nz + extra;
+    const int tpb = recon ? 256 : 128;
+    b = dim3(nx >= 64 ? 64 : 32, 1, 1);
+    int by = 1;
+    while (by * 2 <= (int)(tpb / b.x) && by < ny) by *= 2;
+    b.y = by;
+    g = dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
+}
+
+template <class T, int DIR>
+static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s) {
+    dim3 g, b;
+    split_dims(d, DIR, true, g, b);
+    switch (rec) {
+        case REC_TVD_MM: k_recon<T, DIR, REC_TVD_MM><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_VL: k_recon<T, DIR, REC_TVD_VL><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_MC: k_recon<T, DIR, REC_TVD_MC><<<g, b, 0, s>>>(d); break;
+        case REC_PPM: k_recon<T, DIR, REC_PPM><<<g, b, 0, s>>>(d); break;
+        default: k_recon<T, DIR, REC_WENO><<<g, b, 0, s>>>(d); break;
+    }
+    split_dims(d, DIR, false, g, b);
+    switch (rs) {
+        case RS_LF: k_riemann<T, DIR, RS_LF><<<g, b, 0, s>>>(d); break;
+        case RS_HLL: k_riemann<T, DIR, RS_HLL><<<g, b, 0, s>>>(d); break;
+        case RS_HLLC: k_riemann<T, DIR, RS_HLLC><<<g, b, 0, s>>>(d); break;
+        default: k_riemann<T, DIR, RS_HLLD><<<g, b, 0, s>>>(d); break;
+    }
+}
+template <class T>
+static void launch_split_t(const Dev &d, int dir, int rec, int rs, cudaStream_t s) {
+    if (dir == 0) launch_split_dir<T, 0>(d, rec, rs, s);
+    else if (dir == 1) launch_split_dir<T, 1>(d, rec, rs, s);
+    else launch_split_dir<T, 2>(d, rec, rs, s);
+}
+
 template <class T, int DIR, int REC>
 static void launch_rs(const Dev &d, int rs, dim3 g, dim3 b, size_t sm, cudaStream_t s) {
     switch (rs) {
