@@ -1025,6 +1025,8 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     d.eps_y_out_mode = d.bf[2] == 0 ? 0 : (d.bf[3] == 1 ? 1 : (d.bf[3] >= 2 ? 2 : -1));
     d.fixn = cfg->fix_periodic_normal_faces ? 1 : 0;
     d.pos_fallback = cfg->positivity_fallback ? 1 : 0;
+    d.tpb_recon = 256;
+    d.tpb_riemann = 128;
     d.gamma = cfg->model.gamma; d.cfl = cfg->cfl;
     d.floor_kind = cfg->model.floor_kind; d.source_kind = cfg->model.source_kind; d.bc_kind = cfg->model.bc_kind;
     d.rho_floor = cfg->model.rho_floor; d.eps_floor = cfg->model.eps_floor; d.p_floor = cfg->model.p_floor;

@@ -35,6 +35,7 @@ struct Dev {
     int eps_y_out_mode;     // BOUNDARY1D_NM y-outer rule for epsilon (boundary.f90:243)
     int fixn;               // carry periodic normal faces
     int pos_fallback;       // first-order fallback for non-positive edge rho/p
+    int tpb_recon, tpb_riemann;  // threads per block of the split flux kernels (autotuned)
     signed char bfac[6][12];  // parity per side (xin,xout,yin,yout,zin,zout) and variable 1..11
     double gamma, cfl;
     int floor_kind, source_kind, bc_kind;

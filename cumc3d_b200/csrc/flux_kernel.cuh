@@ -274,8 +274,14 @@ static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &
     if (dir == 0) nx = d.nx + extra;
     if (dir == 1) ny = d.ny + extra;
     if (dir == 2) nz = d.nz + extra;
-    const int tpb = recon ? 256 : 128;
-    b = dim3(nx >= 64 ? 64 : 32, 1, 1);
+    const int tpb = recon ? d.tpb_recon : d.tpb_riemann;
+    // x extent: the warp multiple that wastes the fewest threads on the row
+    int bx = 32, best = ((nx + 31) / 32) * 32;
+    for (int cand = 64; cand <= 128 && cand <= tpb; cand *= 2) {
+        int cover = ((nx + cand - 1) / cand) * cand;
+        if (cover <= best) { best = cover; bx = cand; }
+    }
+    b = dim3(bx, 1, 1);
     int by = 1;
     while (by * 2 <= (int)(tpb / b.x) && by < ny) by *= 2;
     b.y = by;
