@@ -1027,6 +1027,7 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     d.pos_fallback = cfg->positivity_fallback ? 1 : 0;
     d.tpb_recon = 256;
     d.tpb_riemann = 128;
+    d.riemann_minb = 1;
     d.gamma = cfg->model.gamma; d.cfl = cfg->cfl;
     d.floor_kind = cfg->model.floor_kind; d.source_kind = cfg->model.source_kind; d.bc_kind = cfg->model.bc_kind;
     d.rho_floor = cfg->model.rho_floor; d.eps_floor = cfg->model.eps_floor; d.p_floor = cfg->model.p_floor;
@@ -1063,6 +1064,21 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     std::vector<double> wx = build_weights(cfg->recon, nx, dx), wy = build_weights(cfg->recon, ny, dy),
                         wz = build_weights(cfg->recon, nz, dz);
     std::vector<float> wxf(wx.begin(), wx.end()), wyf(wy.begin(), wy.end()), wzf(wz.begin(), wz.end());
+    // uniform-spacing specialisation: identical weight rows over the cells a
+    // sweep reconstructs (0..n+1, or -1..n+2 for TVD) go to kernel parameters
+    {
+        const std::vector<double> *W[3] = {&wx, &wy, &wz};
+        const int nn3[3] = {nx, ny, nz};
+        for (int a = 0; a < 3; ++a) {
+            const int lo = (cfg->recon >= 3) ? 0 : -1, hi = (cfg->recon >= 3) ? nn3[a] + 1 : nn3[a] + 2;
+            const double *r0 = &(*W[a])[(size_t)(lo + 2) * 14];
+            bool same = true;
+            for (int j = lo + 1; j <= hi && same; ++j)
+                same = memcmp(r0, &(*W[a])[(size_t)(j + 2) * 14], 14 * sizeof(double)) == 0;
+            d.wuni[a] = same ? 1 : 0;
+            for (int m = 0; m < 14; ++m) { d.wu[a][m] = r0[m]; d.wuf[a][m] = (float)r0[m]; }
+        }
+    }
 
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         g_create_err = "cudaStreamCreate failed";
@@ -1340,6 +1356,57 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out) {
     int rc = check_scalars(h);
     for (int i = 0; i < PC_N; ++i) ms_out[i] = h->prof_ms[i];
     return rc;
+}
+
+// The project's autotuner: times every candidate launch shape of the face-flux
+// kernels of one stage on the live state (the flux kernels only write face
+// arrays, so repeating them has no side effect) and keeps the fastest.
+int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    struct Cand { int mode, tpb_recon, tpb_riemann, minb; };
+    static const Cand cands[] = {
+        {1, 256, 128, 1}, {1, 256, 128, 4}, {1, 128, 128, 1}, {1, 128, 128, 4},
+        {1, 256, 64, 1}, {1, 512, 128, 1}, {0, 256, 128, 1},
+    };
+    const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
+    double best = 1e300;
+    int bi = 0;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (int i = 0; i < nc; ++i) {
+        h->flux_mode = cands[i].mode;
+        h->d.tpb_recon = cands[i].tpb_recon;
+        h->d.tpb_riemann = cands[i].tpb_riemann;
+        h->d.riemann_minb = cands[i].minb;
+        for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir);  // warm-up
+        CK(cudaEventRecord(a, h->stream));
+        const int reps = 3;
+        for (int r = 0; r < reps; ++r)
+            for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir);
+        CK(cudaEventRecord(b, h->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        CK(cudaGetLastError());
+        if (ms / reps < best) { best = ms / reps; bi = i; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->flux_mode = cands[bi].mode;
+    h->d.tpb_recon = cands[bi].tpb_recon;
+    h->d.tpb_riemann = cands[bi].tpb_riemann;
+    h->d.riemann_minb = cands[bi].minb;
+    // a captured step holds the old launch shapes
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    if (choice_out) {
+        choice_out[0] = cands[bi].mode; choice_out[1] = cands[bi].tpb_recon;
+        choice_out[2] = cands[bi].tpb_riemann; choice_out[3] = cands[bi].minb;
+    }
+    if (best_ms_out) *best_ms_out = best;
+    return CUMC_OK;
 }
 
 int cumc_fp64_peak(double *tflops) {

@@ -36,6 +36,10 @@ struct Dev {
     int fixn;               // carry periodic normal faces
     int pos_fallback;       // first-order fallback for non-positive edge rho/p
     int tpb_recon, tpb_riemann;  // threads per block of the split flux kernels (autotuned)
+    int riemann_minb;            // blocks/SM the Riemann kernel is compiled for (1 or 4; autotuned)
+    int wuni[3];                 // 1: the axis's reconstruction weights are identical in every cell
+    double wu[3][14];            // those weights (FP64 form)
+    float wuf[3][14];            // and in FP32
     signed char bfac[6][12];  // parity per side (xin,xout,yin,yout,zin,zout) and variable 1..11
     double gamma, cfl;
     int floor_kind, source_kind, bc_kind;

@@ -160,7 +160,14 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
 // Face states: QL[v][f] = right edge of cell f, QR[v][f] = left edge of cell
 // f+1, v = rho, vx, vy, vz, p, first and second transverse cell field.
 // ---------------------------------------------------------------------------
-template <class T, int DIR, int REC>
+template <class T> __device__ __forceinline__ T uni_w(const Dev &d, int dir, int m);
+template <> __device__ __forceinline__ double uni_w<double>(const Dev &d, int dir, int m) { return d.wu[dir][m]; }
+template <> __device__ __forceinline__ float uni_w<float>(const Dev &d, int dir, int m) { return d.wuf[dir][m]; }
+
+// UNI = 1: every cell along the sweep has the same weights (uniform spacing
+// along this axis, checked bit for bit on the host); they then come from the
+// kernel parameters and live in uniform registers.
+template <class T, int DIR, int REC, int UNI>
 __global__ void __launch_bounds__(256) k_recon(const Dev d) {
     if (d.S->done) return;
     int c, j, k, l, ns;
@@ -175,11 +182,16 @@ __global__ void __launch_bounds__(256) k_recon(const Dev d) {
     const int ci = cidx(d, j, k, l);
     constexpr int tb1 = (DIR == 0) ? 1 : 0;
     constexpr int tb2 = (DIR == 2) ? 1 : 2;
-    const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
     T w[14];
     constexpr int NW = (REC == REC_PPM) ? 14 : (REC == REC_WENO) ? 10 : 2;
+    if (UNI) {
 #pragma unroll
-    for (int m = 0; m < NW; ++m) w[m] = wp[m];
+        for (int m = 0; m < NW; ++m) w[m] = uni_w<T>(d, DIR, m);
+    } else {
+        const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
+#pragma unroll
+        for (int m = 0; m < NW; ++m) w[m] = wp[m];
+    }
     T *const *QL = reinterpret_cast<T *const *>(d.QL);
     T *const *QR = reinterpret_cast<T *const *>(d.QR);
     T vm_rho = T(0), vp_rho = T(0);
@@ -215,8 +227,8 @@ __global__ void __launch_bounds__(256) k_recon(const Dev d) {
     }
 }
 
-template <class T, int DIR, int RS>
-__global__ void __launch_bounds__(128) k_riemann(const Dev d) {
+template <class T, int DIR, int RS, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_riemann(const Dev d) {
     if (d.S->done) return;
     int f, j, k, l, ns;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -288,24 +300,34 @@ static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &
     g = dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
 }
 
+template <class T, int DIR, int UNI>
+static void launch_recon_u(const Dev &d, int rec, dim3 g, dim3 b, cudaStream_t s) {
+    switch (rec) {
+        case REC_TVD_MM: k_recon<T, DIR, REC_TVD_MM, UNI><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_VL: k_recon<T, DIR, REC_TVD_VL, UNI><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_MC: k_recon<T, DIR, REC_TVD_MC, UNI><<<g, b, 0, s>>>(d); break;
+        case REC_PPM: k_recon<T, DIR, REC_PPM, UNI><<<g, b, 0, s>>>(d); break;
+        default: k_recon<T, DIR, REC_WENO, UNI><<<g, b, 0, s>>>(d); break;
+    }
+}
+template <class T, int DIR, int MINB>
+static void launch_riemann_m(const Dev &d, int rs, dim3 g, dim3 b, cudaStream_t s) {
+    switch (rs) {
+        case RS_LF: k_riemann<T, DIR, RS_LF, MINB><<<g, b, 0, s>>>(d); break;
+        case RS_HLL: k_riemann<T, DIR, RS_HLL, MINB><<<g, b, 0, s>>>(d); break;
+        case RS_HLLC: k_riemann<T, DIR, RS_HLLC, MINB><<<g, b, 0, s>>>(d); break;
+        default: k_riemann<T, DIR, RS_HLLD, MINB><<<g, b, 0, s>>>(d); break;
+    }
+}
 template <class T, int DIR>
 static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s) {
     dim3 g, b;
     split_dims(d, DIR, true, g, b);
-    switch (rec) {
-        case REC_TVD_MM: k_recon<T, DIR, REC_TVD_MM><<<g, b, 0, s>>>(d); break;
-        case REC_TVD_VL: k_recon<T, DIR, REC_TVD_VL><<<g, b, 0, s>>>(d); break;
-        case REC_TVD_MC: k_recon<T, DIR, REC_TVD_MC><<<g, b, 0, s>>>(d); break;
-        case REC_PPM: k_recon<T, DIR, REC_PPM><<<g, b, 0, s>>>(d); break;
-        default: k_recon<T, DIR, REC_WENO><<<g, b, 0, s>>>(d); break;
-    }
+    if (d.wuni[DIR]) launch_recon_u<T, DIR, 1>(d, rec, g, b, s);
+    else launch_recon_u<T, DIR, 0>(d, rec, g, b, s);
     split_dims(d, DIR, false, g, b);
-    switch (rs) {
-        case RS_LF: k_riemann<T, DIR, RS_LF><<<g, b, 0, s>>>(d); break;
-        case RS_HLL: k_riemann<T, DIR, RS_HLL><<<g, b, 0, s>>>(d); break;
-        case RS_HLLC: k_riemann<T, DIR, RS_HLLC><<<g, b, 0, s>>>(d); break;
-        default: k_riemann<T, DIR, RS_HLLD><<<g, b, 0, s>>>(d); break;
-    }
+    if (d.riemann_minb == 4) launch_riemann_m<T, DIR, 4>(d, rs, g, b, s);
+    else launch_riemann_m<T, DIR, 1>(d, rs, g, b, s);
 }
 template <class T>
 static void launch_split_t(const Dev &d, int dir, int rec, int rs, cudaStream_t s) {

@@ -74,12 +74,26 @@ __device__ __forceinline__ void ppmc(const T *__restrict__ w, T vm2, T vm1, T vc
 }
 
 // WENO-Z, solver/mhd/weno_module.f90:315-408 (tau5 = |beta1 - beta3|, eps = 1e-40)
+// epsilon of the WENO-Z weights: the reference's 1e-40 in FP64; the FP32 form
+// uses 1e-30 (1e-40 is subnormal in FP32) and caps the ratio so its square
+// stays finite
+template <class T> struct WenoEps;
+template <> struct WenoEps<double> {
+    static __device__ __forceinline__ double eps() { return 1.0e-40; }
+    static __device__ __forceinline__ double cap(double q) { return q; }
+};
+template <> struct WenoEps<float> {
+    static __device__ __forceinline__ float eps() { return 1.0e-30f; }
+    static __device__ __forceinline__ float cap(float q) { return fminf(q, 1.0e15f); }
+};
+
 template <class T>
 __device__ __forceinline__ T wenoz_combine(T P1, T P2, T P3, T B1, T B2, T B3) {
-    const T smallpara = T(1.0e-40);
+    const T smallpara = WenoEps<T>::eps();
     const T g1 = T(1.0 / 10.0), g2 = T(6.0 / 10.0), g3 = T(3.0 / 10.0);
     T tau5 = dabs(B1 - B3);
-    T q1 = tau5 / (smallpara + B1), q2 = tau5 / (smallpara + B2), q3 = tau5 / (smallpara + B3);
+    T q1 = WenoEps<T>::cap(tau5 / (smallpara + B1)), q2 = WenoEps<T>::cap(tau5 / (smallpara + B2)),
+      q3 = WenoEps<T>::cap(tau5 / (smallpara + B3));
     T w1 = g1 * (T(1) + q1 * q1);
     T w2 = g2 * (T(1) + q2 * q2);
     T w3 = g3 * (T(1) + q3 * q3);

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libcumc3d_gpu.so")
 EXPORTS = [
     "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
-    "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak",
+    "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
     "cumc_last_error",
 ]
 
@@ -61,6 +61,7 @@ def load_library(path=None):
     L.cumc_stream.restype = C.c_void_p
     L.cumc_profile_step.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int]
     L.cumc_fp64_peak.argtypes = [C.POINTER(C.c_double)]
+    L.cumc_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
     if path is None:
@@ -159,6 +160,14 @@ class Solver:
         out = (C.c_double * 8)()
         self._check(self.L.cumc_profile_step(self.h, int(nsteps), out, 8))
         return dict(zip(PROFILE_CLASSES, list(out)))
+
+    def autotune(self):
+        """Pick the fastest face-flux launch shape on the live state."""
+        ch = (C.c_int * 4)()
+        ms = C.c_double()
+        self._check(self.L.cumc_autotune(self.h, ch, C.byref(ms)))
+        return dict(split=bool(ch[0]), tpb_recon=ch[1], tpb_riemann=ch[2], riemann_min_blocks=ch[3],
+                    flux_ms_per_stage=ms.value)
 
     def set_state_ptr(self, prim_ptr, eps_ptr):
         """set_state from raw host pointers (e.g. pinned buffers)."""

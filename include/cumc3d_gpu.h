@@ -181,6 +181,14 @@ void *cumc_stream(cumc_handle *h);
  * recovery + floors + EOS), boundary (ghost fill), dt (CFL reduction). */
 int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
 
+/* Autotuner (no counterpart in the reference): times the candidate launch
+ * shapes of the face-flux kernels (fused or split recon/Riemann, threads per
+ * block, register budget of the Riemann kernel) on the handle's live state and
+ * keeps the fastest for all later steps.  choice_out[0..3] = (split?, recon
+ * threads/block, Riemann threads/block, Riemann min blocks/SM); best_ms_out =
+ * the flux time of one stage with that choice.  Either pointer may be NULL. */
+int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out);
+
 /* Measured FP64 fused-multiply-add throughput of the current device in
  * TFLOP/s (the denominator of the FP64-pipe roofline). */
 int cumc_fp64_peak(double *tflops);
