@@ -1409,6 +1409,20 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
     return CUMC_OK;
 }
 
+int cumc_set_tuning(cumc_handle *h, const int *choice) {
+    if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
+    if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 512 || (choice[1] & 31) ||
+        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4))
+        return fail(h, CUMC_EINVAL, "tuning out of range");
+    h->flux_mode = choice[0];
+    h->d.tpb_recon = choice[1];
+    h->d.tpb_riemann = choice[2];
+    h->d.riemann_minb = choice[3];
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return CUMC_OK;
+}
+
 int cumc_fp64_peak(double *tflops) {
     if (!tflops) return CUMC_EINVAL;
     int dev = 0, nsm = 0;

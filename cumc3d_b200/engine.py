@@ -21,6 +21,7 @@ EXPORTS = [
     "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
+    "cumc_set_tuning",
     "cumc_last_error",
 ]
 
@@ -62,6 +63,7 @@ def load_library(path=None):
     L.cumc_profile_step.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int]
     L.cumc_fp64_peak.argtypes = [C.POINTER(C.c_double)]
     L.cumc_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.cumc_set_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
     if path is None:
@@ -168,6 +170,10 @@ class Solver:
         self._check(self.L.cumc_autotune(self.h, ch, C.byref(ms)))
         return dict(split=bool(ch[0]), tpb_recon=ch[1], tpb_riemann=ch[2], riemann_min_blocks=ch[3],
                     flux_ms_per_stage=ms.value)
+
+    def set_tuning(self, split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1):
+        ch = (C.c_int * 4)(int(split), tpb_recon, tpb_riemann, riemann_min_blocks)
+        self._check(self.L.cumc_set_tuning(self.h, ch))
 
     def set_state_ptr(self, prim_ptr, eps_ptr):
         """set_state from raw host pointers (e.g. pinned buffers)."""

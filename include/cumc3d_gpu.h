@@ -189,6 +189,9 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
  * the flux time of one stage with that choice.  Either pointer may be NULL. */
 int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out);
 
+/* Set the launch shape by hand, same four integers as choice_out above. */
+int cumc_set_tuning(cumc_handle *h, const int *choice);
+
 /* Measured FP64 fused-multiply-add throughput of the current device in
  * TFLOP/s (the denominator of the FP64-pipe roofline). */
 int cumc_fp64_peak(double *tflops);

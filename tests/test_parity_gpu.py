@@ -96,3 +96,31 @@ def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
     assert dg == do
     assert_bitwise(g, o, spec)
     assert np.isfinite(interior(g["prim"], spec)).all()
+
+
+@pytest.mark.parametrize("tuning", [
+    dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4),
+    dict(split=True, tpb_recon=128, tpb_riemann=64, riemann_min_blocks=1),
+    dict(split=False, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1),
+])
+def test_every_launch_shape_is_bitwise_identical(oracle_mod, tuning):
+    """The autotuner's candidates differ in blocking and register budget only."""
+    from cumc3d_b200.engine import Solver
+    spec, prim, eps = models.smooth_state(20, 12, 10, 3, boundary_flag=(1, 1, 0, 0, 2, 2), recon="weno",
+                                          riemann="hlld", seed=11)
+    g = Solver(spec)
+    g.set_state(prim, eps)
+    g.initial_update()
+    g.set_tuning(**tuning)
+    o = oracle_mod.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    for _ in range(3):
+        dt = o.finddt()
+        assert g.finddt() == dt
+        g.rungekutta(dt)
+        o.rk3_step(dt)
+    pg, eg = g.get_state()
+    po, eo = o.get_state()
+    assert np.array_equal(interior(pg, spec), interior(po, spec))
+    assert np.array_equal(interior(eg, spec), interior(eo, spec))
