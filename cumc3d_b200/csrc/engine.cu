@@ -1367,7 +1367,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
     struct Cand { int mode, tpb_recon, tpb_riemann, minb; };
     static const Cand cands[] = {
         {1, 256, 128, 1}, {1, 256, 128, 4}, {1, 128, 128, 1}, {1, 128, 128, 4},
-        {1, 256, 64, 1}, {1, 512, 128, 1}, {0, 256, 128, 1},
+        {1, 256, 64, 1}, {1, 128, 64, 4}, {0, 256, 128, 1},
     };
     const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
     double best = 1e300;
@@ -1411,7 +1411,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
 
 int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
-    if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 512 || (choice[1] & 31) ||
+    if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 256 || (choice[1] & 31) ||
         choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4))
         return fail(h, CUMC_EINVAL, "tuning out of range");
     h->flux_mode = choice[0];
