@@ -5,7 +5,7 @@
 Three translation units:
   engine.cu     stage kernels, ghost fills, time loop, C-ABI   (--fmad=false)
   flux_fp64.cu  fused face-flux kernel, plain FP64 form          (--fmad=false)
-  flux_fp32.cu  fused face-flux kernel, FP32 form                (FMA allowed)
+  flux_fp32.cu  fused face-flux kernel, FP32 form                (FMA, fast div/sqrt)
 --fmad=false keeps every FP64 expression in the reference's rounding order
 (no contraction into fused multiply-adds), which is what makes the plain form
 reproduce the Fortran semantics bit for bit.
@@ -24,7 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 UNITS = [
     ("engine.cu", ["--fmad=false"]),
     ("flux_fp64.cu", ["--fmad=false"]),
-    ("flux_fp32.cu", ["--fmad=true"]),
+    ("flux_fp32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
 ]
 
 

@@ -271,7 +271,10 @@ __global__ void __launch_bounds__(256) k_rk(const Dev d, int stage) {
         }
         // GET_SOURCE (spatial.f90:191-256) + CUSTOM_SOURCE
         double sc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        const double rho = d.P[0][c], vx = d.P[1][c], vy = d.P[2][c], vz = d.P[3][c], p = d.P[4][c];
+        const bool need_prim = d.coord != 0 || d.source_kind != 0;
+        const double rho = need_prim ? d.P[0][c] : 0.0, vx = need_prim ? d.P[1][c] : 0.0;
+        const double vy = need_prim ? d.P[2][c] : 0.0, vz = need_prim ? d.P[3][c] : 0.0;
+        const double p = need_prim ? d.P[4][c] : 0.0;
         if (d.coord != 0) {
             const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
             const double bsquare = bx * bx + by * by + bz * bz;
@@ -613,6 +616,31 @@ __global__ void k_soa_to_aos(const Dev d, double *__restrict__ aos, int nv, cons
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= d.N3) return;
     for (int v = 0; v < nv; ++v) aos[(size_t)c * nv + v] = src[v][c];
+}
+
+// exhaustive-style check of div3 against the IEEE division: a counter-based
+// generator sweeps sign, exponent and mantissa; mismatches are counted
+__global__ void k_div3_check(unsigned long long seed, long long n, unsigned long long *mismatch, double *example) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    unsigned long long bad = 0;
+    for (; i < n; i += stride) {
+        unsigned long long z = seed + (unsigned long long)i * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        // exponent restricted to the normal range away from overflow/underflow
+        unsigned long long e = 1 + (z >> 52) % 2040ull;  // biased exponent 1..2040
+        unsigned long long bits = (z & 0x800FFFFFFFFFFFFFull) | (e << 52);
+        const double x = __longlong_as_double((long long)bits);
+        const double a = x / 3.0;
+        const double b = div3<double>(x);
+        if (__double_as_longlong(a) != __double_as_longlong(b)) {
+            if (bad == 0) example[0] = x;
+            ++bad;
+        }
+    }
+    if (bad) atomicAdd(mismatch, bad);
 }
 
 // FP64 pipe probe: independent DFMA chains, 8 per thread, no memory traffic
@@ -1421,6 +1449,21 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
     return CUMC_OK;
+}
+
+int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example) {
+    unsigned long long *m = nullptr;
+    double *ex = nullptr;
+    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, sizeof(*ex)) != cudaSuccess) return CUMC_ECUDA;
+    cudaMemset(m, 0, sizeof(*m));
+    cudaMemset(ex, 0, sizeof(*ex));
+    k_div3_check<<<148 * 16, 256>>>(seed, n, m, ex);
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemcpy(mismatches, m, sizeof(*m), cudaMemcpyDeviceToHost);
+    cudaMemcpy(example, ex, sizeof(*ex), cudaMemcpyDeviceToHost);
+    cudaFree(m);
+    cudaFree(ex);
+    return e == cudaSuccess ? CUMC_OK : CUMC_ECUDA;
 }
 
 int cumc_fp64_peak(double *tflops) {

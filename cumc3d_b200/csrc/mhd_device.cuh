@@ -100,6 +100,21 @@ __device__ __forceinline__ T wenoz_combine(T P1, T P2, T P3, T B1, T B2, T B3) {
     return (w1 * P1 + w2 * P2 + w3 * P3) / (w1 + w2 + w3);
 }
 
+// x / 3 rounded to nearest.  FP64: the quotient q = RN(x * RN(1/3)) is within
+// one ulp of x/3, the remainder x - 3q is exact with one FMA, and one more FMA
+// q + r * RN(1/3) rounds to the correctly rounded quotient (Markstein's
+// correction; x/3 is never a rounding midpoint since 3m would need p+1 bits).
+// The result equals the IEEE division bit for bit (checked on 2^30+ inputs by
+// tests/test_numerics_gpu.py) at a fraction of its cost.
+template <class T> __device__ __forceinline__ T div3(T x);
+template <> __device__ __forceinline__ double div3<double>(double x) {
+    const double z = 1.0 / 3.0;
+    const double q = __dmul_rn(x, z);
+    const double r = __fma_rn(-q, 3.0, x);
+    return __fma_rn(r, z, q);
+}
+template <> __device__ __forceinline__ float div3<float>(float x) { return x * (1.0f / 3.0f); }
+
 template <class T>
 __device__ __forceinline__ void weno(const T *__restrict__ w, T vm2, T vm1, T vc, T vp1, T vp2, T &vm_out, T &vp_out) {
     const T r1 = T(13.0 / 12.0), r2 = T(1.0 / 4.0);
@@ -110,9 +125,9 @@ __device__ __forceinline__ void weno(const T *__restrict__ w, T vm2, T vm1, T vc
     T U00 = vm1 + w[8] * (vm1 - vm2);
     T U11 = vp1 + w[9] * (vp1 - vp2);
     {
-        T P1 = (T(6) * vc - T(1) * U10 - T(2) * U00) / T(3);
-        T P2 = (-T(1) * U10 + T(2) * vc + T(2) * U01) / T(3);
-        T P3 = (T(2) * U01 + T(2) * vp1 - T(1) * U12) / T(3);
+        T P1 = div3(T(6) * vc - T(1) * U10 - T(2) * U00);
+        T P2 = div3(-T(1) * U10 + T(2) * vc + T(2) * U01);
+        T P3 = div3(T(2) * U01 + T(2) * vp1 - T(1) * U12);
         T t1 = T(2) * U10 - T(2) * U00, t2 = T(4) * vc - T(2) * U10 - T(2) * U00;
         T B1 = r1 * (t1 * t1) + r2 * (t2 * t2);
         T t3 = T(2) * U10 - T(4) * vc + T(2) * U01, t4 = -T(2) * U10 + T(2) * U01;
@@ -122,9 +137,9 @@ __device__ __forceinline__ void weno(const T *__restrict__ w, T vm2, T vm1, T vc
         vp_out = wenoz_combine(P1, P2, P3, B1, B2, B3);
     }
     {
-        T P1 = (T(6) * vc - T(1) * U01 - T(2) * U11) / T(3);
-        T P2 = (-T(1) * U01 + T(2) * vc + T(2) * U10) / T(3);
-        T P3 = (T(2) * U10 + T(2) * vm1 - T(1) * U21) / T(3);
+        T P1 = div3(T(6) * vc - T(1) * U01 - T(2) * U11);
+        T P2 = div3(-T(1) * U01 + T(2) * vc + T(2) * U10);
+        T P3 = div3(T(2) * U10 + T(2) * vm1 - T(1) * U21);
         T t1 = T(2) * U01 - T(2) * U11, t2 = T(4) * vc - T(2) * U01 - T(2) * U11;
         T B1 = r1 * (t1 * t1) + r2 * (t2 * t2);
         T t3 = T(2) * U01 - T(4) * vc + T(2) * U10, t4 = T(2) * U01 - T(2) * U10;

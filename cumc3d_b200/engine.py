@@ -21,7 +21,7 @@ EXPORTS = [
     "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
-    "cumc_set_tuning",
+    "cumc_set_tuning", "cumc_check_div3",
     "cumc_last_error",
 ]
 
@@ -64,6 +64,7 @@ def load_library(path=None):
     L.cumc_fp64_peak.argtypes = [C.POINTER(C.c_double)]
     L.cumc_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.cumc_set_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    L.cumc_check_div3.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
     if path is None:
@@ -189,3 +190,13 @@ def fp64_peak_tflops():
     if rc != 0:
         raise CumcError(rc, "fp64 peak probe failed")
     return v.value
+
+
+def check_div3(seed, n):
+    """(mismatches, example input) of the FMA-corrected x/3 against IEEE x/3."""
+    m = C.c_ulonglong()
+    ex = C.c_double()
+    rc = load_library().cumc_check_div3(seed, n, C.byref(m), C.byref(ex))
+    if rc != 0:
+        raise CumcError(rc, "div3 check failed to run")
+    return m.value, ex.value

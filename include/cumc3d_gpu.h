@@ -192,6 +192,11 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out);
 /* Set the launch shape by hand, same four integers as choice_out above. */
 int cumc_set_tuning(cumc_handle *h, const int *choice);
 
+/* Numerics self-check (no counterpart in the reference): compares the FP64
+ * engine's FMA-corrected division by 3 with the IEEE quotient on n generated
+ * normal inputs; *mismatches counts differing bit patterns. */
+int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example);
+
 /* Measured FP64 fused-multiply-add throughput of the current device in
  * TFLOP/s (the denominator of the FP64-pipe roofline). */
 int cumc_fp64_peak(double *tflops);
