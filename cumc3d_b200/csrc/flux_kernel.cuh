@@ -170,14 +170,23 @@ template <> __device__ __forceinline__ float uni_w<float>(const Dev &d, int dir,
 template <class T, int DIR, int REC, int UNI>
 __global__ void __launch_bounds__(256) k_recon(const Dev d) {
     if (d.S->done) return;
+    // one thread per reconstructed cell, enumerated x fastest with no tail
+    // padding per row: x extent nx+2 (x sweep) or nx, then y, then z
     int c, j, k, l, ns;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = blockIdx.y * blockDim.y + threadIdx.y;
-    const int e = blockIdx.z;
-    if (DIR == 0) { c = a; j = c; k = b + 1; l = e + 1; ns = d.nx; if (k > d.ny) return; }
-    else if (DIR == 1) { c = b; k = c; j = a + 1; l = e + 1; ns = d.ny; if (j > d.nx) return; }
-    else { c = e; l = c; j = a + 1; k = b + 1; ns = d.nz; if (j > d.nx || k > d.ny) return; }
-    if (c > ns + 1) return;
+    {
+        const int ex = (DIR == 0) ? d.nx + 2 : d.nx;
+        const int ey = (DIR == 1) ? d.ny + 2 : d.ny;
+        const int ez = (DIR == 2) ? d.nz + 2 : d.nz;
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (long long)ex * ey * ez) return;
+        const int a = (int)(t % ex);
+        const long long r = t / ex;
+        const int b = (int)(r % ey);
+        const int e = (int)(r / ey);
+        if (DIR == 0) { c = a; j = c; k = b + 1; l = e + 1; ns = d.nx; }
+        else if (DIR == 1) { c = b; k = c; j = a + 1; l = e + 1; ns = d.ny; }
+        else { c = e; l = c; j = a + 1; k = b + 1; ns = d.nz; }
+    }
     const int st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
     const int ci = cidx(d, j, k, l);
     constexpr int tb1 = (DIR == 0) ? 1 : 0;
@@ -231,13 +240,21 @@ template <class T, int DIR, int RS, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_riemann(const Dev d) {
     if (d.S->done) return;
     int f, j, k, l, ns;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = blockIdx.y * blockDim.y + threadIdx.y;
-    const int e = blockIdx.z;
-    if (DIR == 0) { f = a; j = f; k = b + 1; l = e + 1; ns = d.nx; if (k > d.ny) return; }
-    else if (DIR == 1) { f = b; k = f; j = a + 1; l = e + 1; ns = d.ny; if (j > d.nx) return; }
-    else { f = e; l = f; j = a + 1; k = b + 1; ns = d.nz; if (j > d.nx || k > d.ny) return; }
-    if (f > ns) return;
+    {
+        const int ex = (DIR == 0) ? d.nx + 1 : d.nx;
+        const int ey = (DIR == 1) ? d.ny + 1 : d.ny;
+        const int ez = (DIR == 2) ? d.nz + 1 : d.nz;
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= (long long)ex * ey * ez) return;
+        const int a = (int)(t % ex);
+        const long long r = t / ex;
+        const int b = (int)(r % ey);
+        const int e = (int)(r / ey);
+        if (DIR == 0) { f = a; j = f; k = b + 1; l = e + 1; ns = d.nx; }
+        else if (DIR == 1) { f = b; k = f; j = a + 1; l = e + 1; ns = d.ny; }
+        else { f = e; l = f; j = a + 1; k = b + 1; ns = d.nz; }
+    }
+    (void)ns;
     const int ci = cidx(d, j, k, l);
     constexpr int tb1 = (DIR == 0) ? 1 : 0;
     constexpr int tb2 = (DIR == 2) ? 1 : 2;
@@ -279,25 +296,18 @@ __global__ void __launch_bounds__(128, MINB) k_riemann(const Dev d) {
     }
 }
 
-// launch geometry of the split kernels: x fastest, whole warps along x
+// launch geometry of the split kernels: a flat 1D grid over the cells (or
+// faces) of one sweep
 static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &b) {
     const int extra = recon ? 2 : 1;  // cells 0..n+1 or faces 0..n along the sweep
-    int nx = d.nx, ny = d.ny, nz = d.nz;
-    if (dir == 0) nx = d.nx + extra;
-    if (dir == 1) ny = d.ny + extra;
-    if (dir == 2) nz = d.nz + extra;
+    long long nx = d.nx, ny = d.ny, nz = d.nz;
+    if (dir == 0) nx += extra;
+    if (dir == 1) ny += extra;
+    if (dir == 2) nz += extra;
     const int tpb = recon ? d.tpb_recon : d.tpb_riemann;
-    // x extent: the warp multiple that wastes the fewest threads on the row
-    int bx = 32, best = ((nx + 31) / 32) * 32;
-    for (int cand = 64; cand <= 128 && cand <= tpb; cand *= 2) {
-        int cover = ((nx + cand - 1) / cand) * cand;
-        if (cover <= best) { best = cover; bx = cand; }
-    }
-    b = dim3(bx, 1, 1);
-    int by = 1;
-    while (by * 2 <= (int)(tpb / b.x) && by < ny) by *= 2;
-    b.y = by;
-    g = dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz);
+    const long long total = nx * ny * nz;
+    b = dim3(tpb, 1, 1);
+    g = dim3((unsigned)((total + tpb - 1) / tpb), 1, 1);
 }
 
 template <class T, int DIR, int UNI>

@@ -383,6 +383,130 @@ __device__ __forceinline__ void hlld_star(const T *pl, const T *pr, const T *ul,
     }
 }
 
+// conserved state of one side, BUILDSTATES spatial.f90:351-362 (same rounding)
+template <class T>
+__device__ __forceinline__ void cons_state(const T *p, T eps, T *u) {
+    T b2 = p[ibx] * p[ibx] + p[iby] * p[iby] + p[ibz] * p[ibz];
+    T v2 = p[ivx] * p[ivx] + p[ivy] * p[ivy] + p[ivz] * p[ivz];
+    u[irho] = p[irho];
+    u[ivx] = p[ivx] * p[irho];
+    u[ivy] = p[ivy] * p[irho];
+    u[ivz] = p[ivz] * p[irho];
+    u[itau] = p[irho] * (T(0.5) * v2 + eps) + T(0.5) * b2;
+}
+
+// HLLD of rsolver_module.f90:613-750 with the same arithmetic as hlld_star,
+// but the physical fluxes and most conserved components are rebuilt where
+// they are used instead of being held across the whole solve (fewer live
+// registers, higher occupancy; identical results).
+template <class T, int DIR>
+__device__ __forceinline__ void hlld_lean(const T *pl, const T *pr, T epsL, T epsR, T *fo, T sL, T sR, T pLt, T pRt) {
+    using F = Frame<DIR>;
+    constexpr int ivn = F::ivn, ivt1 = F::ivt1, ivt2 = F::ivt2, ibn = F::ibn, ibt1 = F::ibt1, ibt2 = F::ibt2;
+    T usL[9], usR[9], pstL[9], pstR[9];
+    T sM = sstar_hllc(pLt, pRt, pl[irho], pr[irho], pl[ivn], pr[ivn], sL, sR, pl[ibn], pr[ibn]);
+    {
+        T ul[9], ur[9];
+        cons_state<T>(pl, epsL, ul);
+        cons_state<T>(pr, epsR, ur);
+#pragma unroll
+        for (int i = irho; i <= itau; ++i) usL[i] = ul[i] * (sL - pl[ivn]) / (sL - sM);
+#pragma unroll
+        for (int i = irho; i <= itau; ++i) usR[i] = ur[i] * (sR - pr[ivn]) / (sR - sM);
+    }
+    T sstarL = sM - dabs(pl[ibn]) / dsqrt(usL[irho]);
+    T sstarR = sM + dabs(pr[ibn]) / dsqrt(usR[irho]);
+    if (((sstarL - sL) < T(1.0e-4) * (sM - sL)) || ((sstarR - sR) > -T(1.0e-4) * (sR - sM))) {
+        const T flt1 = (pl[ivn] * pl[ibt1] - pl[ivt1] * pl[ibn]), frt1 = (pr[ivn] * pr[ibt1] - pr[ivt1] * pr[ibn]);
+        const T flt2 = (pl[ivn] * pl[ibt2] - pl[ivt2] * pl[ibn]), frt2 = (pr[ivn] * pr[ibt2] - pr[ivt2] * pr[ibn]);
+        usL[ibn] = pl[ibn];
+        usL[ibt1] = hll_state(pl[ibt1], pr[ibt1], flt1, frt1, sL, sR);
+        usL[ibt2] = hll_state(pl[ibt2], pr[ibt2], flt2, frt2, sL, sR);
+        usR[ibn] = pr[ibn];
+        usR[ibt1] = usL[ibt1];
+        usR[ibt2] = usL[ibt2];
+        sstarL = sM;
+        sstarR = sM;
+    } else {
+        T fac_1 = (pl[irho] * (sL - pl[ivn]) * (sL - sM) - pl[ibn] * pl[ibn]);
+        usL[ibn] = pl[ibn];
+        usL[ibt1] = (pl[ibt1] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
+        usL[ibt2] = (pl[ibt2] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
+        fac_1 = (pr[irho] * (sR - pr[ivn]) * (sR - sM) - pr[ibn] * pr[ibn]);
+        usR[ibn] = pr[ibn];
+        usR[ibt1] = (pr[ibt1] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
+        usR[ibt2] = (pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
+    }
+    usL[ivn] = usL[irho] * sM;
+    usL[ivt1] = usL[ivt1] - (usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1]) / (sL - sM);
+    usL[ivt2] = usL[ivt2] - (usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2]) / (sL - sM);
+    usR[ivn] = usR[irho] * sM;
+    usR[ivt1] = usR[ivt1] - (usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1]) / (sR - sM);
+    usR[ivt2] = usR[ivt2] - (usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2]) / (sR - sM);
+    pstL[ivn] = sM;
+    pstL[ivt1] = usL[ivt1] / usL[irho];
+    pstL[ivt2] = usL[ivt2] / usL[irho];
+    pstR[ivn] = sM;
+    pstR[ivt1] = usR[ivt1] / usR[irho];
+    pstR[ivt2] = usR[ivt2] / usR[irho];
+    T pLs = pl[irho] * (sL - pl[ivn]) * (sM - pl[ivn]) + pLt;
+    T pRs = pr[irho] * (sR - pr[ivn]) * (sM - pr[ivn]) + pRt;
+    T bdotu = pl[ibx] * pl[ivx] + pl[iby] * pl[ivy] + pl[ibz] * pl[ivz];
+    T bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
+    usL[itau] = usL[itau] + ((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn]) / (sL - sM);
+    bdotu = pr[ibx] * pr[ivx] + pr[iby] * pr[ivy] + pr[ibz] * pr[ivz];
+    bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
+    usR[itau] = usR[itau] + ((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn]) / (sR - sM);
+    // the side whose fan the face lies in; its flux and state are rebuilt here
+    const bool left = (sstarL >= T(0)) || !(sstarR <= T(0)) && (sM >= T(0));
+    const T *pS = left ? pl : pr;
+    const T epsS = left ? epsL : epsR;
+    const T s = left ? sL : sR;
+    T *usS = left ? usL : usR;
+    T uS[9], fS[9];
+    build_state<T, DIR>(pS, epsS, uS, fS);
+    if (sstarL >= T(0) || sstarR <= T(0)) {
+#pragma unroll
+        for (int i = 1; i <= 8; ++i) fo[i] = fS[i] + s * (usS[i] - uS[i]);
+        return;
+    }
+    T ussL[9], ussR[9], pssL[9], pssR[9];
+    ussL[irho] = usL[irho];
+    ussR[irho] = usR[irho];
+    const T sqL = dsqrt(usL[irho]), sqR = dsqrt(usR[irho]);
+    T fac_1 = T(1) / (sqL + sqR);
+    T fac_2 = sign1(pl[ibn]);
+    pssL[ivn] = sM;
+    pssL[ivt1] = fac_1 * (sqL * pstL[ivt1] + sqR * pstR[ivt1] + (usR[ibt1] - usL[ibt1]) * fac_2);
+    pssL[ivt2] = fac_1 * (sqL * pstL[ivt2] + sqR * pstR[ivt2] + (usR[ibt2] - usL[ibt2]) * fac_2);
+    const T sqLR = dsqrt(usL[irho] * usR[irho]);
+    ussL[ibt1] = fac_1 * (sqL * usR[ibt1] + sqR * usL[ibt1] + sqLR * (pstR[ivt1] - pstL[ivt1]) * fac_2);
+    ussL[ibt2] = fac_1 * (sqL * usR[ibt2] + sqR * usL[ibt2] + sqLR * (pstR[ivt2] - pstL[ivt2]) * fac_2);
+    ussL[ibn] = usL[ibn];
+    ussL[ivn] = ussL[irho] * pssL[ivn];
+    ussL[ivt1] = ussL[irho] * pssL[ivt1];
+    ussL[ivt2] = ussL[irho] * pssL[ivt2];
+    bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
+    T bdotuss = ussL[ibx] * pssL[ivx] + ussL[iby] * pssL[ivy] + ussL[ibz] * pssL[ivz];
+    ussL[itau] = usL[itau] - sqL * (bdotus - bdotuss) * fac_2;
+    pssR[ivn] = sM;
+    pssR[ivt1] = pssL[ivt1];
+    pssR[ivt2] = pssL[ivt2];
+    ussR[ibt1] = ussL[ibt1];
+    ussR[ibt2] = ussL[ibt2];
+    ussR[ibn] = usR[ibn];
+    ussR[ivn] = ussR[irho] * pssR[ivn];
+    ussR[ivt1] = ussR[irho] * pssR[ivt1];
+    ussR[ivt2] = ussR[irho] * pssR[ivt2];
+    bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
+    bdotuss = ussR[ibx] * pssR[ivx] + ussR[iby] * pssR[ivy] + ussR[ibz] * pssR[ivz];
+    ussR[itau] = usR[itau] + sqR * (bdotus - bdotuss) * fac_2;
+    const T sst = left ? sstarL : sstarR;
+    T *ussS = left ? ussL : ussR;
+#pragma unroll
+    for (int i = 1; i <= 8; ++i) fo[i] = fS[i] + s * (usS[i] - uS[i]) + sst * (ussS[i] - usS[i]);
+}
+
 // One face: BUILDSTATES + the chosen solver (LFNM 133-222, HLLNM 227-326,
 // HLLCNM 331-514, HLLDNM 519-767).  pl/pr: primitive L/R states (1-based),
 // epsL/R and csL/R from the face EOS.  fo: flux (1-based, 8 comps).
@@ -390,6 +514,25 @@ template <class T, int DIR, int RS>
 __device__ __forceinline__ void riemann_face(const T *pl, const T *pr, T epsL, T epsR, T csL, T csR, T *fo) {
     using F = Frame<DIR>;
     constexpr int ivn = F::ivn, ibn = F::ibn, ibt1 = F::ibt1, ibt2 = F::ibt2;
+    if (RS == RS_HLLD) {
+        T cfsL = signalspeed(csL, pl[ibn], pl[ibt1], pl[ibt2], pl[irho]);
+        T cfsR = signalspeed(csR, pr[ibn], pr[ibt1], pr[ibt2], pr[irho]);
+        T ubar = roe_avg(pl[ivn], pr[ivn], pl[irho], pr[irho]);
+        T cbar = roe_avg(cfsL, cfsR, pl[irho], pr[irho]);
+        T sL = dmin(pl[ivn] - cfsL, ubar - cbar);
+        T sR = dmax(pr[ivn] + cfsR, ubar + cbar);
+        if (sL >= T(0) || sR <= T(0)) {
+            T u[9];
+            build_state<T, DIR>(sL >= T(0) ? pl : pr, sL >= T(0) ? epsL : epsR, u, fo);
+            return;
+        }
+        T b2L = pl[ibx] * pl[ibx] + pl[iby] * pl[iby] + pl[ibz] * pl[ibz];
+        T b2R = pr[ibx] * pr[ibx] + pr[iby] * pr[iby] + pr[ibz] * pr[ibz];
+        T pLt = pl[itau] + T(0.5) * b2L;
+        T pRt = pr[itau] + T(0.5) * b2R;
+        hlld_lean<T, DIR>(pl, pr, epsL, epsR, fo, sL, sR, pLt, pRt);
+        return;
+    }
     T ul[9], ur[9], fl[9], fr[9];
     build_state<T, DIR>(pl, epsL, ul, fl);
     build_state<T, DIR>(pr, epsR, ur, fr);
