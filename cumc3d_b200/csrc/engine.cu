@@ -233,38 +233,62 @@ __global__ void k_fixpole(const Dev d) {
 // ---------------------------------------------------------------------------
 // du/dt and the Shu-Osher combination over j,k,l = 0..n
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_rk(const Dev d, int stage) {
+__global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
     if (d.S->done) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y;
-    const int l = blockIdx.z;
-    if (j > d.nx || k > d.ny || l > d.nz) return;
+    // flat index over j,k,l = 0..n (x fastest)
+    const int ex = d.nx + 1, ey = d.ny + 1, ez = d.nz + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ex * ey * ez) return;
+    const int j = (int)(t % ex);
+    const long long r = t / ex;
+    const int k = (int)(r % ey);
+    const int l = (int)(r / ey);
     const int c = cidx(d, j, k, l);
     const int sy = d.NX, sz = d.NX * d.NY;
+    const bool interior = (j >= 1 && k >= 1 && l >= 1);
+    // issue every independent load first: this kernel is bound by memory-level
+    // parallelism (about 40 streams per cell), not by its arithmetic
+    double fx0[5], fx1[5], fy0[5], fy1[5], fz0[5], fz1[5];
+    if (interior) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            fx0[i] = d.FX[i][c];
+            fx1[i] = d.FX[i][c - 1];
+            fy0[i] = d.n_dim > 1 ? d.FY[i][c] : 0.0;
+            fy1[i] = d.n_dim > 1 ? d.FY[i][c - sy] : 0.0;
+            fz0[i] = d.n_dim > 2 ? d.FZ[i][c] : 0.0;
+            fz1[i] = d.n_dim > 2 ? d.FZ[i][c - sz] : 0.0;
+        }
+    }
+    const double ex0 = d.EX[c], exz = d.EX[c - sz], exy = d.EX[c - sy];
+    const double ey0 = d.EY[c], eyz = d.EY[c - sz], eyx = d.EY[c - 1];
+    const double ez0 = d.EZ[c], ezy = d.EZ[c - sy], ezx = d.EZ[c - 1];
+    double u[8], u0[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        u[i] = d.U[i][c];
+        u0[i] = (stage == 1) ? u[i] : d.U0[i][c];
+    }
     const double dt = d.S->dt;
     double lr[8];
-    const bool interior = (j >= 1 && k >= 1 && l >= 1);
     if (interior) {
         // FLUX_DIFF, spatial.f90:436-583
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
             double dflux, L;
-            const double *F = d.FX[i];
-            if (d.coord == 0) dflux = (F[c] - F[c - 1]) / (DX(j));
-            else if (d.coord == 1) dflux = (XF(j) * F[c] - XF(j - 1) * F[c - 1]) / (XC(j) * DX(j));
-            else dflux = (XF(j) * XF(j) * F[c] - XF(j - 1) * XF(j - 1) * F[c - 1]) / (DXCB(j) / 3.0);
+            if (d.coord == 0) dflux = (fx0[i] - fx1[i]) / (DX(j));
+            else if (d.coord == 1) dflux = (XF(j) * fx0[i] - XF(j - 1) * fx1[i]) / (XC(j) * DX(j));
+            else dflux = (XF(j) * XF(j) * fx0[i] - XF(j - 1) * XF(j - 1) * fx1[i]) / (DXCB(j) / 3.0);
             L = -dflux;
             if (d.n_dim > 1) {
-                F = d.FY[i];
-                if (d.coord == 0) dflux = (F[c] - F[c - sy]) / (DY(k));
-                else if (d.coord == 1) dflux = (F[c] - F[c - sy]) / (XC(j) * DY(k));
-                else dflux = (SINF(k) * F[c] - SINF(k - 1) * F[c - sy]) / (XBAR(j) * DCOSE(k));
+                if (d.coord == 0) dflux = (fy0[i] - fy1[i]) / (DY(k));
+                else if (d.coord == 1) dflux = (fy0[i] - fy1[i]) / (XC(j) * DY(k));
+                else dflux = (SINF(k) * fy0[i] - SINF(k - 1) * fy1[i]) / (XBAR(j) * DCOSE(k));
                 L = L - dflux;
             }
             if (d.n_dim > 2) {
-                F = d.FZ[i];
-                if (d.coord != 2) dflux = (F[c] - F[c - sz]) / DZ(l);
-                else dflux = (F[c] - F[c - sz]) * DY(k) / (XBAR(j) * DZ(l) * DCOSE(k));
+                if (d.coord != 2) dflux = (fz0[i] - fz1[i]) / DZ(l);
+                else dflux = (fz0[i] - fz1[i]) * DY(k) / (XBAR(j) * DZ(l) * DCOSE(k));
                 L = L - dflux;
             }
             lr[i] = L;
@@ -272,41 +296,41 @@ __global__ void __launch_bounds__(256) k_rk(const Dev d, int stage) {
         // GET_SOURCE (spatial.f90:191-256) + CUSTOM_SOURCE
         double sc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         const bool need_prim = d.coord != 0 || d.source_kind != 0;
-        const double rho = need_prim ? d.P[0][c] : 0.0, vx = need_prim ? d.P[1][c] : 0.0;
-        const double vy = need_prim ? d.P[2][c] : 0.0, vz = need_prim ? d.P[3][c] : 0.0;
-        const double p = need_prim ? d.P[4][c] : 0.0;
-        if (d.coord != 0) {
-            const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
-            const double bsquare = bx * bx + by * by + bz * bz;
-            if (d.coord == 1) {
-                sc[1] = sc[1] + (p + rho * vy * vy + 0.5 * bsquare - by * by) / (XC(j));
-                sc[2] = sc[2] - (rho * vx * vy - bx * by) / (XC(j));
-            } else {
-                const double G = 3.0 * XC(j) * DX(j) / DXCB(j);
-                const double tf = DSINE(k) / DCOSE(k);
-                sc[1] = sc[1] + (2.0 * p + bx * bx + rho * (vy * vy + vz * vz)) * G;
-                sc[2] = sc[2] + (p + rho * vz * vz + 0.5 * bsquare - bz * bz) * G * tf - (rho * vx * vy - bx * by) * G;
-                sc[3] = sc[3] - (rho * vx * vz - bx * bz) * G - (rho * vy * vz - by * bz) * G * tf;
+        if (need_prim) {
+            const double rho = d.P[0][c], vx = d.P[1][c], vy = d.P[2][c], vz = d.P[3][c], p = d.P[4][c];
+            if (d.coord != 0) {
+                const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
+                const double bsquare = bx * bx + by * by + bz * bz;
+                if (d.coord == 1) {
+                    sc[1] = sc[1] + (p + rho * vy * vy + 0.5 * bsquare - by * by) / (XC(j));
+                    sc[2] = sc[2] - (rho * vx * vy - bx * by) / (XC(j));
+                } else {
+                    const double G = 3.0 * XC(j) * DX(j) / DXCB(j);
+                    const double tf = DSINE(k) / DCOSE(k);
+                    sc[1] = sc[1] + (2.0 * p + bx * bx + rho * (vy * vy + vz * vz)) * G;
+                    sc[2] = sc[2] + (p + rho * vz * vz + 0.5 * bsquare - bz * bz) * G * tf - (rho * vx * vy - bx * by) * G;
+                    sc[3] = sc[3] - (rho * vx * vz - bx * bz) * G - (rho * vy * vz - by * bz) * G * tf;
+                }
             }
-        }
-        if (d.source_kind == 1) {  // model/riemann/src/custom.f90:299-312
-            sc[2] = sc[2] - d.g_const * rho;
-        } else if (d.source_kind == 2) {  // model/torus-cyn/src/custom.f90:298-314
-            const double diff = rho - d.rho_floor;
-            const double factor = dmax(sign1(diff), 0.0);
-            const double xj = XC(j), zl = ZC(l);
-            const double radius = sqrt(xj * xj + zl * zl);
-            const double dphidr = xj / radius / ((radius - d.r_sh) * (radius - d.r_sh));
-            const double dphidz = zl / radius / ((radius - d.r_sh) * (radius - d.r_sh));
-            sc[1] = sc[1] + (-(factor * rho * dphidr));
-            sc[3] = sc[3] + (-(factor * rho * dphidz));
-            sc[4] = sc[4] + (-(factor * rho * (vx * dphidr + vz * dphidz)));
-        } else if (d.source_kind == 3) {  // model/torus-sph/src/custom.f90 (radial)
-            const double diff = rho - d.rho_floor;
-            const double factor = dmax(sign1(diff), 0.0);
-            const double dphidr = 1.0 / ((XC(j) - d.r_sh) * (XC(j) - d.r_sh));
-            sc[1] = sc[1] + (-(factor * rho * dphidr));
-            sc[4] = sc[4] + (-(factor * rho * vx * dphidr));
+            if (d.source_kind == 1) {  // model/riemann/src/custom.f90:299-312
+                sc[2] = sc[2] - d.g_const * rho;
+            } else if (d.source_kind == 2) {  // model/torus-cyn/src/custom.f90:298-314
+                const double diff = rho - d.rho_floor;
+                const double factor = dmax(sign1(diff), 0.0);
+                const double xj = XC(j), zl = ZC(l);
+                const double radius = sqrt(xj * xj + zl * zl);
+                const double dphidr = xj / radius / ((radius - d.r_sh) * (radius - d.r_sh));
+                const double dphidz = zl / radius / ((radius - d.r_sh) * (radius - d.r_sh));
+                sc[1] = sc[1] + (-(factor * rho * dphidr));
+                sc[3] = sc[3] + (-(factor * rho * dphidz));
+                sc[4] = sc[4] + (-(factor * rho * (vx * dphidr + vz * dphidz)));
+            } else if (d.source_kind == 3) {  // model/torus-sph/src/custom.f90 (radial)
+                const double diff = rho - d.rho_floor;
+                const double factor = dmax(sign1(diff), 0.0);
+                const double dphidr = 1.0 / ((XC(j) - d.r_sh) * (XC(j) - d.r_sh));
+                sc[1] = sc[1] + (-(factor * rho * dphidr));
+                sc[4] = sc[4] + (-(factor * rho * vx * dphidr));
+            }
         }
 #pragma unroll
         for (int i = 0; i < 5; ++i) lr[i] = lr[i] + sc[i];
@@ -315,34 +339,30 @@ __global__ void __launch_bounds__(256) k_rk(const Dev d, int stage) {
         for (int i = 0; i < 5; ++i) lr[i] = 0.0;  // undefined in the reference, never read back
     }
     // l_operator face-B induction, spatial.f90:639-702
-    {
-        const double *EX = d.EX, *EY = d.EY, *EZ = d.EZ;
-        if (d.coord == 0) {
-            lr[5] = -((EZ[c] - EZ[c - sy]) / (DY(k)) - (EY[c] - EY[c - sz]) / (DZ(l)));
-            lr[6] = -((EX[c] - EX[c - sz]) / (DZ(l)) - (EZ[c] - EZ[c - 1]) / (DX(j)));
-            lr[7] = -((EY[c] - EY[c - 1]) / (DX(j)) - (EX[c] - EX[c - sy]) / (DY(k)));
-        } else if (d.coord == 1) {
-            lr[5] = -(EZ[c] - EZ[c - sy]) / (XF(j) * DY(k)) + (EY[c] - EY[c - sz]) / (DZ(l));
-            lr[6] = -(EX[c] - EX[c - sz]) / (DZ(l)) + (EZ[c] - EZ[c - 1]) / (DX(j));
-            lr[7] = -(XF(j) * EY[c] - XF(j - 1) * EY[c - 1]) / (XC(j) * DX(j)) + (EX[c] - EX[c - sy]) / (XC(j) * DY(k));
-        } else {
-            lr[5] = (-(SINF(k) * EZ[c] - SINF(k - 1) * EZ[c - sy]) + (EY[c] - EY[c - sz]) * (DY(k) / DZ(l))) / (XF(j) * DCOSE(k) + small_num);
-            lr[6] = (-(EX[c] - EX[c - sz]) / (XBAR(j) * SINF(k) * DZ(l) + small_num) + (XF(j) * EZ[c] - XF(j - 1) * EZ[c - 1]) / (XC(j) * DX(j)));
-            lr[7] = (-(XF(j) * EY[c] - XF(j - 1) * EY[c - 1]) / (XC(j) * DX(j)) + (EX[c] - EX[c - sy]) / (XBAR(j) * DY(k)));
-        }
+    if (d.coord == 0) {
+        lr[5] = -((ez0 - ezy) / (DY(k)) - (ey0 - eyz) / (DZ(l)));
+        lr[6] = -((ex0 - exz) / (DZ(l)) - (ez0 - ezx) / (DX(j)));
+        lr[7] = -((ey0 - eyx) / (DX(j)) - (ex0 - exy) / (DY(k)));
+    } else if (d.coord == 1) {
+        lr[5] = -(ez0 - ezy) / (XF(j) * DY(k)) + (ey0 - eyz) / (DZ(l));
+        lr[6] = -(ex0 - exz) / (DZ(l)) + (ez0 - ezx) / (DX(j));
+        lr[7] = -(XF(j) * ey0 - XF(j - 1) * eyx) / (XC(j) * DX(j)) + (ex0 - exy) / (XC(j) * DY(k));
+    } else {
+        lr[5] = (-(SINF(k) * ez0 - SINF(k - 1) * ezy) + (ey0 - eyz) * (DY(k) / DZ(l))) / (XF(j) * DCOSE(k) + small_num);
+        lr[6] = (-(ex0 - exz) / (XBAR(j) * SINF(k) * DZ(l) + small_num) + (XF(j) * ez0 - XF(j - 1) * ezx) / (XC(j) * DX(j)));
+        lr[7] = (-(XF(j) * ey0 - XF(j - 1) * eyx) / (XC(j) * DX(j)) + (ex0 - exy) / (XBAR(j) * DY(k)));
     }
     // rungekutta.f90:61-167
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const double u = d.U[i][c];
         double un;
         if (stage == 1) {
-            d.U0[i][c] = u;
-            un = u + dt * lr[i];
+            d.U0[i][c] = u[i];
+            un = u[i] + dt * lr[i];
         } else if (stage == 2) {
-            un = rk20 * d.U0[i][c] + rk21 * u + rk22 * dt * lr[i];
+            un = rk20 * u0[i] + rk21 * u[i] + rk22 * dt * lr[i];
         } else {
-            un = rk30 * d.U0[i][c] + rk31 * u + rk32 * dt * lr[i];
+            un = rk30 * u0[i] + rk31 * u[i] + rk32 * dt * lr[i];
         }
         d.U[i][c] = un;
     }
@@ -959,7 +979,10 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     }
     prof_end(h, PC_EMF);
     prof_begin(h);
-    k_rk<<<g, b, 0, h->stream>>>(d, stage);
+    {
+        const long long cells = (long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+        k_rk<<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
+    }
     h->launches++;
     prof_end(h, PC_RK);
     prof_begin(h);
