@@ -185,6 +185,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--tuning", default="auto",
+                    help="'auto' (the engine's autotuner) or split,tpb_recon,tpb_riemann,min_blocks "
+                         "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -209,7 +212,12 @@ def main():
     s = engine.Solver(spec)
     s.set_state(prim, eps)
     s.initial_update()
-    tuning = s.autotune()
+    if args.tuning == "auto":
+        tuning = s.autotune()
+    else:
+        sp, tr, tm, mb = (int(v) for v in args.tuning.split(","))
+        s.set_tuning(bool(sp), tr, tm, mb)
+        tuning = dict(split=bool(sp), tpb_recon=tr, tpb_riemann=tm, riemann_min_blocks=mb, pinned=True)
     s.evolve(1e30, args.warmup)
     s.sync()
     stream = torch.cuda.ExternalStream(s.stream())
@@ -277,7 +285,10 @@ def main():
         s2 = engine.Solver(spec)
         s2.set_state(prim, eps)  # untimed: the tuner needs a live state
         s2.initial_update()
-        s2.autotune()
+        if args.tuning == "auto":
+            s2.autotune()
+        else:
+            s2.set_tuning(tuning["split"], tuning["tpb_recon"], tuning["tpb_riemann"], tuning["riemann_min_blocks"])
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
