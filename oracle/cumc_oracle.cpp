@@ -1426,6 +1426,44 @@ double orc_max_divb(void *p) {
     Handle *h = (Handle *)p;
     return h->counting ? h->c->find_divb() : h->d->find_divb();
 }
+/* unit hooks for the invariant tests */
+void orc_recon_cell(int rec, const double *w, const double *v5, double *vm, double *vp) {
+    double a, b;
+    if (rec == CUMC_RECON_PPM) Sim<double>::ppmc(w, v5[0], v5[1], v5[2], v5[3], v5[4], a, b);
+    else if (rec == CUMC_RECON_WENO) Sim<double>::weno(w, v5[0], v5[1], v5[2], v5[3], v5[4], a, b);
+    else Sim<double>::tvd(rec, w, v5[1], v5[2], v5[3], a, b);
+    *vm = a; *vp = b;
+}
+void orc_weights(int rec, const double *d5, double *w) {
+    if (rec == CUMC_RECON_PPM) Sim<double>::ppm_interpolant(d5[0], d5[1], d5[2], d5[3], d5[4], w);
+    else if (rec == CUMC_RECON_WENO) Sim<double>::weno_interpolant(d5[0], d5[1], d5[2], d5[3], d5[4], w);
+    else { w[0] = (d5[2] + d5[3]) / d5[2]; w[1] = (d5[2] + d5[1]) / d5[2]; }
+}
+/* one face: BUILDSTATES + solver, states 1-based in arrays of 9 */
+void orc_riemann_face(int dir, int rs, double gamma, const double *pl8, const double *pr8, double *fo8, double *fphys8) {
+    cumc_config c;
+    memset(&c, 0, sizeof c);
+    Sim<double> s;
+    s.cfg = c;
+    s.cfg.riemann = rs;
+    s.ggas = gamma;
+    s.nx = s.ny = s.nz = 1; s.NX = s.NY = s.NZ = 7;
+    size_t n3 = 343;
+    s.primL.assign(8 * n3, 0.0); s.primR.assign(8 * n3, 0.0); s.uL.assign(8 * n3, 0.0); s.uR.assign(8 * n3, 0.0);
+    s.fluxL.assign(8 * n3, 0.0); s.fluxR.assign(8 * n3, 0.0); s.flux.assign(8 * n3, 0.0);
+    s.epsL.assign(n3, 0.0); s.epsR.assign(n3, 0.0); s.csL.assign(n3, 0.0); s.csR.assign(n3, 0.0);
+    const int j = 1, k = 1, l = 1;
+    for (int i = 1; i <= 8; ++i) { s.PL(i, j, k, l) = pl8[i - 1]; s.PR(i, j, k, l) = pr8[i - 1]; }
+    size_t cc = s.c3(j, k, l);
+    s.epsL[cc] = s.eos_eps(pl8[0], pl8[4]); s.epsR[cc] = s.eos_eps(pr8[0], pr8[4]);
+    s.csL[cc] = s.eos_cs(pl8[4], pl8[0], s.epsL[cc]); s.csR[cc] = s.eos_cs(pr8[4], pr8[0], s.epsR[cc]);
+    /* restrict the face loops to the single face (1,1,1) */
+    s.nx = s.ny = s.nz = 1;
+    s.buildstates(dir);
+    s.riemann(dir);
+    for (int i = 1; i <= 8; ++i) { fo8[i - 1] = s.FL(i, j, k, l); fphys8[i - 1] = s.FXL(i, j, k, l); }
+}
+
 void orc_reset_counts(void) { g_ops = OpCounts(); }
 void orc_get_counts(uint64_t *out5) {
     out5[0] = g_ops.add; out5[1] = g_ops.mul; out5[2] = g_ops.div; out5[3] = g_ops.sqrt; out5[4] = g_ops.cmp;

@@ -57,6 +57,9 @@ def lib():
         L.orc_max_divb.restype = C.c_double
         L.orc_get_counts.argtypes = [C.POINTER(C.c_uint64)]
         L.orc_num_threads.restype = C.c_int
+        L.orc_recon_cell.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_weights.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_riemann_face.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -133,3 +136,28 @@ def get_counts():
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+def weights(rec, d5):
+    d5 = np.ascontiguousarray(d5, dtype=np.float64)
+    w = np.zeros(14)
+    lib().orc_weights(rec, d5.ctypes.data, w.ctypes.data)
+    return w
+
+
+def recon_cell(rec, w, v5):
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    v5 = np.ascontiguousarray(v5, dtype=np.float64)
+    vm, vp = C.c_double(), C.c_double()
+    lib().orc_recon_cell(rec, w.ctypes.data, v5.ctypes.data, C.byref(vm), C.byref(vp))
+    return vm.value, vp.value
+
+
+def riemann_face(dir_, rs, gamma, pl, pr):
+    """(Riemann flux, physical flux of the left state) for one face; dir_ 1..3."""
+    pl = np.ascontiguousarray(pl, dtype=np.float64)
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    fo = np.zeros(8)
+    fp = np.zeros(8)
+    lib().orc_riemann_face(dir_, rs, gamma, pl.ctypes.data, pr.ctypes.data, fo.ctypes.data, fp.ctypes.data)
+    return fo, fp
