@@ -1,0 +1,118 @@
+!-------------------------------------------------------------------------------
+! cumc_gpu.f90 -- ISO_C_BINDING interface to libcumc3d_gpu.so (the B200 MHD
+! stage engine, include/cumc3d_gpu.h) for the CUMC3D Fortran host code.
+!
+! With this module the reference's main loop (solver/mhd/main.f90:56-139)
+! keeps its structure: GET_MODEL fills prim/epsilon on the host as before,
+! then the device owns the state.  The routine names mirror the ones they
+! replace: CUMC_INITIAL_UPDATE (INITIAL_UPDATE), CUMC_FINDDT (FINDDT),
+! CUMC_RUNGEKUTTA (RUNGEKUTTA), CUMC_FIND_DIVB (FIND_DIVB).
+!
+! This file is not compiled in this repository (no Fortran compiler in the
+! build image); the C entry points it binds are exercised by tests/.
+!-------------------------------------------------------------------------------
+MODULE CUMC_GPU
+USE ISO_C_BINDING
+IMPLICIT NONE
+
+INTEGER(C_INT), PARAMETER :: CUMC_OK = 0
+INTEGER(C_INT), PARAMETER :: CUMC_RECON_TVD_MM = 0, CUMC_RECON_TVD_VL = 1, CUMC_RECON_TVD_MC = 2
+INTEGER(C_INT), PARAMETER :: CUMC_RECON_PPM = 3, CUMC_RECON_WENO = 4
+INTEGER(C_INT), PARAMETER :: CUMC_RS_LF = 0, CUMC_RS_HLL = 1, CUMC_RS_HLLC = 2, CUMC_RS_HLLD = 3
+INTEGER(C_INT), PARAMETER :: CUMC_FP64 = 0, CUMC_FP32 = 1
+
+! cumc_model (include/cumc3d_gpu.h)
+TYPE, BIND(C) :: cumc_model
+  REAL(C_DOUBLE) :: gamma
+  INTEGER(C_INT) :: floor_kind
+  REAL(C_DOUBLE) :: rho_floor, eps_floor, p_floor
+  INTEGER(C_INT) :: source_kind
+  REAL(C_DOUBLE) :: g_const, r_sh
+  INTEGER(C_INT) :: bc_kind
+END TYPE
+
+! cumc_config (include/cumc3d_gpu.h)
+TYPE, BIND(C) :: cumc_config
+  INTEGER(C_INT) :: nx, ny, nz, n_dim, coordinate_flag
+  INTEGER(C_INT) :: boundary_flag(6)
+  TYPE(C_PTR) :: xF, yF, zF
+  REAL(C_DOUBLE) :: cfl
+  INTEGER(C_INT) :: recon, riemann, precision, learned, fixpole
+  INTEGER(C_INT) :: fix_periodic_normal_faces, positivity_fallback
+  TYPE(cumc_model) :: model
+END TYPE
+
+INTERFACE
+  INTEGER(C_INT) FUNCTION cumc_create(cfg, h) BIND(C, NAME='cumc_create')
+    IMPORT :: C_INT, C_PTR, cumc_config
+    TYPE(cumc_config), INTENT(IN) :: cfg
+    TYPE(C_PTR), INTENT(OUT) :: h
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_destroy(h) BIND(C, NAME='cumc_destroy')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_set_state(h, prim, eps) BIND(C, NAME='cumc_set_state')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(IN) :: prim(*), eps(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_get_state(h, prim, eps) BIND(C, NAME='cumc_get_state')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(OUT) :: prim(*), eps(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_initial_update(h) BIND(C, NAME='cumc_initial_update')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_finddt(h, dt) BIND(C, NAME='cumc_finddt')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(OUT) :: dt
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_rk3_step(h, dt) BIND(C, NAME='cumc_rk3_step')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), VALUE :: dt
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_evolve(h, t_end, max_steps, t, steps) BIND(C, NAME='cumc_evolve')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), VALUE :: t_end
+    INTEGER(C_INT), VALUE :: max_steps
+    REAL(C_DOUBLE), INTENT(INOUT) :: t
+    INTEGER(C_INT), INTENT(OUT) :: steps
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_max_divb(h, divb) BIND(C, NAME='cumc_max_divb')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(OUT) :: divb
+  END FUNCTION
+  TYPE(C_PTR) FUNCTION cumc_last_error(h) BIND(C, NAME='cumc_last_error')
+    IMPORT :: C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+END INTERFACE
+
+TYPE(C_PTR), SAVE :: cumc_h = C_NULL_PTR
+
+CONTAINS
+
+  ! STOP with the engine's message, as the reference STOPs on bad setup
+  SUBROUTINE CUMC_CHECK(rc)
+    INTEGER(C_INT), INTENT(IN) :: rc
+    CHARACTER(KIND=C_CHAR), POINTER :: msg(:)
+    INTEGER :: n
+    IF (rc /= CUMC_OK) THEN
+      CALL C_F_POINTER(cumc_last_error(cumc_h), msg, [512])
+      n = 0
+      DO WHILE (n < 512)
+        IF (msg(n + 1) == C_NULL_CHAR) EXIT
+        n = n + 1
+      END DO
+      WRITE(*,*) 'cumc3d_gpu error ', rc, ': ', msg(1:n)
+      STOP 'cumc3d_gpu'
+    END IF
+  END SUBROUTINE
+END MODULE CUMC_GPU
