@@ -142,6 +142,8 @@ def reference_arm(args):
     from cumc3d_b200 import models
     from oracle import oracle as O
     O.build()
+    if args.workload == "batch1d":
+        return reference_batch(args, world)
     n = 48
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
     spec["positivity_fallback"] = 1
@@ -172,12 +174,164 @@ def reference_arm(args):
     return 0
 
 
+def batch_specs(precision, t_end=0.1):
+    """The batched workload: 512 seeded 1D Riemann problems, n log-uniform in
+    [128, 4096] (seed 20261203), HLLD + PPM, CFL 0.8, t_end 0.1."""
+    from cumc3d_b200 import models
+    params = models.batch_problems(512)
+    return params, [models.riemann_1d(p["n"], p["left"], p["right"], p["bx"], t_end=t_end, precision=precision)
+                    for p in params]
+
+
+def bench_batch(args, world, rank, local, dist):
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import engine
+    params, probs = batch_specs(args.precision)
+    b = engine.BatchSolver([sp for sp, _, _ in probs], positivity_fallback=1)
+
+    def upload():
+        for i, (_, prim, eps) in enumerate(probs):
+            b.set_state(i, prim, eps)
+
+    for _ in range(args.warmup):
+        upload()
+        b.run()
+    stream = torch.cuda.ExternalStream(b.stream())
+    total_ms, zu = 0.0, 0
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.steps):
+        upload()  # untimed: the initial state of every problem
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, steps, status = b.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        zu += int(sum(p["n"] * int(k) for p, k in zip(params, steps)))
+    clk = clocks.stop()
+    ms = total_ms
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * zu / (ms * 1e-3)
+    # end to end through the C-ABI with host buffers: upload, run, download
+    e2e = None
+    if not args.no_e2e:
+        rows = [(np.empty((p["n"] + 6, 8)), np.empty(p["n"] + 6)) for p in params]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        upload()
+        _, steps, _ = b.run()
+        for i, (pr, ep) in enumerate(rows):
+            b.L.cumc_batch_get_state(b.h, i, pr.ctypes.data, ep.ctypes.data)
+        el = time.perf_counter() - t0
+        zu1 = int(sum(p["n"] * int(k) for p, k in zip(params, steps)))
+        h2d = sum(pr.nbytes + ep.nbytes for _, pr, ep in probs)
+        d2h = sum(pr.nbytes + ep.nbytes for pr, ep in rows)
+        e2e = {"value": world * zu1 / el, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "wall_s": el,
+               "note": "a step is one whole batched run (512 problems to t_end)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        sample = [i for i in np.argsort([p["n"] for p in params])[::37]][:8]
+        t0 = time.perf_counter()
+        zc = 0
+        for i in sample:
+            sp, prim, eps = probs[i]
+            o = O.Oracle(dict(sp, positivity_fallback=1))
+            o.set_state(prim, eps)
+            o.initial_update()
+            _, k = o.evolve(sp["t_end"], 10 ** 7)
+            zc += params[i]["n"] * k
+            o.close()
+        el = time.perf_counter() - t0
+        cpu = {"value": zc / el, "unit": "zone-updates/s", "cores": O.num_threads(), "kind": "port",
+               "sample": "CPU oracle, %d of the 512 problems run to t_end one after another (%.1f s)" % (
+                   len(sample), el)}
+    b.close()
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+            "config": {"workload": "batch1d_512_riemann_ppm_hlld_cfl0.8_t0.1", "problems": 512,
+                       "n_range": [128, 4096], "seed": 20261203, "precision": args.precision,
+                       "positivity_fallback": 1,
+                       "step": "one whole batched run: INITIAL_UPDATE + every problem's time loop",
+                       "l2": "per-problem rows are L2-resident by design; state re-uploaded between runs",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def reference_batch(args, world):
+    """The CPU oracle on the batched workload: a sample of its problems, each
+    run to t_end as the reference runs one problem per execution."""
+    import numpy as np
+    from oracle import oracle as O
+    params, probs = batch_specs("fp64")
+    sample = [i for i in np.argsort([p["n"] for p in params])[::37]][:6]
+
+    def one_pass():
+        zc = 0
+        for i in sample:
+            sp, prim, eps = probs[i]
+            o = O.Oracle(dict(sp, positivity_fallback=1))
+            o.set_state(prim, eps)
+            o.initial_update()
+            _, k = o.evolve(sp["t_end"], 10 ** 7)
+            zc += params[i]["n"] * k
+            o.close()
+        return zc
+
+    for _ in range(min(args.warmup, 1)):
+        one_pass()
+    t0 = time.perf_counter()
+    zc = 0
+    nsteps = max(1, min(args.steps, 3))
+    for _ in range(nsteps):
+        zc += one_pass()
+    el = time.perf_counter() - t0
+    value = zc / el
+    sample_txt = "%d of the 512 problems (every 37th by size) run to t_end, %d passes" % (len(sample), nsteps)
+    line = {
+        "impl": "reference", "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+        "n_gpus": world, "steps": nsteps, "warmup": args.warmup, "ms_per_step": el / nsteps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch1d_512_riemann_ppm_hlld_cfl0.8_t0.1 (reference arm: CPU oracle sample)"},
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": sample_txt},
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 200 RK3 steps of the blast; 5 whole runs of the batch)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "batch1d"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--recon", default="weno")
     ap.add_argument("--riemann", default="hlld")
@@ -189,6 +343,8 @@ def main():
                     help="'auto' (the engine's autotuner) or split,tpb_recon,tpb_riemann,min_blocks "
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 200 if args.workload == "blast3d" else 5
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -201,6 +357,8 @@ def main():
     from cumc3d_b200 import engine, models
     torch.cuda.set_device(local)
     engine.load_library()
+    if args.workload == "batch1d":
+        return bench_batch(args, world, rank, local, dist)
 
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)

@@ -25,6 +25,9 @@ UNITS = [
     ("engine.cu", ["--fmad=false"]),
     ("flux_fp64.cu", ["--fmad=false"]),
     ("flux_fp32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
+    ("batch_host.cu", ["--fmad=false"]),
+    ("batch_fp64.cu", ["--fmad=false"]),
+    ("batch_fp32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
 ]
 
 

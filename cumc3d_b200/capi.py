@@ -68,6 +68,19 @@ class CumcConfig(C.Structure):
     ]
 
 
+class CumcBatchConfig(C.Structure):
+    _fields_ = [
+        ("n_problems", C.c_int),
+        ("nx", C.POINTER(C.c_int)),
+        ("xF", C.POINTER(C.POINTER(C.c_double))),
+        ("t_end", C.POINTER(C.c_double)),
+        ("cfl", C.c_double), ("gamma", C.c_double),
+        ("recon", C.c_int), ("riemann", C.c_int), ("precision", C.c_int),
+        ("floor_kind", C.c_int),
+        ("positivity_fallback", C.c_int),
+    ]
+
+
 def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 

@@ -22,6 +22,8 @@ EXPORTS = [
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
     "cumc_set_tuning", "cumc_check_div3",
+    "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
+    "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_last_error",
     "cumc_last_error",
 ]
 
@@ -67,6 +69,16 @@ def load_library(path=None):
     L.cumc_check_div3.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
+    L.cumc_batch_create.argtypes = [C.POINTER(capi.CumcBatchConfig), C.POINTER(C.c_void_p)]
+    L.cumc_batch_destroy.argtypes = [C.c_void_p]
+    L.cumc_batch_set_state.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.cumc_batch_get_state.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    L.cumc_batch_run.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.cumc_batch_sync.argtypes = [C.c_void_p]
+    L.cumc_batch_stream.argtypes = [C.c_void_p]
+    L.cumc_batch_stream.restype = C.c_void_p
+    L.cumc_batch_last_error.argtypes = [C.c_void_p]
+    L.cumc_batch_last_error.restype = C.c_char_p
     if path is None:
         _lib = L
     return L
@@ -182,6 +194,109 @@ class Solver:
 
     def get_state_ptr(self, prim_ptr, eps_ptr):
         self._check(self.L.cumc_get_state(self.h, prim_ptr, eps_ptr))
+
+
+class BatchSolver:
+    """Many independent 1D problems (each a reference n_dim = 1 run of
+    solver/mhd/main.f90) advanced in one persistent launch.
+
+    ``specs`` are 1D specs (ny = nz = 1, outflow everywhere, Cartesian) that
+    share cfl, gamma, the scheme and the precision; each keeps its own grid,
+    initial state and ``t_end``.
+    """
+
+    def __init__(self, specs, positivity_fallback=0):
+        if not specs:
+            raise ValueError("no problems")
+        s0 = specs[0]
+        for sp in specs:
+            if sp["ny"] != 1 or sp["nz"] != 1 or sp["n_dim"] != 1 or sp.get("coordinate_flag", 0) != 0:
+                raise ValueError("batched problems are 1D Cartesian")
+            if tuple(sp["boundary_flag"]) != (1, 1, 1, 1, 1, 1):
+                raise ValueError("batched problems use outflow boundaries")
+            for key in ("cfl", "recon", "riemann", "precision"):
+                if sp[key] != s0[key]:
+                    raise ValueError("batched problems must share %s" % key)
+            if sp["model"].get("gamma") != s0["model"].get("gamma"):
+                raise ValueError("batched problems must share gamma")
+        self.L = load_library()
+        self.specs = specs
+        self.n = [int(sp["nx"]) for sp in specs]
+        self._xf = [np.ascontiguousarray(sp["xF"], dtype=np.float64) for sp in specs]
+        nprob = len(specs)
+        self._nx = (C.c_int * nprob)(*self.n)
+        self._xfp = (C.POINTER(C.c_double) * nprob)(*[a.ctypes.data_as(C.POINTER(C.c_double)) for a in self._xf])
+        self._tend = (C.c_double * nprob)(*[float(sp["t_end"]) for sp in specs])
+        cfg = capi.CumcBatchConfig()
+        cfg.n_problems = nprob
+        cfg.nx = self._nx
+        cfg.xF = self._xfp
+        cfg.t_end = self._tend
+        cfg.cfl = float(s0["cfl"])
+        cfg.gamma = float(s0["model"].get("gamma", 5.0 / 3.0))
+        cfg.recon = capi.RECON[s0["recon"]]
+        cfg.riemann = capi.RIEMANN[s0["riemann"]]
+        cfg.precision = capi.PRECISION[s0["precision"]]
+        cfg.floor_kind = capi.FLOOR[s0["model"].get("floor", "eps")]
+        cfg.positivity_fallback = int(positivity_fallback)
+        self._cfg = cfg
+        h = C.c_void_p()
+        rc = self.L.cumc_batch_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise CumcError(rc, self.L.cumc_batch_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CumcError(rc, self.L.cumc_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cumc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, p, prim, eps):
+        """GET_MODEL output of problem p, shape (7, 7, n+6, 8) / (7, 7, n+6)."""
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        shape = (7, 7, self.n[p] + 6)
+        if prim.shape != shape + (8,) or eps.shape != shape:
+            raise ValueError("state of problem %d must have shape %s" % (p, shape))
+        self._check(self.L.cumc_batch_set_state(self.h, p, prim.ctypes.data, eps.ctypes.data))
+
+    def get_state(self, p):
+        """(prim (n+6, 8), eps (n+6,)) of the (k, l) = (1, 1) row of problem p."""
+        prim = np.empty((self.n[p] + 6, 8))
+        eps = np.empty(self.n[p] + 6)
+        self._check(self.L.cumc_batch_get_state(self.h, p, prim.ctypes.data, eps.ctypes.data))
+        return prim, eps
+
+    def run(self, max_steps=0, check=True):
+        """INITIAL_UPDATE + every time loop; returns (t, steps, status) arrays.
+
+        A problem that reaches a non-finite or non-positive state stops there
+        with status CUMC_ESTATE; with ``check`` the call then raises, without
+        it the per-problem results are returned as they are."""
+        m = len(self.n)
+        t = np.zeros(m)
+        steps = np.zeros(m, dtype=np.int32)
+        status = np.zeros(m, dtype=np.int32)
+        rc = self.L.cumc_batch_run(self.h, int(max_steps), t.ctypes.data, steps.ctypes.data, status.ctypes.data)
+        if rc != 0 and (check or rc != capi.CUMC_ESTATE):
+            self._check(rc)
+        return t, steps, status
+
+    def sync(self):
+        self._check(self.L.cumc_batch_sync(self.h))
+
+    def stream(self):
+        return int(self.L.cumc_batch_stream(self.h) or 0)
 
 
 def fp64_peak_tflops():

@@ -201,6 +201,40 @@ int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mi
  * TFLOP/s (the denominator of the FP64-pipe roofline). */
 int cumc_fp64_peak(double *tflops);
 
+/* ---------------- batched 1D problems ----------------
+ * Many independent 1D MHD problems of uneven size (the reference's n_dim = 1
+ * build, one problem per run, solver/mhd/main.f90) advanced in ONE persistent
+ * launch: each CTA runs INITIAL_UPDATE and the whole time loop of one problem
+ * (own dt, own t_end, own step count) before taking the next, largest first.
+ * Scope: Cartesian 1D, outflow boundaries on every side (the reference's 1D
+ * Riemann tests, model/riemann/src/riemann1d.f90), ideal gas, no sources;
+ * results are bit-identical to running each problem through cumc_create with
+ * ny = nz = 1. */
+typedef struct cumc_batch_config {
+    int n_problems;
+    const int *nx;               /* zones per problem                            */
+    const double *const *xF;     /* per problem: face coordinates -3..nx+3       */
+    const double *t_end;         /* per problem total_time                        */
+    double cfl, gamma;
+    int recon, riemann, precision;
+    int floor_kind;              /* CUMC_FLOOR_NONE or CUMC_FLOOR_EPS            */
+    int positivity_fallback;
+} cumc_batch_config;
+typedef struct cumc_batch cumc_batch;
+int cumc_batch_create(const cumc_batch_config *cfg, cumc_batch **out);
+int cumc_batch_destroy(cumc_batch *b);
+/* prim(8, -2:nx+3, -2:4, -2:4) and epsilon(-2:nx+3, -2:4, -2:4) of problem p
+ * in the reference's 1D layout (GET_MODEL output) */
+int cumc_batch_set_state(cumc_batch *b, int p, const double *prim, const double *eps);
+/* prim(8, -2:nx+3) and epsilon(-2:nx+3) of the (k,l) = (1,1) row of problem p */
+int cumc_batch_get_state(cumc_batch *b, int p, double *prim_row, double *eps_row);
+/* INITIAL_UPDATE + the time loop of every problem, one launch.  Per problem:
+ * t_out = time reached, steps_out = steps taken, status_out = 0 or CUMC_ESTATE. */
+int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, int *status_out);
+int cumc_batch_sync(cumc_batch *b);
+void *cumc_batch_stream(cumc_batch *b);
+const char *cumc_batch_last_error(cumc_batch *b);
+
 /* Message of the last failed call on this handle (or of the last failed
  * cumc_create when h is NULL). */
 const char *cumc_last_error(cumc_handle *h);

@@ -41,7 +41,9 @@ def test_struct_layout_matches_header():
 #include <stddef.h>
 #include "cumc3d_gpu.h"
 int main(void){printf("%zu %zu %zu %zu %zu\n", sizeof(cumc_model), sizeof(cumc_config),
- offsetof(cumc_config, xF), offsetof(cumc_config, cfl), offsetof(cumc_config, model));return 0;}
+ offsetof(cumc_config, xF), offsetof(cumc_config, cfl), offsetof(cumc_config, model));
+ printf("%zu %zu %zu %zu\n", sizeof(cumc_batch_config), offsetof(cumc_batch_config, t_end),
+ offsetof(cumc_batch_config, cfl), offsetof(cumc_batch_config, positivity_fallback));return 0;}
 '''
     import tempfile
     with tempfile.TemporaryDirectory() as d:
@@ -51,7 +53,9 @@ int main(void){printf("%zu %zu %zu %zu %zu\n", sizeof(cumc_model), sizeof(cumc_c
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         vals = list(map(int, subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()))
     assert vals == [C.sizeof(capi.CumcModel), C.sizeof(capi.CumcConfig), capi.CumcConfig.xF.offset,
-                    capi.CumcConfig.cfl.offset, capi.CumcConfig.model.offset]
+                    capi.CumcConfig.cfl.offset, capi.CumcConfig.model.offset,
+                    C.sizeof(capi.CumcBatchConfig), capi.CumcBatchConfig.t_end.offset,
+                    capi.CumcBatchConfig.cfl.offset, capi.CumcBatchConfig.positivity_fallback.offset]
 
 
 def test_create_rejects_bad_configs_before_touching_the_device():
