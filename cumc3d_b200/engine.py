@@ -24,6 +24,7 @@ EXPORTS = [
     "cumc_set_tuning", "cumc_check_div3",
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_last_error",
+    "cumc_batch_run1_noalloc",
     "cumc_last_error",
 ]
 
@@ -79,6 +80,9 @@ def load_library(path=None):
     L.cumc_batch_stream.restype = C.c_void_p
     L.cumc_batch_last_error.argtypes = [C.c_void_p]
     L.cumc_batch_last_error.restype = C.c_char_p
+    L.cumc_batch_run1_noalloc.argtypes = [C.POINTER(capi.CumcBatchConfig), C.c_void_p, C.c_void_p, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_char_p, C.c_size_t]
     if path is None:
         _lib = L
     return L
@@ -297,6 +301,46 @@ class BatchSolver:
 
     def stream(self):
         return int(self.L.cumc_batch_stream(self.h) or 0)
+
+
+def batch_run1_noalloc(spec, prim, eps, max_steps=0, positivity_fallback=0, stream=0):
+    """One 1D problem through ``cumc_batch_run1_noalloc`` (no device
+    allocation; at most 4096 zones).  Returns (prim row (n+6, 8), eps row,
+    t, steps); raises CumcError on a non-zero status."""
+    L = load_library()
+    n = int(spec["nx"])
+    xf = np.ascontiguousarray(spec["xF"], dtype=np.float64)
+    prim = np.ascontiguousarray(prim, dtype=np.float64)
+    eps = np.ascontiguousarray(eps, dtype=np.float64)
+    if prim.shape != (7, 7, n + 6, 8) or eps.shape != (7, 7, n + 6):
+        raise ValueError("state must have shape (7, 7, n+6, 8) / (7, 7, n+6)")
+    nx = (C.c_int * 1)(n)
+    xfp = (C.POINTER(C.c_double) * 1)(xf.ctypes.data_as(C.POINTER(C.c_double)))
+    tend = (C.c_double * 1)(float(spec["t_end"]))
+    cfg = capi.CumcBatchConfig()
+    cfg.n_problems = 1
+    cfg.nx = nx
+    cfg.xF = xfp
+    cfg.t_end = tend
+    cfg.cfl = float(spec["cfl"])
+    cfg.gamma = float(spec["model"].get("gamma", 5.0 / 3.0))
+    cfg.recon = capi.RECON[spec["recon"]]
+    cfg.riemann = capi.RIEMANN[spec["riemann"]]
+    cfg.precision = capi.PRECISION[spec["precision"]]
+    cfg.floor_kind = capi.FLOOR[spec["model"].get("floor", "eps")]
+    cfg.positivity_fallback = int(positivity_fallback)
+    prow = np.empty((n + 6, 8))
+    erow = np.empty(n + 6)
+    t = C.c_double()
+    steps = C.c_int()
+    status = C.c_int()
+    err = C.create_string_buffer(256)
+    rc = L.cumc_batch_run1_noalloc(C.byref(cfg), prim.ctypes.data, eps.ctypes.data, int(max_steps),
+                                   C.c_void_p(stream), prow.ctypes.data, erow.ctypes.data, C.addressof(t),
+                                   C.addressof(steps), C.addressof(status), err, 256)
+    if rc != 0:
+        raise CumcError(rc, err.value.decode())
+    return prow, erow, t.value, steps.value
 
 
 def fp64_peak_tflops():

@@ -235,6 +235,33 @@ int cumc_batch_sync(cumc_batch *b);
 void *cumc_batch_stream(cumc_batch *b);
 const char *cumc_batch_last_error(cumc_batch *b);
 
+/* cumc_batch_run1_noalloc -- NO REFERENCE COUNTERPART (an addition of this
+ * library; the reference allocates its arrays itself at start-up).
+ * One problem of the batched 1D engine, run without any device allocation:
+ * every device buffer comes from one static array per device (about 3.5 MB)
+ * instead of cudaMalloc, and nothing is freed.  For host programs that own
+ * all device memory and let no library allocate: a Fortran/OpenACC code that
+ * maps its arrays once and sizes its pool to what remains, or a time loop that
+ * must not call cudaMalloc/cudaFree because they can synchronise the device
+ * and stall the host's other streams.
+ *   cfg        n_problems must be 1; nx[0] <= 4096, else CUMC_EINVAL ("at most
+ *              4096 zones without allocation") before any device work;
+ *   prim, eps  host, the reference's 1D layout as for cumc_batch_set_state;
+ *   stream     cudaStream_t to run on (NULL: the default stream); the call
+ *              returns after synchronising it;
+ *   prim_row, eps_row  host outputs as for cumc_batch_get_state;
+ *   t_out, steps_out, status_out  as for cumc_batch_run (may be NULL);
+ *   err, err_len  optional buffer for the failure message.
+ * The first call on each device, with that device current, does the set-up
+ * (looks up the static array's address); make it before any stream capture.
+ * Each call clears the work counter and the scratch rows before use.  Calls
+ * that overlap in time on one device share the static array and race:
+ * serialise them.  Results equal cumc_batch_create/_set_state/_run/_get_state
+ * on the same single problem. */
+int cumc_batch_run1_noalloc(const cumc_batch_config *cfg, const double *prim, const double *eps, int max_steps,
+                            void *stream, double *prim_row, double *eps_row, double *t_out, int *steps_out,
+                            int *status_out, char *err, size_t err_len);
+
 /* Message of the last failed call on this handle (or of the last failed
  * cumc_create when h is NULL). */
 const char *cumc_last_error(cumc_handle *h);
