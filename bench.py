@@ -324,6 +324,116 @@ def reference_batch(args, world):
     return 0
 
 
+def _evolve_timed(engine, torch, spec, prim, eps, warmup, steps=None, t_end=None, tuning="auto"):
+    """Run one handle: W warm-up steps, then time the rest (to t_end, or K
+    more steps) with CUDA events on the engine stream.  Returns the handle
+    (still open), timed steps and milliseconds."""
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.initial_update()
+    if tuning == "auto":
+        s.autotune()
+    te = t_end if t_end is not None else 1e30
+    s.evolve(te, warmup)
+    s.sync()
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    _, n = s.evolve(te, steps if steps is not None else 2 ** 31 - 1)
+    e1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    return s, n, e0.elapsed_time(e1)
+
+
+def bench_config(args, world, rank, local, dist):
+    """Other configurations of the path: Brio-Wu (1D, PPM + HLLD), the CP
+    Alfven wave (256^3, one period, FP64 and FP32 with their relative L1), and
+    the cylindrical torus (192 x 128 x 192, WENO + HLLD, 2000 steps)."""
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import capi, engine, models
+    extra = {}
+    clocks = ClockSampler(local)
+    if args.workload == "briowu":
+        spec, prim, eps = models.brio_wu(800, recon=args.recon_c or "ppm", riemann=args.riemann,
+                                         precision=args.precision)
+        zones = 800
+        clocks.start()
+        s, n, ms = _evolve_timed(engine, torch, spec, prim, eps, args.warmup, t_end=spec["t_end"])
+        clk = clocks.stop()
+        name = "briowu_800_%s_%s_cfl0.8_t0.1" % (spec["recon"], spec["riemann"])
+        extra["time_reached"] = s.time
+        s.close()
+    elif args.workload == "alfven3d":
+        n3 = args.n
+        recon = args.recon_c or "ppm"
+        spec, prim, eps = models.alfven_3d(n3, recon=recon, riemann=args.riemann)
+        zones = n3 ** 3
+        out = {}
+        clocks.start()
+        for prec in ("fp64", "fp32"):
+            sp = dict(spec, precision=prec)
+            s, k, t_ms = _evolve_timed(engine, torch, sp, prim, eps, args.warmup, t_end=spec["t_end"])
+            out[prec] = dict(cons=s.get_array(capi.ARR_CONS), divb=s.find_divb(), steps=k, ms=t_ms,
+                             t=s.time)
+            s.close()
+        clk = clocks.stop()
+        # the exact solution after one period is the initial state
+        s0 = engine.Solver(spec)
+        s0.set_state(prim, eps)
+        s0.initial_update()
+        c0 = s0.get_array(capi.ARR_CONS)
+        s0.close()
+        sl = (slice(3, n3 + 3),) * 3
+
+        def rel_l1(a, b):
+            a, b = a[sl].reshape(-1, 8), b[sl].reshape(-1, 8)
+            den = np.abs(b).sum(axis=0)
+            return (np.abs(a - b).sum(axis=0) / np.where(den == 0, 1, den)).tolist()
+        l1_32 = rel_l1(out["fp32"]["cons"], out["fp64"]["cons"])
+        extra.update({
+            "l1_fp32_vs_fp64_per_var": l1_32, "l1_fp32_vs_fp64_max": max(l1_32),
+            "l1_fp64_vs_exact_per_var": rel_l1(out["fp64"]["cons"], c0),
+            "max_divb": {p: out[p]["divb"] for p in out},
+            "fp32_zone_updates_per_s": zones * out["fp32"]["steps"] / (out["fp32"]["ms"] * 1e-3),
+            "fp64_zone_updates_per_s": zones * out["fp64"]["steps"] / (out["fp64"]["ms"] * 1e-3),
+            "period": spec["t_end"], "time_reached": {p: out[p]["t"] for p in out},
+        })
+        extra["fp32_over_fp64"] = extra["fp32_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
+        key = args.precision
+        n, ms = out[key]["steps"], out[key]["ms"]
+        name = "alfven3d_%d^3_%s_%s_cfl0.4_one_period" % (n3, recon, args.riemann)
+    else:  # torus
+        spec, prim, eps = models.torus_cyl(recon=args.recon_c or "weno", riemann=args.riemann,
+                                           precision=args.precision)
+        spec["positivity_fallback"] = 1
+        zones = spec["nx"] * spec["ny"] * spec["nz"]
+        clocks.start()
+        s, n, ms = _evolve_timed(engine, torch, spec, prim, eps, args.warmup, steps=args.steps)
+        clk = clocks.stop()
+        extra["max_divb"] = s.find_divb()
+        extra["time_reached"] = s.time
+        s.close()
+        name = "torus_cyl_192x128x192_%s_%s_ct_cfl0.4" % (spec["recon"], spec["riemann"])
+    value = zones * n / (ms * 1e-3)
+    if rank == 0:
+        line = {"metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+                "steps": n, "warmup": args.warmup, "ms_per_step": ms / max(n, 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+                "config": {"workload": name, "precision": args.precision}, "results": extra,
+                "e2e": None, "cpu_baseline": None, "clocks": clk}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,7 +441,8 @@ def main():
                     help="timed steps (default 200 RK3 steps of the blast; 5 whole runs of the batch)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "batch1d"])
+    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus"])
+    ap.add_argument("--recon-c", default=None, help="reconstruction of the briowu/alfven3d/torus workloads")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--recon", default="weno")
     ap.add_argument("--riemann", default="hlld")
@@ -344,7 +455,7 @@ def main():
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 200 if args.workload == "blast3d" else 5
+        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -359,6 +470,8 @@ def main():
     engine.load_library()
     if args.workload == "batch1d":
         return bench_batch(args, world, rank, local, dist)
+    if args.workload in ("briowu", "alfven3d", "torus"):
+        return bench_config(args, world, rank, local, dist)
 
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)

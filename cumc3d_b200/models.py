@@ -162,13 +162,15 @@ def alfven_3d(n=256, recon="ppm", riemann="hlld", cfl=0.4, precision="fp64", amp
     kvec = kk * np.array([1.0, 1.0, 1.0])
     kmag = np.linalg.norm(kvec)
 
-    # vector potential A = B_par/2 (e1 x r) + amp/|k| (sin(phase) e2 + cos(phase) e3) gives
-    # curl A = B_par e1 + amp (cos(phase) e2 + sin(phase) e3) (uniform part via the first term)
+    # vector potential A = B_par/2 (e1 x r) - amp/|k| (cos(phase) e2 + sin(phase) e3):
+    # curl of f(phase) w is k x f'(phase) w, and e1 x e2 = e3, e1 x e3 = -e2, so
+    # curl A = B_par e1 + amp (cos(phase) e2 + sin(phase) e3), the same transverse
+    # field the velocity below is built from (an exact travelling Alfven wave)
     def A(px, py, pz):
         phase = kvec[0] * px + kvec[1] * py + kvec[2] * pz
         r = np.stack(np.broadcast_arrays(px, py, pz), axis=-1)
         uni = 0.5 * bpar * np.cross(e1, r)
-        wav = (amp / kmag) * (np.sin(phase)[..., None] * e2 + np.cos(phase)[..., None] * e3)
+        wav = -(amp / kmag) * (np.cos(phase)[..., None] * e2 + np.sin(phase)[..., None] * e3)
         return uni + wav
 
     prim = np.zeros((n + 6, n + 6, n + 6, 8), dtype=np.float64)
