@@ -29,6 +29,7 @@ UNITS = [
     ("batch_fp64.cu", ["--fmad=false"]),
     ("batch_fp32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("noalloc.cu", ["--fmad=false"]),
+    ("learned.cu", ["--fmad=false"]),
 ]
 
 

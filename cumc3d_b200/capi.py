@@ -81,6 +81,18 @@ class CumcBatchConfig(C.Structure):
     ]
 
 
+class CumcTrainConfig(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int), ("batch", C.c_int),
+        ("lr", C.c_float), ("delta", C.c_float),
+        ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+        ("seed", C.c_ulonglong),
+    ]
+
+
+LEARN_NP, LEARN_NF, LEARN_ROW = 2657, 35, 37
+
+
 def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 

@@ -29,6 +29,7 @@
 
 #include "../../include/cumc3d_gpu.h"
 #include "engine.cuh"
+#include "learned.cuh"
 #include "mhd_device.cuh"
 
 namespace cumc {
@@ -856,6 +857,11 @@ static void default_flux_blocks(cumc_handle *h) {
 
 static void launch_flux(cumc_handle *h, int dir) {
     const Dev &d = h->d;
+    if (d.learned) {  // FP32 WENO with the learned smooth-face flag (split kernels)
+        launch_split_learned_fp32(d, dir, h->cfg.riemann, h->stream);
+        h->launches += 2;
+        return;
+    }
     if (h->flux_mode == 1) {
         if (h->cfg.precision == CUMC_FP32) launch_split_fp32(d, dir, h->cfg.recon, h->cfg.riemann, h->stream);
         else launch_split_fp64(d, dir, h->cfg.recon, h->cfg.riemann, h->stream);
@@ -1024,7 +1030,11 @@ static int check_scalars(cumc_handle *h) {
         int c = h->S_host->err_cell;
         const Dev &d = h->d;
         int j = c >= 0 ? c % d.NX - 2 : 0, k = c >= 0 ? (c / d.NX) % d.NY - 2 : 0, l = c >= 0 ? c / (d.NX * d.NY) - 2 : 0;
-        snprintf(buf, sizeof buf, "non-finite or non-positive state at cell (%d,%d,%d), stage %d", j, k, l, h->S_host->err_stage);
+        if (h->S_host->err_stage == -1)
+            snprintf(buf, sizeof buf, "learned inference: a tensor-core MMA of tile %d did not complete", c);
+        else
+            snprintf(buf, sizeof buf, "non-finite or non-positive state at cell (%d,%d,%d), stage %d", j, k, l,
+                     h->S_host->err_stage);
         int code = h->S_host->err_code;
         // clear so the handle stays usable after the caller repairs the state
         Scalars z = *h->S_host;
@@ -1051,6 +1061,8 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     if (cfg->recon < 0 || cfg->recon > 4 || cfg->riemann < 0 || cfg->riemann > 3 || cfg->precision < 0 || cfg->precision > 1)
         return fail(nullptr, CUMC_EINVAL, "bad recon/riemann/precision option");
     if (!cfg->xF || !cfg->yF || !cfg->zF) return fail(nullptr, CUMC_EINVAL, "face coordinates missing");
+    if (cfg->learned && (cfg->precision != CUMC_FP32 || cfg->recon != CUMC_RECON_WENO))
+        return fail(nullptr, CUMC_EINVAL, "the learned smooth-face flag needs the FP32 form with WENO reconstruction");
     const int nn[3] = {nx, ny, nz};
     for (int a = 0; a < 3; ++a) {
         int fi = cfg->boundary_flag[2 * a], fo = cfg->boundary_flag[2 * a + 1];
@@ -1183,6 +1195,21 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     if (dv) h->allocs.push_back(dv);
     h->divb_dev = (unsigned long long *)dv;
     ok = ok && cudaMallocHost((void **)&h->S_host, sizeof(Scalars)) == cudaSuccess;
+    if (cfg->learned) {
+        // parameters, per-tile fallback flags, audit counters (the path stays
+        // off until cumc_learn_set supplies parameters)
+        auto B = [&](size_t bytes) -> void * {
+            void *p = nullptr;
+            if (cudaMalloc(&p, bytes) != cudaSuccess) { ok = false; return nullptr; }
+            cudaMemset(p, 0, bytes);
+            h->allocs.push_back(p);
+            return p;
+        };
+        d.mlp = B(sizeof(MlpPacked));
+        for (int a = 0; a < 3; ++a) d.lfb[a] = (unsigned char *)B((size_t)learned_tiles(d, a) + 1);
+        d.lstats = (unsigned long long *)B(sizeof(unsigned long long) * LEARN_STAT_SLOTS * LEARN_STAT_FIELDS);
+        d.learned = 0;
+    }
     if (!ok) {
         g_create_err = "device allocation failed";
         cumc_destroy(h);
@@ -1471,6 +1498,64 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     h->d.riemann_minb = choice[3];
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return CUMC_OK;
+}
+
+int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int audit_interval, float audit_tol) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->cfg.learned || !h->d.mlp) return fail(h, CUMC_EINVAL, "handle was created without the learned flag");
+    if (audit_interval < 0 || !(audit_tol >= 0.0f)) return fail(h, CUMC_EINVAL, "bad audit settings");
+    Dev &d = h->d;
+    if (params) {
+        for (int i = 0; i < LEARN_NP; ++i)
+            if (!std::isfinite(params[i])) return fail(h, CUMC_EINVAL, "non-finite network parameter");
+        MlpPacked hp;
+        learn_pack(params, &hp);
+        CK(cudaMemcpyAsync((void *)d.mlp, &hp, sizeof hp, cudaMemcpyHostToDevice, h->stream));
+    }
+    for (int a = 0; a < 3; ++a) CK(cudaMemsetAsync(d.lfb[a], 0, (size_t)learned_tiles(d, a) + 1, h->stream));
+    CK(cudaMemsetAsync(d.lstats, 0, sizeof(unsigned long long) * LEARN_STAT_SLOTS * LEARN_STAT_FIELDS, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    d.learned = params ? 1 : 0;
+    d.learn_thr = threshold;
+    d.audit_interval = audit_interval;
+    d.audit_tol = audit_tol;
+    // the captured step holds the kernel arguments: capture again
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return CUMC_OK;
+}
+
+int cumc_learn_stats(cumc_handle *h, unsigned long long *out4) {
+    if (!h || !out4) return fail(h, CUMC_EINVAL, "null argument");
+    for (int f = 0; f < LEARN_STAT_FIELDS; ++f) out4[f] = 0;
+    if (!h->d.lstats) return CUMC_OK;
+    unsigned long long buf[LEARN_STAT_SLOTS * LEARN_STAT_FIELDS];
+    CK(cudaMemcpyAsync(buf, h->d.lstats, sizeof buf, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int sl = 0; sl < LEARN_STAT_SLOTS; ++sl)
+        for (int f = 0; f < LEARN_STAT_FIELDS; ++f) out4[f] += buf[sl * LEARN_STAT_FIELDS + f];
+    return CUMC_OK;
+}
+
+int cumc_learn_harvest(cumc_handle *h, int dir, long long stride, float *out, long long cap, long long *rows_out) {
+    if (!h || !out || stride < 1 || dir < 0 || dir > 2) return fail(h, CUMC_EINVAL, "bad argument");
+    if (h->cfg.recon != CUMC_RECON_WENO) return fail(h, CUMC_EINVAL, "harvesting needs WENO reconstruction");
+    if ((dir == 1 && h->d.n_dim < 2) || (dir == 2 && h->d.n_dim < 3))
+        return fail(h, CUMC_EINVAL, "direction not active");
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    const long long rows = harvest_rows(h->d, stride);
+    if (rows_out) *rows_out = rows;
+    if (cap < rows) return fail(h, CUMC_EINVAL, "output buffer too small");
+    float *dbuf = nullptr;
+    CK(cudaMalloc(&dbuf, (size_t)rows * LEARN_ROW * sizeof(float)));
+    launch_harvest(h->d, dir, stride, dbuf, h->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dbuf, (size_t)rows * LEARN_ROW * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dbuf);
+    if (e != cudaSuccess) return fail(h, CUMC_ECUDA, std::string("harvest: ") + cudaGetErrorString(e));
     return CUMC_OK;
 }
 

@@ -63,6 +63,15 @@ struct Dev {
     const double *wx, *wy, *wz;  // reconstruction weights, 14 per cell
     const float *wxf, *wyf, *wzf;
     Scalars *S;
+
+    // learned smooth-face flag of the FP32 WENO form (learned.cuh)
+    int learned;                 // 1: the learned reconstruction kernel replaces k_recon
+    float learn_thr;             // logit above which a cell is flagged smooth
+    int audit_interval;          // full-WENO audit every this many steps (0: never)
+    float audit_tol;             // relative face-value error a tile may show
+    const void *mlp;             // MlpPacked parameters
+    unsigned char *lfb[3];       // per direction, per 128-cell tile: 1 = fall back to WENO-Z
+    unsigned long long *lstats;  // audit counters (LEARN_STAT_SLOTS x LEARN_STAT_FIELDS)
 };
 
 __device__ __forceinline__ int cidx(const Dev &d, int j, int k, int l) {
@@ -74,5 +83,7 @@ void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 bl
 void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
 void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
 void launch_split_fp32(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
+void launch_split_learned_fp32(const Dev &d, int dir, int rs, cudaStream_t s);
+long long learned_tiles(const Dev &d, int dir);
 
 }  // namespace cumc

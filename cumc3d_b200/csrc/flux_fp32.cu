@@ -2,6 +2,7 @@
 // single precision (fused multiply-add allowed); fluxes are widened to FP64
 // before the FP64 CT / RK accumulation in the stage kernels.
 #include "flux_kernel.cuh"
+#include "recon_learned.cuh"
 
 namespace cumc {
 void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
@@ -9,5 +10,28 @@ void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 bl
 }
 void launch_split_fp32(const Dev &d, int dir, int rec, int rs, cudaStream_t s) {
     launch_split_t<float>(d, dir, rec, rs, s);
+}
+
+// tiles of 128 reconstructed cells of one sweep (the learned kernel's CTAs)
+long long learned_tiles(const Dev &d, int dir) {
+    const long long ex = d.nx + (dir == 0 ? 2 : 0), ey = d.ny + (dir == 1 ? 2 : 0), ez = d.nz + (dir == 2 ? 2 : 0);
+    return (ex * ey * ez + 127) / 128;
+}
+
+template <int DIR>
+static void launch_learned_dir(const Dev &d, int rs, cudaStream_t s) {
+    const unsigned tiles = (unsigned)learned_tiles(d, DIR);
+    if (d.wuni[DIR]) k_recon_learned<DIR, 1><<<tiles, 128, 0, s>>>(d);
+    else k_recon_learned<DIR, 0><<<tiles, 128, 0, s>>>(d);
+    dim3 g, b;
+    split_dims(d, DIR, false, g, b);
+    if (d.riemann_minb == 4) launch_riemann_m<float, DIR, 4>(d, rs, g, b, s);
+    else launch_riemann_m<float, DIR, 1>(d, rs, g, b, s);
+}
+
+void launch_split_learned_fp32(const Dev &d, int dir, int rs, cudaStream_t s) {
+    if (dir == 0) launch_learned_dir<0>(d, rs, s);
+    else if (dir == 1) launch_learned_dir<1>(d, rs, s);
+    else launch_learned_dir<2>(d, rs, s);
 }
 }  // namespace cumc

@@ -150,6 +150,78 @@ __device__ __forceinline__ void weno(const T *__restrict__ w, T vm2, T vm1, T vc
     }
 }
 
+// The pieces of weno() above, for the learned smooth-face path: candidate
+// values P and smoothness indicators B of the right (p) and left (m) faces,
+// with the same expressions in the same order.
+template <class T> struct WenoParts { T Pp[3], Bp[3], Pm[3], Bm[3]; };
+template <class T>
+__device__ __forceinline__ void weno_parts(const T *__restrict__ w, T vm2, T vm1, T vc, T vp1, T vp2, WenoParts<T> &o) {
+    const T r1 = T(13.0 / 12.0), r2 = T(1.0 / 4.0);
+    T U01 = w[0] * vc + w[1] * vp1;
+    T U12 = w[2] * vp1 + w[3] * vp2;
+    T U10 = w[4] * vm1 + w[5] * vc;
+    T U21 = w[6] * vm2 + w[7] * vm1;
+    T U00 = vm1 + w[8] * (vm1 - vm2);
+    T U11 = vp1 + w[9] * (vp1 - vp2);
+    o.Pp[0] = div3(T(6) * vc - T(1) * U10 - T(2) * U00);
+    o.Pp[1] = div3(-T(1) * U10 + T(2) * vc + T(2) * U01);
+    o.Pp[2] = div3(T(2) * U01 + T(2) * vp1 - T(1) * U12);
+    {
+        T t1 = T(2) * U10 - T(2) * U00, t2 = T(4) * vc - T(2) * U10 - T(2) * U00;
+        o.Bp[0] = r1 * (t1 * t1) + r2 * (t2 * t2);
+        T t3 = T(2) * U10 - T(4) * vc + T(2) * U01, t4 = -T(2) * U10 + T(2) * U01;
+        o.Bp[1] = r1 * (t3 * t3) + r2 * (t4 * t4);
+        T t5 = T(2) * U01 - T(4) * vp1 + T(2) * U12, t6 = -T(6) * U01 + T(8) * vp1 - T(2) * U12;
+        o.Bp[2] = r1 * (t5 * t5) + r2 * (t6 * t6);
+    }
+    o.Pm[0] = div3(T(6) * vc - T(1) * U01 - T(2) * U11);
+    o.Pm[1] = div3(-T(1) * U01 + T(2) * vc + T(2) * U10);
+    o.Pm[2] = div3(T(2) * U10 + T(2) * vm1 - T(1) * U21);
+    {
+        T t1 = T(2) * U01 - T(2) * U11, t2 = T(4) * vc - T(2) * U01 - T(2) * U11;
+        o.Bm[0] = r1 * (t1 * t1) + r2 * (t2 * t2);
+        T t3 = T(2) * U01 - T(4) * vc + T(2) * U10, t4 = T(2) * U01 - T(2) * U10;
+        o.Bm[1] = r1 * (t3 * t3) + r2 * (t4 * t4);
+        T t5 = T(2) * U10 - T(4) * vm1 + T(2) * U21, t6 = T(8) * vm1 - T(6) * U10 - T(2) * U21;
+        o.Bm[2] = r1 * (t5 * t5) + r2 * (t6 * t6);
+    }
+}
+
+// linear (optimal-weight) fifth-order face values: the WENO candidates
+// combined with g = (0.1, 0.6, 0.3) instead of the nonlinear weights
+template <class T>
+__device__ __forceinline__ void weno_linear(const T *__restrict__ w, T vm2, T vm1, T vc, T vp1, T vp2, T &vm_out,
+                                            T &vp_out) {
+    T U01 = w[0] * vc + w[1] * vp1;
+    T U12 = w[2] * vp1 + w[3] * vp2;
+    T U10 = w[4] * vm1 + w[5] * vc;
+    T U21 = w[6] * vm2 + w[7] * vm1;
+    T U00 = vm1 + w[8] * (vm1 - vm2);
+    T U11 = vp1 + w[9] * (vp1 - vp2);
+    const T g1 = T(1.0 / 10.0), g2 = T(6.0 / 10.0), g3 = T(3.0 / 10.0);
+    vp_out = g1 * div3(T(6) * vc - T(1) * U10 - T(2) * U00) + g2 * div3(-T(1) * U10 + T(2) * vc + T(2) * U01) +
+             g3 * div3(T(2) * U01 + T(2) * vp1 - T(1) * U12);
+    vm_out = g1 * div3(T(6) * vc - T(1) * U01 - T(2) * U11) + g2 * div3(-T(1) * U01 + T(2) * vc + T(2) * U10) +
+             g3 * div3(T(2) * U10 + T(2) * vm1 - T(1) * U21);
+}
+
+// normalised WENO-Z weights (the ones wenoz_combine applies)
+template <class T>
+__device__ __forceinline__ void wenoz_weights(const T B[3], T om[3]) {
+    const T smallpara = WenoEps<T>::eps();
+    const T g1 = T(1.0 / 10.0), g2 = T(6.0 / 10.0), g3 = T(3.0 / 10.0);
+    T tau5 = dabs(B[0] - B[2]);
+    T q1 = WenoEps<T>::cap(tau5 / (smallpara + B[0])), q2 = WenoEps<T>::cap(tau5 / (smallpara + B[1])),
+      q3 = WenoEps<T>::cap(tau5 / (smallpara + B[2]));
+    T w1 = g1 * (T(1) + q1 * q1);
+    T w2 = g2 * (T(1) + q2 * q2);
+    T w3 = g3 * (T(1) + q3 * q3);
+    T sum = w1 + w2 + w3;
+    om[0] = w1 / sum;
+    om[1] = w2 / sum;
+    om[2] = w3 / sum;
+}
+
 // TVD (Mignone 2014) limiters, solver/mhd/tvd_module.f90:279-344
 template <class T, int LIM>
 __device__ __forceinline__ void tvd(const T *__restrict__ w, T vm, T vc, T vp, T &vm_out, T &vp_out) {

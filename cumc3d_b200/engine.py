@@ -25,6 +25,8 @@ EXPORTS = [
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
+    "cumc_learn_set", "cumc_learn_stats", "cumc_learn_harvest", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
 
@@ -80,6 +82,13 @@ def load_library(path=None):
     L.cumc_batch_stream.restype = C.c_void_p
     L.cumc_batch_last_error.argtypes = [C.c_void_p]
     L.cumc_batch_last_error.restype = C.c_char_p
+    L.cumc_learn_set.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_float]
+    L.cumc_learn_stats.argtypes = [C.c_void_p, C.c_void_p]
+    L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
+    L.cumc_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p, C.c_void_p]
+    L.cumc_mlp_train.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(capi.CumcTrainConfig), C.c_void_p, C.c_void_p]
+    L.cumc_mlp_infer.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p]
+    L.cumc_mlp_last_error.restype = C.c_char_p
     L.cumc_batch_run1_noalloc.argtypes = [C.POINTER(capi.CumcBatchConfig), C.c_void_p, C.c_void_p, C.c_int,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_char_p, C.c_size_t]
@@ -191,6 +200,34 @@ class Solver:
     def set_tuning(self, split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1):
         ch = (C.c_int * 4)(int(split), tpb_recon, tpb_riemann, riemann_min_blocks)
         self._check(self.L.cumc_set_tuning(self.h, ch))
+
+    # ---- learned smooth-face flag (FP32 WENO form, handle created with learned=1) ----
+    def learn_set(self, params, threshold=0.0, audit_interval=10, audit_tol=1e-6):
+        """Enable the flag with these parameters (float[2657]); None disables it."""
+        if params is None:
+            self._check(self.L.cumc_learn_set(self.h, None, float(threshold), int(audit_interval), float(audit_tol)))
+            return
+        P = np.ascontiguousarray(params, dtype=np.float32)
+        if P.shape != (capi.LEARN_NP,):
+            raise ValueError("parameters must have %d entries" % capi.LEARN_NP)
+        self._check(self.L.cumc_learn_set(self.h, P.ctypes.data, float(threshold), int(audit_interval),
+                                          float(audit_tol)))
+
+    def learn_stats(self):
+        """Audit counters: cells audited, flagged, tiles set to fall back, audits."""
+        out = (C.c_ulonglong * 4)()
+        self._check(self.L.cumc_learn_stats(self.h, out))
+        return dict(audited=out[0], flagged=out[1], fallback_tiles=out[2], audits=out[3])
+
+    def learn_harvest(self, direction, stride=1):
+        """Samples (rows of 37 floats) of every stride-th interior cell, one sweep."""
+        n = self.spec["nx"] * self.spec["ny"] * self.spec["nz"]
+        rows = (n + stride - 1) // stride
+        out = np.empty((rows, capi.LEARN_ROW), dtype=np.float32)
+        got = C.c_longlong()
+        self._check(self.L.cumc_learn_harvest(self.h, int(direction), int(stride), out.ctypes.data, rows,
+                                              C.byref(got)))
+        return out[:got.value]
 
     def set_state_ptr(self, prim_ptr, eps_ptr):
         """set_state from raw host pointers (e.g. pinned buffers)."""
@@ -341,6 +378,59 @@ def batch_run1_noalloc(spec, prim, eps, max_steps=0, positivity_fallback=0, stre
     if rc != 0:
         raise CumcError(rc, err.value.decode())
     return prow, erow, t.value, steps.value
+
+
+def _mlp_check(L, rc):
+    if rc != 0:
+        raise CumcError(rc, L.cumc_mlp_last_error().decode())
+
+
+def mlp_init(seed=0):
+    """He-uniform initial parameters of the flag network (inputs 35..47 zero)."""
+    rng = np.random.default_rng(seed)
+    P = np.zeros(capi.LEARN_NP, dtype=np.float32)
+    lim1 = np.sqrt(6.0 / capi.LEARN_NF)
+    W1 = np.zeros((32, 48), dtype=np.float32)
+    W1[:, :capi.LEARN_NF] = rng.uniform(-lim1, lim1, (32, capi.LEARN_NF))
+    P[0:1536] = W1.ravel()
+    lim2 = np.sqrt(6.0 / 32)
+    P[1568:2592] = rng.uniform(-lim2, lim2, 32 * 32)
+    P[2624:2656] = rng.uniform(-lim2, lim2, 32)
+    return P
+
+
+def mlp_grad(params, samples, delta):
+    """(mean loss, gradient) of the flag network on the GPU (FP32)."""
+    L = load_library()
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    S = np.ascontiguousarray(samples, dtype=np.float32)
+    g = np.zeros(capi.LEARN_NP, dtype=np.float32)
+    loss = C.c_float()
+    _mlp_check(L, L.cumc_mlp_grad(P.ctypes.data, S.ctypes.data, S.shape[0], float(delta), g.ctypes.data,
+                                  C.byref(loss)))
+    return loss.value, g
+
+
+def mlp_train(samples, params, steps=2000, batch=4096, lr=1e-3, delta=1e-6, seed=1):
+    """Adam on the GPU; returns (parameters, loss per step)."""
+    L = load_library()
+    P = np.array(params, dtype=np.float32, copy=True)
+    S = np.ascontiguousarray(samples, dtype=np.float32)
+    tc = capi.CumcTrainConfig(steps=int(steps), batch=int(batch), lr=float(lr), delta=float(delta), beta1=0.0,
+                              beta2=0.0, eps=0.0, seed=int(seed))
+    losses = np.zeros(int(steps), dtype=np.float32)
+    _mlp_check(L, L.cumc_mlp_train(S.ctypes.data, S.shape[0], C.byref(tc), P.ctypes.data, losses.ctypes.data))
+    return P, losses
+
+
+def mlp_infer(params, features):
+    """Logits of feature rows on the tensor cores (the reconstruction kernel's MLP)."""
+    L = load_library()
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(features, dtype=np.float32)
+    z = np.zeros(X.shape[0], dtype=np.float32)
+    _mlp_check(L, L.cumc_mlp_infer(P.ctypes.data, X.ctypes.data, X.shape[1], X.shape[0], z.ctypes.data))
+    return z
 
 
 def fp64_peak_tflops():

@@ -235,6 +235,47 @@ int cumc_batch_sync(cumc_batch *b);
 void *cumc_batch_stream(cumc_batch *b);
 const char *cumc_batch_last_error(cumc_batch *b);
 
+/* ---------------- learned smooth-face flag (FP32 WENO form) ----------------
+ * No reference counterpart: the reference always applies the WENO-Z
+ * nonlinear weights (solver/mhd/weno_module.f90:363-404).  A 35-32-32-1 MLP
+ * over scale-free stencil features flags cells whose WENO-Z face values are
+ * within a tolerance of the linear optimal-weight fifth-order values; warps
+ * of 32 flagged cells reconstruct with the linear weights.  Inference is
+ * fused into the reconstruction kernel (BF16 tcgen05 MMA, FP32 accumulators
+ * in tensor memory); every audit_interval steps a full WENO-Z audit marks
+ * 128-cell tiles whose flagged cells are off by more than audit_tol to fall
+ * back to WENO-Z until the next audit.
+ * Parameters: float[CUMC_LEARN_NP] = W1[32][48] (out, in; inputs 35..47
+ * unused), b1[32], W2[32][32], b2[32], w3[32], b3.
+ * Samples: rows of CUMC_LEARN_ROW floats = 35 features, the relative
+ * face-value change the linear weights make (FP64 WENO-Z of the plain
+ * method), the largest nonlinear-weight deviation |omega_k - g_k|. */
+#define CUMC_LEARN_NP   2657
+#define CUMC_LEARN_NF   35
+#define CUMC_LEARN_ROW  37
+typedef struct cumc_train_config {
+    int steps, batch;            /* Adam steps, samples per step               */
+    float lr, delta;             /* learning rate; label: change < delta       */
+    float beta1, beta2, eps;     /* Adam (0: 0.9, 0.999, 1e-8)                 */
+    unsigned long long seed;     /* minibatch sampling                         */
+} cumc_train_config;
+/* enable (params != NULL) or disable the flag on a handle created with
+ * learned = 1 (FP32 + WENO); resets the fallback tiles and the counters */
+int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int audit_interval, float audit_tol);
+/* audit counters: cells audited, cells flagged, tiles set to fall back, audits */
+int cumc_learn_stats(cumc_handle *h, unsigned long long *out4);
+/* samples of every stride-th interior cell of the current state, sweep dir */
+int cumc_learn_harvest(cumc_handle *h, int dir, long long stride, float *out, long long cap, long long *rows_out);
+/* mean loss and gradient over n samples (FP32, deterministic order) */
+int cumc_mlp_grad(const float *params, const float *samples, long long n, float delta, float *grad_out,
+                  float *loss_out);
+/* Adam training on the GPU; params in/out, loss per step (may be NULL) */
+int cumc_mlp_train(const float *samples, long long n, const cumc_train_config *tc, float *params_inout,
+                   float *loss_curve);
+/* logits of n feature rows (leading dimension ld >= 35) on the tensor cores */
+int cumc_mlp_infer(const float *params, const float *features, int ld, long long n, float *logits);
+const char *cumc_mlp_last_error(void);
+
 /* cumc_batch_run1_noalloc -- NO REFERENCE COUNTERPART (an addition of this
  * library; the reference allocates its arrays itself at start-up).
  * One problem of the batched 1D engine, run without any device allocation:

@@ -1464,6 +1464,146 @@ void orc_riemann_face(int dir, int rs, double gamma, const double *pl8, const do
     for (int i = 1; i <= 8; ++i) { fo8[i - 1] = s.FL(i, j, k, l); fphys8[i - 1] = s.FXL(i, j, k, l); }
 }
 
+/* ------------------------------------------------------------------ */
+/* Learned smooth-face flag (no reference counterpart): the CPU checker */
+/* of the GPU harvest, trainer and inference.  Features in float        */
+/* arithmetic, labels from the FP64 WENO-Z of weno_module.f90:363-404.  */
+/* ------------------------------------------------------------------ */
+static void lrn_var_features(float a0, float a1, float a2, float a3, float a4, float *f4, float *r) {
+    const float d0 = a1 - a0, d1 = a2 - a1, d2 = a3 - a2, d3 = a4 - a3;
+    const float sum = ((std::fabs(d0) + std::fabs(d1)) + std::fabs(d2)) + std::fabs(d3);
+    const float den = sum + 1.0e-30f;
+    f4[0] = d0 / den;
+    f4[1] = d1 / den;
+    f4[2] = d2 / den;
+    f4[3] = d3 / den;
+    *r = sum / ((std::fabs(a2) + sum) + 1.0e-30f);
+}
+
+/* WENO-Z candidates P and indicators B of the right (p) and left (m) face */
+static void lrn_parts(const double *w, double vm2, double vm1, double vc, double vp1, double vp2, double *Pp,
+                      double *Bp, double *Pm, double *Bm) {
+    double U01 = w[0] * vc + w[1] * vp1;
+    double U12 = w[2] * vp1 + w[3] * vp2;
+    double U10 = w[4] * vm1 + w[5] * vc;
+    double U21 = w[6] * vm2 + w[7] * vm1;
+    double U00 = vm1 + w[8] * (vm1 - vm2);
+    double U11 = vp1 + w[9] * (vp1 - vp2);
+    Pp[0] = (6.0 * vc - 1.0 * U10 - 2.0 * U00) / 3.0;
+    Pp[1] = (-1.0 * U10 + 2.0 * vc + 2.0 * U01) / 3.0;
+    Pp[2] = (2.0 * U01 + 2.0 * vp1 - 1.0 * U12) / 3.0;
+    double t1 = 2.0 * U10 - 2.0 * U00, t2 = 4.0 * vc - 2.0 * U10 - 2.0 * U00;
+    Bp[0] = r_weno_1 * (t1 * t1) + r_weno_2 * (t2 * t2);
+    double t3 = 2.0 * U10 - 4.0 * vc + 2.0 * U01, t4 = -2.0 * U10 + 2.0 * U01;
+    Bp[1] = r_weno_1 * (t3 * t3) + r_weno_2 * (t4 * t4);
+    double t5 = 2.0 * U01 - 4.0 * vp1 + 2.0 * U12, t6 = -6.0 * U01 + 8.0 * vp1 - 2.0 * U12;
+    Bp[2] = r_weno_1 * (t5 * t5) + r_weno_2 * (t6 * t6);
+    Pm[0] = (6.0 * vc - 1.0 * U01 - 2.0 * U11) / 3.0;
+    Pm[1] = (-1.0 * U01 + 2.0 * vc + 2.0 * U10) / 3.0;
+    Pm[2] = (2.0 * U10 + 2.0 * vm1 - 1.0 * U21) / 3.0;
+    t1 = 2.0 * U01 - 2.0 * U11; t2 = 4.0 * vc - 2.0 * U01 - 2.0 * U11;
+    Bm[0] = r_weno_1 * (t1 * t1) + r_weno_2 * (t2 * t2);
+    t3 = 2.0 * U01 - 4.0 * vc + 2.0 * U10; t4 = 2.0 * U01 - 2.0 * U10;
+    Bm[1] = r_weno_1 * (t3 * t3) + r_weno_2 * (t4 * t4);
+    t5 = 2.0 * U10 - 4.0 * vm1 + 2.0 * U21; t6 = 8.0 * vm1 - 6.0 * U10 - 2.0 * U21;
+    Bm[2] = r_weno_1 * (t5 * t5) + r_weno_2 * (t6 * t6);
+}
+
+static void lrn_omega(const double *B, double *om) {
+    const double tau5 = std::fabs(B[0] - B[2]);
+    const double q1 = tau5 / (smallpara + B[0]), q2 = tau5 / (smallpara + B[1]), q3 = tau5 / (smallpara + B[2]);
+    const double w1 = g_weno_1 * (1.0 + q1 * q1), w2 = g_weno_2 * (1.0 + q2 * q2), w3 = g_weno_3 * (1.0 + q3 * q3);
+    const double sum = w1 + w2 + w3;
+    om[0] = w1 / sum;
+    om[1] = w2 / sum;
+    om[2] = w3 / sum;
+}
+
+/* one sample: st = 7 stencils of 5 values (rho, v, p, the two transverse
+ * cell fields), w = the cell's 10 WENO weights; row = 35 features, the
+ * relative face-value change of the linear weights, the largest
+ * nonlinear-weight deviation */
+void orc_learn_sample(const double *st, const double *w, float *row) {
+    const double g[3] = {g_weno_1, g_weno_2, g_weno_3};
+    double change = 0.0, wdev = 0.0;
+    for (int v = 0; v < 7; ++v) {
+        const double *s5 = st + 5 * v;
+        float f4[4], rv;
+        lrn_var_features((float)s5[0], (float)s5[1], (float)s5[2], (float)s5[3], (float)s5[4], f4, &rv);
+        for (int i = 0; i < 4; ++i) row[4 * v + i] = f4[i];
+        row[28 + v] = rv;
+        double Pp[3], Bp[3], Pm[3], Bm[3], om[3];
+        lrn_parts(w, s5[0], s5[1], s5[2], s5[3], s5[4], Pp, Bp, Pm, Bm);
+        lrn_omega(Bp, om);
+        const double vp_z = om[0] * Pp[0] + om[1] * Pp[1] + om[2] * Pp[2];
+        for (int q = 0; q < 3; ++q) wdev = std::fmax(wdev, std::fabs(om[q] - g[q]));
+        lrn_omega(Bm, om);
+        const double vm_z = om[0] * Pm[0] + om[1] * Pm[1] + om[2] * Pm[2];
+        for (int q = 0; q < 3; ++q) wdev = std::fmax(wdev, std::fabs(om[q] - g[q]));
+        const double vp_l = g[0] * Pp[0] + g[1] * Pp[1] + g[2] * Pp[2];
+        const double vm_l = g[0] * Pm[0] + g[1] * Pm[1] + g[2] * Pm[2];
+        const double den = std::fabs(s5[2]) + 1.0e-300;
+        change = std::fmax(change, std::fmax(std::fabs(vp_l - vp_z), std::fabs(vm_l - vm_z)) / den);
+    }
+    row[35] = (float)change;
+    row[36] = (float)wdev;
+}
+
+/* the flag network in FP64: parameters as the C-ABI (W1[32][48], b1,
+ * W2[32][32], b2, w3, b3), samples of 37 floats, label change < delta.
+ * Returns the mean binary cross-entropy; grad = its gradient. */
+enum { L_H = 32, L_K = 48, L_NF = 35, L_ROW = 37, L_W1 = 0, L_B1 = 1536, L_W2 = 1568, L_B2 = 2592, L_W3 = 2624,
+       L_B3 = 2656, L_NP = 2657 };
+static double lrn_forward(const float *P, const float *x, double *h1, double *h2) {
+    for (int o = 0; o < L_H; ++o) {
+        double a = P[L_B1 + o];
+        for (int i = 0; i < L_NF; ++i) a += (double)P[L_W1 + o * L_K + i] * (double)x[i];
+        h1[o] = a > 0.0 ? a : 0.0;
+    }
+    for (int o = 0; o < L_H; ++o) {
+        double a = P[L_B2 + o];
+        for (int i = 0; i < L_H; ++i) a += (double)P[L_W2 + o * L_H + i] * h1[i];
+        h2[o] = a > 0.0 ? a : 0.0;
+    }
+    double z = P[L_B3];
+    for (int i = 0; i < L_H; ++i) z += (double)P[L_W3 + i] * h2[i];
+    return z;
+}
+
+void orc_mlp_forward(const float *P, const float *X, int ld, long long n, double *z) {
+    double h1[L_H], h2[L_H];
+    for (long long s = 0; s < n; ++s) z[s] = lrn_forward(P, X + s * ld, h1, h2);
+}
+
+double orc_mlp_loss_grad(const float *P, const float *X, long long n, float delta, double *grad) {
+    for (int p = 0; p < L_NP; ++p) grad[p] = 0.0;
+    double loss = 0.0;
+    double h1[L_H], h2[L_H], g1[L_H], g2[L_H];
+    for (long long s = 0; s < n; ++s) {
+        const float *x = X + s * L_ROW;
+        const double y = x[L_NF] < delta ? 1.0 : 0.0;
+        const double z = lrn_forward(P, x, h1, h2);
+        loss += std::fmax(z, 0.0) - y * z + std::log1p(std::exp(-std::fabs(z)));
+        const double dz = 1.0 / (1.0 + std::exp(-z)) - y;
+        for (int i = 0; i < L_H; ++i) g2[i] = h2[i] > 0.0 ? dz * (double)P[L_W3 + i] : 0.0;
+        for (int i = 0; i < L_H; ++i) {
+            double a = 0.0;
+            for (int o = 0; o < L_H; ++o) a += (double)P[L_W2 + o * L_H + i] * g2[o];
+            g1[i] = h1[i] > 0.0 ? a : 0.0;
+        }
+        for (int o = 0; o < L_H; ++o) {
+            for (int i = 0; i < L_NF; ++i) grad[L_W1 + o * L_K + i] += g1[o] * (double)x[i];
+            grad[L_B1 + o] += g1[o];
+            for (int i = 0; i < L_H; ++i) grad[L_W2 + o * L_H + i] += g2[o] * h1[i];
+            grad[L_B2 + o] += g2[o];
+            grad[L_W3 + o] += dz * h2[o];
+        }
+        grad[L_B3] += dz;
+    }
+    for (int p = 0; p < L_NP; ++p) grad[p] /= (double)n;
+    return loss / (double)n;
+}
+
 void orc_reset_counts(void) { g_ops = OpCounts(); }
 void orc_get_counts(uint64_t *out5) {
     out5[0] = g_ops.add; out5[1] = g_ops.mul; out5[2] = g_ops.div; out5[3] = g_ops.sqrt; out5[4] = g_ops.cmp;

@@ -60,6 +60,10 @@ def lib():
         L.orc_recon_cell.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_weights.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         L.orc_riemann_face.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_learn_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p]
+        L.orc_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p]
+        L.orc_mlp_loss_grad.restype = C.c_double
         _lib = L
     return _lib
 
@@ -161,3 +165,63 @@ def riemann_face(dir_, rs, gamma, pl, pr):
     fp = np.zeros(8)
     lib().orc_riemann_face(dir_, rs, gamma, pl.ctypes.data, pr.ctypes.data, fo.ctypes.data, fp.ctypes.data)
     return fo, fp
+
+
+# ---------------------------------------------------------------------------
+# learned smooth-face flag: the checker of the GPU harvest, trainer, inference
+# ---------------------------------------------------------------------------
+LEARN_NP, LEARN_NF, LEARN_ROW = 2657, 35, 37
+
+
+def learn_sample(stencils, w10):
+    """stencils (7, 5) FP64, w10 the cell's WENO weights -> 37-float sample row."""
+    st = np.ascontiguousarray(stencils, dtype=np.float64)
+    w = np.ascontiguousarray(w10, dtype=np.float64)
+    row = np.zeros(LEARN_ROW, dtype=np.float32)
+    lib().orc_learn_sample(st.ctypes.data, w.ctypes.data, row.ctypes.data)
+    return row
+
+
+def mlp_forward(params, X):
+    """FP64 forward pass of the flag network on rows of features."""
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    z = np.zeros(X.shape[0])
+    lib().orc_mlp_forward(P.ctypes.data, X.ctypes.data, X.shape[1], X.shape[0], z.ctypes.data)
+    return z
+
+
+def mlp_loss_grad(params, samples, delta):
+    """FP64 mean binary cross-entropy of "change < delta" and its gradient."""
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    S = np.ascontiguousarray(samples, dtype=np.float32)
+    assert S.shape[1] == LEARN_ROW
+    g = np.zeros(LEARN_NP)
+    loss = lib().orc_mlp_loss_grad(P.ctypes.data, S.ctypes.data, S.shape[0], delta, g.ctypes.data)
+    return loss, g
+
+
+def _bf16(a):
+    """Round FP32 values to BF16 (nearest even), returned as FP32."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def mlp_forward_bf16(params, X):
+    """The tensor-core inference emulated: BF16 features, W1, hidden layer and
+    W2, FP32 accumulation (in FP64 here), FP32 output layer."""
+    P = np.asarray(params, dtype=np.float32)
+    W1 = _bf16(P[0:1536]).reshape(32, 48).astype(np.float64)
+    b1 = P[1536:1568].astype(np.float64)
+    W2 = _bf16(P[1568:2592]).reshape(32, 32).astype(np.float64)
+    b2 = P[2592:2624].astype(np.float64)
+    w3 = P[2624:2656].astype(np.float64)
+    b3 = float(P[2656])
+    x = np.zeros((X.shape[0], 48), dtype=np.float32)
+    x[:, :LEARN_NF] = X[:, :LEARN_NF]
+    h1 = np.maximum(_bf16(x).astype(np.float64) @ W1.T + b1, 0.0)
+    h1 = _bf16(h1.astype(np.float32)).astype(np.float64)
+    h2 = np.maximum(h1 @ W2.T + b2, 0.0)
+    return h2 @ w3 + b3
