@@ -324,13 +324,15 @@ def reference_batch(args, world):
     return 0
 
 
-def _evolve_timed(engine, torch, spec, prim, eps, warmup, steps=None, t_end=None, tuning="auto"):
+def _evolve_timed(engine, torch, spec, prim, eps, warmup, steps=None, t_end=None, tuning="auto", setup=None):
     """Run one handle: W warm-up steps, then time the rest (to t_end, or K
     more steps) with CUDA events on the engine stream.  Returns the handle
     (still open), timed steps and milliseconds."""
     s = engine.Solver(spec)
     s.set_state(prim, eps)
     s.initial_update()
+    if setup is not None:
+        setup(s)
     if tuning == "auto":
         s.autotune()
     te = t_end if t_end is not None else 1e30
@@ -374,12 +376,20 @@ def bench_config(args, world, rank, local, dist):
         spec, prim, eps = models.alfven_3d(n3, recon=recon, riemann=args.riemann)
         zones = n3 ** 3
         out = {}
+        forms = [("fp64", dict(spec, precision="fp64"), None), ("fp32", dict(spec, precision="fp32"), None)]
+        lp = args.learned_params
+        if recon == "weno" and lp and os.path.exists(lp):
+            P = np.load(lp)
+
+            def setup(s, P=P):
+                s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5)
+            forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
         clocks.start()
-        for prec in ("fp64", "fp32"):
-            sp = dict(spec, precision=prec)
-            s, k, t_ms = _evolve_timed(engine, torch, sp, prim, eps, args.warmup, t_end=spec["t_end"])
-            out[prec] = dict(cons=s.get_array(capi.ARR_CONS), divb=s.find_divb(), steps=k, ms=t_ms,
-                             t=s.time)
+        for name_f, sp, setup in forms:
+            s, k, t_ms = _evolve_timed(engine, torch, sp, prim, eps, args.warmup, t_end=spec["t_end"], setup=setup)
+            out[name_f] = dict(cons=s.get_array(capi.ARR_CONS), divb=s.find_divb(), steps=k, ms=t_ms, t=s.time)
+            if setup is not None:
+                out[name_f]["stats"] = s.learn_stats()
             s.close()
         clk = clocks.stop()
         # the exact solution after one period is the initial state
@@ -404,6 +414,20 @@ def bench_config(args, world, rank, local, dist):
             "period": spec["t_end"], "time_reached": {p: out[p]["t"] for p in out},
         })
         extra["fp32_over_fp64"] = extra["fp32_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
+        if "fp32+learned" in out:
+            o = out["fp32+learned"]
+            l1_l = rel_l1(o["cons"], out["fp64"]["cons"])
+            st = o["stats"]
+            extra.update({
+                "l1_learned_vs_fp64_per_var": l1_l, "l1_learned_vs_fp64_max": max(l1_l),
+                "l1_learned_vs_exact_per_var": rel_l1(o["cons"], c0),
+                "learned_zone_updates_per_s": zones * o["steps"] / (o["ms"] * 1e-3),
+                "learned_flagged_fraction_at_audits": st["flagged"] / max(1, st["audited"]),
+                "learned_fallback_tiles": st["fallback_tiles"], "learned_audits": st["audits"],
+                "learned_params": os.path.relpath(lp, ROOT),
+            })
+            extra["learned_over_fp64"] = extra["learned_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
+            extra["max_divb"]["fp32+learned"] = o["divb"]
         key = args.precision
         n, ms = out[key]["steps"], out[key]["ms"]
         name = "alfven3d_%d^3_%s_%s_cfl0.4_one_period" % (n3, recon, args.riemann)
@@ -443,6 +467,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blast3d", choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus"])
     ap.add_argument("--recon-c", default=None, help="reconstruction of the briowu/alfven3d/torus workloads")
+    ap.add_argument("--learned-params", default=os.path.join(ROOT, "cumc3d_b200", "data", "flag_mlp.npy"),
+                    help="trained flag network for the FP32+learned form of the alfven3d workload")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--recon", default="weno")
     ap.add_argument("--riemann", default="hlld")

@@ -855,10 +855,10 @@ static void default_flux_blocks(cumc_handle *h) {
     h->fblk[2] = dim3(32, 8, 1);
 }
 
-static void launch_flux(cumc_handle *h, int dir) {
+static void launch_flux(cumc_handle *h, int dir, int stage = 1) {
     const Dev &d = h->d;
     if (d.learned) {  // FP32 WENO with the learned smooth-face flag (split kernels)
-        launch_split_learned_fp32(d, dir, h->cfg.riemann, h->stream);
+        launch_split_learned_fp32(d, dir, h->cfg.riemann, stage, h->stream);
         h->launches += 2;
         return;
     }
@@ -967,7 +967,7 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     const Dev &d = h->d;
     for (int dir = 0; dir < d.n_dim; ++dir) {
         prof_begin(h);
-        launch_flux(h, dir);
+        launch_flux(h, dir, stage);
         prof_end(h, PC_FLUX_X + dir);
     }
     dim3 g, b;
@@ -1206,7 +1206,10 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
             return p;
         };
         d.mlp = B(sizeof(MlpPacked));
-        for (int a = 0; a < 3; ++a) d.lfb[a] = (unsigned char *)B((size_t)learned_tiles(d, a) + 1);
+        for (int a = 0; a < 3; ++a) {
+            d.lfb[a] = (unsigned char *)B((size_t)learned_tiles(d, a) + 1);
+            d.lflag[a] = (unsigned char *)B((size_t)learned_tiles(d, a) * 128);
+        }
         d.lstats = (unsigned long long *)B(sizeof(unsigned long long) * LEARN_STAT_SLOTS * LEARN_STAT_FIELDS);
         d.learned = 0;
     }

@@ -71,6 +71,7 @@ struct Dev {
     float audit_tol;             // relative face-value error a tile may show
     const void *mlp;             // MlpPacked parameters
     unsigned char *lfb[3];       // per direction, per 128-cell tile: 1 = fall back to WENO-Z
+    unsigned char *lflag[3];     // per direction, per reconstructed cell: the stage-1 flag
     unsigned long long *lstats;  // audit counters (LEARN_STAT_SLOTS x LEARN_STAT_FIELDS)
 };
 
@@ -83,7 +84,7 @@ void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 bl
 void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
 void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
 void launch_split_fp32(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
-void launch_split_learned_fp32(const Dev &d, int dir, int rs, cudaStream_t s);
+void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStream_t s);
 long long learned_tiles(const Dev &d, int dir);
 
 }  // namespace cumc

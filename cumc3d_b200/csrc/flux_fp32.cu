@@ -19,19 +19,24 @@ long long learned_tiles(const Dev &d, int dir) {
 }
 
 template <int DIR>
-static void launch_learned_dir(const Dev &d, int rs, cudaStream_t s) {
+static void launch_learned_dir(const Dev &d, int rs, int stage, cudaStream_t s) {
     const unsigned tiles = (unsigned)learned_tiles(d, DIR);
-    if (d.wuni[DIR]) k_recon_learned<DIR, 1><<<tiles, 128, 0, s>>>(d);
-    else k_recon_learned<DIR, 0><<<tiles, 128, 0, s>>>(d);
+    if (stage == 1) {  // the network runs once per step and direction
+        if (d.wuni[DIR]) k_recon_learned<DIR, 1><<<tiles, 128, 0, s>>>(d);
+        else k_recon_learned<DIR, 0><<<tiles, 128, 0, s>>>(d);
+    } else {
+        if (d.wuni[DIR]) k_recon_flagged<DIR, 1><<<(tiles + 1) / 2, 256, 0, s>>>(d);
+        else k_recon_flagged<DIR, 0><<<(tiles + 1) / 2, 256, 0, s>>>(d);
+    }
     dim3 g, b;
     split_dims(d, DIR, false, g, b);
     if (d.riemann_minb == 4) launch_riemann_m<float, DIR, 4>(d, rs, g, b, s);
     else launch_riemann_m<float, DIR, 1>(d, rs, g, b, s);
 }
 
-void launch_split_learned_fp32(const Dev &d, int dir, int rs, cudaStream_t s) {
-    if (dir == 0) launch_learned_dir<0>(d, rs, s);
-    else if (dir == 1) launch_learned_dir<1>(d, rs, s);
-    else launch_learned_dir<2>(d, rs, s);
+void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStream_t s) {
+    if (dir == 0) launch_learned_dir<0>(d, rs, stage, s);
+    else if (dir == 1) launch_learned_dir<1>(d, rs, stage, s);
+    else launch_learned_dir<2>(d, rs, stage, s);
 }
 }  // namespace cumc

@@ -1,11 +1,12 @@
 // recon_learned.cuh -- FP32 WENO reconstruction with the learned smooth-face
-// flag fused in (see learned.cuh).  Same cells, same enumeration and the same
-// outputs (QL/QR face states) as k_recon<float, DIR, REC_WENO, UNI>.
+// flag (see learned.cuh).  Same cells, same enumeration and the same outputs
+// (QL/QR face states) as k_recon<float, DIR, REC_WENO, UNI>.
 //
-// One CTA = 128 consecutive cells of the flat enumeration = one tile:
+// Stage 1 of each RK step, k_recon_learned (one CTA = 128 consecutive cells
+// of the flat enumeration = one tile):
 //   1. each thread loads its cell's 7 stencils and builds the 35 features;
 //   2. the MLP (tcgen05, BF16 operands, FP32 accumulators in TMEM) gives one
-//      logit per cell;
+//      logit per cell; the flag (logit > threshold) is stored per cell;
 //   3. a warp whose 32 cells are all flagged, in a tile not marked to fall
 //      back, reconstructs with the linear optimal weights; every other warp
 //      runs WENO-Z exactly as k_recon does;
@@ -13,11 +14,120 @@
 //      the plain FP32 form), flagged cells also evaluate the linear values,
 //      and the tile is marked to fall back until the next audit if any
 //      flagged cell's relative face-value error exceeds audit_tol.
+// Stages 2 and 3, k_recon_flagged: the stage-1 flags of the cell and of its
+// two neighbours along the sweep (the state moves less than a cell per step)
+// choose linear or WENO-Z per warp, without running the network again.
+//
+// Cells next to the domain boundary along the sweep (c <= 1 or c >= n) always
+// use WENO-Z: on a periodic axis face 0 and face n are one face, and their
+// fluxes (hence the edge EMFs of constrained transport) must come out bit for
+// bit equal from the identical stencils of cells 0/n and 1/n+1.
 #pragma once
 #include "flux_kernel.cuh"
 #include "learned.cuh"
 
 namespace cumc {
+
+struct LearnedCell {
+    int c, ns, st, ci;
+    long long t;
+    bool valid;
+};
+
+template <int DIR>
+__device__ __forceinline__ LearnedCell learned_cell(const Dev &d, long long t0, long long total) {
+    LearnedCell q;
+    q.valid = t0 < total;
+    q.t = q.valid ? t0 : total - 1;  // rows past the end load a real cell, store nothing
+    const int ex = (DIR == 0) ? d.nx + 2 : d.nx;
+    const int ey = (DIR == 1) ? d.ny + 2 : d.ny;
+    int j, k, l;
+    const int a = (int)(q.t % ex);
+    const long long r = q.t / ex;
+    const int b = (int)(r % ey);
+    const int e = (int)(r / ey);
+    if (DIR == 0) { q.c = a; j = q.c; k = b + 1; l = e + 1; q.ns = d.nx; }
+    else if (DIR == 1) { q.c = b; q.ns = d.ny; k = q.c; j = a + 1; l = e + 1; }
+    else { q.c = e; q.ns = d.nz; l = q.c; j = a + 1; k = b + 1; }
+    q.st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
+    q.ci = cidx(d, j, k, l);
+    return q;
+}
+
+template <int DIR, int UNI>
+__device__ __forceinline__ void learned_weights(const Dev &d, int c, float *w) {
+    if (UNI) {
+#pragma unroll
+        for (int m = 0; m < 10; ++m) w[m] = uni_w<float>(d, DIR, m);
+    } else {
+        const float *wp = weights<float>(d, DIR) + (size_t)(c + 2) * 14;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) w[m] = wp[m];
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ void learned_stencils(const Dev &d, const LearnedCell &q, float a[LEARN_NV][5]) {
+    constexpr int tb1 = (DIR == 0) ? 1 : 0;
+    constexpr int tb2 = (DIR == 2) ? 1 : 2;
+#pragma unroll
+    for (int v = 0; v < LEARN_NV; ++v) {
+        const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) a[v][m] = (float)__ldg(src + q.ci + (m - 2) * q.st);
+    }
+}
+
+// the 7 reconstructions of one cell and its stores (as k_recon); with audit,
+// also the largest relative change the linear weights would make
+__device__ __forceinline__ void learned_reconstruct(const Dev &d, const LearnedCell &q, const float *w,
+                                                    float a[LEARN_NV][5], bool linear, bool audit_cell,
+                                                    float &err) {
+    float *const *QL = reinterpret_cast<float *const *>(d.QL);
+    float *const *QR = reinterpret_cast<float *const *>(d.QR);
+    float vm_rho = 0.0f, vp_rho = 0.0f;
+    bool fallback = false;
+#pragma unroll
+    for (int v = 0; v < LEARN_NV; ++v) {
+        float vm, vp;
+        if (linear) {
+            weno_linear<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], vm, vp);
+        } else {
+            weno<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], vm, vp);
+            if (audit_cell) {
+                float lm, lp;
+                weno_linear<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], lm, lp);
+                const float den = fabsf(a[v][2]) + 1.0e-30f;
+                err = fmaxf(err, fmaxf(fabsf(lm - vm), fabsf(lp - vp)) / den);
+            }
+        }
+        if (v == 0) { vm_rho = vm; vp_rho = vp; }
+        if (v == 4 && d.pos_fallback) {
+            fallback = !(vm_rho > 0.0f && vp_rho > 0.0f && vm > 0.0f && vp > 0.0f);
+            if (fallback && q.valid) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float cv = (float)__ldg(d.P[u] + q.ci);
+                    if (q.c <= q.ns) QL[u][q.ci] = cv;
+                    if (q.c >= 1) QR[u][q.ci - q.st] = cv;
+                }
+            }
+        }
+        if (fallback) vm = vp = a[v][2];
+        if (q.valid) {
+            if (q.c <= q.ns) QL[v][q.ci] = vp;
+            if (q.c >= 1) QR[v][q.ci - q.st] = vm;
+        }
+    }
+}
+
+template <int DIR>
+__device__ __forceinline__ long long learned_total(const Dev &d) {
+    const long long ex = (DIR == 0) ? d.nx + 2 : d.nx;
+    const long long ey = (DIR == 1) ? d.ny + 2 : d.ny;
+    const long long ez = (DIR == 2) ? d.nz + 2 : d.nz;
+    return ex * ey * ez;
+}
 
 template <int DIR, int UNI>
 __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d) {
@@ -27,44 +137,12 @@ __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d) {
     __shared__ int s_flag[4];
     const int tid = threadIdx.x;
     mlp_tile_setup(tile, reinterpret_cast<const MlpPacked *>(d.mlp));
-
-    const int ex = (DIR == 0) ? d.nx + 2 : d.nx;
-    const int ey = (DIR == 1) ? d.ny + 2 : d.ny;
-    const int ez = (DIR == 2) ? d.nz + 2 : d.nz;
-    const long long total = (long long)ex * ey * ez;
-    const long long t0 = (long long)blockIdx.x * 128 + tid;
-    const bool valid = t0 < total;
-    const long long t = valid ? t0 : total - 1;  // rows past the end load a real cell, store nothing
-    int c, j, k, l, ns;
-    {
-        const int a = (int)(t % ex);
-        const long long r = t / ex;
-        const int b = (int)(r % ey);
-        const int e = (int)(r / ey);
-        if (DIR == 0) { c = a; j = c; k = b + 1; l = e + 1; ns = d.nx; }
-        else if (DIR == 1) { c = b; k = c; j = a + 1; l = e + 1; ns = d.ny; }
-        else { c = e; l = c; j = a + 1; k = b + 1; ns = d.nz; }
-    }
-    const int st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
-    const int ci = cidx(d, j, k, l);
-    constexpr int tb1 = (DIR == 0) ? 1 : 0;
-    constexpr int tb2 = (DIR == 2) ? 1 : 2;
+    const long long total = learned_total<DIR>(d);
+    const LearnedCell q = learned_cell<DIR>(d, (long long)blockIdx.x * 128 + tid, total);
     float w[14];
-    if (UNI) {
-#pragma unroll
-        for (int m = 0; m < 10; ++m) w[m] = uni_w<float>(d, DIR, m);
-    } else {
-        const float *wp = weights<float>(d, DIR) + (size_t)(c + 2) * 14;
-#pragma unroll
-        for (int m = 0; m < 10; ++m) w[m] = wp[m];
-    }
+    learned_weights<DIR, UNI>(d, q.c, w);
     float a[LEARN_NV][5];
-#pragma unroll
-    for (int v = 0; v < LEARN_NV; ++v) {
-        const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) a[v][m] = (float)__ldg(src + ci + (m - 2) * st);
-    }
+    learned_stencils<DIR>(d, q, a);
     float logit = -1.0e30f;
     {
         float x[LEARN_K];
@@ -84,51 +162,17 @@ __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d) {
         }
     }
     const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
-    const bool flag = valid && logit > d.learn_thr;
-    const bool warp_all = __all_sync(0xffffffffu, flag);
+    const bool flag = q.valid && logit > d.learn_thr;
+    if (q.valid) d.lflag[DIR][q.t] = flag ? 1 : 0;
+    const bool inner = q.c >= 2 && q.c <= q.ns - 1;
+    const bool warp_all = __all_sync(0xffffffffu, flag && inner);
     const bool linear = warp_all && !audit && d.lfb[DIR][blockIdx.x] == 0;
-
-    float *const *QL = reinterpret_cast<float *const *>(d.QL);
-    float *const *QR = reinterpret_cast<float *const *>(d.QR);
-    float vm_rho = 0.0f, vp_rho = 0.0f;
-    bool fallback = false;
     float err = 0.0f;
-#pragma unroll
-    for (int v = 0; v < LEARN_NV; ++v) {
-        float vm, vp;
-        if (linear) {
-            weno_linear<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], vm, vp);
-        } else {
-            weno<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], vm, vp);
-            if (audit && flag) {
-                float lm, lp;
-                weno_linear<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], lm, lp);
-                const float den = fabsf(a[v][2]) + 1.0e-30f;
-                err = fmaxf(err, fmaxf(fabsf(lm - vm), fabsf(lp - vp)) / den);
-            }
-        }
-        if (v == 0) { vm_rho = vm; vp_rho = vp; }
-        if (v == 4 && d.pos_fallback) {
-            fallback = !(vm_rho > 0.0f && vp_rho > 0.0f && vm > 0.0f && vp > 0.0f);
-            if (fallback && valid) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const float cv = (float)__ldg(d.P[u] + ci);
-                    if (c <= ns) QL[u][ci] = cv;
-                    if (c >= 1) QR[u][ci - st] = cv;
-                }
-            }
-        }
-        if (fallback) vm = vp = a[v][2];
-        if (valid) {
-            if (c <= ns) QL[v][ci] = vp;
-            if (c >= 1) QR[v][ci - st] = vm;
-        }
-    }
+    learned_reconstruct(d, q, w, a, linear, audit && flag && inner, err);
     if (audit) {
         // tile verdict: the largest error of a flagged cell against the tolerance
         float e = err;
-        int nf = flag ? 1 : 0;
+        int nf = (flag && inner) ? 1 : 0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
@@ -154,6 +198,31 @@ __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d) {
         }
     }
     mlp_tile_teardown(tile);
+}
+
+// stages 2 and 3: the stage-1 flags, dilated by one cell along the sweep
+template <int DIR, int UNI>
+__global__ void __launch_bounds__(256) k_recon_flagged(const Dev d) {
+    if (d.S->done) return;
+    const long long total = learned_total<DIR>(d);
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((t0 & ~31ll) >= total) return;  // whole warps past the end
+    const LearnedCell q = learned_cell<DIR>(d, t0, total);
+    const long long sweep = (DIR == 0) ? 1 : (DIR == 1) ? (long long)d.nx : (long long)d.nx * d.ny;
+    const bool inner = q.c >= 2 && q.c <= q.ns - 1;
+    const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
+    bool ok = false;
+    if (q.valid && inner && !audit) {
+        const unsigned char *f = d.lflag[DIR];
+        ok = f[q.t] && f[q.t - sweep] && f[q.t + sweep] && d.lfb[DIR][q.t >> 7] == 0;
+    }
+    const bool linear = __all_sync(0xffffffffu, ok);
+    float w[14];
+    learned_weights<DIR, UNI>(d, q.c, w);
+    float a[LEARN_NV][5];
+    learned_stencils<DIR>(d, q, a);
+    float err = 0.0f;
+    learned_reconstruct(d, q, w, a, linear, false, err);
 }
 
 }  // namespace cumc

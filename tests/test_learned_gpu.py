@@ -140,7 +140,8 @@ def test_audit_every_step_reproduces_plain_fp32_and_no_audit_does_not():
     plain, _ = fp32_run(spec, prim, eps, 6)
     audited, st = fp32_run(spec, prim, eps, 6, dict(params=flag_all_params(), threshold=0.0, audit_interval=1,
                                                       audit_tol=0.0))
-    assert st["audits"] >= 6 and st["flagged"] == st["audited"]
+    # every cell but the two next to each end of a sweep is flagged
+    assert st["audits"] >= 6 and st["flagged"] > 0.8 * st["audited"]
     assert np.array_equal(interior(plain, spec), interior(audited, spec))
     linear, st2 = fp32_run(spec, prim, eps, 6, dict(params=flag_all_params(), threshold=0.0, audit_interval=0,
                                                       audit_tol=0.0))
@@ -175,3 +176,24 @@ def test_trained_flag_separates_smooth_from_shocked_cells():
     # clearly non-smooth cells (change > 100 delta) are almost never flagged
     rough = held[:, 35] > 100 * DELTA
     assert rough.sum() > 100 and (z[rough] > 0).mean() < 0.02
+
+
+def test_trained_flag_keeps_div_b_at_roundoff_on_a_periodic_box():
+    """Face 0 and face n of a periodic axis are one face: the cells next to
+    the ends of a sweep always use WENO-Z so both copies get the same flux
+    and constrained transport keeps div B at roundoff."""
+    import os
+    P = np.load(os.path.join(os.path.dirname(engine.__file__), "data", "flag_mlp.npy"))
+    spec, prim, eps = models.alfven_3d(48, recon="weno")
+    sp = dict(spec, precision="fp32", learned=1)
+    s = engine.Solver(sp)
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5)
+    s.evolve(1e30, 30)
+    divb = s.find_divb()
+    st = s.learn_stats()
+    s.close()
+    assert st["flagged"] > 0
+    # |B| ~ 1, dx = 1/48: roundoff level is ~1e-13
+    assert divb < 1e-11, divb
