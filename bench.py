@@ -382,7 +382,7 @@ def bench_config(args, world, rank, local, dist):
             P = np.load(lp)
 
             def setup(s, P=P):
-                s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5)
+                s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5, flag_interval=4)
             forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
         clocks.start()
         for name_f, sp, setup in forms:
@@ -477,7 +477,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--tuning", default="auto",
-                    help="'auto' (the engine's autotuner) or split,tpb_recon,tpb_riemann,min_blocks "
+                    help="'auto' (the engine's autotuner) or split,tpb_recon,tpb_riemann,min_blocks[,recon_tile] "
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.steps is None:
@@ -512,9 +512,11 @@ def main():
     if args.tuning == "auto":
         tuning = s.autotune()
     else:
-        sp, tr, tm, mb = (int(v) for v in args.tuning.split(","))
-        s.set_tuning(bool(sp), tr, tm, mb)
-        tuning = dict(split=bool(sp), tpb_recon=tr, tpb_riemann=tm, riemann_min_blocks=mb, pinned=True)
+        vals = [int(v) for v in args.tuning.split(",")] + [0]
+        sp, tr, tm, mb, rt = vals[:5]
+        s.set_tuning(bool(sp), tr, tm, mb, rt)
+        tuning = dict(split=bool(sp), tpb_recon=tr, tpb_riemann=tm, riemann_min_blocks=mb, recon_tile=rt,
+                      pinned=True)
     s.evolve(1e30, args.warmup)
     s.sync()
     stream = torch.cuda.ExternalStream(s.stream())
@@ -585,7 +587,8 @@ def main():
         if args.tuning == "auto":
             s2.autotune()
         else:
-            s2.set_tuning(tuning["split"], tuning["tpb_recon"], tuning["tpb_riemann"], tuning["riemann_min_blocks"])
+            s2.set_tuning(tuning["split"], tuning["tpb_recon"], tuning["tpb_riemann"], tuning["riemann_min_blocks"],
+                          tuning["recon_tile"])
         if dist:
             dist.barrier()
         torch.cuda.synchronize()

@@ -1212,6 +1212,11 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
         }
         d.lstats = (unsigned long long *)B(sizeof(unsigned long long) * LEARN_STAT_SLOTS * LEARN_STAT_FIELDS);
         d.learned = 0;
+        d.flag_interval = 1;
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        d.num_sms = nsm;
     }
     if (!ok) {
         g_create_err = "device allocation failed";
@@ -1445,10 +1450,11 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out) {
 int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
     if (!h) return fail(h, CUMC_EINVAL, "null handle");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
-    struct Cand { int mode, tpb_recon, tpb_riemann, minb; };
+    struct Cand { int mode, tpb_recon, tpb_riemann, minb, tile; };
     static const Cand cands[] = {
-        {1, 256, 128, 1}, {1, 256, 128, 4}, {1, 128, 128, 1}, {1, 128, 128, 4},
-        {1, 256, 64, 1}, {1, 128, 64, 4}, {0, 256, 128, 1},
+        {1, 256, 128, 1, 0}, {1, 256, 128, 4, 0}, {1, 128, 128, 1, 0}, {1, 128, 128, 4, 0},
+        {1, 256, 64, 1, 0},  {1, 128, 64, 4, 0},  {0, 256, 128, 1, 0},
+        {1, 256, 128, 1, 1}, {1, 256, 128, 4, 1}, {1, 256, 128, 1, 2}, {1, 256, 128, 4, 2},
     };
     const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
     double best = 1e300;
@@ -1461,6 +1467,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
         h->d.tpb_recon = cands[i].tpb_recon;
         h->d.tpb_riemann = cands[i].tpb_riemann;
         h->d.riemann_minb = cands[i].minb;
+        h->d.recon_tile = cands[i].tile;
         for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir);  // warm-up
         CK(cudaEventRecord(a, h->stream));
         const int reps = 3;
@@ -1479,12 +1486,14 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
     h->d.tpb_recon = cands[bi].tpb_recon;
     h->d.tpb_riemann = cands[bi].tpb_riemann;
     h->d.riemann_minb = cands[bi].minb;
+    h->d.recon_tile = cands[bi].tile;
     // a captured step holds the old launch shapes
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
     if (choice_out) {
         choice_out[0] = cands[bi].mode; choice_out[1] = cands[bi].tpb_recon;
         choice_out[2] = cands[bi].tpb_riemann; choice_out[3] = cands[bi].minb;
+        choice_out[4] = cands[bi].tile;
     }
     if (best_ms_out) *best_ms_out = best;
     return CUMC_OK;
@@ -1493,8 +1502,10 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
 int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
     if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 256 || (choice[1] & 31) ||
-        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4))
+        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4) ||
+        choice[4] < 0 || choice[4] > 2)
         return fail(h, CUMC_EINVAL, "tuning out of range");
+    h->d.recon_tile = choice[4];
     h->flux_mode = choice[0];
     h->d.tpb_recon = choice[1];
     h->d.tpb_riemann = choice[2];
@@ -1504,10 +1515,12 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     return CUMC_OK;
 }
 
-int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int audit_interval, float audit_tol) {
+int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int flag_interval, int audit_interval,
+                   float audit_tol) {
     if (!h) return fail(h, CUMC_EINVAL, "null handle");
     if (!h->cfg.learned || !h->d.mlp) return fail(h, CUMC_EINVAL, "handle was created without the learned flag");
-    if (audit_interval < 0 || !(audit_tol >= 0.0f)) return fail(h, CUMC_EINVAL, "bad audit settings");
+    if (audit_interval < 0 || !(audit_tol >= 0.0f) || flag_interval < 1)
+        return fail(h, CUMC_EINVAL, "bad flag or audit interval");
     Dev &d = h->d;
     if (params) {
         for (int i = 0; i < LEARN_NP; ++i)
@@ -1521,6 +1534,7 @@ int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int aud
     CK(cudaStreamSynchronize(h->stream));
     d.learned = params ? 1 : 0;
     d.learn_thr = threshold;
+    d.flag_interval = flag_interval;
     d.audit_interval = audit_interval;
     d.audit_tol = audit_tol;
     // the captured step holds the kernel arguments: capture again

@@ -37,6 +37,7 @@ struct Dev {
     int pos_fallback;       // first-order fallback for non-positive edge rho/p
     int tpb_recon, tpb_riemann;  // threads per block of the split flux kernels (autotuned)
     int riemann_minb;            // blocks/SM the Riemann kernel is compiled for (1 or 4; autotuned)
+    int recon_tile;              // 0: per-cell stencil loads; 1, 2: staged tiles, cells per thread (autotuned)
     int wuni[3];                 // 1: the axis's reconstruction weights are identical in every cell
     double wu[3][14];            // those weights (FP64 form)
     float wuf[3][14];            // and in FP32
@@ -67,6 +68,8 @@ struct Dev {
     // learned smooth-face flag of the FP32 WENO form (learned.cuh)
     int learned;                 // 1: the learned reconstruction kernel replaces k_recon
     float learn_thr;             // logit above which a cell is flagged smooth
+    int flag_interval;           // the network runs every this many steps (stage 1)
+    int num_sms;                 // persistent grids
     int audit_interval;          // full-WENO audit every this many steps (0: never)
     float audit_tol;             // relative face-value error a tile may show
     const void *mlp;             // MlpPacked parameters

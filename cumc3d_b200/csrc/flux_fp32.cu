@@ -21,13 +21,15 @@ long long learned_tiles(const Dev &d, int dir) {
 template <int DIR>
 static void launch_learned_dir(const Dev &d, int rs, int stage, cudaStream_t s) {
     const unsigned tiles = (unsigned)learned_tiles(d, DIR);
-    if (stage == 1) {  // the network runs once per step and direction
-        if (d.wuni[DIR]) k_recon_learned<DIR, 1><<<tiles, 128, 0, s>>>(d);
-        else k_recon_learned<DIR, 0><<<tiles, 128, 0, s>>>(d);
-    } else {
-        if (d.wuni[DIR]) k_recon_flagged<DIR, 1><<<(tiles + 1) / 2, 256, 0, s>>>(d);
-        else k_recon_flagged<DIR, 0><<<(tiles + 1) / 2, 256, 0, s>>>(d);
+    if (stage == 1) {
+        // the network kernel (persistent, 4 CTAs per SM) runs on refresh steps,
+        // the flag kernel on the others; whichever does not apply exits at once
+        const unsigned pg = tiles < (unsigned)(4 * d.num_sms) ? tiles : (unsigned)(4 * d.num_sms);
+        if (d.wuni[DIR]) k_recon_learned<DIR, 1><<<pg, 128, 0, s>>>(d, stage);
+        else k_recon_learned<DIR, 0><<<pg, 128, 0, s>>>(d, stage);
     }
+    if (d.wuni[DIR]) k_recon_flagged<DIR, 1><<<(tiles + 1) / 2, 256, 0, s>>>(d, stage);
+    else k_recon_flagged<DIR, 0><<<(tiles + 1) / 2, 256, 0, s>>>(d, stage);
     dim3 g, b;
     split_dims(d, DIR, false, g, b);
     if (d.riemann_minb == 4) launch_riemann_m<float, DIR, 4>(d, rs, g, b, s);

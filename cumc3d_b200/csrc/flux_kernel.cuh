@@ -310,8 +310,33 @@ static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &
     g = dim3((unsigned)((total + tpb - 1) / tpb), 1, 1);
 }
 
+}  // namespace cumc
+#include "recon_tile.cuh"
+namespace cumc {
+
+template <class T, int DIR, int UNI, int CPT>
+static void launch_recon_tile_c(const Dev &d, int rec, cudaStream_t s) {
+    const dim3 g = recon_tile_grid(d, DIR, CPT), b(32, 8, 1);
+    switch (rec) {
+        case REC_TVD_MM: k_recon_tile<T, DIR, REC_TVD_MM, UNI, CPT><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_VL: k_recon_tile<T, DIR, REC_TVD_VL, UNI, CPT><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_MC: k_recon_tile<T, DIR, REC_TVD_MC, UNI, CPT><<<g, b, 0, s>>>(d); break;
+        case REC_PPM: k_recon_tile<T, DIR, REC_PPM, UNI, CPT><<<g, b, 0, s>>>(d); break;
+        default: k_recon_tile<T, DIR, REC_WENO, UNI, CPT><<<g, b, 0, s>>>(d); break;
+    }
+}
+template <class T, int DIR, int UNI>
+static void launch_recon_tile(const Dev &d, int rec, cudaStream_t s) {
+    if (d.recon_tile == 2) launch_recon_tile_c<T, DIR, UNI, 2>(d, rec, s);
+    else launch_recon_tile_c<T, DIR, UNI, 1>(d, rec, s);
+}
+
 template <class T, int DIR, int UNI>
 static void launch_recon_u(const Dev &d, int rec, dim3 g, dim3 b, cudaStream_t s) {
+    if (d.recon_tile) {
+        launch_recon_tile<T, DIR, UNI>(d, rec, s);
+        return;
+    }
     switch (rec) {
         case REC_TVD_MM: k_recon<T, DIR, REC_TVD_MM, UNI><<<g, b, 0, s>>>(d); break;
         case REC_TVD_VL: k_recon<T, DIR, REC_TVD_VL, UNI><<<g, b, 0, s>>>(d); break;

@@ -48,12 +48,12 @@ __host__ __device__ inline void learn_var_features(float a0, float a1, float a2,
                                                    float *r) {
     const float d0 = a1 - a0, d1 = a2 - a1, d2 = a3 - a2, d3 = a4 - a3;
     const float s = ((fabsf(d0) + fabsf(d1)) + fabsf(d2)) + fabsf(d3);
-    const float den = s + 1.0e-30f;
-    f4[0] = d0 / den;
-    f4[1] = d1 / den;
-    f4[2] = d2 / den;
-    f4[3] = d3 / den;
-    *r = s / ((fabsf(a2) + s) + 1.0e-30f);
+    const float inv = 1.0f / (s + 1.0e-30f);
+    f4[0] = d0 * inv;
+    f4[1] = d1 * inv;
+    f4[2] = d2 * inv;
+    f4[3] = d3 * inv;
+    *r = s * (1.0f / ((fabsf(a2) + s) + 1.0e-30f));
 }
 
 // element offset of (row r, column k) in a K-major BF16 tile of K columns in

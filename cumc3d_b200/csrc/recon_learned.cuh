@@ -2,8 +2,8 @@
 // flag (see learned.cuh).  Same cells, same enumeration and the same outputs
 // (QL/QR face states) as k_recon<float, DIR, REC_WENO, UNI>.
 //
-// Stage 1 of each RK step, k_recon_learned (one CTA = 128 consecutive cells
-// of the flat enumeration = one tile):
+// Stage 1 of every flag_interval-th RK step, k_recon_learned (a tile = 128
+// consecutive cells of the flat enumeration; persistent CTAs walk the tiles):
 //   1. each thread loads its cell's 7 stencils and builds the 35 features;
 //   2. the MLP (tcgen05, BF16 operands, FP32 accumulators in TMEM) gives one
 //      logit per cell; the flag (logit > threshold) is stored per cell;
@@ -14,9 +14,9 @@
 //      the plain FP32 form), flagged cells also evaluate the linear values,
 //      and the tile is marked to fall back until the next audit if any
 //      flagged cell's relative face-value error exceeds audit_tol.
-// Stages 2 and 3, k_recon_flagged: the stage-1 flags of the cell and of its
-// two neighbours along the sweep (the state moves less than a cell per step)
-// choose linear or WENO-Z per warp, without running the network again.
+// All other stages, k_recon_flagged: the stored flags of the cell and of its
+// neighbours within two cells along the sweep choose linear or WENO-Z per
+// warp, without running the network.
 //
 // Cells next to the domain boundary along the sweep (c <= 1 or c >= n) always
 // use WENO-Z: on a periodic axis face 0 and face n are one face, and their
@@ -129,50 +129,129 @@ __device__ __forceinline__ long long learned_total(const Dev &d) {
     return ex * ey * ez;
 }
 
+// Steps on which the network runs: every flag_interval steps, stage 1.
+__device__ __forceinline__ bool learned_refresh(const Dev &d, int stage) {
+    return stage == 1 && (d.flag_interval <= 1 || (d.S->steps % d.flag_interval) == 0);
+}
+__device__ __forceinline__ bool learned_audit(const Dev &d) {
+    return d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
+}
+
+// Network + reconstruction, persistent: each CTA allocates tensor memory and
+// loads the weights once, then walks tiles blockIdx.x, +gridDim.x, ...
+// Runs on refresh stages only (uniform early exit otherwise).
 template <int DIR, int UNI>
-__global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d) {
-    if (d.S->done) return;
+__global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d, int stage) {
+    if (d.S->done || !learned_refresh(d, stage)) return;
     __shared__ MlpTile tile;
     __shared__ float s_err[4];
     __shared__ int s_flag[4];
     const int tid = threadIdx.x;
     mlp_tile_setup(tile, reinterpret_cast<const MlpPacked *>(d.mlp));
     const long long total = learned_total<DIR>(d);
-    const LearnedCell q = learned_cell<DIR>(d, (long long)blockIdx.x * 128 + tid, total);
+    const long long ntiles = (total + 127) / 128;
+    const bool audit = learned_audit(d);
+    uint32_t phase = 0;
+    bool mma_ok = true;
+    for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        const LearnedCell q = learned_cell<DIR>(d, tl * 128 + tid, total);
+        float w[14];
+        learned_weights<DIR, UNI>(d, q.c, w);
+        float a[LEARN_NV][5];
+        learned_stencils<DIR>(d, q, a);
+        float logit = -1.0e30f;
+        {
+            float x[LEARN_K];
+#pragma unroll
+            for (int v = 0; v < LEARN_NV; ++v)
+                learn_var_features(a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], &x[4 * v], &x[4 * LEARN_NV + v]);
+#pragma unroll
+            for (int m = LEARN_NF; m < LEARN_K; ++m) x[m] = 0.0f;
+            if (!mlp_tile_logit(tile, x, phase, logit) || !mma_ok) {
+                // an MMA never completed: no cell is flagged, the error is reported
+                logit = -1.0e30f;
+                if (mma_ok && atomicCAS(&d.S->err_code, 0, LEARN_ERR_MMA) == 0) {
+                    d.S->err_cell = (int)tl;
+                    d.S->err_stage = -1;
+                }
+                mma_ok = false;
+            }
+        }
+        const bool flag = q.valid && logit > d.learn_thr;
+        if (q.valid) d.lflag[DIR][q.t] = flag ? 1 : 0;
+        const bool inner = q.c >= 2 && q.c <= q.ns - 1;
+        const bool warp_all = __all_sync(0xffffffffu, flag && inner);
+        const bool linear = warp_all && !audit && d.lfb[DIR][tl] == 0;
+        float err = 0.0f;
+        learned_reconstruct(d, q, w, a, linear, audit && flag && inner, err);
+        if (audit) {
+            // tile verdict: the largest error of a flagged cell against the tolerance
+            float e = err;
+            int nf = (flag && inner) ? 1 : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
+                nf += __shfl_xor_sync(0xffffffffu, nf, o);
+            }
+            if ((tid & 31) == 0) {
+                s_err[tid >> 5] = e;
+                s_flag[tid >> 5] = nf;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                const float te = fmaxf(fmaxf(s_err[0], s_err[1]), fmaxf(s_err[2], s_err[3]));
+                const int tf = s_flag[0] + s_flag[1] + s_flag[2] + s_flag[3];
+                const unsigned char fb = te > d.audit_tol ? 1 : 0;
+                d.lfb[DIR][tl] = fb;
+                const long long nvalid = total - tl * 128;
+                // counters spread over 64 slots (summed on the host)
+                unsigned long long *ls = d.lstats + (tl & (LEARN_STAT_SLOTS - 1)) * LEARN_STAT_FIELDS;
+                atomicAdd(&ls[0], (unsigned long long)(nvalid < 128 ? nvalid : 128));
+                atomicAdd(&ls[1], (unsigned long long)tf);
+                atomicAdd(&ls[2], (unsigned long long)fb);
+                if (tl == 0 && DIR == 0) atomicAdd(&ls[3], 1ull);
+            }
+            __syncthreads();
+        }
+    }
+    mlp_tile_teardown(tile);
+}
+
+// Every other stage: the flags of the last network run, dilated by two cells
+// along the sweep (the state moves less than half a cell per step at the
+// CFL numbers of the workloads, so two cells cover the steps between runs;
+// transverse motion is left to the audit).  On audit steps every cell uses
+// WENO-Z; on the stage-1 audit the tile verdict is taken as above.
+template <int DIR, int UNI>
+__global__ void __launch_bounds__(256) k_recon_flagged(const Dev d, int stage) {
+    if (d.S->done || learned_refresh(d, stage)) return;
+    __shared__ float s_err[8];
+    __shared__ int s_flag[8];
+    const long long total = learned_total<DIR>(d);
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const LearnedCell q = learned_cell<DIR>(d, t0, total);
+    const long long sweep = (DIR == 0) ? 1 : (DIR == 1) ? (long long)d.nx : (long long)d.nx * d.ny;
+    const bool inner = q.c >= 2 && q.c <= q.ns - 1;
+    const bool audit = learned_audit(d);
+    bool flag = false;
+    if (q.valid && inner) {
+        const unsigned char *f = d.lflag[DIR];
+        // c-2 .. c+2 lie within 0 .. n+1, the cells of the enumeration
+        flag = f[q.t] && f[q.t - sweep] && f[q.t + sweep] && f[q.t - 2 * sweep] && f[q.t + 2 * sweep];
+    }
+    const bool linear = __all_sync(0xffffffffu, flag && d.lfb[DIR][q.t >> 7] == 0) && !audit;
     float w[14];
     learned_weights<DIR, UNI>(d, q.c, w);
     float a[LEARN_NV][5];
     learned_stencils<DIR>(d, q, a);
-    float logit = -1.0e30f;
-    {
-        float x[LEARN_K];
-#pragma unroll
-        for (int v = 0; v < LEARN_NV; ++v)
-            learn_var_features(a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], &x[4 * v], &x[4 * LEARN_NV + v]);
-#pragma unroll
-        for (int m = LEARN_NF; m < LEARN_K; ++m) x[m] = 0.0f;
-        uint32_t phase = 0;
-        if (!mlp_tile_logit(tile, x, phase, logit)) {
-            // the MMA never completed: no cell is flagged, the error is reported
-            logit = -1.0e30f;
-            if (atomicCAS(&d.S->err_code, 0, LEARN_ERR_MMA) == 0) {
-                d.S->err_cell = blockIdx.x;
-                d.S->err_stage = -1;
-            }
-        }
-    }
-    const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
-    const bool flag = q.valid && logit > d.learn_thr;
-    if (q.valid) d.lflag[DIR][q.t] = flag ? 1 : 0;
-    const bool inner = q.c >= 2 && q.c <= q.ns - 1;
-    const bool warp_all = __all_sync(0xffffffffu, flag && inner);
-    const bool linear = warp_all && !audit && d.lfb[DIR][blockIdx.x] == 0;
     float err = 0.0f;
-    learned_reconstruct(d, q, w, a, linear, audit && flag && inner, err);
-    if (audit) {
-        // tile verdict: the largest error of a flagged cell against the tolerance
+    const bool verdict = audit && stage == 1;
+    learned_reconstruct(d, q, w, a, linear, verdict && flag, err);
+    if (verdict) {
+        // two 128-cell tiles per CTA: warps 0-3 and 4-7
+        const int tid = threadIdx.x;
         float e = err;
-        int nf = (flag && inner) ? 1 : 0;
+        int nf = flag ? 1 : 0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
@@ -183,46 +262,23 @@ __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d) {
             s_flag[tid >> 5] = nf;
         }
         __syncthreads();
-        if (tid == 0) {
-            const float te = fmaxf(fmaxf(s_err[0], s_err[1]), fmaxf(s_err[2], s_err[3]));
-            const int tf = s_flag[0] + s_flag[1] + s_flag[2] + s_flag[3];
-            const unsigned char fb = te > d.audit_tol ? 1 : 0;
-            d.lfb[DIR][blockIdx.x] = fb;
-            const long long nvalid = total - (long long)blockIdx.x * 128;
-            // counters spread over 64 slots (summed on the host)
-            unsigned long long *ls = d.lstats + (blockIdx.x & (LEARN_STAT_SLOTS - 1)) * LEARN_STAT_FIELDS;
-            atomicAdd(&ls[0], (unsigned long long)(nvalid < 128 ? nvalid : 128));
-            atomicAdd(&ls[1], (unsigned long long)tf);
-            atomicAdd(&ls[2], (unsigned long long)fb);
-            if (blockIdx.x == 0 && DIR == 0) atomicAdd(&ls[3], 1ull);
+        if ((tid & 127) == 0) {
+            const int h = tid >> 7;
+            const long long tl = (long long)blockIdx.x * 2 + h;
+            if (tl * 128 < total) {
+                const float te = fmaxf(fmaxf(s_err[4 * h], s_err[4 * h + 1]), fmaxf(s_err[4 * h + 2], s_err[4 * h + 3]));
+                const int tf = s_flag[4 * h] + s_flag[4 * h + 1] + s_flag[4 * h + 2] + s_flag[4 * h + 3];
+                const unsigned char fb = te > d.audit_tol ? 1 : 0;
+                d.lfb[DIR][tl] = fb;
+                const long long nvalid = total - tl * 128;
+                unsigned long long *ls = d.lstats + (tl & (LEARN_STAT_SLOTS - 1)) * LEARN_STAT_FIELDS;
+                atomicAdd(&ls[0], (unsigned long long)(nvalid < 128 ? nvalid : 128));
+                atomicAdd(&ls[1], (unsigned long long)tf);
+                atomicAdd(&ls[2], (unsigned long long)fb);
+                if (tl == 0 && DIR == 0) atomicAdd(&ls[3], 1ull);
+            }
         }
     }
-    mlp_tile_teardown(tile);
-}
-
-// stages 2 and 3: the stage-1 flags, dilated by one cell along the sweep
-template <int DIR, int UNI>
-__global__ void __launch_bounds__(256) k_recon_flagged(const Dev d) {
-    if (d.S->done) return;
-    const long long total = learned_total<DIR>(d);
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if ((t0 & ~31ll) >= total) return;  // whole warps past the end
-    const LearnedCell q = learned_cell<DIR>(d, t0, total);
-    const long long sweep = (DIR == 0) ? 1 : (DIR == 1) ? (long long)d.nx : (long long)d.nx * d.ny;
-    const bool inner = q.c >= 2 && q.c <= q.ns - 1;
-    const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
-    bool ok = false;
-    if (q.valid && inner && !audit) {
-        const unsigned char *f = d.lflag[DIR];
-        ok = f[q.t] && f[q.t - sweep] && f[q.t + sweep] && d.lfb[DIR][q.t >> 7] == 0;
-    }
-    const bool linear = __all_sync(0xffffffffu, ok);
-    float w[14];
-    learned_weights<DIR, UNI>(d, q.c, w);
-    float a[LEARN_NV][5];
-    learned_stencils<DIR>(d, q, a);
-    float err = 0.0f;
-    learned_reconstruct(d, q, w, a, linear, false, err);
 }
 
 }  // namespace cumc

@@ -1,0 +1,128 @@
+// recon_tile.cuh -- face reconstruction with the stencils staged in shared
+// memory.  Same cells, same arithmetic (recon_cell) and the same outputs as
+// k_recon; each state value of the tile is loaded from HBM once, coalesced
+// along x, and converted to T once, instead of once per stencil that uses it.
+//
+// CTA = 32 x 8 threads.  Tile:
+//   x sweep (DIR 0): 32 cells along x  x  8*CPT rows along y, halo H in x;
+//   y/z sweep:       32 cells along x  x  8*CPT cells along the sweep,
+//                    halo H rows along the sweep;
+// H = 2 for the 5-point stencils (PPM, WENO), 1 for TVD.  CPT (cells per
+// thread, 1 or 2) trades halo overhead for registers; the autotuner picks.
+#pragma once
+#include "engine.cuh"
+#include "mhd_device.cuh"
+
+namespace cumc {
+
+template <class T, int DIR, int REC, int UNI, int CPT>
+__global__ void __launch_bounds__(256) k_recon_tile(const Dev d) {
+    if (d.S->done) return;
+    constexpr int TX = 32, TY = 8;
+    constexpr int H = (REC == REC_PPM || REC == REC_WENO) ? 2 : 1;
+    constexpr int NR = TY * CPT;                    // rows of reconstructed cells
+    constexpr int SX = (DIR == 0) ? TX + 2 * H : TX;  // staged row length
+    constexpr int SR = (DIR == 0) ? NR : NR + 2 * H;  // staged rows
+    __shared__ T s[7][SR][SX];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * TX + tx;
+    constexpr int tb1 = (DIR == 0) ? 1 : 0;
+    constexpr int tb2 = (DIR == 2) ? 1 : 2;
+
+    // ---- stage the tile ----
+    const int c0 = (DIR == 0) ? blockIdx.x * TX : blockIdx.y * NR;  // first reconstructed cell
+    for (int idx = tid; idx < SR * SX; idx += TX * TY) {
+        const int sr = idx / SX, sx = idx - sr * SX;
+        int x, y, z;
+        bool ok;
+        if (DIR == 0) {
+            x = c0 - H + sx; y = blockIdx.y * NR + sr + 1; z = blockIdx.z + 1;
+            ok = x <= d.nx + 3 && y <= d.ny;
+        } else if (DIR == 1) {
+            x = blockIdx.x * TX + sx + 1; y = c0 - H + sr; z = blockIdx.z + 1;
+            ok = x <= d.nx && y <= d.ny + 3;
+        } else {
+            x = blockIdx.x * TX + sx + 1; y = blockIdx.z + 1; z = c0 - H + sr;
+            ok = x <= d.nx && z <= d.nz + 3;
+        }
+        if (ok) {
+            const int ci = cidx(d, x, y, z);
+#pragma unroll
+            for (int v = 0; v < 7; ++v) {
+                const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
+                s[v][sr][sx] = (T)__ldg(src + ci);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- reconstruct CPT cells per thread ----
+    T *const *QL = reinterpret_cast<T *const *>(d.QL);
+    T *const *QR = reinterpret_cast<T *const *>(d.QR);
+    const int st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+        const int r = ty + TY * i;  // row within the tile
+        int c, j, k, l, ns;
+        bool valid;
+        if (DIR == 0) {
+            c = c0 + tx; j = c; k = blockIdx.y * NR + r + 1; l = blockIdx.z + 1; ns = d.nx;
+            valid = c <= d.nx + 1 && k <= d.ny;
+        } else if (DIR == 1) {
+            c = c0 + r; k = c; j = blockIdx.x * TX + tx + 1; l = blockIdx.z + 1; ns = d.ny;
+            valid = j <= d.nx && c <= d.ny + 1;
+        } else {
+            c = c0 + r; l = c; j = blockIdx.x * TX + tx + 1; k = blockIdx.z + 1; ns = d.nz;
+            valid = j <= d.nx && c <= d.nz + 1;
+        }
+        if (!valid) continue;
+        const int ci = cidx(d, j, k, l);
+        T w[14];
+        constexpr int NW = (REC == REC_PPM) ? 14 : (REC == REC_WENO) ? 10 : 2;
+        if (UNI) {
+#pragma unroll
+            for (int m = 0; m < NW; ++m) w[m] = uni_w<T>(d, DIR, m);
+        } else {
+            const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
+#pragma unroll
+            for (int m = 0; m < NW; ++m) w[m] = wp[m];
+        }
+        T vm_rho = T(0), vp_rho = T(0);
+        bool fallback = false;
+#pragma unroll
+        for (int v = 0; v < 7; ++v) {
+            // the stencil c-H .. c+H of variable v
+            auto at = [&](int m) -> T { return (DIR == 0) ? s[v][r][tx + H + m] : s[v][r + H + m][tx]; };
+            T a0 = T(0), a4 = T(0);
+            if (H == 2) { a0 = at(-2); a4 = at(2); }
+            const T a1 = at(-1), a2 = at(0), a3 = at(1);
+            T vm, vp;
+            recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
+            if (v == 0) { vm_rho = vm; vp_rho = vp; }
+            if (v == 4 && d.pos_fallback) {
+                fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
+                if (fallback) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const T cv = (DIR == 0) ? s[u][r][tx + H] : s[u][r + H][tx];
+                        if (c <= ns) QL[u][ci] = cv;
+                        if (c >= 1) QR[u][ci - st] = cv;
+                    }
+                }
+            }
+            if (fallback) vm = vp = a2;
+            if (c <= ns) QL[v][ci] = vp;      // left state of face c
+            if (c >= 1) QR[v][ci - st] = vm;  // right state of face c-1
+        }
+    }
+}
+
+// grid of the tiled reconstruction for one sweep
+static inline dim3 recon_tile_grid(const Dev &d, int dir, int cpt) {
+    const int nr = 8 * cpt;
+    if (dir == 0) return dim3((d.nx + 2 + 31) / 32, (d.ny + nr - 1) / nr, d.nz);
+    if (dir == 1) return dim3((d.nx + 31) / 32, (d.ny + 2 + nr - 1) / nr, d.nz);
+    return dim3((d.nx + 31) / 32, (d.nz + 2 + nr - 1) / nr, d.ny);
+}
+
+}  // namespace cumc

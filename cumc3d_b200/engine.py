@@ -82,7 +82,7 @@ def load_library(path=None):
     L.cumc_batch_stream.restype = C.c_void_p
     L.cumc_batch_last_error.argtypes = [C.c_void_p]
     L.cumc_batch_last_error.restype = C.c_char_p
-    L.cumc_learn_set.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_float]
+    L.cumc_learn_set.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_float]
     L.cumc_learn_stats.argtypes = [C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
     L.cumc_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p, C.c_void_p]
@@ -191,26 +191,27 @@ class Solver:
 
     def autotune(self):
         """Pick the fastest face-flux launch shape on the live state."""
-        ch = (C.c_int * 4)()
+        ch = (C.c_int * 5)()
         ms = C.c_double()
         self._check(self.L.cumc_autotune(self.h, ch, C.byref(ms)))
         return dict(split=bool(ch[0]), tpb_recon=ch[1], tpb_riemann=ch[2], riemann_min_blocks=ch[3],
-                    flux_ms_per_stage=ms.value)
+                    recon_tile=ch[4], flux_ms_per_stage=ms.value)
 
-    def set_tuning(self, split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1):
-        ch = (C.c_int * 4)(int(split), tpb_recon, tpb_riemann, riemann_min_blocks)
+    def set_tuning(self, split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1, recon_tile=0):
+        ch = (C.c_int * 5)(int(split), tpb_recon, tpb_riemann, riemann_min_blocks, int(recon_tile))
         self._check(self.L.cumc_set_tuning(self.h, ch))
 
     # ---- learned smooth-face flag (FP32 WENO form, handle created with learned=1) ----
-    def learn_set(self, params, threshold=0.0, audit_interval=10, audit_tol=1e-6):
-        """Enable the flag with these parameters (float[2657]); None disables it."""
-        if params is None:
-            self._check(self.L.cumc_learn_set(self.h, None, float(threshold), int(audit_interval), float(audit_tol)))
-            return
-        P = np.ascontiguousarray(params, dtype=np.float32)
-        if P.shape != (capi.LEARN_NP,):
-            raise ValueError("parameters must have %d entries" % capi.LEARN_NP)
-        self._check(self.L.cumc_learn_set(self.h, P.ctypes.data, float(threshold), int(audit_interval),
+    def learn_set(self, params, threshold=0.0, audit_interval=10, audit_tol=1e-6, flag_interval=1):
+        """Enable the flag with these parameters (float[2657]); None disables it.
+        The network runs every flag_interval steps; audits every audit_interval."""
+        ptr = None
+        if params is not None:
+            P = np.ascontiguousarray(params, dtype=np.float32)
+            if P.shape != (capi.LEARN_NP,):
+                raise ValueError("parameters must have %d entries" % capi.LEARN_NP)
+            ptr = P.ctypes.data
+        self._check(self.L.cumc_learn_set(self.h, ptr, float(threshold), int(flag_interval), int(audit_interval),
                                           float(audit_tol)))
 
     def learn_stats(self):

@@ -184,12 +184,14 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
 /* Autotuner (no counterpart in the reference): times the candidate launch
  * shapes of the face-flux kernels (fused or split recon/Riemann, threads per
  * block, register budget of the Riemann kernel) on the handle's live state and
- * keeps the fastest for all later steps.  choice_out[0..3] = (split?, recon
- * threads/block, Riemann threads/block, Riemann min blocks/SM); best_ms_out =
- * the flux time of one stage with that choice.  Either pointer may be NULL. */
+ * keeps the fastest for all later steps.  choice_out[0..4] = (split?, recon
+ * threads/block, Riemann threads/block, Riemann min blocks/SM, staged
+ * reconstruction: 0 = per-cell loads, 1 or 2 = stencils staged in shared
+ * memory with that many cells per thread); best_ms_out = the flux time of
+ * one stage with that choice.  Either pointer may be NULL. */
 int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out);
 
-/* Set the launch shape by hand, same four integers as choice_out above. */
+/* Set the launch shape by hand, same five integers as choice_out above. */
 int cumc_set_tuning(cumc_handle *h, const int *choice);
 
 /* Numerics self-check (no counterpart in the reference): compares the FP64
@@ -260,8 +262,11 @@ typedef struct cumc_train_config {
     unsigned long long seed;     /* minibatch sampling                         */
 } cumc_train_config;
 /* enable (params != NULL) or disable the flag on a handle created with
- * learned = 1 (FP32 + WENO); resets the fallback tiles and the counters */
-int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int audit_interval, float audit_tol);
+ * learned = 1 (FP32 + WENO); resets the fallback tiles and the counters.
+ * The network runs at stage 1 of every flag_interval-th step (>= 1); the
+ * other stages reuse its flags, dilated by two cells along the sweep. */
+int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int flag_interval, int audit_interval,
+                   float audit_tol);
 /* audit counters: cells audited, cells flagged, tiles set to fall back, audits */
 int cumc_learn_stats(cumc_handle *h, unsigned long long *out4);
 /* samples of every stride-th interior cell of the current state, sweep dir */

@@ -1472,12 +1472,12 @@ void orc_riemann_face(int dir, int rs, double gamma, const double *pl8, const do
 static void lrn_var_features(float a0, float a1, float a2, float a3, float a4, float *f4, float *r) {
     const float d0 = a1 - a0, d1 = a2 - a1, d2 = a3 - a2, d3 = a4 - a3;
     const float sum = ((std::fabs(d0) + std::fabs(d1)) + std::fabs(d2)) + std::fabs(d3);
-    const float den = sum + 1.0e-30f;
-    f4[0] = d0 / den;
-    f4[1] = d1 / den;
-    f4[2] = d2 / den;
-    f4[3] = d3 / den;
-    *r = sum / ((std::fabs(a2) + sum) + 1.0e-30f);
+    const float inv = 1.0f / (sum + 1.0e-30f);
+    f4[0] = d0 * inv;
+    f4[1] = d1 * inv;
+    f4[2] = d2 * inv;
+    f4[3] = d3 * inv;
+    *r = sum * (1.0f / ((std::fabs(a2) + sum) + 1.0e-30f));
 }
 
 /* WENO-Z candidates P and indicators B of the right (p) and left (m) face */

@@ -178,7 +178,8 @@ def test_trained_flag_separates_smooth_from_shocked_cells():
     assert rough.sum() > 100 and (z[rough] > 0).mean() < 0.02
 
 
-def test_trained_flag_keeps_div_b_at_roundoff_on_a_periodic_box():
+@pytest.mark.parametrize("flag_interval", [1, 4])
+def test_trained_flag_keeps_div_b_at_roundoff_on_a_periodic_box(flag_interval):
     """Face 0 and face n of a periodic axis are one face: the cells next to
     the ends of a sweep always use WENO-Z so both copies get the same flux
     and constrained transport keeps div B at roundoff."""
@@ -189,7 +190,7 @@ def test_trained_flag_keeps_div_b_at_roundoff_on_a_periodic_box():
     s = engine.Solver(sp)
     s.set_state(prim, eps)
     s.initial_update()
-    s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5)
+    s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5, flag_interval=flag_interval)
     s.evolve(1e30, 30)
     divb = s.find_divb()
     st = s.learn_stats()

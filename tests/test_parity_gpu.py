@@ -102,11 +102,15 @@ def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4),
     dict(split=True, tpb_recon=128, tpb_riemann=64, riemann_min_blocks=1),
     dict(split=False, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1),
+    dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1, recon_tile=1),
+    dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=2),
 ])
-def test_every_launch_shape_is_bitwise_identical(oracle_mod, tuning):
-    """The autotuner's candidates differ in blocking and register budget only."""
+@pytest.mark.parametrize("recon", ["weno", "ppm", "tvdmc"])
+def test_every_launch_shape_is_bitwise_identical(oracle_mod, tuning, recon):
+    """The autotuner's candidates differ in blocking, staging and register
+    budget only (grid extents not multiples of the tiles)."""
     from cumc3d_b200.engine import Solver
-    spec, prim, eps = models.smooth_state(20, 12, 10, 3, boundary_flag=(1, 1, 0, 0, 2, 2), recon="weno",
+    spec, prim, eps = models.smooth_state(20, 12, 10, 3, boundary_flag=(1, 1, 0, 0, 2, 2), recon=recon,
                                           riemann="hlld", seed=11)
     g = Solver(spec)
     g.set_state(prim, eps)
