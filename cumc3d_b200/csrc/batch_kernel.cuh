@@ -188,7 +188,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
             const double a2 = b.CS[c] * b.CS[c];
             const double a4 = a2 * a2;
             const double bx = b.BC[0][c], by = b.BC[1][c], bz = b.BC[2][c];
-            const double b2x = (bx * bx / rho), b2y = (by * by / rho), b2z = (bz * bz / rho);
+            const double b2x = dv(bx * bx, rho), b2y = dv(by * by, rho), b2z = dv(bz * bz, rho);
             const double b2 = b2x + b2y + b2z;
             const double b4 = b2 * b2;
             const double cfx = sqrt(0.5 * (a2 + b2 + sqrt((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2x)));
@@ -299,7 +299,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 if (j >= 1) {
 #pragma unroll
                     for (int i = 0; i < 5; ++i) {
-                        const double dflux = (b.F[i][c] - b.F[i][c - 1]) / (dxj);
+                        const double dflux = dv(b.F[i][c] - b.F[i][c - 1], dxj);
                         lr[i] = -dflux;
                         lr[i] = lr[i] + 0.0;  // + sc (no sources)
                     }
@@ -313,8 +313,8 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 const double lbx = -((zero) / 1.0 - (zero) / 1.0);
                 const double ezd = (j >= 1) ? (b.EZ[c] - b.EZ[c - 1]) : 0.0;
                 const double eyd = (j >= 1) ? (b.EY[c] - b.EY[c - 1]) : 0.0;
-                const double lby = -((zero) / 1.0 - ezd / (dxj));
-                const double lbz = -(eyd / (dxj) - (zero) / 1.0);
+                const double lby = -((zero) / 1.0 - dv(ezd, dxj));
+                const double lbz = -(dv(eyd, dxj) - (zero) / 1.0);
                 auto combo = [&](double *Uarr, double *Oarr, double lrv) {
                     const double u = Uarr[c];
                     double un;
@@ -343,7 +343,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 const double byu = 0.5 * (b.UBY1[c] + b.UBY0[c]);
                 const double bzu = 0.5 * (b.UBZ1[c] + b.UBZ0[c]);
                 const double u0 = b.U[0][c];
-                const double vx = b.U[1][c] / u0, vy = b.U[2][c] / u0, vz = b.U[3][c] / u0;
+                const double vx = dv(b.U[1][c], u0), vy = dv(b.U[2][c], u0), vz = dv(b.U[3][c], u0);
                 const double bsquare = bxu * bxu + byu * byu + bzu * bzu;
                 const double vsquare = vx * vx + vy * vy + vz * vz;
                 double e = (b.U[4][c] - 0.5 * bsquare) / u0 - 0.5 * vsquare;

@@ -234,6 +234,7 @@ __global__ void k_fixpole(const Dev d) {
 // ---------------------------------------------------------------------------
 // du/dt and the Shu-Osher combination over j,k,l = 0..n
 // ---------------------------------------------------------------------------
+template <class FT>  // storage type of the hydro face fluxes (double, or float in the FP32 form)
 __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
     if (d.S->done) return;
     // flat index over j,k,l = 0..n (x fastest)
@@ -253,12 +254,15 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
     if (interior) {
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
-            fx0[i] = d.FX[i][c];
-            fx1[i] = d.FX[i][c - 1];
-            fy0[i] = d.n_dim > 1 ? d.FY[i][c] : 0.0;
-            fy1[i] = d.n_dim > 1 ? d.FY[i][c - sy] : 0.0;
-            fz0[i] = d.n_dim > 2 ? d.FZ[i][c] : 0.0;
-            fz1[i] = d.n_dim > 2 ? d.FZ[i][c - sz] : 0.0;
+            const FT *FXi = reinterpret_cast<const FT *>(d.FX[i]);
+            const FT *FYi = reinterpret_cast<const FT *>(d.FY[i]);
+            const FT *FZi = reinterpret_cast<const FT *>(d.FZ[i]);
+            fx0[i] = (double)FXi[c];
+            fx1[i] = (double)FXi[c - 1];
+            fy0[i] = d.n_dim > 1 ? (double)FYi[c] : 0.0;
+            fy1[i] = d.n_dim > 1 ? (double)FYi[c - sy] : 0.0;
+            fz0[i] = d.n_dim > 2 ? (double)FZi[c] : 0.0;
+            fz1[i] = d.n_dim > 2 ? (double)FZi[c - sz] : 0.0;
         }
     }
     const double ex0 = d.EX[c], exz = d.EX[c - sz], exy = d.EX[c - sy];
@@ -277,19 +281,19 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
             double dflux, L;
-            if (d.coord == 0) dflux = (fx0[i] - fx1[i]) / (DX(j));
-            else if (d.coord == 1) dflux = (XF(j) * fx0[i] - XF(j - 1) * fx1[i]) / (XC(j) * DX(j));
-            else dflux = (XF(j) * XF(j) * fx0[i] - XF(j - 1) * XF(j - 1) * fx1[i]) / (DXCB(j) / 3.0);
+            if (d.coord == 0) dflux = dv(fx0[i] - fx1[i], DX(j));
+            else if (d.coord == 1) dflux = dv(XF(j) * fx0[i] - XF(j - 1) * fx1[i], XC(j) * DX(j));
+            else dflux = dv(XF(j) * XF(j) * fx0[i] - XF(j - 1) * XF(j - 1) * fx1[i], DXCB(j) / 3.0);
             L = -dflux;
             if (d.n_dim > 1) {
-                if (d.coord == 0) dflux = (fy0[i] - fy1[i]) / (DY(k));
-                else if (d.coord == 1) dflux = (fy0[i] - fy1[i]) / (XC(j) * DY(k));
-                else dflux = (SINF(k) * fy0[i] - SINF(k - 1) * fy1[i]) / (XBAR(j) * DCOSE(k));
+                if (d.coord == 0) dflux = dv(fy0[i] - fy1[i], DY(k));
+                else if (d.coord == 1) dflux = dv(fy0[i] - fy1[i], XC(j) * DY(k));
+                else dflux = dv(SINF(k) * fy0[i] - SINF(k - 1) * fy1[i], XBAR(j) * DCOSE(k));
                 L = L - dflux;
             }
             if (d.n_dim > 2) {
-                if (d.coord != 2) dflux = (fz0[i] - fz1[i]) / DZ(l);
-                else dflux = (fz0[i] - fz1[i]) * DY(k) / (XBAR(j) * DZ(l) * DCOSE(k));
+                if (d.coord != 2) dflux = dv(fz0[i] - fz1[i], DZ(l));
+                else dflux = dv((fz0[i] - fz1[i]) * DY(k), XBAR(j) * DZ(l) * DCOSE(k));
                 L = L - dflux;
             }
             lr[i] = L;
@@ -303,8 +307,8 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
                 const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
                 const double bsquare = bx * bx + by * by + bz * bz;
                 if (d.coord == 1) {
-                    sc[1] = sc[1] + (p + rho * vy * vy + 0.5 * bsquare - by * by) / (XC(j));
-                    sc[2] = sc[2] - (rho * vx * vy - bx * by) / (XC(j));
+                    sc[1] = sc[1] + dv(p + rho * vy * vy + 0.5 * bsquare - by * by, XC(j));
+                    sc[2] = sc[2] - dv(rho * vx * vy - bx * by, XC(j));
                 } else {
                     const double G = 3.0 * XC(j) * DX(j) / DXCB(j);
                     const double tf = DSINE(k) / DCOSE(k);
@@ -341,13 +345,13 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
     }
     // l_operator face-B induction, spatial.f90:639-702
     if (d.coord == 0) {
-        lr[5] = -((ez0 - ezy) / (DY(k)) - (ey0 - eyz) / (DZ(l)));
-        lr[6] = -((ex0 - exz) / (DZ(l)) - (ez0 - ezx) / (DX(j)));
-        lr[7] = -((ey0 - eyx) / (DX(j)) - (ex0 - exy) / (DY(k)));
+        lr[5] = -(dv(ez0 - ezy, DY(k)) - dv(ey0 - eyz, DZ(l)));
+        lr[6] = -(dv(ex0 - exz, DZ(l)) - dv(ez0 - ezx, DX(j)));
+        lr[7] = -(dv(ey0 - eyx, DX(j)) - dv(ex0 - exy, DY(k)));
     } else if (d.coord == 1) {
-        lr[5] = -(ez0 - ezy) / (XF(j) * DY(k)) + (ey0 - eyz) / (DZ(l));
-        lr[6] = -(ex0 - exz) / (DZ(l)) + (ez0 - ezx) / (DX(j));
-        lr[7] = -(XF(j) * ey0 - XF(j - 1) * eyx) / (XC(j) * DX(j)) + (ex0 - exy) / (XC(j) * DY(k));
+        lr[5] = dv(-(ez0 - ezy), XF(j) * DY(k)) + dv(ey0 - eyz, DZ(l));
+        lr[6] = dv(-(ex0 - exz), DZ(l)) + dv(ez0 - ezx, DX(j));
+        lr[7] = dv(-(XF(j) * ey0 - XF(j - 1) * eyx), XC(j) * DX(j)) + dv(ex0 - exy, XC(j) * DY(k));
     } else {
         lr[5] = (-(SINF(k) * ez0 - SINF(k - 1) * ezy) + (ey0 - eyz) * (DY(k) / DZ(l))) / (XF(j) * DCOSE(k) + small_num);
         lr[6] = (-(ex0 - exz) / (XBAR(j) * SINF(k) * DZ(l) + small_num) + (XF(j) * ez0 - XF(j - 1) * ezx) / (XC(j) * DX(j)));
@@ -422,9 +426,9 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
         cell_b(d, j, k, l, bfx, Ux[c - 1], bfy, Uy[c - sy], bfz, Uz[c - sz], bc);
         const double u0 = d.U[0][c];
         rho = u0;
-        vx = d.U[1][c] / u0;
-        vy = d.U[2][c] / u0;
-        vz = d.U[3][c] / u0;
+        vx = dv(d.U[1][c], u0);
+        vy = dv(d.U[2][c], u0);
+        vz = dv(d.U[3][c], u0);
         const double bsquare = bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2];
         const double vsquare = vx * vx + vy * vy + vz * vz;
         e = (d.U[4][c] - 0.5 * bsquare) / u0 - 0.5 * vsquare;
@@ -524,9 +528,9 @@ __global__ void __launch_bounds__(256) k_finddt(const Dev d) {
         const double a2 = d.CS[c] * d.CS[c];
         const double a4 = a2 * a2;
         const double bx = d.BC[0][c], by = d.BC[1][c], bz = d.BC[2][c];
-        const double b2x = (bx * bx / rho);
-        const double b2y = (by * by / rho);
-        const double b2z = (bz * bz / rho);
+        const double b2x = dv(bx * bx, rho);
+        const double b2y = dv(by * by, rho);
+        const double b2z = dv(bz * bz, rho);
         const double b2 = b2x + b2y + b2z;
         const double b4 = b2 * b2;
         const double cfx = sqrt(0.5 * (a2 + b2 + sqrt((a4 + 2.0 * a2 * b2 + b4) - 4.0 * a2 * b2x)));
@@ -609,7 +613,7 @@ __global__ void k_divb(const Dev d, unsigned long long *out) {
         const double bx = d.P[5][c], bxm = d.P[5][c - 1], by = d.P[6][c], bym = d.P[6][c - sy];
         const double bz = d.P[7][c], bzm = d.P[7][c - sz];
         double v;
-        if (d.coord == 0) v = (bx - bxm) / (DX(j)) + (by - bym) / (DY(k)) + (bz - bzm) / (DZ(l));
+        if (d.coord == 0) v = dv(bx - bxm, DX(j)) + dv(by - bym, DY(k)) + dv(bz - bzm, DZ(l));
         else if (d.coord == 1)
             v = (XF(j) * bx - XF(j - 1) * bxm) / (XC(j) * DX(j)) + (by - bym) / (XC(j) * DY(k)) + (bz - bzm) / (DZ(l));
         else
@@ -987,7 +991,8 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     prof_begin(h);
     {
         const long long cells = (long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
-        k_rk<<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
+        if (h->cfg.precision == CUMC_FP32) k_rk<float><<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
+        else k_rk<double><<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
     }
     h->launches++;
     prof_end(h, PC_RK);

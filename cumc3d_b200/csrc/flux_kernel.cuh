@@ -33,6 +33,15 @@ __device__ __forceinline__ T eos_cs(T p, T rho, T e, T g) {
     return dsqrt(dpdden + dpdint * p / (rho * rho));
 }
 
+// hydro face fluxes are stored in the precision of the flux arithmetic: FP64
+// in the plain form, FP32 in the FP32 form (the RK accumulation that reads
+// them stays FP64); the arrays are FP64-sized either way
+template <class T> __device__ __forceinline__ void store_flux(double *a, int i, T v);
+template <> __device__ __forceinline__ void store_flux<double>(double *a, int i, double v) { a[i] = v; }
+template <> __device__ __forceinline__ void store_flux<float>(double *a, int i, float v) {
+    reinterpret_cast<float *>(a)[i] = v;
+}
+
 template <class T> __device__ __forceinline__ const T *weights(const Dev &d, int dir);
 template <> __device__ __forceinline__ const double *weights<double>(const Dev &d, int dir) {
     return dir == 0 ? d.wx : dir == 1 ? d.wy : d.wz;
@@ -139,7 +148,7 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
 
     double *const *FO = (DIR == 0) ? d.FX : (DIR == 1) ? d.FY : d.FZ;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) FO[v][ci] = (double)fo[1 + v];
+    for (int v = 0; v < 5; ++v) store_flux<T>(FO[v], ci, fo[1 + v]);
     // MHD_FLUX, solver/mhd/mhd_module.f90:229-270
     if (DIR == 0) {
         d.EF[e_yx][ci] = (double)fo[ibz];
@@ -283,7 +292,7 @@ __global__ void __launch_bounds__(128, MINB) k_riemann(const Dev d) {
     riemann_face<T, DIR, RS>(pl, pr, epsL, epsR, csL, csR, fo);
     double *const *FO = (DIR == 0) ? d.FX : (DIR == 1) ? d.FY : d.FZ;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) FO[v][ci] = (double)fo[1 + v];
+    for (int v = 0; v < 5; ++v) store_flux<T>(FO[v], ci, fo[1 + v]);
     if (DIR == 0) {
         d.EF[e_yx][ci] = (double)fo[ibz];
         d.EF[e_zx][ci] = -(double)fo[iby];

@@ -26,6 +26,28 @@ template <> __device__ __forceinline__ float dsqrt<float>(float x) { return sqrt
 template <class T> __device__ __forceinline__ T dabs(T x);
 template <> __device__ __forceinline__ double dabs<double>(double x) { return fabs(x); }
 template <> __device__ __forceinline__ float dabs<float>(float x) { return fabsf(x); }
+// x / y bit for bit, minus the FP64 division's slow path for x == 0 (a
+// zero numerator is common: fluid at rest, zero field components, flat
+// stencils).  For x == +-0 and a normal y the quotient of a stand-in
+// numerator (chosen in inline PTX, so the optimizer cannot put x back) is
+// discarded and the signed zero sign(x) * sign(y) returned; every other case
+// is the ordinary division.  The tests run on the integer pipe, which the
+// FP64-bound kernels leave idle.  FP32 divides directly.
+template <class T> __device__ __forceinline__ T dv(T x, T y) { return x / y; }
+template <> __device__ __forceinline__ double dv<double>(double x, double y) {
+    const unsigned long long xb = (unsigned long long)__double_as_longlong(x);
+    const unsigned long long yb = (unsigned long long)__double_as_longlong(y);
+    const unsigned ye = (unsigned)(yb >> 52) & 0x7FFu;  // biased exponent of y
+    const int z = ((xb << 1) == 0ull) & ((ye - 1u) < 0x7FEu);
+    unsigned long long nb;
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\tselp.b64 %0, 0x3FF0000000000000, %1, p;\n\t}"
+        : "=l"(nb)
+        : "l"(xb), "r"(z));
+    const double q = __longlong_as_double((long long)nb) / y;
+    const unsigned long long zb = (xb ^ yb) & 0x8000000000000000ull;
+    return z ? __longlong_as_double((long long)zb) : q;
+}
+
 // Fortran SIGN(1, x)
 template <class T> __device__ __forceinline__ T sign1(T x);
 template <> __device__ __forceinline__ double sign1<double>(double x) { return copysign(1.0, x); }
@@ -92,12 +114,12 @@ __device__ __forceinline__ T wenoz_combine(T P1, T P2, T P3, T B1, T B2, T B3) {
     const T smallpara = WenoEps<T>::eps();
     const T g1 = T(1.0 / 10.0), g2 = T(6.0 / 10.0), g3 = T(3.0 / 10.0);
     T tau5 = dabs(B1 - B3);
-    T q1 = WenoEps<T>::cap(tau5 / (smallpara + B1)), q2 = WenoEps<T>::cap(tau5 / (smallpara + B2)),
-      q3 = WenoEps<T>::cap(tau5 / (smallpara + B3));
+    T q1 = WenoEps<T>::cap(dv(tau5, smallpara + B1)), q2 = WenoEps<T>::cap(dv(tau5, smallpara + B2)),
+      q3 = WenoEps<T>::cap(dv(tau5, smallpara + B3));
     T w1 = g1 * (T(1) + q1 * q1);
     T w2 = g2 * (T(1) + q2 * q2);
     T w3 = g3 * (T(1) + q3 * q3);
-    return (w1 * P1 + w2 * P2 + w3 * P3) / (w1 + w2 + w3);
+    return dv(w1 * P1 + w2 * P2 + w3 * P3, w1 + w2 + w3);
 }
 
 // x / 3 rounded to nearest.  FP64: the quotient q = RN(x * RN(1/3)) is within
@@ -211,8 +233,8 @@ __device__ __forceinline__ void wenoz_weights(const T B[3], T om[3]) {
     const T smallpara = WenoEps<T>::eps();
     const T g1 = T(1.0 / 10.0), g2 = T(6.0 / 10.0), g3 = T(3.0 / 10.0);
     T tau5 = dabs(B[0] - B[2]);
-    T q1 = WenoEps<T>::cap(tau5 / (smallpara + B[0])), q2 = WenoEps<T>::cap(tau5 / (smallpara + B[1])),
-      q3 = WenoEps<T>::cap(tau5 / (smallpara + B[2]));
+    T q1 = WenoEps<T>::cap(dv(tau5, smallpara + B[0])), q2 = WenoEps<T>::cap(dv(tau5, smallpara + B[1])),
+      q3 = WenoEps<T>::cap(dv(tau5, smallpara + B[2]));
     T w1 = g1 * (T(1) + q1 * q1);
     T w2 = g2 * (T(1) + q2 * q2);
     T w3 = g3 * (T(1) + q3 * q3);
@@ -226,19 +248,19 @@ __device__ __forceinline__ void wenoz_weights(const T B[3], T om[3]) {
 template <class T, int LIM>
 __device__ __forceinline__ void tvd(const T *__restrict__ w, T vm, T vc, T vp, T &vm_out, T &vp_out) {
     const T cf = w[0], cb = w[1];
-    T dqf = T(2) * (vp - vc) / cf;
-    T dqb = T(2) * (vc - vm) / cb;
+    T dqf = dv(T(2) * (vp - vc), cf);
+    T dqb = dv(T(2) * (vc - vm), cb);
     T slope;
     if (LIM == REC_TVD_MM) {
         slope = T(0.5) * (sign1(dqf) + sign1(dqb)) * dmin(dabs(dqf), dabs(dqb));
     } else if (LIM == REC_TVD_VL) {
         T dq2 = dqf * dqb;
         if (dq2 <= T(0)) slope = T(0);
-        else slope = (dq2 * (cf * dqb + cb * dqf) / (dqb * dqb + dqf * dqf + dq2 * (cf + cb - T(2))));
+        else slope = dv(dq2 * (cf * dqb + cb * dqf), dqb * dqb + dqf * dqf + dq2 * (cf + cb - T(2)));
     } else {
         if (dqf == T(0)) slope = T(0);
         else {
-            T v_tvd = dqb / dqf;
+            T v_tvd = dv(dqb, dqf);
             slope = dmax(T(0), dmin3(T(0.5) * (T(1) + v_tvd), cf, cb * v_tvd));
             slope = dqf * slope;
         }
@@ -261,25 +283,25 @@ template <class T>
 __device__ __forceinline__ T signalspeed(T cs, T bn, T bt1, T bt2, T rho) {  // 32-48
     T a2 = cs * cs;
     T a4 = a2 * a2;
-    T b2n = (bn * bn / rho);
-    T b2t1 = (bt1 * bt1 / rho);
-    T b2t2 = (bt2 * bt2 / rho);
+    T b2n = dv(bn * bn, rho);
+    T b2t1 = dv(bt1 * bt1, rho);
+    T b2t2 = dv(bt2 * bt2, rho);
     T b2 = b2n + b2t1 + b2t2;
     T b4 = b2 * b2;
     return dsqrt(T(0.5) * (a2 + b2 + dsqrt(dmax((a4 + b4 + T(2) * b2 * a2) - T(4) * a2 * b2n, T(0)))));
 }
 template <class T> __device__ __forceinline__ T hll_state(T ul, T ur, T fl, T fr, T sl, T sr) {  // 54-59
-    return (sr * ur - sl * ul - (fr - fl)) / (sr - sl);
+    return dv(sr * ur - sl * ul - (fr - fl), sr - sl);
 }
 template <class T> __device__ __forceinline__ T hll_flux(T yl, T yr, T xl, T xr, T sl, T sr) {  // 61-66
-    return (sr * yl - sl * yr + sl * sr * (xr - xl)) / (sr - sl);
+    return dv(sr * yl - sl * yr + sl * sr * (xr - xl), sr - sl);
 }
 template <class T> __device__ __forceinline__ T roe_avg(T xl, T xr, T rhol, T rhor) {  // 68-73
-    return (dsqrt(rhol) * xl + dsqrt(rhor) * xr) / (dsqrt(rhol) + dsqrt(rhor));
+    return dv(dsqrt(rhol) * xl + dsqrt(rhor) * xr, dsqrt(rhol) + dsqrt(rhor));
 }
 template <class T>
 __device__ __forceinline__ T sstar_hllc(T pl, T pr, T rhol, T rhor, T vl, T vr, T sl, T sr, T bl, T br) {  // 86-93
-    return (rhor * vr * (sr - vr) - rhol * vl * (sl - vl) + pl - pr + br * br - bl * bl) / (rhor * (sr - vr) - rhol * (sl - vl));
+    return dv(rhor * vr * (sr - vr) - rhol * vl * (sl - vl) + pl - pr + br * br - bl * bl, rhor * (sr - vr) - rhol * (sl - vl));
 }
 
 // direction -> (normal, transverse) component indices, BUILDSTATES spatial.f90:306-331
@@ -330,14 +352,14 @@ __device__ __forceinline__ void hllc_star(const T *pl, const T *pr, const T *ul,
     u_hll[ivt1] = hll_state(ul[ivt1], ur[ivt1], fl[ivt1], fr[ivt1], sL, sR);
     u_hll[ivt2] = hll_state(ul[ivt2], ur[ivt2], fl[ivt2], fr[ivt2], sL, sR);
     p_hll[ivn] = sstar;
-    p_hll[ivt1] = u_hll[ivt1] / u_hll[irho];
-    p_hll[ivt2] = u_hll[ivt2] / u_hll[irho];
+    p_hll[ivt1] = dv(u_hll[ivt1], u_hll[irho]);
+    p_hll[ivt2] = dv(u_hll[ivt2], u_hll[irho]);
     const bool left = (sstar >= T(0));
     const T *pS = left ? pl : pr;
     const T *uS = left ? ul : ur;
     const T *fS = left ? fl : fr;
     const T s = left ? sL : sR, pSt = left ? pLt : pRt;
-    us[irho] = uS[irho] * (s - pS[ivn]) / (s - sstar);
+    us[irho] = dv(uS[irho] * (s - pS[ivn]), s - sstar);
     T vb = pS[ibx] * pS[ivx] + pS[iby] * pS[ivy] + pS[ibz] * pS[ivz];
     T vbhll = u_hll[ibx] * p_hll[ivx] + u_hll[iby] * p_hll[ivy] + u_hll[ibz] * p_hll[ivz];
     T ps = pS[irho] * (s - pS[ivn]) * (sstar - pS[ivn]) + pSt;
@@ -345,9 +367,9 @@ __device__ __forceinline__ void hllc_star(const T *pl, const T *pr, const T *ul,
     us[ibt1] = u_hll[ibt1];
     us[ibt2] = u_hll[ibt2];
     us[ivn] = us[irho] * sstar;
-    us[ivt1] = (uS[ivt1] * (s - pS[ivn]) - (us[ibn] * us[ibt1] - pS[ibn] * pS[ibt1])) / (s - sstar);
-    us[ivt2] = (uS[ivt2] * (s - pS[ivn]) - (us[ibn] * us[ibt2] - pS[ibn] * pS[ibt2])) / (s - sstar);
-    us[itau] = (uS[itau] * (s - pS[ivn]) + (ps * sstar - pSt * pS[ivn]) - ((vbhll * us[ibn] - vb * pS[ibn]))) / (s - sstar);
+    us[ivt1] = dv(uS[ivt1] * (s - pS[ivn]) - (us[ibn] * us[ibt1] - pS[ibn] * pS[ibt1]), s - sstar);
+    us[ivt2] = dv(uS[ivt2] * (s - pS[ivn]) - (us[ibn] * us[ibt2] - pS[ibn] * pS[ibt2]), s - sstar);
+    us[itau] = dv(uS[itau] * (s - pS[ivn]) + (ps * sstar - pSt * pS[ivn]) - ((vbhll * us[ibn] - vb * pS[ibn])), s - sstar);
 #pragma unroll
     for (int i = 1; i <= 8; ++i) fo[i] = fS[i] + s * (us[i] - uS[i]);
 }
@@ -363,11 +385,11 @@ __device__ __forceinline__ void hlld_star(const T *pl, const T *pr, const T *ul,
     T usL[9], usR[9], pstL[9], pstR[9];
     T sM = sstar_hllc(pLt, pRt, pl[irho], pr[irho], pl[ivn], pr[ivn], sL, sR, pl[ibn], pr[ibn]);
 #pragma unroll
-    for (int i = irho; i <= itau; ++i) usL[i] = ul[i] * (sL - pl[ivn]) / (sL - sM);
+    for (int i = irho; i <= itau; ++i) usL[i] = dv(ul[i] * (sL - pl[ivn]), sL - sM);
 #pragma unroll
-    for (int i = irho; i <= itau; ++i) usR[i] = ur[i] * (sR - pr[ivn]) / (sR - sM);
-    T sstarL = sM - dabs(pl[ibn]) / dsqrt(usL[irho]);
-    T sstarR = sM + dabs(pr[ibn]) / dsqrt(usR[irho]);
+    for (int i = irho; i <= itau; ++i) usR[i] = dv(ur[i] * (sR - pr[ivn]), sR - sM);
+    T sstarL = sM - dv(dabs(pl[ibn]), dsqrt(usL[irho]));
+    T sstarR = sM + dv(dabs(pr[ibn]), dsqrt(usR[irho]));
     if (((sstarL - sL) < T(1.0e-4) * (sM - sL)) || ((sstarR - sR) > -T(1.0e-4) * (sR - sM))) {
         usL[ibn] = pl[ibn];
         usL[ibt1] = hll_state(pl[ibt1], pr[ibt1], fl[ibt1], fr[ibt1], sL, sR);
@@ -380,33 +402,33 @@ __device__ __forceinline__ void hlld_star(const T *pl, const T *pr, const T *ul,
     } else {
         T fac_1 = (pl[irho] * (sL - pl[ivn]) * (sL - sM) - pl[ibn] * pl[ibn]);
         usL[ibn] = pl[ibn];
-        usL[ibt1] = (pl[ibt1] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
-        usL[ibt2] = (pl[ibt2] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
+        usL[ibt1] = dv(pl[ibt1] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn]), fac_1);
+        usL[ibt2] = dv(pl[ibt2] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn]), fac_1);
         fac_1 = (pr[irho] * (sR - pr[ivn]) * (sR - sM) - pr[ibn] * pr[ibn]);
         usR[ibn] = pr[ibn];
-        usR[ibt1] = (pr[ibt1] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
-        usR[ibt2] = (pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
+        usR[ibt1] = dv(pr[ibt1] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn]), fac_1);
+        usR[ibt2] = dv(pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn]), fac_1);
     }
     usL[ivn] = usL[irho] * sM;
-    usL[ivt1] = usL[ivt1] - (usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1]) / (sL - sM);
-    usL[ivt2] = usL[ivt2] - (usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2]) / (sL - sM);
+    usL[ivt1] = usL[ivt1] - dv(usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1], sL - sM);
+    usL[ivt2] = usL[ivt2] - dv(usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2], sL - sM);
     usR[ivn] = usR[irho] * sM;
-    usR[ivt1] = usR[ivt1] - (usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1]) / (sR - sM);
-    usR[ivt2] = usR[ivt2] - (usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2]) / (sR - sM);
+    usR[ivt1] = usR[ivt1] - dv(usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1], sR - sM);
+    usR[ivt2] = usR[ivt2] - dv(usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2], sR - sM);
     pstL[ivn] = sM;
-    pstL[ivt1] = usL[ivt1] / usL[irho];
-    pstL[ivt2] = usL[ivt2] / usL[irho];
+    pstL[ivt1] = dv(usL[ivt1], usL[irho]);
+    pstL[ivt2] = dv(usL[ivt2], usL[irho]);
     pstR[ivn] = sM;
-    pstR[ivt1] = usR[ivt1] / usR[irho];
-    pstR[ivt2] = usR[ivt2] / usR[irho];
+    pstR[ivt1] = dv(usR[ivt1], usR[irho]);
+    pstR[ivt2] = dv(usR[ivt2], usR[irho]);
     T pLs = pl[irho] * (sL - pl[ivn]) * (sM - pl[ivn]) + pLt;
     T pRs = pr[irho] * (sR - pr[ivn]) * (sM - pr[ivn]) + pRt;
     T bdotu = pl[ibx] * pl[ivx] + pl[iby] * pl[ivy] + pl[ibz] * pl[ivz];
     T bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
-    usL[itau] = usL[itau] + ((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn]) / (sL - sM);
+    usL[itau] = usL[itau] + dv((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn], sL - sM);
     bdotu = pr[ibx] * pr[ivx] + pr[iby] * pr[ivy] + pr[ibz] * pr[ivz];
     bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
-    usR[itau] = usR[itau] + ((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn]) / (sR - sM);
+    usR[itau] = usR[itau] + dv((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn], sR - sM);
     if (sstarL >= T(0)) {
 #pragma unroll
         for (int i = 1; i <= 8; ++i) fo[i] = fl[i] + sL * (usL[i] - ul[i]);
@@ -482,12 +504,12 @@ __device__ __forceinline__ void hlld_lean(const T *pl, const T *pr, T epsL, T ep
         cons_state<T>(pl, epsL, ul);
         cons_state<T>(pr, epsR, ur);
 #pragma unroll
-        for (int i = irho; i <= itau; ++i) usL[i] = ul[i] * (sL - pl[ivn]) / (sL - sM);
+        for (int i = irho; i <= itau; ++i) usL[i] = dv(ul[i] * (sL - pl[ivn]), sL - sM);
 #pragma unroll
-        for (int i = irho; i <= itau; ++i) usR[i] = ur[i] * (sR - pr[ivn]) / (sR - sM);
+        for (int i = irho; i <= itau; ++i) usR[i] = dv(ur[i] * (sR - pr[ivn]), sR - sM);
     }
-    T sstarL = sM - dabs(pl[ibn]) / dsqrt(usL[irho]);
-    T sstarR = sM + dabs(pr[ibn]) / dsqrt(usR[irho]);
+    T sstarL = sM - dv(dabs(pl[ibn]), dsqrt(usL[irho]));
+    T sstarR = sM + dv(dabs(pr[ibn]), dsqrt(usR[irho]));
     if (((sstarL - sL) < T(1.0e-4) * (sM - sL)) || ((sstarR - sR) > -T(1.0e-4) * (sR - sM))) {
         const T flt1 = (pl[ivn] * pl[ibt1] - pl[ivt1] * pl[ibn]), frt1 = (pr[ivn] * pr[ibt1] - pr[ivt1] * pr[ibn]);
         const T flt2 = (pl[ivn] * pl[ibt2] - pl[ivt2] * pl[ibn]), frt2 = (pr[ivn] * pr[ibt2] - pr[ivt2] * pr[ibn]);
@@ -502,33 +524,33 @@ __device__ __forceinline__ void hlld_lean(const T *pl, const T *pr, T epsL, T ep
     } else {
         T fac_1 = (pl[irho] * (sL - pl[ivn]) * (sL - sM) - pl[ibn] * pl[ibn]);
         usL[ibn] = pl[ibn];
-        usL[ibt1] = (pl[ibt1] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
-        usL[ibt2] = (pl[ibt2] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn])) / fac_1;
+        usL[ibt1] = dv(pl[ibt1] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn]), fac_1);
+        usL[ibt2] = dv(pl[ibt2] * (pl[irho] * (sL - pl[ivn]) * (sL - pl[ivn]) - pl[ibn] * pl[ibn]), fac_1);
         fac_1 = (pr[irho] * (sR - pr[ivn]) * (sR - sM) - pr[ibn] * pr[ibn]);
         usR[ibn] = pr[ibn];
-        usR[ibt1] = (pr[ibt1] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
-        usR[ibt2] = (pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn])) / fac_1;
+        usR[ibt1] = dv(pr[ibt1] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn]), fac_1);
+        usR[ibt2] = dv(pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn]), fac_1);
     }
     usL[ivn] = usL[irho] * sM;
-    usL[ivt1] = usL[ivt1] - (usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1]) / (sL - sM);
-    usL[ivt2] = usL[ivt2] - (usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2]) / (sL - sM);
+    usL[ivt1] = usL[ivt1] - dv(usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1], sL - sM);
+    usL[ivt2] = usL[ivt2] - dv(usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2], sL - sM);
     usR[ivn] = usR[irho] * sM;
-    usR[ivt1] = usR[ivt1] - (usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1]) / (sR - sM);
-    usR[ivt2] = usR[ivt2] - (usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2]) / (sR - sM);
+    usR[ivt1] = usR[ivt1] - dv(usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1], sR - sM);
+    usR[ivt2] = usR[ivt2] - dv(usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2], sR - sM);
     pstL[ivn] = sM;
-    pstL[ivt1] = usL[ivt1] / usL[irho];
-    pstL[ivt2] = usL[ivt2] / usL[irho];
+    pstL[ivt1] = dv(usL[ivt1], usL[irho]);
+    pstL[ivt2] = dv(usL[ivt2], usL[irho]);
     pstR[ivn] = sM;
-    pstR[ivt1] = usR[ivt1] / usR[irho];
-    pstR[ivt2] = usR[ivt2] / usR[irho];
+    pstR[ivt1] = dv(usR[ivt1], usR[irho]);
+    pstR[ivt2] = dv(usR[ivt2], usR[irho]);
     T pLs = pl[irho] * (sL - pl[ivn]) * (sM - pl[ivn]) + pLt;
     T pRs = pr[irho] * (sR - pr[ivn]) * (sM - pr[ivn]) + pRt;
     T bdotu = pl[ibx] * pl[ivx] + pl[iby] * pl[ivy] + pl[ibz] * pl[ivz];
     T bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
-    usL[itau] = usL[itau] + ((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn]) / (sL - sM);
+    usL[itau] = usL[itau] + dv((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn], sL - sM);
     bdotu = pr[ibx] * pr[ivx] + pr[iby] * pr[ivy] + pr[ibz] * pr[ivz];
     bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
-    usR[itau] = usR[itau] + ((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn]) / (sR - sM);
+    usR[itau] = usR[itau] + dv((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn], sR - sM);
     // the side whose fan the face lies in; its flux and state are rebuilt here
     const bool left = (sstarL >= T(0)) || !(sstarR <= T(0)) && (sM >= T(0));
     const T *pS = left ? pl : pr;
