@@ -174,11 +174,12 @@ def reference_arm(args):
     return 0
 
 
-def batch_specs(precision, t_end=0.1):
+def batch_specs(precision, t_end=0.1, count=512):
     """The batched workload: 512 seeded 1D Riemann problems, n log-uniform in
-    [128, 4096] (seed 20261203), HLLD + PPM, CFL 0.8, t_end 0.1."""
+    [128, 4096] (seed 20261203), HLLD + PPM, CFL 0.8, t_end 0.1 (the first
+    `count` of them for profiler runs)."""
     from cumc3d_b200 import models
-    params = models.batch_problems(512)
+    params = models.batch_problems(512)[:count]
     return params, [models.riemann_1d(p["n"], p["left"], p["right"], p["bx"], t_end=t_end, precision=precision)
                     for p in params]
 
@@ -188,7 +189,7 @@ def bench_batch(args, world, rank, local, dist):
     import torch
 
     from cumc3d_b200 import engine
-    params, probs = batch_specs(args.precision)
+    params, probs = batch_specs(args.precision, count=args.batch_problems)
     b = engine.BatchSolver([sp for sp, _, _ in probs], positivity_fallback=1)
 
     def upload():
@@ -266,7 +267,7 @@ def bench_batch(args, world, rank, local, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-            "config": {"workload": "batch1d_512_riemann_ppm_hlld_cfl0.8_t0.1", "problems": 512,
+            "config": {"workload": "batch1d_512_riemann_ppm_hlld_cfl0.8_t0.1", "problems": len(params),
                        "n_range": [128, 4096], "seed": 20261203, "precision": args.precision,
                        "positivity_fallback": 1,
                        "step": "one whole batched run: INITIAL_UPDATE + every problem's time loop",
@@ -467,6 +468,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blast3d", choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus"])
     ap.add_argument("--recon-c", default=None, help="reconstruction of the briowu/alfven3d/torus workloads")
+    ap.add_argument("--batch-problems", type=int, default=512,
+                    help="batch1d: run only the first N problems (profiler runs); the workload is 512")
     ap.add_argument("--learned-params", default=os.path.join(ROOT, "cumc3d_b200", "data", "flag_mlp.npy"),
                     help="trained flag network for the FP32+learned form of the alfven3d workload")
     ap.add_argument("--n", type=int, default=256)
@@ -551,7 +554,11 @@ def main():
     peak_gbs, peak_kind = load_peaks()
     if dominant.startswith("flux"):
         bytes_launch = FLUX_BYTES_PER_ZONE * zones
-        kname = "k_flux<%s,%s,%s>" % (dominant[-1], args.recon, args.riemann)
+        if tuning.get("split", True):
+            kname = "%s + k_riemann, %s sweep (%s, %s)" % ("k_recon_tile" if tuning.get("recon_tile") else "k_recon",
+                                                           dominant[-1], args.recon, args.riemann)
+        else:
+            kname = "k_flux<%s,%s,%s>" % (dominant[-1], args.recon, args.riemann)
     else:
         bytes_launch = None
         kname = dominant
@@ -568,6 +575,15 @@ def main():
                 "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peak_kind,
                 "avg_launch_ms": avg_ms, "class_ms_per_step": {k: v / args.profile_steps for k, v in prof.items()}}
+    fp64_pipe = None
+    fpath = os.path.join(ROOT, "profiles", "fp64_pipe.json")
+    if os.path.exists(fpath) and args.precision == "fp64":
+        with open(fpath) as f:
+            fp64_pipe = json.load(f).get("%s/%s/fp64" % (args.recon, args.riemann))
+    if fp64_pipe is not None:
+        roofline["fp64_pipe_frac_ncu"] = fp64_pipe
+        roofline["note"] = ("the flux kernels are FP64-pipe bound (fp64_pipe_frac_ncu); the HBM fraction is "
+                            "reported against the algorithmic bytes of a fused pass")
     step_gbs = STEP_BYTES_PER_ZONE * value / world / 1e9
     try:
         fp64_peak = engine.fp64_peak_tflops()
