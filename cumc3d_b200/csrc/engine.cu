@@ -1460,6 +1460,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
         {1, 256, 128, 1, 0}, {1, 256, 128, 4, 0}, {1, 128, 128, 1, 0}, {1, 128, 128, 4, 0},
         {1, 256, 64, 1, 0},  {1, 128, 64, 4, 0},  {0, 256, 128, 1, 0},
         {1, 256, 128, 1, 1}, {1, 256, 128, 4, 1}, {1, 256, 128, 1, 2}, {1, 256, 128, 4, 2},
+        {1, 256, 128, 5, 1}, {1, 256, 128, 6, 1}, {1, 256, 128, 5, 2}, {1, 256, 128, 6, 2},
     };
     const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
     double best = 1e300;
@@ -1507,7 +1508,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
 int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
     if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 256 || (choice[1] & 31) ||
-        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4) ||
+        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4 && choice[3] != 5 && choice[3] != 6) ||
         choice[4] < 0 || choice[4] > 2)
         return fail(h, CUMC_EINVAL, "tuning out of range");
     h->d.recon_tile = choice[4];

@@ -32,8 +32,12 @@ static void launch_learned_dir(const Dev &d, int rs, int stage, cudaStream_t s) 
     else k_recon_flagged<DIR, 0><<<(tiles + 1) / 2, 256, 0, s>>>(d, stage);
     dim3 g, b;
     split_dims(d, DIR, false, g, b);
-    if (d.riemann_minb == 4) launch_riemann_m<float, DIR, 4>(d, rs, g, b, s);
-    else launch_riemann_m<float, DIR, 1>(d, rs, g, b, s);
+    switch (d.riemann_minb) {
+        case 4: launch_riemann_m<float, DIR, 4>(d, rs, g, b, s); break;
+        case 5: launch_riemann_m<float, DIR, 5>(d, rs, g, b, s); break;
+        case 6: launch_riemann_m<float, DIR, 6>(d, rs, g, b, s); break;
+        default: launch_riemann_m<float, DIR, 1>(d, rs, g, b, s); break;
+    }
 }
 
 void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStream_t s) {

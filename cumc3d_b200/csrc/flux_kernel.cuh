@@ -370,8 +370,12 @@ static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s) {
     if (d.wuni[DIR]) launch_recon_u<T, DIR, 1>(d, rec, g, b, s);
     else launch_recon_u<T, DIR, 0>(d, rec, g, b, s);
     split_dims(d, DIR, false, g, b);
-    if (d.riemann_minb == 4) launch_riemann_m<T, DIR, 4>(d, rs, g, b, s);
-    else launch_riemann_m<T, DIR, 1>(d, rs, g, b, s);
+    switch (d.riemann_minb) {
+        case 4: launch_riemann_m<T, DIR, 4>(d, rs, g, b, s); break;
+        case 5: launch_riemann_m<T, DIR, 5>(d, rs, g, b, s); break;
+        case 6: launch_riemann_m<T, DIR, 6>(d, rs, g, b, s); break;
+        default: launch_riemann_m<T, DIR, 1>(d, rs, g, b, s); break;
+    }
 }
 template <class T>
 static void launch_split_t(const Dev &d, int dir, int rec, int rs, cudaStream_t s) {

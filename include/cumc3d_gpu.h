@@ -185,7 +185,7 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
  * shapes of the face-flux kernels (fused or split recon/Riemann, threads per
  * block, register budget of the Riemann kernel) on the handle's live state and
  * keeps the fastest for all later steps.  choice_out[0..4] = (split?, recon
- * threads/block, Riemann threads/block, Riemann min blocks/SM, staged
+ * threads/block, Riemann threads/block, Riemann min blocks/SM (1, 4, 5, 6), staged
  * reconstruction: 0 = per-cell loads, 1 or 2 = stencils staged in shared
  * memory with that many cells per thread); best_ms_out = the flux time of
  * one stage with that choice.  Either pointer may be NULL. */
