@@ -383,8 +383,9 @@ def bench_config(args, world, rank, local, dist):
             P = np.load(lp)
 
             def setup(s, P=P):
-                s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5, flag_interval=4)
+                s.learn_set(P, threshold=0.0, audit_interval=20, audit_tol=1e-5, flag_interval=4)
             forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
+            forms.append(("fp64+learned", dict(spec, precision="fp64", learned=1), setup))
         clocks.start()
         for name_f, sp, setup in forms:
             s, k, t_ms = _evolve_timed(engine, torch, sp, prim, eps, args.warmup, t_end=spec["t_end"], setup=setup)
@@ -428,7 +429,14 @@ def bench_config(args, world, rank, local, dist):
                 "learned_params": os.path.relpath(lp, ROOT),
             })
             extra["learned_over_fp64"] = extra["learned_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
-            extra["max_divb"]["fp32+learned"] = o["divb"]
+            o64 = out["fp64+learned"]
+            l1_64 = rel_l1(o64["cons"], out["fp64"]["cons"])
+            extra.update({
+                "fp64_learned_zone_updates_per_s": zones * o64["steps"] / (o64["ms"] * 1e-3),
+                "l1_fp64_learned_vs_fp64_max": max(l1_64),
+                "fp64_learned_flagged_fraction_at_audits": o64["stats"]["flagged"] / max(1, o64["stats"]["audited"]),
+            })
+            extra["fp64_learned_over_fp64"] = extra["fp64_learned_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
         key = args.precision
         n, ms = out[key]["steps"], out[key]["ms"]
         name = "alfven3d_%d^3_%s_%s_cfl0.4_one_period" % (n3, recon, args.riemann)

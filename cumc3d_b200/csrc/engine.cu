@@ -861,8 +861,9 @@ static void default_flux_blocks(cumc_handle *h) {
 
 static void launch_flux(cumc_handle *h, int dir, int stage = 1) {
     const Dev &d = h->d;
-    if (d.learned) {  // FP32 WENO with the learned smooth-face flag (split kernels)
-        launch_split_learned_fp32(d, dir, h->cfg.riemann, stage, h->stream);
+    if (d.learned) {  // WENO with the learned smooth-face flag (split kernels)
+        if (h->cfg.precision == CUMC_FP32) launch_split_learned_fp32(d, dir, h->cfg.riemann, stage, h->stream);
+        else launch_split_learned_fp64(d, dir, h->cfg.riemann, stage, h->stream);
         h->launches += 2;
         return;
     }
@@ -1066,8 +1067,8 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     if (cfg->recon < 0 || cfg->recon > 4 || cfg->riemann < 0 || cfg->riemann > 3 || cfg->precision < 0 || cfg->precision > 1)
         return fail(nullptr, CUMC_EINVAL, "bad recon/riemann/precision option");
     if (!cfg->xF || !cfg->yF || !cfg->zF) return fail(nullptr, CUMC_EINVAL, "face coordinates missing");
-    if (cfg->learned && (cfg->precision != CUMC_FP32 || cfg->recon != CUMC_RECON_WENO))
-        return fail(nullptr, CUMC_EINVAL, "the learned smooth-face flag needs the FP32 form with WENO reconstruction");
+    if (cfg->learned && cfg->recon != CUMC_RECON_WENO)
+        return fail(nullptr, CUMC_EINVAL, "the learned smooth-face flag needs WENO reconstruction");
     const int nn[3] = {nx, ny, nz};
     for (int a = 0; a < 3; ++a) {
         int fi = cfg->boundary_flag[2 * a], fo = cfg->boundary_flag[2 * a + 1];

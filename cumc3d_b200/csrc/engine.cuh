@@ -88,6 +88,8 @@ void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 bl
 void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
 void launch_split_fp32(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
 void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStream_t s);
+void launch_split_learned_fp64(const Dev &d, int dir, int rs, int stage, cudaStream_t s);
+void launch_learned_flags(const Dev &d, int dir, int stage, cudaStream_t s);
 long long learned_tiles(const Dev &d, int dir);
 
 }  // namespace cumc

@@ -22,14 +22,23 @@ template <int DIR>
 static void launch_learned_dir(const Dev &d, int rs, int stage, cudaStream_t s) {
     const unsigned tiles = (unsigned)learned_tiles(d, DIR);
     if (stage == 1) {
-        // the network kernel (persistent, 4 CTAs per SM) runs on refresh steps,
-        // the flag kernel on the others; whichever does not apply exits at once
+        // the network kernel (persistent, 4 CTAs per SM) runs on refresh
+        // stages, the staged flag kernel on the others; whichever does not
+        // apply exits at once
         const unsigned pg = tiles < (unsigned)(4 * d.num_sms) ? tiles : (unsigned)(4 * d.num_sms);
-        if (d.wuni[DIR]) k_recon_learned<DIR, 1><<<pg, 128, 0, s>>>(d, stage);
-        else k_recon_learned<DIR, 0><<<pg, 128, 0, s>>>(d, stage);
+        if (d.wuni[DIR]) k_recon_learned<DIR, 1, 1><<<pg, 128, 0, s>>>(d, stage);
+        else k_recon_learned<DIR, 0, 1><<<pg, 128, 0, s>>>(d, stage);
     }
-    if (d.wuni[DIR]) k_recon_flagged<DIR, 1><<<(tiles + 1) / 2, 256, 0, s>>>(d, stage);
-    else k_recon_flagged<DIR, 0><<<(tiles + 1) / 2, 256, 0, s>>>(d, stage);
+    const dim3 tb(32, 8, 1);
+    if (d.recon_tile == 1) {
+        const dim3 g = recon_tile_grid(d, DIR, 1);
+        if (d.wuni[DIR]) k_recon_tile<float, DIR, REC_WENO, 1, 1, 1><<<g, tb, 0, s>>>(d, stage);
+        else k_recon_tile<float, DIR, REC_WENO, 0, 1, 1><<<g, tb, 0, s>>>(d, stage);
+    } else {
+        const dim3 g = recon_tile_grid(d, DIR, 2);
+        if (d.wuni[DIR]) k_recon_tile<float, DIR, REC_WENO, 1, 2, 1><<<g, tb, 0, s>>>(d, stage);
+        else k_recon_tile<float, DIR, REC_WENO, 0, 2, 1><<<g, tb, 0, s>>>(d, stage);
+    }
     dim3 g, b;
     split_dims(d, DIR, false, g, b);
     switch (d.riemann_minb) {
@@ -38,6 +47,21 @@ static void launch_learned_dir(const Dev &d, int rs, int stage, cudaStream_t s) 
         case 6: launch_riemann_m<float, DIR, 6>(d, rs, g, b, s); break;
         default: launch_riemann_m<float, DIR, 1>(d, rs, g, b, s); break;
     }
+}
+
+// the flags-only network kernel of the FP64 form (refresh stages)
+template <int DIR>
+static void launch_flags_dir(const Dev &d, int stage, cudaStream_t s) {
+    const unsigned tiles = (unsigned)learned_tiles(d, DIR);
+    const unsigned pg = tiles < (unsigned)(4 * d.num_sms) ? tiles : (unsigned)(4 * d.num_sms);
+    if (d.wuni[DIR]) k_recon_learned<DIR, 1, 0><<<pg, 128, 0, s>>>(d, stage);
+    else k_recon_learned<DIR, 0, 0><<<pg, 128, 0, s>>>(d, stage);
+}
+void launch_learned_flags(const Dev &d, int dir, int stage, cudaStream_t s) {
+    if (stage != 1) return;
+    if (dir == 0) launch_flags_dir<0>(d, stage, s);
+    else if (dir == 1) launch_flags_dir<1>(d, stage, s);
+    else launch_flags_dir<2>(d, stage, s);
 }
 
 void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStream_t s) {

@@ -14,7 +14,8 @@
 //      the plain FP32 form), flagged cells also evaluate the linear values,
 //      and the tile is marked to fall back until the next audit if any
 //      flagged cell's relative face-value error exceeds audit_tol.
-// All other stages, k_recon_flagged: the stored flags of the cell and of its
+// All other stages, k_recon_tile<float, DIR, REC_WENO, UNI, CPT, 1>: the
+// staged reconstruction, where the stored flags of the cell and of its
 // neighbours within two cells along the sweep choose linear or WENO-Z per
 // warp, without running the network.
 //
@@ -129,10 +130,9 @@ __device__ __forceinline__ long long learned_total(const Dev &d) {
     return ex * ey * ez;
 }
 
-// Steps on which the network runs: every flag_interval steps, stage 1.
-__device__ __forceinline__ bool learned_refresh(const Dev &d, int stage) {
-    return stage == 1 && (d.flag_interval <= 1 || (d.S->steps % d.flag_interval) == 0);
-}
+// Steps on which the network runs: stage 1 of every flag_interval-th step
+// (learned_refresh_stage, recon_tile.cuh).  Audits are taken there too: set
+// audit_interval to a multiple of flag_interval.
 __device__ __forceinline__ bool learned_audit(const Dev &d) {
     return d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
 }
@@ -140,9 +140,27 @@ __device__ __forceinline__ bool learned_audit(const Dev &d) {
 // Network + reconstruction, persistent: each CTA allocates tensor memory and
 // loads the weights once, then walks tiles blockIdx.x, +gridDim.x, ...
 // Runs on refresh stages only (uniform early exit otherwise).
-template <int DIR, int UNI>
+// largest relative change the linear weights make to the 7 face pairs of a
+// cell (FP32), for the audit of the flags-only network kernel
+__device__ __forceinline__ float learned_linear_change(const float *w, float a[LEARN_NV][5]) {
+    float err = 0.0f;
+#pragma unroll
+    for (int v = 0; v < LEARN_NV; ++v) {
+        float vm, vp, lm, lp;
+        weno<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], vm, vp);
+        weno_linear<float>(w, a[v][0], a[v][1], a[v][2], a[v][3], a[v][4], lm, lp);
+        const float den = fabsf(a[v][2]) + 1.0e-30f;
+        err = fmaxf(err, fmaxf(fabsf(lm - vm), fabsf(lp - vp)) / den);
+    }
+    return err;
+}
+
+// RECON = 1: the FP32 form (network + FP32 reconstruction of the refresh
+// stage).  RECON = 0: flags (and the audit verdict) only, for the FP64 form,
+// whose reconstruction runs in k_recon_tile<double, ..., LRN = 2>.
+template <int DIR, int UNI, int RECON>
 __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d, int stage) {
-    if (d.S->done || !learned_refresh(d, stage)) return;
+    if (d.S->done || !learned_refresh_stage(d, stage)) return;
     __shared__ MlpTile tile;
     __shared__ float s_err[4];
     __shared__ int s_flag[4];
@@ -183,7 +201,8 @@ __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d, int stage
         const bool warp_all = __all_sync(0xffffffffu, flag && inner);
         const bool linear = warp_all && !audit && d.lfb[DIR][tl] == 0;
         float err = 0.0f;
-        learned_reconstruct(d, q, w, a, linear, audit && flag && inner, err);
+        if (RECON) learned_reconstruct(d, q, w, a, linear, audit && flag && inner, err);
+        else if (audit && flag && inner) err = learned_linear_change(w, a);
         if (audit) {
             // tile verdict: the largest error of a flagged cell against the tolerance
             float e = err;
@@ -215,70 +234,6 @@ __global__ void __launch_bounds__(128, 4) k_recon_learned(const Dev d, int stage
         }
     }
     mlp_tile_teardown(tile);
-}
-
-// Every other stage: the flags of the last network run, dilated by two cells
-// along the sweep (the state moves less than half a cell per step at the
-// CFL numbers of the workloads, so two cells cover the steps between runs;
-// transverse motion is left to the audit).  On audit steps every cell uses
-// WENO-Z; on the stage-1 audit the tile verdict is taken as above.
-template <int DIR, int UNI>
-__global__ void __launch_bounds__(256) k_recon_flagged(const Dev d, int stage) {
-    if (d.S->done || learned_refresh(d, stage)) return;
-    __shared__ float s_err[8];
-    __shared__ int s_flag[8];
-    const long long total = learned_total<DIR>(d);
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const LearnedCell q = learned_cell<DIR>(d, t0, total);
-    const long long sweep = (DIR == 0) ? 1 : (DIR == 1) ? (long long)d.nx : (long long)d.nx * d.ny;
-    const bool inner = q.c >= 2 && q.c <= q.ns - 1;
-    const bool audit = learned_audit(d);
-    bool flag = false;
-    if (q.valid && inner) {
-        const unsigned char *f = d.lflag[DIR];
-        // c-2 .. c+2 lie within 0 .. n+1, the cells of the enumeration
-        flag = f[q.t] && f[q.t - sweep] && f[q.t + sweep] && f[q.t - 2 * sweep] && f[q.t + 2 * sweep];
-    }
-    const bool linear = __all_sync(0xffffffffu, flag && d.lfb[DIR][q.t >> 7] == 0) && !audit;
-    float w[14];
-    learned_weights<DIR, UNI>(d, q.c, w);
-    float a[LEARN_NV][5];
-    learned_stencils<DIR>(d, q, a);
-    float err = 0.0f;
-    const bool verdict = audit && stage == 1;
-    learned_reconstruct(d, q, w, a, linear, verdict && flag, err);
-    if (verdict) {
-        // two 128-cell tiles per CTA: warps 0-3 and 4-7
-        const int tid = threadIdx.x;
-        float e = err;
-        int nf = flag ? 1 : 0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
-            nf += __shfl_xor_sync(0xffffffffu, nf, o);
-        }
-        if ((tid & 31) == 0) {
-            s_err[tid >> 5] = e;
-            s_flag[tid >> 5] = nf;
-        }
-        __syncthreads();
-        if ((tid & 127) == 0) {
-            const int h = tid >> 7;
-            const long long tl = (long long)blockIdx.x * 2 + h;
-            if (tl * 128 < total) {
-                const float te = fmaxf(fmaxf(s_err[4 * h], s_err[4 * h + 1]), fmaxf(s_err[4 * h + 2], s_err[4 * h + 3]));
-                const int tf = s_flag[4 * h] + s_flag[4 * h + 1] + s_flag[4 * h + 2] + s_flag[4 * h + 3];
-                const unsigned char fb = te > d.audit_tol ? 1 : 0;
-                d.lfb[DIR][tl] = fb;
-                const long long nvalid = total - tl * 128;
-                unsigned long long *ls = d.lstats + (tl & (LEARN_STAT_SLOTS - 1)) * LEARN_STAT_FIELDS;
-                atomicAdd(&ls[0], (unsigned long long)(nvalid < 128 ? nvalid : 128));
-                atomicAdd(&ls[1], (unsigned long long)tf);
-                atomicAdd(&ls[2], (unsigned long long)fb);
-                if (tl == 0 && DIR == 0) atomicAdd(&ls[3], 1ull);
-            }
-        }
-    }
 }
 
 }  // namespace cumc

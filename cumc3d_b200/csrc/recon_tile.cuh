@@ -15,9 +15,20 @@
 
 namespace cumc {
 
-template <class T, int DIR, int REC, int UNI, int CPT>
-__global__ void __launch_bounds__(256) k_recon_tile(const Dev d) {
+// LRN = 1 (FP32 WENO with the learned flag, stages the network does not
+// run) or 2 (FP64 WENO with the learned flag, every stage; the network only
+// sets the flags): a warp whose 32 cells carry the stored flag, dilated by
+// two cells along the sweep, in 128-cell tiles not marked to fall back,
+// reconstructs with the linear optimal weights (recon_learned.cuh).  With
+// no cell flagged the arithmetic is that of LRN = 0.
+__device__ __forceinline__ bool learned_refresh_stage(const Dev &d, int stage) {
+    return stage == 1 && (d.flag_interval <= 1 || (d.S->steps % d.flag_interval) == 0);
+}
+
+template <class T, int DIR, int REC, int UNI, int CPT, int LRN = 0>
+__global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) {
     if (d.S->done) return;
+    if (LRN == 1 && learned_refresh_stage(d, stage)) return;  // the network kernel reconstructs this stage
     constexpr int TX = 32, TY = 8;
     constexpr int H = (REC == REC_PPM || REC == REC_WENO) ? 2 : 1;
     constexpr int NR = TY * CPT;                    // rows of reconstructed cells
@@ -75,6 +86,23 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d) {
             c = c0 + r; l = c; j = blockIdx.x * TX + tx + 1; k = blockIdx.z + 1; ns = d.nz;
             valid = j <= d.nx && c <= d.nz + 1;
         }
+        bool linear = false;
+        if (LRN) {
+            // the flat index of this cell in the sweep's enumeration (x fastest)
+            long long t, sweep;
+            if (DIR == 0) { t = c + (long long)(d.nx + 2) * ((k - 1) + (long long)d.ny * (l - 1)); sweep = 1; }
+            else if (DIR == 1) { t = (j - 1) + (long long)d.nx * (c + (long long)(d.ny + 2) * (l - 1)); sweep = d.nx; }
+            else { t = (j - 1) + (long long)d.nx * ((k - 1) + (long long)d.ny * c); sweep = (long long)d.nx * d.ny; }
+            bool ok = false;
+            const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
+            if (valid && c >= 2 && c <= ns - 1 && !audit) {
+                const unsigned char *f = d.lflag[DIR];
+                // c-2 .. c+2 lie within 0 .. n+1, the cells of the enumeration
+                ok = f[t] && f[t - sweep] && f[t + sweep] && f[t - 2 * sweep] && f[t + 2 * sweep] &&
+                     d.lfb[DIR][t >> 7] == 0;
+            }
+            linear = __all_sync(0xffffffffu, ok);
+        }
         if (!valid) continue;
         const int ci = cidx(d, j, k, l);
         T w[14];
@@ -97,7 +125,8 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d) {
             if (H == 2) { a0 = at(-2); a4 = at(2); }
             const T a1 = at(-1), a2 = at(0), a3 = at(1);
             T vm, vp;
-            recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
+            if (LRN && linear) weno_linear<T>(w, a0, a1, a2, a3, a4, vm, vp);
+            else recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
             if (v == 0) { vm_rho = vm; vp_rho = vp; }
             if (v == 4 && d.pos_fallback) {
                 fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));

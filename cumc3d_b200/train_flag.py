@@ -1,8 +1,9 @@
 """Train the learned smooth-face flag from the plain method's own runs.
 
 Samples come from FP64 WENO runs of the engine itself (the plain form): a
-circularly polarised Alfven wave (smooth) and a magnetised blast (shocks,
-contacts, smooth ambient), several snapshots each, all three sweeps.  Each
+circularly polarised Alfven wave (smooth) at 64^3, 128^3 and 256^3 and a
+magnetised blast (shocks, contacts, smooth ambient) at 64^3 and 128^3,
+several snapshots each, all three sweeps.  Each
 sample holds the 35 features the reconstruction kernel computes and the
 relative change the linear optimal weights would make to the cell's face
 values.  The network is trained on the GPU (cumc_mlp_train) to predict
@@ -40,13 +41,19 @@ def harvest(spec, prim, eps, snapshots, stride):
 
 
 def training_set(n=64, stride=3):
-    sa, pa, ea = models.alfven_3d(n, recon="weno")
-    sb, pb, eb = models.blast_3d(n, radius=0.2, p_in=1.0)
-    sb["positivity_fallback"] = 1
-    sb["fix_periodic_normal_faces"] = 1
-    smooth = harvest(sa, pa, ea, [0, 20, 60], stride)
-    rough = harvest(sb, pb, eb, [10, 30, 60], stride)
-    return smooth, rough
+    """Snapshots at n^3 and at 2n, 4n (strides scaled to keep each grid's
+    share similar): the features of smooth data shift with resolution (the
+    relative variation across a stencil falls as 1/n)."""
+    smooth, rough = [], []
+    for m, st in ((n, stride), (2 * n, 8 * stride), (4 * n, 64 * stride)):
+        sa, pa, ea = models.alfven_3d(m, recon="weno")
+        smooth.append(harvest(sa, pa, ea, [0, 20], st))
+        if m <= 2 * n:
+            sb, pb, eb = models.blast_3d(m, radius=0.2, p_in=1.0)
+            sb["positivity_fallback"] = 1
+            sb["fix_periodic_normal_faces"] = 1
+            rough.append(harvest(sb, pb, eb, [10, 30, 60], st))
+    return np.concatenate(smooth), np.concatenate(rough)
 
 
 def main(argv=None):

@@ -237,7 +237,7 @@ int cumc_batch_sync(cumc_batch *b);
 void *cumc_batch_stream(cumc_batch *b);
 const char *cumc_batch_last_error(cumc_batch *b);
 
-/* ---------------- learned smooth-face flag (FP32 WENO form) ----------------
+/* ---------------- learned smooth-face flag (WENO, FP32 or FP64 form) ----------------
  * No reference counterpart: the reference always applies the WENO-Z
  * nonlinear weights (solver/mhd/weno_module.f90:363-404).  A 35-32-32-1 MLP
  * over scale-free stencil features flags cells whose WENO-Z face values are
@@ -262,7 +262,12 @@ typedef struct cumc_train_config {
     unsigned long long seed;     /* minibatch sampling                         */
 } cumc_train_config;
 /* enable (params != NULL) or disable the flag on a handle created with
- * learned = 1 (FP32 + WENO); resets the fallback tiles and the counters.
+ * learned = 1 (WENO; FP32 form: the network is fused into the FP32
+ * reconstruction of its stage; FP64 form: the network only sets the flags
+ * and the FP64 reconstruction reads them; with no cell flagged the FP64 form
+ * is bit-identical to the plain form); resets the fallback tiles and the
+ * counters.  Audits are taken on refresh steps: set audit_interval to a
+ * multiple of flag_interval.
  * The network runs at stage 1 of every flag_interval-th step (>= 1); the
  * other stages reuse its flags, dilated by two cells along the sweep. */
 int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int flag_interval, int audit_interval,

@@ -190,7 +190,7 @@ def test_trained_flag_keeps_div_b_at_roundoff_on_a_periodic_box(flag_interval):
     s = engine.Solver(sp)
     s.set_state(prim, eps)
     s.initial_update()
-    s.learn_set(P, threshold=0.0, audit_interval=10, audit_tol=1e-5, flag_interval=flag_interval)
+    s.learn_set(P, threshold=0.0, audit_interval=8, audit_tol=1e-5, flag_interval=flag_interval)
     s.evolve(1e30, 30)
     divb = s.find_divb()
     st = s.learn_stats()
@@ -198,3 +198,58 @@ def test_trained_flag_keeps_div_b_at_roundoff_on_a_periodic_box(flag_interval):
     assert st["flagged"] > 0
     # |B| ~ 1, dx = 1/48: roundoff level is ~1e-13
     assert divb < 1e-11, divb
+
+
+def fp64_learned_run(spec, prim, eps, steps, learned):
+    sp = dict(spec, precision="fp64", learned=1)
+    s = engine.Solver(sp)
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.learn_set(**learned)
+    s.evolve(1e30, steps)
+    cons = s.get_array(capi.ARR_CONS)
+    divb = s.find_divb()
+    stats = s.learn_stats()
+    s.close()
+    return cons, divb, stats
+
+
+def plain_fp64(spec, prim, eps, steps):
+    s = engine.Solver(dict(spec, precision="fp64"))
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.evolve(1e30, steps)
+    cons = s.get_array(capi.ARR_CONS)
+    s.close()
+    return cons
+
+
+def test_fp64_learned_without_flags_is_the_plain_form(oracle_mod):
+    """The FP64 form with the flag network but no cell flagged runs the plain
+    FP64 arithmetic: bit-identical to the plain form and to the oracle."""
+    spec, prim, eps = models.alfven_3d(24, recon="weno")
+    cons, _, st = fp64_learned_run(spec, prim, eps, 6, dict(params=flag_all_params(-100.0), threshold=0.0,
+                                                               audit_interval=4, audit_tol=1e-6, flag_interval=2))
+    assert st["flagged"] == 0 and st["audits"] >= 1
+    ref = plain_fp64(spec, prim, eps, 6)
+    assert np.array_equal(interior(cons, spec), interior(ref, spec))
+    o = oracle_mod.Oracle(dict(spec, precision="fp64"))
+    o.set_state(prim, eps)
+    o.initial_update()
+    o.evolve(1e30, 6)
+    assert np.array_equal(interior(cons, spec), interior(o.get_array(capi.ARR_CONS), spec))
+    o.close()
+
+
+def test_fp64_learned_with_trained_flag_stays_close_to_plain():
+    import os
+    P = np.load(os.path.join(os.path.dirname(engine.__file__), "data", "flag_mlp.npy"))
+    spec, prim, eps = models.alfven_3d(48, recon="weno")
+    cons, divb, st = fp64_learned_run(spec, prim, eps, 30, dict(params=P, threshold=0.0, audit_interval=8,
+                                                                  audit_tol=1e-5, flag_interval=4))
+    ref = plain_fp64(spec, prim, eps, 30)
+    a, b = interior(cons, spec).reshape(-1, 8), interior(ref, spec).reshape(-1, 8)
+    l1 = np.abs(a - b).sum(0) / np.abs(b).sum(0)
+    assert st["flagged"] > 0.5 * st["audited"]
+    assert l1.max() < 1e-5, l1
+    assert divb < 1e-11
