@@ -42,6 +42,18 @@ TYPE, BIND(C) :: cumc_config
   TYPE(cumc_model) :: model
 END TYPE
 
+! cumc_batch_config (include/cumc3d_gpu.h): many 1D problems in one launch
+TYPE, BIND(C) :: cumc_batch_config
+  INTEGER(C_INT) :: n_problems
+  TYPE(C_PTR) :: nx             ! INTEGER(C_INT) nx(n_problems)
+  TYPE(C_PTR) :: xF             ! TYPE(C_PTR) xF(n_problems), each -3:nx+3 faces
+  TYPE(C_PTR) :: t_end          ! REAL(C_DOUBLE) t_end(n_problems)
+  REAL(C_DOUBLE) :: cfl, gamma
+  INTEGER(C_INT) :: recon, riemann, precision, floor_kind, positivity_fallback
+END TYPE
+
+INTEGER(C_INT), PARAMETER :: CUMC_LEARN_NP = 2657
+
 INTERFACE
   INTEGER(C_INT) FUNCTION cumc_create(cfg, h) BIND(C, NAME='cumc_create')
     IMPORT :: C_INT, C_PTR, cumc_config
@@ -92,6 +104,44 @@ INTERFACE
   TYPE(C_PTR) FUNCTION cumc_last_error(h) BIND(C, NAME='cumc_last_error')
     IMPORT :: C_PTR
     TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  ! batched 1D problems (the n_dim = 1 build of main.f90, many at once)
+  INTEGER(C_INT) FUNCTION cumc_batch_create(cfg, b) BIND(C, NAME='cumc_batch_create')
+    IMPORT :: C_INT, C_PTR, cumc_batch_config
+    TYPE(cumc_batch_config), INTENT(IN) :: cfg
+    TYPE(C_PTR), INTENT(OUT) :: b
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_batch_set_state(b, p, prim, eps) BIND(C, NAME='cumc_batch_set_state')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: b
+    INTEGER(C_INT), VALUE :: p
+    REAL(C_DOUBLE), INTENT(IN) :: prim(*), eps(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_batch_run(b, max_steps, t, steps, status) BIND(C, NAME='cumc_batch_run')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: b
+    INTEGER(C_INT), VALUE :: max_steps
+    REAL(C_DOUBLE), INTENT(OUT) :: t(*)
+    INTEGER(C_INT), INTENT(OUT) :: steps(*), status(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_batch_get_state(b, p, prim_row, eps_row) BIND(C, NAME='cumc_batch_get_state')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: b
+    INTEGER(C_INT), VALUE :: p
+    REAL(C_DOUBLE), INTENT(OUT) :: prim_row(*), eps_row(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_batch_destroy(b) BIND(C, NAME='cumc_batch_destroy')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: b
+  END FUNCTION
+  ! learned smooth-face flag (a handle created with cfg%learned = 1, WENO)
+  INTEGER(C_INT) FUNCTION cumc_learn_set(h, params, threshold, flag_interval, audit_interval, audit_tol) &
+      BIND(C, NAME='cumc_learn_set')
+    IMPORT :: C_INT, C_PTR, C_FLOAT
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_FLOAT), INTENT(IN) :: params(*)
+    REAL(C_FLOAT), VALUE :: threshold, audit_tol
+    INTEGER(C_INT), VALUE :: flag_interval, audit_interval
   END FUNCTION
 END INTERFACE
 
