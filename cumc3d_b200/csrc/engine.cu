@@ -880,7 +880,9 @@ static void launch_flux(cumc_handle *h, int dir, int stage = 1) {
     else if (dir == 1) g = dim3((d.nx + b.x - 1) / b.x, (d.ny + 1 + TS - 2) / (TS - 1), d.nz);
     else g = dim3((d.nx + b.x - 1) / b.x, (d.nz + 1 + TS - 2) / (TS - 1), d.ny);
     const bool f32 = h->cfg.precision == CUMC_FP32;
-    const size_t smem = 2 * 7 * (size_t)b.x * b.y * (f32 ? sizeof(float) : sizeof(double));
+    // face states of the tile + its staged stencils (2-cell halo along the sweep)
+    const size_t staged = 7 * (size_t)(dir == 0 ? (b.x + 4) * b.y : b.x * (b.y + 4));
+    const size_t smem = (2 * 7 * (size_t)b.x * b.y + staged) * (f32 ? sizeof(float) : sizeof(double));
     if (f32) launch_flux_fp32(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, h->stream);
     else launch_flux_fp64(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, h->stream);
     h->launches++;

@@ -82,6 +82,42 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
     constexpr int tb1 = (DIR == 0) ? 1 : 0;  // bcell index 0..2
     constexpr int tb2 = (DIR == 2) ? 1 : 2;
 
+    // stage the stencils of the tile in shared memory: every state value
+    // loaded and converted once (2-cell halo along the sweep)
+    const int SX = (DIR == 0) ? (int)blockDim.x + 4 : (int)blockDim.x;
+    const int SR = (DIR == 0) ? (int)blockDim.y : (int)blockDim.y + 4;
+    T *sS = sVP + 7 * nthr;  // [7][SR][SX]
+    {
+        const int c0 = (DIR == 0) ? (int)blockIdx.x * (TS - 1) : (int)blockIdx.y * (TS - 1);
+        for (int idx = tid; idx < SR * SX; idx += nthr) {
+            const int sr = idx / SX, sx = idx - sr * SX;
+            int x, y, z;
+            bool ok;
+            if (DIR == 0) {
+                x = c0 - 2 + sx; y = blockIdx.y * blockDim.y + sr + 1; z = blockIdx.z + 1;
+                ok = x <= d.nx + 3 && y <= d.ny;
+            } else if (DIR == 1) {
+                x = blockIdx.x * blockDim.x + sx + 1; y = c0 - 2 + sr; z = blockIdx.z + 1;
+                ok = x <= d.nx && y <= d.ny + 3;
+            } else {
+                x = blockIdx.x * blockDim.x + sx + 1; y = blockIdx.z + 1; z = c0 - 2 + sr;
+                ok = x <= d.nx && z <= d.nz + 3;
+            }
+            if (ok) {
+                const int cc = cidx(d, x, y, z);
+#pragma unroll
+                for (int v = 0; v < 7; ++v) {
+                    const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
+                    sS[(v * SR + sr) * SX + sx] = (T)__ldg(src + cc);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // this cell's stencil c-2 .. c+2 in the staged tile
+    const int sb = (DIR == 0) ? (int)threadIdx.y * SX + ls + 2 : (ls + 2) * SX + (int)threadIdx.x;
+    const int sm = (DIR == 0) ? 1 : SX;
+
     if (rvalid) {
         const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
         T w[14];
@@ -91,15 +127,15 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
         bool fallback = false;
 #pragma unroll
         for (int v = 0; v < 7; ++v) {
-            const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
+            const T *sv = sS + v * SR * SX + sb;
             T a0 = T(0), a4 = T(0);
             if (REC == REC_PPM || REC == REC_WENO) {
-                a0 = (T)__ldg(src + ci - 2 * st);
-                a4 = (T)__ldg(src + ci + 2 * st);
+                a0 = sv[-2 * sm];
+                a4 = sv[2 * sm];
             }
-            T a1 = (T)__ldg(src + ci - st);
-            T a2 = (T)__ldg(src + ci);
-            T a3 = (T)__ldg(src + ci + st);
+            T a1 = sv[-sm];
+            T a2 = sv[0];
+            T a3 = sv[sm];
             T vm, vp;
             recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
             if (v == 4 && d.pos_fallback) {
@@ -109,7 +145,7 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
                 if (fallback) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        const T cv = (T)__ldg(d.P[u] + ci);
+                        const T cv = sS[u * SR * SX + sb];
                         sVM[u * nthr + tid] = cv;
                         sVP[u * nthr + tid] = cv;
                     }
@@ -384,8 +420,18 @@ static void launch_split_t(const Dev &d, int dir, int rec, int rs, cudaStream_t 
     else launch_split_dir<T, 2>(d, rec, rs, s);
 }
 
+template <class T, int DIR, int REC, int RS>
+static void flux_smem(size_t sm) {
+    if (sm > 48 * 1024) cudaFuncSetAttribute(k_flux<T, DIR, REC, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+}
 template <class T, int DIR, int REC>
 static void launch_rs(const Dev &d, int rs, dim3 g, dim3 b, size_t sm, cudaStream_t s) {
+    switch (rs) {
+        case RS_LF: flux_smem<T, DIR, REC, RS_LF>(sm); break;
+        case RS_HLL: flux_smem<T, DIR, REC, RS_HLL>(sm); break;
+        case RS_HLLC: flux_smem<T, DIR, REC, RS_HLLC>(sm); break;
+        default: flux_smem<T, DIR, REC, RS_HLLD>(sm); break;
+    }
     switch (rs) {
         case RS_LF: k_flux<T, DIR, REC, RS_LF><<<g, b, sm, s>>>(d); break;
         case RS_HLL: k_flux<T, DIR, REC, RS_HLL><<<g, b, sm, s>>>(d); break;
