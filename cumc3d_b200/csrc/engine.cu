@@ -420,18 +420,27 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
     const int c = cidx(d, j, k, l);
     const int sy = d.NX, sz = d.NX * d.NY;
     double rho, vx, vy, vz, e, bfx, bfy, bfz, bc[3];
+    // every load of the cell issued before any arithmetic (the kernel waits on
+    // memory, not on its few flops); the lower-face operands of FROMRVETOU are
+    // selected afterwards from loads of both candidates
+    double ux_m = 0.0, uy_m = 0.0, uz_m = 0.0, u_c[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double px_m = d.P[5][c - 1], py_m = d.P[6][c - sy], pz_m = d.P[7][c - sz];
     if (!INIT) {
-        const double *Ux = d.U[5], *Uy = d.U[6], *Uz = d.U[7];
-        bfx = Ux[c]; bfy = Uy[c]; bfz = Uz[c];
-        cell_b(d, j, k, l, bfx, Ux[c - 1], bfy, Uy[c - sy], bfz, Uz[c - sz], bc);
-        const double u0 = d.U[0][c];
+        bfx = d.U[5][c]; bfy = d.U[6][c]; bfz = d.U[7][c];
+        ux_m = d.U[5][c - 1]; uy_m = d.U[6][c - sy]; uz_m = d.U[7][c - sz];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) u_c[i] = d.U[i][c];
+    }
+    if (!INIT) {
+        cell_b(d, j, k, l, bfx, ux_m, bfy, uy_m, bfz, uz_m, bc);
+        const double u0 = u_c[0];
         rho = u0;
-        vx = dv(d.U[1][c], u0);
-        vy = dv(d.U[2][c], u0);
-        vz = dv(d.U[3][c], u0);
+        vx = dv(u_c[1], u0);
+        vy = dv(u_c[2], u0);
+        vz = dv(u_c[3], u0);
         const double bsquare = bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2];
         const double vsquare = vx * vx + vy * vy + vz * vz;
-        e = (d.U[4][c] - 0.5 * bsquare) / u0 - 0.5 * vsquare;
+        e = (u_c[4] - 0.5 * bsquare) / u0 - 0.5 * vsquare;
     } else {
         rho = d.P[0][c]; vx = d.P[1][c]; vy = d.P[2][c]; vz = d.P[3][c];
         e = d.EPS[c];
@@ -443,13 +452,13 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
     // index-0 layer, which FROMUTORVE leaves untouched (fromrvetou.f90:201)
     double fxm, fym, fzm;
     if (!INIT) {
-        fxm = (j > 1) ? d.U[5][c - 1] : d.P[5][c - 1];
-        fym = (k > 1) ? d.U[6][c - sy] : d.P[6][c - sy];
-        fzm = (l > 1) ? d.U[7][c - sz] : d.P[7][c - sz];
+        fxm = (j > 1) ? ux_m : px_m;
+        fym = (k > 1) ? uy_m : py_m;
+        fzm = (l > 1) ? uz_m : pz_m;
     } else {
-        fxm = d.P[5][c - 1];
-        fym = d.P[6][c - sy];
-        fzm = d.P[7][c - sz];
+        fxm = px_m;
+        fym = py_m;
+        fzm = pz_m;
     }
     cell_b(d, j, k, l, bfx, fxm, bfy, fym, bfz, fzm, bc);
     const double vsquare = vx * vx + vy * vy + vz * vz;
