@@ -116,22 +116,33 @@ def dist_setup(n_gpus):
     return world, rank, local, dist
 
 
-def cpu_oracle_rate(n, nz_slab, steps, workload):
-    """Wall-clock zone-updates/s of the CPU oracle on a slab of the workload."""
-    from cumc3d_b200 import models
+def cpu_baseline_of(build, steps, sample):
+    """The CPU oracle (a restatement of the reference's Fortran, OpenMP) on a
+    bounded sample of a workload, on all host cores and on the reference's
+    hard-coded 4 threads (solver/mhd/main.f90:31)."""
     from oracle import oracle as O
-    spec, prim, eps = workload(n, nz=nz_slab)
-    o = O.Oracle(spec)
-    o.set_state(prim, eps)
-    o.initial_update()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        dt = o.finddt()
-        o.rk3_step(dt)
-    el = time.perf_counter() - t0
-    zones = spec["nx"] * spec["ny"] * spec["nz"]
-    o.close()
-    return zones * steps / el, O.num_threads(), el
+    out = {"unit": "zone-updates/s", "kind": "port", "sample": sample}
+    try:
+        allc = os.cpu_count() or 1
+        for threads, key in ((allc, "value"), (4, "value_4_threads")):
+            O.set_num_threads(threads)
+            spec, prim, eps = build()
+            o = O.Oracle(spec)
+            o.set_state(prim, eps)
+            o.initial_update()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                o.rk3_step(o.finddt())
+            el = time.perf_counter() - t0
+            out[key] = spec["nx"] * spec["ny"] * spec["nz"] * steps / el
+            if key == "value":
+                out["cores"] = O.num_threads()
+                out["seconds"] = el
+            o.close()
+        O.set_num_threads(allc)
+    except Exception as ex:  # the baseline must not hide the GPU number
+        out.update({"value": None, "cores": None, "sample": "failed: %s" % ex})
+    return out
 
 
 def reference_arm(args):
@@ -362,6 +373,7 @@ def bench_config(args, world, rank, local, dist):
 
     from cumc3d_b200 import capi, engine, models
     extra = {}
+    cpu = None
     clocks = ClockSampler(local)
     if args.workload == "briowu":
         spec, prim, eps = models.brio_wu(800, recon=args.recon_c or "ppm", riemann=args.riemann,
@@ -373,6 +385,9 @@ def bench_config(args, world, rank, local, dist):
         name = "briowu_800_%s_%s_cfl0.8_t0.1" % (spec["recon"], spec["riemann"])
         extra["time_reached"] = s.time
         s.close()
+        if not args.no_cpu:
+            cpu = cpu_baseline_of(lambda: models.brio_wu(800, recon=spec["recon"], riemann=spec["riemann"]), 100,
+                                  "CPU oracle, Brio-Wu 800 zones, 100 RK3 steps")
     elif args.workload == "alfven3d":
         n3 = args.n
         recon = args.recon_c or "ppm"
@@ -418,6 +433,9 @@ def bench_config(args, world, rank, local, dist):
             "period": spec["t_end"], "time_reached": {p: out[p]["t"] for p in out},
         })
         extra["fp32_over_fp64"] = extra["fp32_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
+        if not args.no_cpu:
+            cpu = cpu_baseline_of(lambda: models.alfven_3d(128, recon=recon, riemann=args.riemann), 2,
+                                  "CPU oracle, the same wave on a 128^3 grid, 2 RK3 steps")
         if "fp32+learned" in out:
             o = out["fp32+learned"]
             l1_l = rel_l1(o["cons"], out["fp64"]["cons"])
@@ -443,17 +461,47 @@ def bench_config(args, world, rank, local, dist):
         n, ms = out[key]["steps"], out[key]["ms"]
         name = "alfven3d_%d^3_%s_%s_cfl0.4_one_period" % (n3, recon, args.riemann)
     else:  # torus
-        spec, prim, eps = models.torus_cyl(recon=args.recon_c or "weno", riemann=args.riemann,
-                                           precision=args.precision)
+        recon = args.recon_c or "weno"
+        spec, prim, eps = models.torus_cyl(recon=recon, riemann=args.riemann, precision="fp64")
         spec["positivity_fallback"] = 1
         zones = spec["nx"] * spec["ny"] * spec["nz"]
+        forms = [("fp64", dict(spec), None), ("fp32", dict(spec, precision="fp32"), None)]
+        lp = args.learned_params
+        if recon == "weno" and lp and os.path.exists(lp):
+            P = np.load(lp)
+
+            def setup(s, P=P):
+                s.learn_set(P, threshold=0.0, audit_interval=20, audit_tol=1e-5, flag_interval=4)
+            forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
+        out = {}
         clocks.start()
-        s, n, ms = _evolve_timed(engine, torch, spec, prim, eps, args.warmup, steps=args.steps)
+        for name_f, sp, setup in forms:
+            s, k, t_ms = _evolve_timed(engine, torch, sp, prim, eps, args.warmup, steps=args.steps, setup=setup)
+            out[name_f] = dict(cons=s.get_array(capi.ARR_CONS), divb=s.find_divb(), steps=k, ms=t_ms, t=s.time,
+                               stats=s.learn_stats() if setup is not None else None)
+            s.close()
         clk = clocks.stop()
-        extra["max_divb"] = s.find_divb()
-        extra["time_reached"] = s.time
-        s.close()
-        name = "torus_cyl_192x128x192_%s_%s_ct_cfl0.4" % (spec["recon"], spec["riemann"])
+        sl = (slice(3, spec["nz"] + 3), slice(3, spec["ny"] + 3), slice(3, spec["nx"] + 3))
+
+        def rel_l1(a, b):
+            a, b = a[sl].reshape(-1, 8), b[sl].reshape(-1, 8)
+            den = np.abs(b).sum(axis=0)
+            return (np.abs(a - b).sum(axis=0) / np.where(den == 0, 1, den)).tolist()
+        extra["max_divb"] = {f: out[f]["divb"] for f in out}
+        extra["time_reached"] = {f: out[f]["t"] for f in out}
+        for f in out:
+            extra["%s_zone_updates_per_s" % f] = zones * out[f]["steps"] / (out[f]["ms"] * 1e-3)
+            if f != "fp64":
+                extra["l1_%s_vs_fp64_max" % f] = max(rel_l1(out[f]["cons"], out["fp64"]["cons"]))
+        if "fp32+learned" in out:
+            st = out["fp32+learned"]["stats"]
+            extra["learned_flagged_fraction_at_audits"] = st["flagged"] / max(1, st["audited"])
+        key = args.precision if args.precision in out else "fp64"
+        n, ms = out[key]["steps"], out[key]["ms"]
+        name = "torus_cyl_192x128x192_%s_%s_ct_cfl0.4" % (recon, args.riemann)
+        if not args.no_cpu:
+            cpu = cpu_baseline_of(lambda: models.torus_cyl(nr=96, nphi=64, nz=96, recon=recon, riemann=args.riemann),
+                                  2, "CPU oracle, the same torus on a 96x64x96 grid, 2 RK3 steps")
     value = zones * n / (ms * 1e-3)
     if rank == 0:
         line = {"metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
@@ -461,7 +509,7 @@ def bench_config(args, world, rank, local, dist):
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
                 "config": {"workload": name, "precision": args.precision}, "results": extra,
-                "e2e": None, "cpu_baseline": None, "clocks": clk}
+                "e2e": None, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -638,19 +686,15 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        try:
-            nz_slab = 64
-            def slab(nn, nz):
-                sp, pr, ep = models.blast_3d(nn, nz=nz, recon=args.recon, riemann=args.riemann)
-                sp["positivity_fallback"] = 1
-                sp["fix_periodic_normal_faces"] = 1
-                return sp, pr, ep
-            rate, cores, el = cpu_oracle_rate(n, nz_slab, 2, slab)
-            cpu = {"value": rate, "unit": "zone-updates/s", "cores": cores, "kind": "port",
-                   "sample": "CPU oracle, %dx%dx%d periodic slab of the blast, 2 RK3 steps (%.1f s)" % (
-                       n, n, nz_slab, el)}
-        except Exception as ex:  # the baseline must not hide the GPU number
-            cpu = {"value": None, "unit": "zone-updates/s", "cores": None, "kind": "port", "sample": "failed: %s" % ex}
+        nz_slab = 64
+
+        def slab():
+            sp, pr, ep = models.blast_3d(n, nz=nz_slab, recon=args.recon, riemann=args.riemann)
+            sp["positivity_fallback"] = 1
+            sp["fix_periodic_normal_faces"] = 1
+            return sp, pr, ep
+        cpu = cpu_baseline_of(slab, 2, "CPU oracle, %dx%dx%d periodic slab of the blast, 2 RK3 steps" % (
+            n, n, nz_slab))
 
     s.close()
     if rank == 0:

@@ -1608,6 +1608,16 @@ void orc_reset_counts(void) { g_ops = OpCounts(); }
 void orc_get_counts(uint64_t *out5) {
     out5[0] = g_ops.add; out5[1] = g_ops.mul; out5[2] = g_ops.div; out5[3] = g_ops.sqrt; out5[4] = g_ops.cmp;
 }
+/* OpenMP threads of the following calls (the reference hard-codes 4,
+ * solver/mhd/main.f90:31; the baselines also run on every host core) */
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -57,6 +57,7 @@ def lib():
         L.orc_max_divb.restype = C.c_double
         L.orc_get_counts.argtypes = [C.POINTER(C.c_uint64)]
         L.orc_num_threads.restype = C.c_int
+        L.orc_set_num_threads.argtypes = [C.c_int]
         L.orc_recon_cell.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_weights.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         L.orc_riemann_face.argtypes = [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -140,6 +141,10 @@ def get_counts():
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+def set_num_threads(n):
+    lib().orc_set_num_threads(int(n))
 
 
 def weights(rec, d5):
