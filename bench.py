@@ -385,6 +385,27 @@ def bench_config(args, world, rank, local, dist):
         name = "briowu_800_%s_%s_cfl0.8_t0.1" % (spec["recon"], spec["riemann"])
         extra["time_reached"] = s.time
         s.close()
+        # the same problem through the persistent 1D kernel (cumc_batch_*, one
+        # problem; bit-identical to the 3D engine): one launch instead of ~60
+        # graph nodes per step
+        bs = engine.BatchSolver([spec])
+        for _ in range(args.warmup):
+            bs.set_state(0, prim, eps)
+            bs.run()
+        bs.set_state(0, prim, eps)
+        stb = torch.cuda.ExternalStream(bs.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stb)
+        _, bsteps, _ = bs.run()
+        e1.record(stb)
+        torch.cuda.synchronize()
+        bms = e0.elapsed_time(e1)
+        bs.close()
+        extra["persistent_1d_kernel"] = {"zone_updates_per_s": zones * int(bsteps[0]) / (bms * 1e-3),
+                                         "steps": int(bsteps[0]), "ms": bms,
+                                         "note": "cumc_batch_run with this one problem (INITIAL_UPDATE included)"}
         if not args.no_cpu:
             cpu = cpu_baseline_of(lambda: models.brio_wu(800, recon=spec["recon"], riemann=spec["riemann"]), 100,
                                   "CPU oracle, Brio-Wu 800 zones, 100 RK3 steps")
