@@ -219,6 +219,7 @@ def bench_batch(args, world, rank, local, dist):
     total_ms, zu = 0.0, 0
     clocks = ClockSampler(local)
     clocks.start()
+    l0 = b.launch_count()
     for _ in range(args.steps):
         upload()  # untimed: the initial state of every problem
         if dist:
@@ -233,6 +234,7 @@ def bench_batch(args, world, rank, local, dist):
         total_ms += e0.elapsed_time(e1)
         zu += int(sum(p["n"] * int(k) for p, k in zip(params, steps)))
     clk = clocks.stop()
+    launches = b.launch_count() - l0
     ms = shard.max_over_ranks(total_ms, dist, "cuda")
     zu = shard.sum_over_ranks(zu, dist, "cuda")
     value = zu / (ms * 1e-3)
@@ -286,7 +288,7 @@ def bench_batch(args, world, rank, local, dist):
                        "step": "one whole batched run: INITIAL_UPDATE + every problem's time loop",
                        "l2": "per-problem rows are L2-resident by design; state re-uploaded between runs",
                        "parallelism": "problems sharded over %d ranks" % world if world > 1 else "single"},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         }
         print(json.dumps(line))
     if dist:

@@ -243,5 +243,6 @@ int cumc_batch_sync(cumc_batch *b) {
 }
 
 void *cumc_batch_stream(cumc_batch *b) { return b ? (void *)b->stream : nullptr; }
+int64_t cumc_batch_launch_count(cumc_batch *b) { return b ? b->launches : 0; }
 
 }  // extern "C"

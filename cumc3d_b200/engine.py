@@ -23,7 +23,7 @@ EXPORTS = [
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
     "cumc_set_tuning", "cumc_check_div3",
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
-    "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_last_error",
+    "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
     "cumc_learn_set", "cumc_learn_stats", "cumc_learn_harvest", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
@@ -80,6 +80,8 @@ def load_library(path=None):
     L.cumc_batch_sync.argtypes = [C.c_void_p]
     L.cumc_batch_stream.argtypes = [C.c_void_p]
     L.cumc_batch_stream.restype = C.c_void_p
+    L.cumc_batch_launch_count.argtypes = [C.c_void_p]
+    L.cumc_batch_launch_count.restype = C.c_int64
     L.cumc_batch_last_error.argtypes = [C.c_void_p]
     L.cumc_batch_last_error.restype = C.c_char_p
     L.cumc_learn_set.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_float]
@@ -339,6 +341,10 @@ class BatchSolver:
 
     def stream(self):
         return int(self.L.cumc_batch_stream(self.h) or 0)
+
+    def launch_count(self):
+        """Kernel launches issued since creation."""
+        return int(self.L.cumc_batch_launch_count(self.h))
 
 
 def batch_run1_noalloc(spec, prim, eps, max_steps=0, positivity_fallback=0, stream=0):

@@ -235,6 +235,9 @@ int cumc_batch_get_state(cumc_batch *b, int p, double *prim_row, double *eps_row
 int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, int *status_out);
 int cumc_batch_sync(cumc_batch *b);
 void *cumc_batch_stream(cumc_batch *b);
+/* Number of kernel launches the batch issued since creation (one per
+ * cumc_batch_run). */
+int64_t cumc_batch_launch_count(cumc_batch *b);
 const char *cumc_batch_last_error(cumc_batch *b);
 
 /* ---------------- learned smooth-face flag (WENO, FP32 or FP64 form) ----------------
