@@ -12,6 +12,7 @@
 //   k_rk                FLUX_DIFF + GET_SOURCE + CUSTOM_SOURCE + l_operator
 //                       + the Shu-Osher stage combination                   (spatial.f90:167-713,
 //                                                                            rungekutta.f90:61-167)
+//   k_rk_cart           the same for the FP32 form on Cartesian grids without sources
 //   k_recover           FROMUTORVE + CUSTOM_CHECKRHO + FROMRVETOU
 //                       + FINDPRESSURE on the interior                       (fromrvetou.f90, update.f90)
 //   k_cons0             FROMRVETOU on the index-0 ghost layer (face fields)
@@ -358,6 +359,82 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
         lr[7] = (-(XF(j) * ey0 - XF(j - 1) * eyx) / (XC(j) * DX(j)) + (ex0 - exy) / (XBAR(j) * DY(k)));
     }
     // rungekutta.f90:61-167
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        double un;
+        if (stage == 1) {
+            d.U0[i][c] = u[i];
+            un = u[i] + dt * lr[i];
+        } else if (stage == 2) {
+            un = rk20 * u0[i] + rk21 * u[i] + rk22 * dt * lr[i];
+        } else {
+            un = rk30 * u0[i] + rk31 * u[i] + rk32 * dt * lr[i];
+        }
+        d.U[i][c] = un;
+    }
+}
+
+// k_rk of the FP32 form on Cartesian grids without sources (GET_SOURCE and
+// CUSTOM_SOURCE add nothing there): every operand is loaded before any
+// store, the face fluxes kept in their FP32 storage type (30 registers
+// instead of 60), so the kernel runs without spills at 256 threads and two
+// blocks per SM.  Same expressions in the same order as k_rk, so the same
+// bits.  (For the FP64 form the hoisted FP64 fluxes spill; k_rk stays.)
+template <class FT>
+__global__ void __launch_bounds__(256, 2) k_rk_cart(const Dev d, int stage) {
+    if (d.S->done) return;
+    const unsigned ex = d.nx + 1, ey = d.ny + 1, ez = d.nz + 1;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ex * ey * ez) return;
+    const unsigned r = t / ex;
+    const int j = (int)(t - r * ex);
+    const int k = (int)(r % ey);
+    const int l = (int)(r / ey);
+    const int c = cidx(d, j, k, l);
+    const int sy = d.NX, sz = d.NX * d.NY;
+    const bool interior = j >= 1 && k >= 1 && l >= 1;
+    FT f[5][6];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) f[i][m] = FT(0);
+    }
+    if (interior) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+            const FT *FXi = reinterpret_cast<const FT *>(d.FX[i]);
+            const FT *FYi = reinterpret_cast<const FT *>(d.FY[i]);
+            const FT *FZi = reinterpret_cast<const FT *>(d.FZ[i]);
+            f[i][0] = __ldg(FXi + c);
+            f[i][1] = __ldg(FXi + c - 1);
+            if (d.n_dim > 1) { f[i][2] = __ldg(FYi + c); f[i][3] = __ldg(FYi + c - sy); }
+            if (d.n_dim > 2) { f[i][4] = __ldg(FZi + c); f[i][5] = __ldg(FZi + c - sz); }
+        }
+    }
+    const double ex0 = __ldg(d.EX + c), exz = __ldg(d.EX + c - sz), exy = __ldg(d.EX + c - sy);
+    const double ey0 = __ldg(d.EY + c), eyz = __ldg(d.EY + c - sz), eyx = __ldg(d.EY + c - 1);
+    const double ez0 = __ldg(d.EZ + c), ezy = __ldg(d.EZ + c - sy), ezx = __ldg(d.EZ + c - 1);
+    double u[8], u0[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        u[i] = d.U[i][c];
+        u0[i] = (stage == 1) ? u[i] : __ldg(d.U0[i] + c);
+    }
+    const double dt = d.S->dt;
+    double lr[8];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        lr[i] = 0.0;
+        if (interior) {
+            double L = -dv((double)f[i][0] - (double)f[i][1], DX(j));
+            if (d.n_dim > 1) L = L - dv((double)f[i][2] - (double)f[i][3], DY(k));
+            if (d.n_dim > 2) L = L - dv((double)f[i][4] - (double)f[i][5], DZ(l));
+            lr[i] = L + 0.0;
+        }
+    }
+    lr[5] = -(dv(ez0 - ezy, DY(k)) - dv(ey0 - eyz, DZ(l)));
+    lr[6] = -(dv(ex0 - exz, DZ(l)) - dv(ez0 - ezx, DX(j)));
+    lr[7] = -(dv(ey0 - eyx, DX(j)) - dv(ex0 - exy, DY(k)));
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         double un;
@@ -873,7 +950,8 @@ static void launch_flux(cumc_handle *h, int dir, int stage = 1) {
     if (d.learned) {  // WENO with the learned smooth-face flag (split kernels)
         if (h->cfg.precision == CUMC_FP32) launch_split_learned_fp32(d, dir, h->cfg.riemann, stage, h->stream);
         else launch_split_learned_fp64(d, dir, h->cfg.riemann, stage, h->stream);
-        h->launches += 2;
+        // stage 1: network + per-warp decisions + staged reconstruction + Riemann
+        h->launches += (stage == 1) ? 4 : 2;
         return;
     }
     if (h->flux_mode == 1) {
@@ -1003,8 +1081,14 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     prof_begin(h);
     {
         const long long cells = (long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
-        if (h->cfg.precision == CUMC_FP32) k_rk<float><<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
-        else k_rk<double><<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
+        const bool fp32 = h->cfg.precision == CUMC_FP32;
+        if (fp32 && d.coord == 0 && d.source_kind == 0 && cells < (1LL << 31)) {
+            k_rk_cart<float><<<(unsigned)((cells + 255) / 256), 256, 0, h->stream>>>(d, stage);
+        } else if (fp32) {
+            k_rk<float><<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
+        } else {
+            k_rk<double><<<(unsigned)((cells + 127) / 128), 128, 0, h->stream>>>(d, stage);
+        }
     }
     h->launches++;
     prof_end(h, PC_RK);
@@ -1226,6 +1310,7 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
         for (int a = 0; a < 3; ++a) {
             d.lfb[a] = (unsigned char *)B((size_t)learned_tiles(d, a) + 1);
             d.lflag[a] = (unsigned char *)B((size_t)learned_tiles(d, a) * 128);
+            d.lwarp[a] = (unsigned char *)B((size_t)learned_warps(d, a));
         }
         d.lstats = (unsigned long long *)B(sizeof(unsigned long long) * LEARN_STAT_SLOTS * LEARN_STAT_FIELDS);
         d.learned = 0;
@@ -1486,11 +1571,15 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
         h->d.tpb_riemann = cands[i].tpb_riemann;
         h->d.riemann_minb = cands[i].minb;
         h->d.recon_tile = cands[i].tile;
-        for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir);  // warm-up
+        // with the learned flag, stage 1 of a refresh step also runs the flag
+        // network, the same work for every candidate; stage 2 times the
+        // kernels the candidates differ in, as every non-refresh stage runs them
+        const int stage = h->d.learned ? 2 : 1;
+        for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir, stage);  // warm-up
         CK(cudaEventRecord(a, h->stream));
         const int reps = 3;
         for (int r = 0; r < reps; ++r)
-            for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir);
+            for (int dir = 0; dir < h->d.n_dim; ++dir) launch_flux(h, dir, stage);
         CK(cudaEventRecord(b, h->stream));
         CK(cudaEventSynchronize(b));
         float ms = 0.f;
@@ -1547,7 +1636,12 @@ int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int fla
         learn_pack(params, &hp);
         CK(cudaMemcpyAsync((void *)d.mlp, &hp, sizeof hp, cudaMemcpyHostToDevice, h->stream));
     }
-    for (int a = 0; a < 3; ++a) CK(cudaMemsetAsync(d.lfb[a], 0, (size_t)learned_tiles(d, a) + 1, h->stream));
+    // flags of an earlier network do not carry over: WENO-Z until the next refresh
+    for (int a = 0; a < 3; ++a) {
+        CK(cudaMemsetAsync(d.lfb[a], 0, (size_t)learned_tiles(d, a) + 1, h->stream));
+        CK(cudaMemsetAsync(d.lflag[a], 0, (size_t)learned_tiles(d, a) * 128, h->stream));
+        CK(cudaMemsetAsync(d.lwarp[a], 0, (size_t)learned_warps(d, a), h->stream));
+    }
     CK(cudaMemsetAsync(d.lstats, 0, sizeof(unsigned long long) * LEARN_STAT_SLOTS * LEARN_STAT_FIELDS, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     d.learned = params ? 1 : 0;
@@ -1570,6 +1664,24 @@ int cumc_learn_stats(cumc_handle *h, unsigned long long *out4) {
     CK(cudaStreamSynchronize(h->stream));
     for (int sl = 0; sl < LEARN_STAT_SLOTS; ++sl)
         for (int f = 0; f < LEARN_STAT_FIELDS; ++f) out4[f] += buf[sl * LEARN_STAT_FIELDS + f];
+    return CUMC_OK;
+}
+
+int cumc_learn_flags(cumc_handle *h, int dir, unsigned char *flags, unsigned char *warps, unsigned char *tiles,
+                     long long *sizes_out) {
+    if (!h || !sizes_out || dir < 0 || dir > 2) return fail(h, CUMC_EINVAL, "bad argument");
+    const Dev &d = h->d;
+    if (!h->cfg.learned || !d.lflag[0]) return fail(h, CUMC_EINVAL, "handle was created without the learned flag");
+    if ((dir == 1 && d.n_dim < 2) || (dir == 2 && d.n_dim < 3)) return fail(h, CUMC_EINVAL, "direction not active");
+    const long long nf = (long long)(d.nx + (dir == 0 ? 2 : 0)) * (d.ny + (dir == 1 ? 2 : 0)) * (d.nz + (dir == 2 ? 2 : 0));
+    const long long nw = learned_warps(d, dir), nt = learned_tiles(d, dir);
+    sizes_out[0] = nf;
+    sizes_out[1] = nw;
+    sizes_out[2] = nt;
+    if (flags) CK(cudaMemcpyAsync(flags, d.lflag[dir], (size_t)nf, cudaMemcpyDeviceToHost, h->stream));
+    if (warps) CK(cudaMemcpyAsync(warps, d.lwarp[dir], (size_t)nw, cudaMemcpyDeviceToHost, h->stream));
+    if (tiles) CK(cudaMemcpyAsync(tiles, d.lfb[dir], (size_t)nt, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return CUMC_OK;
 }
 

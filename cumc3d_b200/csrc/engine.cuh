@@ -75,6 +75,7 @@ struct Dev {
     const void *mlp;             // MlpPacked parameters
     unsigned char *lfb[3];       // per direction, per 128-cell tile: 1 = fall back to WENO-Z
     unsigned char *lflag[3];     // per direction, per reconstructed cell: the stage-1 flag
+    unsigned char *lwarp[3];     // per direction, per warp of the staged reconstruction: 1 = linear
     unsigned long long *lstats;  // audit counters (LEARN_STAT_SLOTS x LEARN_STAT_FIELDS)
 };
 
@@ -91,5 +92,17 @@ void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStr
 void launch_split_learned_fp64(const Dev &d, int dir, int rs, int stage, cudaStream_t s);
 void launch_learned_flags(const Dev &d, int dir, int stage, cudaStream_t s);
 long long learned_tiles(const Dev &d, int dir);
+// The warps of the staged reconstruction (a warp = 32 consecutive x-cells of
+// one row of the tile, for every cells-per-thread): their number along x and
+// in all, per sweep direction.
+__device__ __host__ __forceinline__ int learned_warp_nx(const Dev &d, int dir) {
+    return dir == 0 ? (d.nx + 2 + 31) / 32 : (d.nx + 31) / 32;
+}
+__device__ __host__ __forceinline__ long long learned_warps(const Dev &d, int dir) {
+    const long long nxc = learned_warp_nx(d, dir);
+    if (dir == 0) return nxc * d.ny * d.nz;
+    if (dir == 1) return nxc * (d.ny + 2) * d.nz;
+    return nxc * d.ny * (d.nz + 2);
+}
 
 }  // namespace cumc

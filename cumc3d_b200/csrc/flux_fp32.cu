@@ -28,6 +28,7 @@ static void launch_learned_dir(const Dev &d, int rs, int stage, cudaStream_t s) 
         const unsigned pg = tiles < (unsigned)(4 * d.num_sms) ? tiles : (unsigned)(4 * d.num_sms);
         if (d.wuni[DIR]) k_recon_learned<DIR, 1, 1><<<pg, 128, 0, s>>>(d, stage);
         else k_recon_learned<DIR, 0, 1><<<pg, 128, 0, s>>>(d, stage);
+        k_learned_warps<DIR><<<2 * d.num_sms, dim3(32, 8, 1), 0, s>>>(d, stage);
     }
     const dim3 tb(32, 8, 1);
     if (d.recon_tile == 1) {
@@ -56,6 +57,7 @@ static void launch_flags_dir(const Dev &d, int stage, cudaStream_t s) {
     const unsigned pg = tiles < (unsigned)(4 * d.num_sms) ? tiles : (unsigned)(4 * d.num_sms);
     if (d.wuni[DIR]) k_recon_learned<DIR, 1, 0><<<pg, 128, 0, s>>>(d, stage);
     else k_recon_learned<DIR, 0, 0><<<pg, 128, 0, s>>>(d, stage);
+    k_learned_warps<DIR><<<2 * d.num_sms, dim3(32, 8, 1), 0, s>>>(d, stage);
 }
 void launch_learned_flags(const Dev &d, int dir, int stage, cudaStream_t s) {
     if (stage != 1) return;

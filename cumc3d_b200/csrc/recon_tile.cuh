@@ -19,10 +19,79 @@ namespace cumc {
 // run) or 2 (FP64 WENO with the learned flag, every stage; the network only
 // sets the flags): a warp whose 32 cells carry the stored flag, dilated by
 // two cells along the sweep, in 128-cell tiles not marked to fall back,
-// reconstructs with the linear optimal weights (recon_learned.cuh).  With
-// no cell flagged the arithmetic is that of LRN = 0.
+// reconstructs with the linear optimal weights (recon_learned.cuh); the
+// decision is made once per refresh, per warp (k_learned_warps).  With no
+// cell flagged the arithmetic is that of LRN = 0.
 __device__ __forceinline__ bool learned_refresh_stage(const Dev &d, int stage) {
     return stage == 1 && (d.flag_interval <= 1 || (d.S->steps % d.flag_interval) == 0);
+}
+
+// grid of the tiled reconstruction for one sweep
+__host__ __device__ inline dim3 recon_tile_grid(const Dev &d, int dir, int cpt) {
+    const int nr = 8 * cpt;
+    if (dir == 0) return dim3((d.nx + 2 + 31) / 32, (d.ny + nr - 1) / nr, d.nz);
+    if (dir == 1) return dim3((d.nx + 31) / 32, (d.ny + 2 + nr - 1) / nr, d.nz);
+    return dim3((d.nx + 31) / 32, (d.nz + 2 + nr - 1) / nr, d.ny);
+}
+
+// The index of the warp of the staged reconstruction (learned_warps in
+// engine.cuh) with x-chunk bx, sweep cell c (DIR 1, 2) or row k (DIR 0) and
+// the remaining coordinate o (l for DIR 0 and 1, k for DIR 2).
+template <int DIR>
+__device__ __forceinline__ long long learned_warp(const Dev &d, int bx, int c, int o) {
+    const long long nxc = learned_warp_nx(d, DIR);
+    if (DIR == 0) return bx + nxc * ((c - 1) + (long long)d.ny * (o - 1));
+    if (DIR == 1) return bx + nxc * (c + (long long)(d.ny + 2) * (o - 1));
+    return bx + nxc * ((o - 1) + (long long)d.ny * c);
+}
+
+// After the flag network (refresh stages only): the linear decision of every
+// warp of the staged reconstruction, from the flags of its 32 cells and of
+// their neighbours within two cells along the sweep and from the per-tile
+// fallback marks -- the test the staged kernel would otherwise make per cell
+// with five flag loads.  A small persistent grid of 32 x 8 blocks walks the
+// blocks of recon_tile_grid(d, DIR, 1), so that on the other stages (the
+// kernel sits in every captured step) it costs only its early exit.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_learned_warps(const Dev d, int stage) {
+    if (d.S->done || !learned_refresh_stage(d, stage)) return;
+    const dim3 tg = recon_tile_grid(d, DIR, 1);
+    const long long nblk = (long long)tg.x * tg.y * tg.z;
+    const int tx = threadIdx.x, r = threadIdx.y;
+    for (long long bid = blockIdx.x; bid < nblk; bid += gridDim.x) {
+        const int bx = (int)(bid % tg.x);
+        const long long rest = bid / tg.x;
+        const int by = (int)(rest % tg.y), bz = (int)(rest / tg.y);
+        const int c0 = (DIR == 0) ? bx * 32 : by * 8;
+        int c, j, k, l, ns, o;
+        bool valid, row;
+        if (DIR == 0) {
+            c = c0 + tx; j = c; k = by * 8 + r + 1; l = bz + 1; ns = d.nx; o = l;
+            valid = c <= d.nx + 1 && k <= d.ny;
+            row = k <= d.ny;
+        } else if (DIR == 1) {
+            c = c0 + r; k = c; j = bx * 32 + tx + 1; l = bz + 1; ns = d.ny; o = l;
+            valid = j <= d.nx && c <= d.ny + 1;
+            row = c <= d.ny + 1;
+        } else {
+            c = c0 + r; l = c; j = bx * 32 + tx + 1; k = bz + 1; ns = d.nz; o = k;
+            valid = j <= d.nx && c <= d.nz + 1;
+            row = c <= d.nz + 1;
+        }
+        bool ok = false;
+        if (valid && c >= 2 && c <= ns - 1) {
+            long long t, sweep;
+            if (DIR == 0) { t = c + (long long)(d.nx + 2) * ((k - 1) + (long long)d.ny * (l - 1)); sweep = 1; }
+            else if (DIR == 1) { t = (j - 1) + (long long)d.nx * (c + (long long)(d.ny + 2) * (l - 1)); sweep = d.nx; }
+            else { t = (j - 1) + (long long)d.nx * ((k - 1) + (long long)d.ny * c); sweep = (long long)d.nx * d.ny; }
+            const unsigned char *f = d.lflag[DIR];
+            // c-2 .. c+2 lie within 0 .. n+1, the cells of the enumeration
+            ok = f[t] && f[t - sweep] && f[t + sweep] && f[t - 2 * sweep] && f[t + 2 * sweep] &&
+                 d.lfb[DIR][t >> 7] == 0;
+        }
+        const bool all = __all_sync(0xffffffffu, ok);
+        if (tx == 0 && row) d.lwarp[DIR][learned_warp<DIR>(d, bx, (DIR == 0) ? k : c, o)] = all ? 1 : 0;
+    }
 }
 
 template <class T, int DIR, int REC, int UNI, int CPT, int LRN = 0>
@@ -88,20 +157,11 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) 
         }
         bool linear = false;
         if (LRN) {
-            // the flat index of this cell in the sweep's enumeration (x fastest)
-            long long t, sweep;
-            if (DIR == 0) { t = c + (long long)(d.nx + 2) * ((k - 1) + (long long)d.ny * (l - 1)); sweep = 1; }
-            else if (DIR == 1) { t = (j - 1) + (long long)d.nx * (c + (long long)(d.ny + 2) * (l - 1)); sweep = d.nx; }
-            else { t = (j - 1) + (long long)d.nx * ((k - 1) + (long long)d.ny * c); sweep = (long long)d.nx * d.ny; }
-            bool ok = false;
+            // the warp's decision, made once per refresh by k_learned_warps;
+            // audit steps reconstruct with WENO-Z everywhere
+            const bool row = (DIR == 0) ? k <= d.ny : (DIR == 1) ? c <= d.ny + 1 : c <= d.nz + 1;
             const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
-            if (valid && c >= 2 && c <= ns - 1 && !audit) {
-                const unsigned char *f = d.lflag[DIR];
-                // c-2 .. c+2 lie within 0 .. n+1, the cells of the enumeration
-                ok = f[t] && f[t - sweep] && f[t + sweep] && f[t - 2 * sweep] && f[t + 2 * sweep] &&
-                     d.lfb[DIR][t >> 7] == 0;
-            }
-            linear = __all_sync(0xffffffffu, ok);
+            if (row && !audit) linear = d.lwarp[DIR][learned_warp<DIR>(d, blockIdx.x, DIR == 0 ? k : c, DIR == 2 ? k : l)] != 0;
         }
         if (!valid) continue;
         const int ci = cidx(d, j, k, l);
@@ -144,14 +204,6 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) 
             if (c >= 1) QR[v][ci - st] = vm;  // right state of face c-1
         }
     }
-}
-
-// grid of the tiled reconstruction for one sweep
-static inline dim3 recon_tile_grid(const Dev &d, int dir, int cpt) {
-    const int nr = 8 * cpt;
-    if (dir == 0) return dim3((d.nx + 2 + 31) / 32, (d.ny + nr - 1) / nr, d.nz);
-    if (dir == 1) return dim3((d.nx + 31) / 32, (d.ny + 2 + nr - 1) / nr, d.nz);
-    return dim3((d.nx + 31) / 32, (d.nz + 2 + nr - 1) / nr, d.ny);
 }
 
 }  // namespace cumc

@@ -25,7 +25,7 @@ EXPORTS = [
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
-    "cumc_learn_set", "cumc_learn_stats", "cumc_learn_harvest", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
@@ -86,6 +86,7 @@ def load_library(path=None):
     L.cumc_batch_last_error.restype = C.c_char_p
     L.cumc_learn_set.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_float]
     L.cumc_learn_stats.argtypes = [C.c_void_p, C.c_void_p]
+    L.cumc_learn_flags.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
     L.cumc_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p, C.c_void_p]
     L.cumc_mlp_train.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(capi.CumcTrainConfig), C.c_void_p, C.c_void_p]
@@ -221,6 +222,16 @@ class Solver:
         out = (C.c_ulonglong * 4)()
         self._check(self.L.cumc_learn_stats(self.h, out))
         return dict(audited=out[0], flagged=out[1], fallback_tiles=out[2], audits=out[3])
+
+    def learn_flags(self, direction):
+        """The stored learned-flag state of one sweep: per-cell flags, per-warp
+        linear decisions of the staged reconstruction, per-tile fallback marks."""
+        sizes = (C.c_longlong * 3)()
+        self._check(self.L.cumc_learn_flags(self.h, int(direction), None, None, None, sizes))
+        f, w, t = (np.empty(int(n), dtype=np.uint8) for n in sizes)
+        self._check(self.L.cumc_learn_flags(self.h, int(direction), f.ctypes.data, w.ctypes.data, t.ctypes.data,
+                                            sizes))
+        return f, w, t
 
     def learn_harvest(self, direction, stride=1):
         """Samples (rows of 37 floats) of every stride-th interior cell, one sweep."""

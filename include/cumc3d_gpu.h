@@ -277,6 +277,15 @@ int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int fla
                    float audit_tol);
 /* audit counters: cells audited, cells flagged, tiles set to fall back, audits */
 int cumc_learn_stats(cumc_handle *h, unsigned long long *out4);
+/* For inspection (no counterpart in the reference): the learned-flag state of
+ * sweep dir as the last refresh left it.  flags = one byte per cell of the
+ * sweep's enumeration (x fastest; cells 0..n+1 along the sweep, interior
+ * across it), warps = the linear decision of each warp of the staged
+ * reconstruction (32 consecutive x-cells of one row), tiles = the per
+ * 128-cell fallback marks.  sizes_out[0..2] receives the three byte counts;
+ * any of the buffers may be NULL to ask for the sizes only. */
+int cumc_learn_flags(cumc_handle *h, int dir, unsigned char *flags, unsigned char *warps, unsigned char *tiles,
+                     long long *sizes_out);
 /* samples of every stride-th interior cell of the current state, sweep dir */
 int cumc_learn_harvest(cumc_handle *h, int dir, long long stride, float *out, long long cap, long long *rows_out);
 /* mean loss and gradient over n samples (FP32, deterministic order) */

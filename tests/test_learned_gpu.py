@@ -253,3 +253,59 @@ def test_fp64_learned_with_trained_flag_stays_close_to_plain():
     assert st["flagged"] > 0.5 * st["audited"]
     assert l1.max() < 1e-5, l1
     assert divb < 1e-11
+
+
+def expected_warps(flags, tiles, spec, direction):
+    """The linear decision of each warp of the staged reconstruction, restated
+    from the stored per-cell flags: a warp (32 consecutive x-cells of one row)
+    is linear when every one of its cells lies two or more cells inside the
+    sweep, carries the flag together with its neighbours within two cells
+    along the sweep, and sits in a 128-cell tile not marked to fall back."""
+    nx, ny, nz = spec["nx"], spec["ny"], spec["nz"]
+    shape = [(nz, ny, nx + 2), (nz, ny + 2, nx), (nz + 2, ny, nx)][direction]
+    sweep_axis = [2, 1, 0][direction]
+    n = [nx, ny, nz][direction]
+    g = np.moveaxis(flags.reshape(shape) != 0, sweep_axis, -1)
+    tile_ok = np.moveaxis((tiles[np.arange(flags.size) >> 7] == 0).reshape(shape), sweep_axis, -1)
+    ok = np.zeros_like(g)
+    for c in range(2, n):
+        ok[..., c] = g[..., c - 2:c + 3].all(-1) & tile_ok[..., c]
+    ok = np.moveaxis(ok, -1, sweep_axis)
+    nxc = (shape[2] + 31) // 32
+    pad = np.zeros(shape[:2] + (nxc * 32,), dtype=bool)
+    pad[..., :shape[2]] = ok
+    return pad.reshape(shape[:2] + (nxc, 32)).all(-1).reshape(-1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("case", ["all", "all_fallback", "trained"])
+def test_warp_decisions_follow_the_dilated_flags(precision, case):
+    """The per-warp decisions written after the network (k_learned_warps) equal
+    the dilated per-cell rule restated in numpy, on a grid whose rows end in
+    partial warps (72 cells: 74 along the x sweep).  Cases: every cell
+    flagged (linear exactly where a warp lies two cells inside the sweep);
+    the same with a zero-tolerance audit each step, which marks tiles to fall
+    back; the trained network."""
+    import os
+    spec, prim, eps = models.alfven_3d(72, recon="weno")
+    if case == "trained":
+        P = np.load(os.path.join(os.path.dirname(engine.__file__), "data", "flag_mlp.npy"))
+        learn = dict(params=P, threshold=0.0, audit_interval=0, audit_tol=1e-5)
+    else:
+        learn = dict(params=flag_all_params(), threshold=0.0, audit_interval=1 if case == "all_fallback" else 0,
+                     audit_tol=0.0)
+    s = engine.Solver(dict(spec, precision=precision, learned=1))
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.learn_set(flag_interval=1, **learn)
+    s.evolve(1e30, 1)
+    for d in range(3):
+        flags, warps, tiles = s.learn_flags(d)
+        exp = expected_warps(flags, tiles, spec, d)
+        assert warps.shape == exp.shape
+        assert np.array_equal(warps != 0, exp), (d, int((warps != 0).sum()), int(exp.sum()))
+        if case == "all":
+            assert 0 < exp.sum() < exp.size and not tiles.any()
+        if case == "all_fallback":
+            assert tiles.any()
+    s.close()
