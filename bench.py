@@ -423,7 +423,8 @@ def bench_config(args, world, rank, local, dist):
             P = np.load(lp)
 
             def setup(s, P=P):
-                s.learn_set(P, threshold=0.0, audit_interval=20, audit_tol=1e-5, flag_interval=4)
+                s.learn_set(P, threshold=args.learn_threshold, audit_interval=args.audit_interval, audit_tol=1e-5,
+                            flag_interval=args.flag_interval)
             forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
             forms.append(("fp64+learned", dict(spec, precision="fp64", learned=1), setup))
         clocks.start()
@@ -470,6 +471,8 @@ def bench_config(args, world, rank, local, dist):
                 "learned_flagged_fraction_at_audits": st["flagged"] / max(1, st["audited"]),
                 "learned_fallback_tiles": st["fallback_tiles"], "learned_audits": st["audits"],
                 "learned_params": os.path.relpath(lp, ROOT),
+                "learned_flag_interval": args.flag_interval, "learned_audit_interval": args.audit_interval,
+                "learned_threshold": args.learn_threshold,
             })
             extra["learned_over_fp64"] = extra["learned_zone_updates_per_s"] / extra["fp64_zone_updates_per_s"]
             o64 = out["fp64+learned"]
@@ -498,7 +501,8 @@ def bench_config(args, world, rank, local, dist):
             P = np.load(lp)
 
             def setup(s, P=P):
-                s.learn_set(P, threshold=0.0, audit_interval=20, audit_tol=1e-5, flag_interval=4)
+                s.learn_set(P, threshold=args.learn_threshold, audit_interval=args.audit_interval, audit_tol=1e-5,
+                            flag_interval=args.flag_interval)
             forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
         out = {}
         clocks.start()
@@ -523,6 +527,8 @@ def bench_config(args, world, rank, local, dist):
         if "fp32+learned" in out:
             st = out["fp32+learned"]["stats"]
             extra["learned_flagged_fraction_at_audits"] = st["flagged"] / max(1, st["audited"])
+            extra["learned_settings"] = {"flag_interval": args.flag_interval, "audit_interval": args.audit_interval,
+                                         "threshold": args.learn_threshold, "audit_tol": 1e-5}
         key = args.precision if args.precision in out else "fp64"
         n, ms = out[key]["steps"], out[key]["ms"]
         name = "torus_cyl_192x128x192_%s_%s_ct_cfl0.4" % (recon, args.riemann)
@@ -557,6 +563,14 @@ def main():
                     help="batch1d: run only the first N problems (profiler runs); the workload is 512")
     ap.add_argument("--learned-params", default=os.path.join(ROOT, "cumc3d_b200", "data", "flag_mlp.npy"),
                     help="trained flag network for the FP32+learned form of the alfven3d workload")
+    ap.add_argument("--flag-interval", type=int, default=8,
+                    help="learned forms: the flag network runs every this many steps")
+    ap.add_argument("--audit-interval", type=int, default=24,
+                    help="learned forms: full-WENO audit every this many steps (a multiple of --flag-interval)")
+    ap.add_argument("--learn-threshold", type=float, default=-4.0,
+                    help="learned forms: a cell is flagged smooth when the network's logit exceeds this; below 0 "
+                         "also flags the borderline cells, whose scatter would otherwise keep whole warps on "
+                         "WENO-Z (the audits bound the error)")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--recon", default="weno")
     ap.add_argument("--riemann", default="hlld")
