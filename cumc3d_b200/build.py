@@ -30,6 +30,7 @@ UNITS = [
     ("batch_fp32.cu", ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
     ("noalloc.cu", ["--fmad=false"]),
     ("learned.cu", ["--fmad=false"]),
+    ("poisson.cu", ["--fmad=false"]),
 ]
 
 

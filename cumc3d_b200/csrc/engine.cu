@@ -32,6 +32,7 @@
 #include "engine.cuh"
 #include "learned.cuh"
 #include "mhd_device.cuh"
+#include "poisson.cuh"
 
 namespace cumc {
 
@@ -800,6 +801,14 @@ struct cumc_handle {
     int prof_class = -1;           // >= 0 while cumc_profile_step is recording
     cudaEvent_t ev[2] = {nullptr, nullptr};
     double prof_ms[16];
+    // self-gravity potential (cumc_poisson_*): host copies of the cell
+    // centres (offset +2), the solver's device state and its step graph
+    std::vector<double> xc_host, yc_host, zc_host;
+    SorDev sor{};
+    bool sor_ready = false;
+    double sor_rho_atm = 0.0;
+    cudaGraph_t sor_graph = nullptr;
+    cudaGraphExec_t sor_exec = nullptr;
 };
 
 static std::string g_create_err;
@@ -1225,6 +1234,9 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
         F(yF, 0) = 0.0; F(yF, ny) = 4.0 * std::atan(1.0);
         sinf[3] = 0.0; sinf[ny + 3] = 0.0;
     }
+    h->xc_host = x;
+    h->yc_host = y;
+    h->zc_host = z;
     std::vector<double> wx = build_weights(cfg->recon, nx, dx), wy = build_weights(cfg->recon, ny, dy),
                         wz = build_weights(cfg->recon, nz, dz);
     std::vector<float> wxf(wx.begin(), wx.end()), wyf(wy.begin(), wy.end()), wzf(wz.begin(), wz.end());
@@ -1347,6 +1359,8 @@ int cumc_destroy(cumc_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->sor_exec) cudaGraphExecDestroy(h->sor_exec);
+    if (h->sor_graph) cudaGraphDestroy(h->sor_graph);
     for (void *p : h->allocs) cudaFree(p);
     for (int i = 0; i < 2; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -1665,6 +1679,163 @@ int cumc_learn_stats(cumc_handle *h, unsigned long long *out4) {
     for (int sl = 0; sl < LEARN_STAT_SLOTS; ++sl)
         for (int f = 0; f < LEARN_STAT_FIELDS; ++f) out4[f] += buf[sl * LEARN_STAT_FIELDS + f];
     return CUMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// self-gravity potential of the collapsar model (poisson.cu)
+// ---------------------------------------------------------------------------
+int cumc_poisson_setup(cumc_handle *h, double rho_atm, double omega) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    const Dev &d = h->d;
+    if (d.coord != 2) return fail(h, CUMC_EINVAL, "the self-gravity solver needs a spherical grid");
+    if (!(omega > 0.0 && omega < 2.0)) return fail(h, CUMC_EINVAL, "over-relaxation factor outside (0, 2)");
+    if (!(rho_atm == rho_atm)) return fail(h, CUMC_EINVAL, "atmosphere density is NaN");
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    SorDev &s = h->sor;
+    const long long px = nx + 2, py = (long long)(nx + 2) * (ny + 2), n3 = py * (nz + 2);
+    const int hx = (nx + 3) / 2;
+    const long long half = (long long)hx * (ny + 2) * (nz + 2);
+    if (!h->sor_ready) {
+        bool ok = true;
+        auto A = [&](size_t bytes) -> void * {
+            void *p = nullptr;
+            if (cudaMalloc(&p, bytes) != cudaSuccess) { ok = false; return nullptr; }
+            h->allocs.push_back(p);
+            return p;
+        };
+        s.nx = nx; s.ny = ny; s.nz = nz; s.hx = hx;
+        for (int c = 0; c < 2; ++c) {
+            s.phi[c] = (double *)A(half * sizeof(double));
+            s.clp1[c] = (double *)A(half * sizeof(double));
+            s.clm1[c] = (double *)A(half * sizeof(double));
+            s.epsc[c] = (double *)A(half * sizeof(double));
+            s.src[c] = (double *)A(half * sizeof(double));
+        }
+        s.ajp1 = (double *)A(px * sizeof(double));
+        s.ajm1 = (double *)A(px * sizeof(double));
+        s.bkp1 = (double *)A(py * sizeof(double));
+        s.bkm1 = (double *)A(py * sizeof(double));
+        s.err = (unsigned long long *)A(sizeof(unsigned long long));
+        s.state = (int *)A(4 * sizeof(int));
+        s.tol = (double *)A(sizeof(double));
+        s.err_last = (double *)A(sizeof(double));
+        if (!ok) return fail(h, CUMC_ENOMEM, "self-gravity arrays: out of device memory");
+        // coefficients (poisson.f90, computed once as GET_MODEL does), split by colour
+        std::vector<double> aj1(px, 0.0), aj0(px, 0.0), bk1(py, 0.0), bk0(py, 0.0), cl1(n3, 0.0), cl0(n3, 0.0),
+            ep(n3, 0.0);
+        sor_coefficients(nx, ny, nz, h->xc_host.data() + 2, h->yc_host.data() + 2, h->zc_host.data() + 2, aj1.data(),
+                         aj0.data(), bk1.data(), bk0.data(), cl1.data(), cl0.data(), ep.data());
+        std::vector<double> split[2][3];
+        for (int c = 0; c < 2; ++c)
+            for (int a = 0; a < 3; ++a) split[c][a].assign(half, 0.0);
+        for (int l = 0; l <= nz + 1; ++l)
+            for (int k = 0; k <= ny + 1; ++k)
+                for (int j = 0; j <= nx + 1; ++j) {
+                    const long long n = j + px * k + py * l, q = sor_index(s, j, k, l);
+                    const int c = (j + k + l) & 1;
+                    split[c][0][q] = cl1[n];
+                    split[c][1][q] = cl0[n];
+                    split[c][2][q] = ep[n];
+                }
+        for (int c = 0; c < 2; ++c) {
+            CK(cudaMemcpyAsync((void *)s.clp1[c], split[c][0].data(), half * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync((void *)s.clm1[c], split[c][1].data(), half * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync((void *)s.epsc[c], split[c][2].data(), half * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemsetAsync(s.src[c], 0, half * sizeof(double), h->stream));
+        }
+        CK(cudaMemcpyAsync((void *)s.ajp1, aj1.data(), px * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync((void *)s.ajm1, aj0.data(), px * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync((void *)s.bkp1, bk1.data(), py * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync((void *)s.bkm1, bk0.data(), py * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));  // the host buffers go out of scope
+    }
+    s.omega = omega;
+    h->sor_rho_atm = rho_atm;
+    // the initial model's guess: phi = 0 everywhere, ghosts included (custom.f90:498-507)
+    for (int c = 0; c < 2; ++c) CK(cudaMemsetAsync(s.phi[c], 0, half * sizeof(double), h->stream));
+    // omega lives in the captured kernel parameters: capture again
+    if (h->sor_exec) { cudaGraphExecDestroy(h->sor_exec); h->sor_exec = nullptr; }
+    if (h->sor_graph) { cudaGraphDestroy(h->sor_graph); h->sor_graph = nullptr; }
+    CK(cudaStreamSynchronize(h->stream));
+    h->sor_ready = true;
+    return CUMC_OK;
+}
+
+int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out, double *err_out,
+                       int *converged_out) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->sor_ready) return fail(h, CUMC_ENOTREADY, "cumc_poisson_setup first");
+    if (max_iter < 1 || !(tol >= 0.0)) return fail(h, CUMC_EINVAL, "bad iteration limit or tolerance");
+    if (!h->have_state) return fail(h, CUMC_ENOTREADY, "no state: cumc_set_state first");
+    SorDev &s = h->sor;
+    const Dev &d = h->d;
+    launch_sor_source(s, d.P[0], d.NX, d.NY, h->sor_rho_atm, h->stream);
+    const int lim[1] = {max_iter};
+    CK(cudaMemcpyAsync(s.state + 2, lim, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(s.tol, &tol, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    launch_sor_reset(s, h->stream);
+    if (!h->sor_exec) {
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        launch_sor_iteration(s, h->stream);
+        CK(cudaStreamEndCapture(h->stream, &h->sor_graph));
+        CK(cudaGraphInstantiate(&h->sor_exec, h->sor_graph, 0));
+    }
+    // replay in chunks; once the device marks the loop finished, the
+    // remaining launches of a chunk return at once
+    int st[3] = {0, 0, 0};
+    while (true) {
+        const int left = max_iter - st[0];
+        const int chunk = left < 32 ? left : 32;
+        for (int i = 0; i < chunk; ++i) CK(cudaGraphLaunch(h->sor_exec, h->stream));
+        h->launches += 4LL * chunk;
+        CK(cudaMemcpyAsync(st, s.state, 3 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (st[1] != 0) break;
+    }
+    double e = 0.0;
+    CK(cudaMemcpyAsync(&e, s.err_last, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (iters_out) *iters_out = st[0];
+    if (err_out) *err_out = e;
+    if (converged_out) *converged_out = st[1] == 1 ? 1 : 0;
+    return CUMC_OK;
+}
+
+// phi in the natural layout: (nx+2) (ny+2) (nz+2) doubles, j,k,l = 0..n+1, j fastest
+static int poisson_copy(cumc_handle *h, double *out, const double *in) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->sor_ready) return fail(h, CUMC_ENOTREADY, "cumc_poisson_setup first");
+    SorDev &s = h->sor;
+    const long long px = s.nx + 2, py = (long long)(s.nx + 2) * (s.ny + 2);
+    const long long half = (long long)s.hx * (s.ny + 2) * (s.nz + 2);
+    std::vector<double> part[2];
+    for (int c = 0; c < 2; ++c) part[c].assign(half, 0.0);
+    if (out) {
+        for (int c = 0; c < 2; ++c)
+            CK(cudaMemcpyAsync(part[c].data(), s.phi[c], half * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    for (int l = 0; l <= s.nz + 1; ++l)
+        for (int k = 0; k <= s.ny + 1; ++k)
+            for (int j = 0; j <= s.nx + 1; ++j) {
+                const long long n = j + px * k + py * l, q = sor_index(s, j, k, l);
+                if (out) out[n] = part[(j + k + l) & 1][q];
+                else part[(j + k + l) & 1][q] = in[n];
+            }
+    if (in) {
+        for (int c = 0; c < 2; ++c)
+            CK(cudaMemcpyAsync(s.phi[c], part[c].data(), half * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return CUMC_OK;
+}
+int cumc_poisson_get(cumc_handle *h, double *phi) {
+    if (!phi) return fail(h, CUMC_EINVAL, "null argument");
+    return poisson_copy(h, phi, nullptr);
+}
+int cumc_poisson_set(cumc_handle *h, const double *phi) {
+    if (!phi) return fail(h, CUMC_EINVAL, "null argument");
+    return poisson_copy(h, nullptr, phi);
 }
 
 int cumc_learn_flags(cumc_handle *h, int dir, unsigned char *flags, unsigned char *warps, unsigned char *tiles,

@@ -25,7 +25,8 @@ EXPORTS = [
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
-    "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest",
+    "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
@@ -86,6 +87,11 @@ def load_library(path=None):
     L.cumc_batch_last_error.restype = C.c_char_p
     L.cumc_learn_set.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_int, C.c_float]
     L.cumc_learn_stats.argtypes = [C.c_void_p, C.c_void_p]
+    L.cumc_poisson_setup.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.cumc_poisson_solve.argtypes = [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_int)]
+    L.cumc_poisson_get.argtypes = [C.c_void_p, C.c_void_p]
+    L.cumc_poisson_set.argtypes = [C.c_void_p, C.c_void_p]
     L.cumc_learn_flags.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
     L.cumc_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p, C.c_void_p]
@@ -222,6 +228,33 @@ class Solver:
         out = (C.c_ulonglong * 4)()
         self._check(self.L.cumc_learn_stats(self.h, out))
         return dict(audited=out[0], flagged=out[1], fallback_tiles=out[2], audits=out[3])
+
+    # ---- self-gravity potential of the collapsar model (spherical grids) ----
+    def poisson_setup(self, rho_atm, omega=1.9):
+        """Coefficients of the red-black SOR solver; phi = 0 everywhere."""
+        self._check(self.L.cumc_poisson_setup(self.h, float(rho_atm), float(omega)))
+
+    def poisson_solve(self, max_iter=100000, tol=1e-10):
+        """Relax phi with the current density.  Returns (iterations, last
+        max |dphi/phi_old|, converged)."""
+        it, err, conv = C.c_int(), C.c_double(), C.c_int()
+        self._check(self.L.cumc_poisson_solve(self.h, int(max_iter), float(tol), C.byref(it), C.byref(err),
+                                              C.byref(conv)))
+        return it.value, err.value, bool(conv.value)
+
+    def poisson_get(self):
+        """phi as (nz+2, ny+2, nx+2), cells 0..n+1 of each axis."""
+        sp = self.spec
+        out = np.empty((sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2))
+        self._check(self.L.cumc_poisson_get(self.h, out.ctypes.data))
+        return out
+
+    def poisson_set(self, phi):
+        sp = self.spec
+        P = np.ascontiguousarray(phi, dtype=np.float64)
+        if P.shape != (sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2):
+            raise ValueError("phi must be (nz+2, ny+2, nx+2)")
+        self._check(self.L.cumc_poisson_set(self.h, P.ctypes.data))
 
     def learn_flags(self, direction):
         """The stored learned-flag state of one sweep: per-cell flags, per-warp

@@ -288,6 +288,45 @@ def torus_cyl(nr=192, nphi=128, nz=192, r_range=(2.0, 42.0), z_range=(-20.0, 20.
 
 
 # ---------------------------------------------------------------------------
+# self-gravitating star on a spherical grid: the setting of the collapsar
+# model's gravity solve (model/collapsar/src/custom.f90:489-620).  The
+# reference reads a progenitor profile from files it does not ship
+# (model/collapsar/src/model.f90:40-90); this stand-in is an analytic,
+# seeded one of the same shape: a centrally condensed star inside a
+# tenuous atmosphere, rotating differentially.
+# ---------------------------------------------------------------------------
+def star_sph(nr=96, ntheta=48, nphi=48, r_range=(2.0, 40.0), theta_range=(0.1 * math.pi, 0.9 * math.pi), rho_c=1.0,
+             r_core=2.0, r_star=20.0, rho_atm=1e-6, p_atm=1e-8, asym=0.05, seed=20261203, recon="weno",
+             riemann="hlld", cfl=0.4, precision="fp64"):
+    """rho = rho_c / (1 + (r / r_core)^2)^1.5 inside r_star (times
+    1 + asym * sin(theta) cos(phi) + 1% seeded noise), rho_atm outside;
+    p = K rho^(5/3) with K = 1; v = 0, B = 0.  Returns (spec, prim, eps).
+
+    The default theta range keeps clear of the axis: with cells next to the
+    poles, whose phi-coefficients grow as 1/sin^2(theta), the reference's
+    over-relaxation factor 1.9 makes the red-black iteration diverge on
+    these grids (1.7 converges)."""
+    g = 5.0 / 3.0
+    full = theta_range[0] == 0.0 and theta_range[1] == math.pi
+    spec = _base_spec(nr, ntheta, nphi, 3, (1, 1, 3 if full else 1, 3 if full else 1, 0, 0), r_range, theta_range,
+                      (0.0, 2.0 * math.pi), coordinate_flag=2, cfl=cfl, recon=recon, riemann=riemann,
+                      precision=precision, fixpole=1 if full else 0, name="star_sph_%dx%dx%d" % (nr, ntheta, nphi))
+    r, th, ph = centers(spec["xF"]), centers(spec["yF"]), centers(spec["zF"])
+    P3, T3, R3 = np.meshgrid(ph, th, r, indexing="ij")
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rho = rho_c / (1.0 + (R3 / r_core) ** 2) ** 1.5
+    rho = rho * (1.0 + asym * np.sin(T3) * np.cos(P3)) * (1.0 + 0.01 * (rng.random(R3.shape) - 0.5) / 0.5)
+    rho = np.where(R3 < r_star, rho, rho_atm)
+    prim = np.zeros((nphi + 6, ntheta + 6, nr + 6, 8), dtype=np.float64)
+    prim[..., IRHO] = rho
+    prim[..., ITAU] = np.where(R3 < r_star, rho ** g, p_atm)
+    eps = prim[..., ITAU] / prim[..., IRHO] / (g - 1.0)
+    spec["model"] = dict(gamma=g, floor="eps", source="none", bc="none", rho_floor=rho_atm)
+    spec["rho_atm"] = rho_atm
+    return spec, prim, np.ascontiguousarray(eps)
+
+
+# ---------------------------------------------------------------------------
 # named workloads
 # ---------------------------------------------------------------------------
 WORKLOADS = {

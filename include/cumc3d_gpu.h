@@ -277,6 +277,34 @@ int cumc_learn_set(cumc_handle *h, const float *params, float threshold, int fla
                    float audit_tol);
 /* audit counters: cells audited, cells flagged, tiles set to fall back, audits */
 int cumc_learn_stats(cumc_handle *h, unsigned long long *out4);
+/* ---------------- self-gravity potential of the collapsar model ----------------
+ * Red-black successive over-relaxation of the Poisson equation on the
+ * handle's spherical grid (coordinate_flag 2), as CUSTOM_UPDATE of the
+ * collapsar model does it (model/collapsar/src/custom.f90:489-620; the
+ * coefficients are POISSON_COEF, model/collapsar/src/poisson.f90:34-64).
+ * phi lives on cells 0..n+1 of each axis.
+ *
+ * cumc_poisson_setup: computes the coefficients once (GET_POISSON,
+ * poisson.f90:6-27), sets phi = 0 everywhere (the initial model's guess,
+ * custom.f90:498-507).  rho_atm = the atmosphere density prim_a(irho): cells
+ * at or below it carry no mass in the source; omega = omega_weight (1.9 in
+ * the reference's def.f90).  CUMC_EINVAL for a non-spherical grid. */
+int cumc_poisson_setup(cumc_handle *h, double rho_atm, double omega);
+/* The relaxation loop (custom.f90:511-620) from the current phi, with the
+ * density of the handle's current state: per iteration the red cells
+ * ((-1)**(j+k+l) > 0), the black cells, the ghost layers (phi(0) = phi(1),
+ * phi(nx+1) = -1, copies along theta, periodic along phi) and the test
+ * max |dphi / phi_old| <= tol over the interior.  iters_out = iterations
+ * taken, err_out = that maximum at the last one, converged_out = 1 if it
+ * reached tol, 0 if max_iter ran out (where the reference STOPs).  An error
+ * that is NaN (0/0 where phi stays exactly zero) counts as not converged. */
+int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out, double *err_out,
+                       int *converged_out);
+/* phi (nx+2)*(ny+2)*(nz+2) doubles, j fastest, j,k,l = 0..n+1: read it back,
+ * or set it (a warm start, or a restart from a checkpoint). */
+int cumc_poisson_get(cumc_handle *h, double *phi);
+int cumc_poisson_set(cumc_handle *h, const double *phi);
+
 /* For inspection (no counterpart in the reference): the learned-flag state of
  * sweep dir as the last refresh left it.  flags = one byte per cell of the
  * sweep's enumeration (x fastest; cells 0..n+1 along the sweep, interior

@@ -1604,6 +1604,104 @@ double orc_mlp_loss_grad(const float *P, const float *X, long long n, float delt
     return loss / (double)n;
 }
 
+/* Self-gravity potential of the collapsar model: GET_POISSON + POISSON_COEF
+ * (model/collapsar/src/poisson.f90:6-64) and the red-black SOR loop of
+ * CUSTOM_UPDATE (model/collapsar/src/custom.f90:511-620), restated with the
+ * Fortran's loops and order: phi_old backup, abserror = 1e-50, red cells
+ * ((-1)**(j+k+l) > 0) in l,k,j order, black cells, the error maximum, the
+ * ghost layers, the exit test.  rho: interior, nx*ny*nz, j fastest; phi:
+ * (nx+2)*(ny+2)*(nz+2), j fastest, j,k,l = 0..n+1, in/out.  A NaN error
+ * (0/0 where phi stays zero) is kept as the maximum and fails the test.
+ * Returns 1 when the error reached tol, 0 when max_iter ran out. */
+int orc_poisson_solve(const cumc_config *cfg, const double *rho, double rho_atm, double omega, double tol,
+                      int max_iter, double *phi, int *iters, double *err) {
+    const int nx = cfg->nx, ny = cfg->ny, nz = cfg->nz;
+    const long long px = nx + 2, py = (long long)(nx + 2) * (ny + 2);
+    // cell centres x(j) = (xF(j) + xF(j-1)) / 2 for j = 0..n+1 (getgrid.f90:55-63);
+    // the face arrays start at index -3
+    auto centre = [](const double *f, int j) { return (f[j + 3] + f[j + 2]) / 2.0; };
+    std::vector<double> x(nx + 2), y(ny + 2), z(nz + 2);
+    for (int j = 0; j <= nx + 1; ++j) x[j] = centre(cfg->xF, j);
+    for (int k = 0; k <= ny + 1; ++k) y[k] = centre(cfg->yF, k);
+    for (int l = 0; l <= nz + 1; ++l) z[l] = centre(cfg->zF, l);
+    std::vector<double> ajp1(px), ajm1(px), bkp1(py), bkm1(py), clp1(py * (nz + 2)), clm1(py * (nz + 2)),
+        epsc(py * (nz + 2));
+    auto I3 = [&](int j, int k, int l) { return j + px * k + py * l; };
+    for (int i = 1; i <= nx; ++i)
+        for (int j = 1; j <= ny; ++j)
+            for (int k = 1; k <= nz; ++k) {
+                const double xm1 = x[i - 1], xc = x[i], xp1 = x[i + 1];
+                const double ym1 = y[j - 1], yc = y[j], yp1 = y[j + 1];
+                const double zm1 = z[k - 1], zc = z[k], zp1 = z[k + 1];
+                epsc[I3(i, j, k)] = 2.0 * (xp1 + xm1 - 3.0 * xc) / xc / (xp1 - xc) / (xc - xm1) +
+                                    (yp1 + ym1 - 2.0 * yc - 2.0 * std::tan(yc)) / (xc * xc) / std::tan(yc) /
+                                        (yp1 - yc) / (yc - ym1) -
+                                    2.0 / (xc * xc) / (std::sin(yc) * std::sin(yc)) / (zp1 - zc) / (zc - zm1);
+                ajp1[i] = 2.0 * (2.0 * xc - xm1) / (xp1 - xm1) / (xp1 - xc) / xc;
+                ajm1[i] = 2.0 * (2.0 * xc - xp1) / (xp1 - xm1) / (xc - xm1) / xc;
+                bkp1[i + px * j] = (2.0 * std::tan(yc) + yc - ym1) / (xc * xc) / std::tan(yc) / (yp1 - yc) / (yp1 - ym1);
+                bkm1[i + px * j] = (2.0 * std::tan(yc) + yc - yp1) / (xc * xc) / std::tan(yc) / (yp1 - ym1) / (yc - ym1);
+                clp1[I3(i, j, k)] = 2.0 / (xc * xc) / (std::sin(yc) * std::sin(yc)) / (zp1 - zm1) / (zp1 - zc);
+                clm1[I3(i, j, k)] = 2.0 / (xc * xc) / (std::sin(yc) * std::sin(yc)) / (zp1 - zm1) / (zc - zm1);
+            }
+    const double pi = 4.0 * std::atan(1.0);
+    std::vector<double> phi_old(py * (nz + 2));
+    auto sweep = [&](int parity) {
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    if (((j + k + l) & 1) != parity) continue;
+                    const double r = rho[(j - 1) + (long long)nx * ((k - 1) + (long long)ny * (l - 1))];
+                    const double diff = r - rho_atm;
+                    const double factor = diff > 0.0 ? 1.0 : 0.0;
+                    const double rho_in = factor * r;
+                    const long long c = I3(j, k, l);
+                    const double rhs = (4.0 * pi * rho_in -
+                                        (ajp1[j] * phi[c + 1] + ajm1[j] * phi[c - 1] + bkp1[j + px * k] * phi[c + px] +
+                                         bkm1[j + px * k] * phi[c - px] + clp1[c] * phi[c + py] + clm1[c] * phi[c - py])) /
+                                       epsc[c];
+                    phi[c] = (1.0 - omega) * phi[c] + omega * rhs;
+                }
+    };
+    int n = 0, converged = 0;
+    double abserror = 0.0;
+    for (n = 1; n <= max_iter; ++n) {
+        for (long long c = 0; c < py * (nz + 2); ++c) phi_old[c] = phi[c];
+        abserror = 1.0e-50;
+        sweep(0);  // red: (-1)**(j+k+l) > 0
+        sweep(1);  // black
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k)
+                for (int j = 1; j <= nx; ++j) {
+                    const long long c = I3(j, k, l);
+                    const double v = std::fabs((phi[c] - phi_old[c]) / phi_old[c]);
+                    if (v != v || v > abserror) abserror = v;
+                }
+        for (int l = 1; l <= nz; ++l)
+            for (int k = 1; k <= ny; ++k) {
+                phi[I3(0, k, l)] = phi[I3(1, k, l)];
+                phi[I3(nx + 1, k, l)] = -1.0;
+            }
+        for (int l = 1; l <= nz; ++l)
+            for (int j = 1; j <= nx; ++j) {
+                phi[I3(j, 0, l)] = phi[I3(j, 1, l)];
+                phi[I3(j, ny + 1, l)] = phi[I3(j, ny, l)];
+            }
+        for (int k = 1; k <= ny; ++k)
+            for (int j = 1; j <= nx; ++j) {
+                phi[I3(j, k, 0)] = phi[I3(j, k, nz)];
+                phi[I3(j, k, nz + 1)] = phi[I3(j, k, 1)];
+            }
+        if (abserror <= tol) {
+            converged = 1;
+            break;
+        }
+    }
+    if (iters) *iters = converged ? n : max_iter;
+    if (err) *err = abserror;
+    return converged;
+}
+
 void orc_reset_counts(void) { g_ops = OpCounts(); }
 void orc_get_counts(uint64_t *out5) {
     out5[0] = g_ops.add; out5[1] = g_ops.mul; out5[2] = g_ops.div; out5[3] = g_ops.sqrt; out5[4] = g_ops.cmp;

@@ -65,6 +65,9 @@ def lib():
         L.orc_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p]
         L.orc_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p]
         L.orc_mlp_loss_grad.restype = C.c_double
+        L.orc_poisson_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_poisson_solve.restype = C.c_int
         _lib = L
     return _lib
 
@@ -230,3 +233,20 @@ def mlp_forward_bf16(params, X):
     h1 = _bf16(h1.astype(np.float32)).astype(np.float64)
     h2 = np.maximum(h1 @ W2.T + b2, 0.0)
     return h2 @ w3 + b3
+
+
+def poisson_solve(spec, rho, rho_atm, omega=1.9, tol=1e-10, max_iter=100000, phi=None):
+    """Red-black SOR for the collapsar self-gravity potential (the oracle's
+    restatement of model/collapsar/src/custom.f90:511-620).  rho: interior
+    (nz, ny, nx); phi: (nz+2, ny+2, nx+2) start value (zeros if None).
+    Returns (phi, iterations, last error, converged)."""
+    from cumc3d_b200.capi import make_config  # structures only
+    cfg, keep = make_config(spec)
+    nx, ny, nz = spec["nx"], spec["ny"], spec["nz"]
+    r = np.ascontiguousarray(rho, dtype=np.float64).reshape(nz, ny, nx)
+    p = np.zeros((nz + 2, ny + 2, nx + 2)) if phi is None else np.array(phi, dtype=np.float64, copy=True)
+    it, err = C.c_int(), C.c_double()
+    conv = lib().orc_poisson_solve(C.byref(cfg), r.ctypes.data, float(rho_atm), float(omega), float(tol),
+                                   int(max_iter), p.ctypes.data, C.byref(it), C.byref(err))
+    del keep
+    return p, it.value, err.value, bool(conv)
