@@ -340,6 +340,117 @@ def reference_batch(args, world):
     return 0
 
 
+def bench_poisson(args, world, rank, local, dist):
+    """Self-gravity of the collapsar model: the red-black SOR of the spherical
+    Poisson equation (model/collapsar/src/custom.f90:511-620) on an
+    nr x ntheta x nphi grid of the seeded star (models.star_sph).  A step =
+    --sor-iters iterations continuing from the current potential (as the
+    model re-solves every 10 hydro steps); metric = cell-updates/s (interior
+    cells x iterations per second).  Also reported: a full solve from phi = 0
+    to 1e-10, the initial model's solve."""
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import engine, models, shard
+    nr, nth, nph = (int(v) for v in args.sor_grid.split(","))
+    spec, prim, eps = models.star_sph(nr, nth, nph)
+    cells = nr * nth * nph
+    ra = spec["rho_atm"]
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.poisson_setup(ra, 1.9)
+    it_step = args.sor_iters
+    for _ in range(args.warmup):
+        s.poisson_solve(max_iter=it_step, tol=0.0)  # tol 0: exactly it_step iterations
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = s.launch_count()
+    e0.record(stream)
+    total = 0
+    for _ in range(args.steps):
+        it, _, _ = s.poisson_solve(max_iter=it_step, tol=0.0)
+        total += it
+    e1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = s.launch_count() - l0
+    ms = shard.max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    value = world * cells * total / (ms * 1e-3)
+    t_iter = ms / total
+    # one iteration moves 56 B per interior cell: the cell's own phi read and
+    # written (16), its three coefficients (24), its source term (8), and its
+    # phi once more as the other colour's neighbour (8)
+    peak_gbs, peak_kind = load_peaks()
+    achieved = 56.0 * cells / (t_iter * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_sor_sweep<0,2> + k_sor_sweep<1,2> + k_sor_ghosts (one iteration)",
+                "achieved": achieved, "peak": peak_gbs,
+                "unit": "GB/s", "frac": achieved / peak_gbs, "traffic": None, "bytes_per_cell_iteration": 56,
+                "avg_iteration_ms": t_iter, "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peak_kind}
+    # the initial model's solve: phi = 0, to 1e-10
+    full = None
+    if args.sor_full:
+        s.poisson_setup(ra, 1.9)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        it_full, err_full, conv_full = s.poisson_solve(max_iter=100000, tol=1e-10)
+        e1.record(stream)
+        s.sync()
+        torch.cuda.synchronize()
+        full = {"iterations": it_full, "converged": conv_full, "final_error": err_full,
+                "ms": e0.elapsed_time(e1), "tol": 1e-10, "omega": 1.9}
+    # end to end through the C-ABI with host buffers: density state and the
+    # start potential up, one step of iterations, the potential back
+    e2e = None
+    if not args.no_e2e:
+        phi0 = s.poisson_get()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.set_state(prim, eps)
+        s.poisson_set(phi0)
+        it_e, _, _ = s.poisson_solve(max_iter=it_step, tol=0.0)
+        phi1 = s.poisson_get()
+        el = time.perf_counter() - t0
+        e2e = {"value": world * cells * it_e / el, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": int(prim.nbytes + eps.nbytes + phi0.nbytes), "d2h_bytes_per_step": int(phi1.nbytes),
+               "wall_s": el, "note": "set_state + poisson_set + one step of %d iterations + poisson_get" % it_step}
+    s.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        sp2, pr2, _ = models.star_sph(128, 64, 64)
+        n_it = 300
+        t0 = time.perf_counter()
+        O.poisson_solve(sp2, pr2[3:-3, 3:-3, 3:-3, 0], sp2["rho_atm"], omega=1.9, tol=0.0, max_iter=n_it)
+        el = time.perf_counter() - t0
+        cpu = {"value": 128 * 64 * 64 * n_it / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": "CPU oracle (the reference's loops in order, one thread), the star on a "
+                         "128x64x64 grid, %d iterations (%.1f s; coefficient setup included)" % (n_it, el)}
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "collapsar_self_gravity_sor_%dx%dx%d_star" % (nr, nth, nph),
+                       "iterations_per_step": it_step, "omega": 1.9,
+                       "l2": "colour arrays %.1f GB, larger than L2" % (cells * 56 / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": roofline, "full_solve_from_zero": full, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def _evolve_timed(engine, torch, spec, prim, eps, warmup, steps=None, t_end=None, tuning="auto", setup=None):
     """Run one handle: W warm-up steps, then time the rest (to t_end, or K
     more steps) with CUDA events on the engine stream.  Returns the handle
@@ -557,7 +668,11 @@ def main():
                     help="timed steps (default 200 RK3 steps of the blast; 5 whole runs of the batch)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="blast3d", choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus"])
+    ap.add_argument("--workload", default="blast3d",
+                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "poisson"])
+    ap.add_argument("--sor-grid", default="384,192,192", help="poisson: nr,ntheta,nphi of the star")
+    ap.add_argument("--sor-iters", type=int, default=100, help="poisson: SOR iterations per step")
+    ap.add_argument("--sor-full", type=int, default=1, help="poisson: also time the full solve from phi = 0 (0: skip)")
     ap.add_argument("--recon-c", default=None, help="reconstruction of the briowu/alfven3d/torus workloads")
     ap.add_argument("--batch-problems", type=int, default=512,
                     help="batch1d: run only the first N problems (profiler runs); the workload is 512")
@@ -583,7 +698,7 @@ def main():
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000}.get(args.workload, 0)
+        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "poisson": 20}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -600,6 +715,8 @@ def main():
         return bench_batch(args, world, rank, local, dist)
     if args.workload in ("briowu", "alfven3d", "torus"):
         return bench_config(args, world, rank, local, dist)
+    if args.workload == "poisson":
+        return bench_poisson(args, world, rank, local, dist)
 
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)

@@ -1787,7 +1787,7 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
         const int left = max_iter - st[0];
         const int chunk = left < 32 ? left : 32;
         for (int i = 0; i < chunk; ++i) CK(cudaGraphLaunch(h->sor_exec, h->stream));
-        h->launches += 4LL * chunk;
+        h->launches += 3LL * chunk;
         CK(cudaMemcpyAsync(st, s.state, 3 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         if (st[1] != 0) break;

@@ -143,6 +143,31 @@ INTERFACE
     REAL(C_FLOAT), VALUE :: threshold, audit_tol
     INTEGER(C_INT), VALUE :: flag_interval, audit_interval
   END FUNCTION
+  ! self-gravity potential of the collapsar model (spherical grids)
+  INTEGER(C_INT) FUNCTION cumc_poisson_setup(h, rho_atm, omega) BIND(C, NAME='cumc_poisson_setup')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), VALUE :: rho_atm, omega
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_poisson_solve(h, max_iter, tol, iters, err, converged) &
+      BIND(C, NAME='cumc_poisson_solve')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: max_iter
+    REAL(C_DOUBLE), VALUE :: tol
+    INTEGER(C_INT), INTENT(OUT) :: iters, converged
+    REAL(C_DOUBLE), INTENT(OUT) :: err
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_poisson_get(h, phi) BIND(C, NAME='cumc_poisson_get')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(OUT) :: phi(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_poisson_set(h, phi) BIND(C, NAME='cumc_poisson_set')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(IN) :: phi(*)
+  END FUNCTION
 END INTERFACE
 
 TYPE(C_PTR), SAVE :: cumc_h = C_NULL_PTR
