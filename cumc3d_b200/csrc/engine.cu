@@ -51,6 +51,7 @@ static const double small_num = 2.2250738585072014e-308;  // TINY(1.0D0)
 #define SINF(k) d.sinf[(k) + 3]
 #define DCOSE(k) d.dcose[(k) + 2]
 #define DSINE(k) d.dsine[(k) + 2]
+#define YC(k) d.y[(k) + 2]
 #define ZC(l) d.z[(l) + 2]
 #define DZ(l) d.dz[(l) + 2]
 
@@ -234,6 +235,53 @@ __global__ void k_fixpole(const Dev d) {
 }
 
 // ---------------------------------------------------------------------------
+// the collapsar model's black hole after each RK stage (CUSTOM_UPDATE,
+// model/collapsar/src/custom.f90:450-485): mdot from the stage's inner-face
+// mass flux (GETFLUX_X, custom.f90:222-240: flux(irho,0,k,l)), its mass by
+// the stage's Shu-Osher weights, r_sh = 2 m_bh / c^2.  One block of 1024
+// threads: thread t sums the terms t, t+1024, ... of the (k fastest) face
+// sequence in order, then a pairwise tree; the oracle sums in that order.
+// ---------------------------------------------------------------------------
+template <class FT>
+__global__ void __launch_bounds__(1024) k_bh_update(const Dev d, int stage) {
+    if (d.S->done) return;
+    __shared__ double part[1024];
+    const int t = threadIdx.x;
+    const FT *F0 = reinterpret_cast<const FT *>(d.FX[0]);
+    const double xf0 = XF(0);
+    double acc = 0.0;
+    const int n = d.ny * d.nz;
+    for (int i = t; i < n; i += 1024) {
+        const int k = i % d.ny + 1, l = i / d.ny + 1;
+        const double mflux = (double)F0[cidx(d, 0, k, l)];
+        acc = acc + (-mflux) * xf0 * xf0 * DCOSE(k) * DZ(l);
+    }
+    part[t] = acc;
+    __syncthreads();
+    for (int s = 512; s > 0; s >>= 1) {
+        if (t < s) part[t] = part[t] + part[t + s];
+        __syncthreads();
+    }
+    if (t == 0) {
+        const double mdot = dmax(part[0], 0.0);
+        const double dt = d.S->dt;
+        double m = d.S->m_bh;
+        if (stage == 1) {
+            d.S->mbh_old = m;
+            m = m + dt * mdot;
+        } else if (stage == 2) {
+            m = rk20 * d.S->mbh_old + rk21 * m + rk22 * dt * mdot;
+        } else {
+            m = rk30 * d.S->mbh_old + rk31 * m + rk32 * dt * mdot;
+        }
+        d.S->m_bh = m;
+        const double r_sh = 2.0 * m / (d.c_code * d.c_code);
+        d.S->r_sh = r_sh;
+        if (r_sh >= xf0) set_error(d, CUMC_ESTATE, -1, -2);  // the reference STOPs here
+    }
+}
+
+// ---------------------------------------------------------------------------
 // du/dt and the Shu-Osher combination over j,k,l = 0..n
 // ---------------------------------------------------------------------------
 template <class FT>  // storage type of the hydro face fluxes (double, or float in the FP32 form)
@@ -331,6 +379,27 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
                 sc[1] = sc[1] + (-(factor * rho * dphidr));
                 sc[3] = sc[3] + (-(factor * rho * dphidz));
                 sc[4] = sc[4] + (-(factor * rho * (vx * dphidr + vz * dphidz)));
+            } else if (d.source_kind == 4) {  // model/collapsar/src/custom.f90:355-385
+                const double diff = rho - d.rho_floor;
+                const double factor = dmax(sign1(diff), 0.0);
+                auto ph = [&](int a, int b, int c) {
+                    return d.phi[(a + b + c) & 1][(a >> 1) + (long long)d.phx * (b + (long long)(d.ny + 2) * c)];
+                };
+                // first_derivative (custom.f90:402-409) on the non-uniform centres
+                auto fd = [](double xm1, double xc, double xp1, double fm1, double fc, double fp1) {
+                    const double h2 = xp1 - xc, h1 = xc - xm1;
+                    return ((fp1 - fc) * h1 * h1 + (fc - fm1) * h2 * h2) / (h1 * h2 * (h1 + h2));
+                };
+                const double p0 = ph(j, k, l);
+                double dphidx = fd(XC(j - 1), XC(j), XC(j + 1), ph(j - 1, k, l), p0, ph(j + 1, k, l));
+                const double dphidy = fd(YC(k - 1), YC(k), YC(k + 1), ph(j, k - 1, l), p0, ph(j, k + 1, l));
+                const double dphidz = fd(ZC(l - 1), ZC(l), ZC(l + 1), ph(j, k, l - 1), p0, ph(j, k, l + 1));
+                const double m_bh = d.S->m_bh, r_sh = d.S->r_sh;
+                dphidx = dphidx + m_bh / ((XC(j) - r_sh) * (XC(j) - r_sh));
+                sc[1] = sc[1] - factor * rho * dphidx;
+                sc[2] = sc[2] - factor * rho * dphidy / XC(j);
+                sc[3] = sc[3] - factor * rho * dphidz / XC(j) / SINE(k);
+                sc[4] = sc[4] - factor * rho * (vx * dphidx + vy * dphidy / XC(j) + vz * dphidz / XC(j) / SINE(k));
             } else if (d.source_kind == 3) {  // model/torus-sph/src/custom.f90 (radial)
                 const double diff = rho - d.rho_floor;
                 const double factor = dmax(sign1(diff), 0.0);
@@ -483,6 +552,16 @@ __device__ __forceinline__ void apply_floor(const Dev &d, double &rho, double &v
         vx = factor * vx;
         vy = factor * vy;
         vz = factor * vz;
+        e = factor * e + (1.0 - factor) * d.eps_floor;
+        if (e < 0.0) e = d.eps_floor;
+    } else if (d.floor_kind == 3) {  // model/collapsar/src/custom.f90:289-304
+        // prim(irho:ivz) = factor*prim + (1-factor)*prim_a, prim_a = (rho_a, 0, 0, 0)
+        const double diff = rho - d.rho_floor;
+        const double factor = dmax(sign1(diff), 0.0);
+        rho = factor * rho + (1.0 - factor) * d.rho_floor;
+        vx = factor * vx + (1.0 - factor) * 0.0;
+        vy = factor * vy + (1.0 - factor) * 0.0;
+        vz = factor * vz + (1.0 - factor) * 0.0;
         e = factor * e + (1.0 - factor) * d.eps_floor;
         if (e < 0.0) e = d.eps_floor;
     }
@@ -804,6 +883,7 @@ struct cumc_handle {
     // self-gravity potential (cumc_poisson_*): host copies of the cell
     // centres (offset +2), the solver's device state and its step graph
     std::vector<double> xc_host, yc_host, zc_host;
+    double xf0 = 0.0;  // the inner radial face xF(0)
     SorDev sor{};
     bool sor_ready = false;
     double sor_rho_atm = 0.0;
@@ -1110,6 +1190,11 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     prof_begin(h);
     launch_fills(h, false);
     prof_end(h, PC_BND);
+    if (d.source_kind == 4) {
+        if (h->cfg.precision == CUMC_FP32) k_bh_update<float><<<1, 1024, 0, h->stream>>>(d, stage);
+        else k_bh_update<double><<<1, 1024, 0, h->stream>>>(d, stage);
+        h->launches++;
+    }
 }
 
 static void enqueue_finddt(cumc_handle *h, int clamp) {
@@ -1142,6 +1227,9 @@ static int check_scalars(cumc_handle *h) {
         int j = c >= 0 ? c % d.NX - 2 : 0, k = c >= 0 ? (c / d.NX) % d.NY - 2 : 0, l = c >= 0 ? c / (d.NX * d.NY) - 2 : 0;
         if (h->S_host->err_stage == -1)
             snprintf(buf, sizeof buf, "learned inference: a tensor-core MMA of tile %d did not complete", c);
+        else if (h->S_host->err_stage == -2)
+            snprintf(buf, sizeof buf, "black hole event horizon exceeds computational grid (r_sh %.17g >= xF(0))",
+                     h->S_host->r_sh);
         else
             snprintf(buf, sizeof buf, "non-finite or non-positive state at cell (%d,%d,%d), stage %d", j, k, l,
                      h->S_host->err_stage);
@@ -1235,6 +1323,7 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
         sinf[3] = 0.0; sinf[ny + 3] = 0.0;
     }
     h->xc_host = x;
+    h->xf0 = F(xF, 0);
     h->yc_host = y;
     h->zc_host = z;
     std::vector<double> wx = build_weights(cfg->recon, nx, dx), wy = build_weights(cfg->recon, ny, dy),
@@ -1461,6 +1550,8 @@ int cumc_rk3_step(cumc_handle *h, double dt) {
     if (!h) return fail(h, CUMC_EINVAL, "null handle");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, CUMC_EINVAL, "dt must be positive and finite");
+    if (h->d.source_kind == CUMC_SRC_COLLAPSAR && !h->d.phi[0])
+        return fail(h, CUMC_ENOTREADY, "the collapsar source needs cumc_poisson_setup first");
     CK(cudaMemcpyAsync(&h->d.S->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
     enqueue_step(h, false, false);
     CK(cudaGetLastError());
@@ -1471,6 +1562,8 @@ int cumc_evolve(cumc_handle *h, double t_end, int max_steps, double *t_inout, in
     if (!h || !t_inout) return fail(h, CUMC_EINVAL, "null argument");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
     if (steps_out) *steps_out = 0;
+    if (h->d.source_kind == CUMC_SRC_COLLAPSAR && !h->d.phi[0])
+        return fail(h, CUMC_ENOTREADY, "the collapsar source needs cumc_poisson_setup first");
     if (max_steps <= 0 || !(*t_inout < t_end)) return CUMC_OK;
     // device-side loop state
     Scalars s;
@@ -1547,6 +1640,8 @@ void *cumc_stream(cumc_handle *h) { return h ? (void *)h->stream : nullptr; }
 int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out) {
     if (!h || !ms_out || n_out < PC_N) return fail(h, CUMC_EINVAL, "need 8 output slots");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    if (h->d.source_kind == CUMC_SRC_COLLAPSAR && !h->d.phi[0])
+        return fail(h, CUMC_ENOTREADY, "the collapsar source needs cumc_poisson_setup first");
     for (int i = 0; i < PC_N; ++i) h->prof_ms[i] = 0.0;
     h->prof_class = 0;
     for (int s = 0; s < nsteps; ++s) {
@@ -1751,6 +1846,12 @@ int cumc_poisson_setup(cumc_handle *h, double rho_atm, double omega) {
     }
     s.omega = omega;
     h->sor_rho_atm = rho_atm;
+    // the collapsar source reads the potential: the step graph holds the old Dev
+    h->d.phi[0] = s.phi[0];
+    h->d.phi[1] = s.phi[1];
+    h->d.phx = s.hx;
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
     // the initial model's guess: phi = 0 everywhere, ghosts included (custom.f90:498-507)
     for (int c = 0; c < 2; ++c) CK(cudaMemsetAsync(s.phi[c], 0, half * sizeof(double), h->stream));
     // omega lives in the captured kernel parameters: capture again
@@ -1798,6 +1899,40 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
     if (iters_out) *iters_out = st[0];
     if (err_out) *err_out = e;
     if (converged_out) *converged_out = st[1] == 1 ? 1 : 0;
+    return CUMC_OK;
+}
+
+int cumc_collapsar_set(cumc_handle *h, double m_bh, double c_code) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (h->d.source_kind != CUMC_SRC_COLLAPSAR || h->d.coord != 2)
+        return fail(h, CUMC_EINVAL, "the black hole belongs to a spherical handle with the collapsar source");
+    if (!(m_bh >= 0.0) || !(c_code > 0.0)) return fail(h, CUMC_EINVAL, "bad black hole mass or speed of light");
+    // r_sh as CUSTOM_UPDATE computes it (custom.f90:481)
+    const double r_sh = 2.0 * m_bh / (c_code * c_code);
+    if (r_sh >= h->xf0) return fail(h, CUMC_EINVAL, "black hole event horizon exceeds computational grid");
+    Scalars sc;
+    CK(cudaMemcpyAsync(&sc, h->d.S, sizeof sc, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    sc.m_bh = m_bh;
+    sc.mbh_old = m_bh;
+    sc.r_sh = r_sh;
+    CK(cudaMemcpyAsync(h->d.S, &sc, sizeof sc, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->d.c_code != c_code) {
+        h->d.c_code = c_code;
+        if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+        if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    }
+    return CUMC_OK;
+}
+
+int cumc_collapsar_get(cumc_handle *h, double *m_bh, double *r_sh) {
+    if (!h || !m_bh || !r_sh) return fail(h, CUMC_EINVAL, "null argument");
+    Scalars sc;
+    CK(cudaMemcpyAsync(&sc, h->d.S, sizeof sc, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *m_bh = sc.m_bh;
+    *r_sh = sc.r_sh;
     return CUMC_OK;
 }
 

@@ -25,6 +25,9 @@ struct Scalars {
     int err_cell;                // padded linear index of that cell
     int err_stage;
     int pad[2];
+    // the collapsar model's black hole: mass, its value at the step's start,
+    // the pseudo-Newtonian radius 2 m_bh / c^2
+    double m_bh, mbh_old, r_sh;
 };
 
 struct Dev {
@@ -76,6 +79,11 @@ struct Dev {
     unsigned char *lfb[3];       // per direction, per 128-cell tile: 1 = fall back to WENO-Z
     unsigned char *lflag[3];     // per direction, per reconstructed cell: the stage-1 flag
     unsigned char *lwarp[3];     // per direction, per warp of the staged reconstruction: 1 = linear
+    // the collapsar model: the self-gravity potential (colour-split, see
+    // poisson.cuh; null until cumc_poisson_setup) and c in code units
+    const double *phi[2];
+    int phx;
+    double c_code;
     unsigned long long *lstats;  // audit counters (LEARN_STAT_SLOTS x LEARN_STAT_FIELDS)
 };
 

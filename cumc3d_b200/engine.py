@@ -26,7 +26,8 @@ EXPORTS = [
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
     "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest",
-    "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set",
+    "cumc_collapsar_set", "cumc_collapsar_get", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
@@ -92,6 +93,8 @@ def load_library(path=None):
                                      C.POINTER(C.c_int)]
     L.cumc_poisson_get.argtypes = [C.c_void_p, C.c_void_p]
     L.cumc_poisson_set.argtypes = [C.c_void_p, C.c_void_p]
+    L.cumc_collapsar_set.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.cumc_collapsar_get.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.cumc_learn_flags.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
     L.cumc_mlp_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p, C.c_void_p]
@@ -255,6 +258,16 @@ class Solver:
         if P.shape != (sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2):
             raise ValueError("phi must be (nz+2, ny+2, nx+2)")
         self._check(self.L.cumc_poisson_set(self.h, P.ctypes.data))
+
+    def collapsar_set(self, m_bh, c_code):
+        """The collapsar model's black hole: mass and c in code units."""
+        self._check(self.L.cumc_collapsar_set(self.h, float(m_bh), float(c_code)))
+
+    def collapsar_get(self):
+        """(m_bh, r_sh) as the last stage left them."""
+        m, r = C.c_double(), C.c_double()
+        self._check(self.L.cumc_collapsar_get(self.h, C.byref(m), C.byref(r)))
+        return m.value, r.value
 
     def learn_flags(self, direction):
         """The stored learned-flag state of one sweep: per-cell flags, per-warp

@@ -20,6 +20,9 @@ INTEGER(C_INT), PARAMETER :: CUMC_RECON_TVD_MM = 0, CUMC_RECON_TVD_VL = 1, CUMC_
 INTEGER(C_INT), PARAMETER :: CUMC_RECON_PPM = 3, CUMC_RECON_WENO = 4
 INTEGER(C_INT), PARAMETER :: CUMC_RS_LF = 0, CUMC_RS_HLL = 1, CUMC_RS_HLLC = 2, CUMC_RS_HLLD = 3
 INTEGER(C_INT), PARAMETER :: CUMC_FP64 = 0, CUMC_FP32 = 1
+INTEGER(C_INT), PARAMETER :: CUMC_FLOOR_NONE = 0, CUMC_FLOOR_EPS = 1, CUMC_FLOOR_TORUS = 2, CUMC_FLOOR_COLLAPSAR = 3
+INTEGER(C_INT), PARAMETER :: CUMC_SRC_NONE = 0, CUMC_SRC_CONST_GY = 1, CUMC_SRC_PM_CYL = 2, CUMC_SRC_PM_SPH = 3
+INTEGER(C_INT), PARAMETER :: CUMC_SRC_COLLAPSAR = 4
 
 ! cumc_model (include/cumc3d_gpu.h)
 TYPE, BIND(C) :: cumc_model
@@ -167,6 +170,17 @@ INTERFACE
     IMPORT :: C_INT, C_PTR, C_DOUBLE
     TYPE(C_PTR), VALUE :: h
     REAL(C_DOUBLE), INTENT(IN) :: phi(*)
+  END FUNCTION
+  ! the collapsar model's black hole
+  INTEGER(C_INT) FUNCTION cumc_collapsar_set(h, m_bh, c_code) BIND(C, NAME='cumc_collapsar_set')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), VALUE :: m_bh, c_code
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_collapsar_get(h, m_bh, r_sh) BIND(C, NAME='cumc_collapsar_get')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(OUT) :: m_bh, r_sh
   END FUNCTION
 END INTERFACE
 

@@ -326,6 +326,31 @@ def star_sph(nr=96, ntheta=48, nphi=48, r_range=(2.0, 40.0), theta_range=(0.1 * 
     return spec, prim, np.ascontiguousarray(eps)
 
 
+def collapsar_sph(nr=96, ntheta=48, nphi=48, m_bh=0.2, c_code=20.0, v_in=0.02, rho_c=0.01, **kw):
+    """The star of star_sph set up as the collapsar model runs it: its
+    floors (the atmosphere state prim_a = the outermost cell, zero velocity,
+    model/collapsar/src/model.f90:238-242) and its source (self-gravity of
+    the potential plus a black hole of mass m_bh; c_code = the speed of light
+    in code units, r_sh = 2 m_bh / c_code^2), and an inflow of speed v_in
+    that fades outward, so the hole accretes.  No magnetic field.  Returns
+    (spec, prim, eps)."""
+    g = 5.0 / 3.0
+    spec, prim, eps = star_sph(nr, ntheta, nphi, rho_c=rho_c, **kw)
+    r = centers(spec["xF"])
+    rho_a = float(prim[3, 3, nr + 2, IRHO])   # prim(irho, nx, 1, 1)
+    p_a = float(prim[3, 3, nr + 2, ITAU])
+    prim[..., IVX] = -v_in * np.exp(-(r[None, None, :] - r[3]) / 4.0)
+    eps = prim[..., ITAU] / prim[..., IRHO] / (g - 1.0)
+    spec["boundary_flag"] = [1, 1] + list(spec["boundary_flag"][2:])
+    spec["model"] = dict(gamma=g, floor="collapsar", rho_floor=rho_a, eps_floor=p_a / rho_a / (g - 1.0),
+                         source="collapsar", bc="none")
+    spec["rho_atm"] = rho_a
+    spec["m_bh"] = m_bh
+    spec["c_code"] = c_code
+    spec["name"] = "collapsar_sph_%dx%dx%d" % (nr, ntheta, nphi)
+    return spec, prim, np.ascontiguousarray(eps)
+
+
 # ---------------------------------------------------------------------------
 # named workloads
 # ---------------------------------------------------------------------------

@@ -64,11 +64,20 @@ extern "C" {
 #define CUMC_FLOOR_EPS   1   /* model/riemann/src/custom.f90:260-284          */
 #define CUMC_FLOOR_TORUS 2   /* model/torus-cyn/src/custom.f90:240-275,
                                 model/torus-cyn/src/findpressure.f90:7-37    */
+#define CUMC_FLOOR_COLLAPSAR 3 /* model/collapsar/src/custom.f90:269-330: the
+                                atmosphere prim_a = (rho_floor, v = 0, eps_floor)
+                                blended in below it; ideal-gas FINDPRESSURE
+                                (model/collapsar/src/findpressure.f90)         */
 /* model source terms (CUSTOM_SOURCE) */
 #define CUMC_SRC_NONE     0
 #define CUMC_SRC_CONST_GY 1  /* model/riemann/src/custom.f90:289-316          */
 #define CUMC_SRC_PM_CYL   2  /* model/torus-cyn/src/custom.f90:280-320        */
 #define CUMC_SRC_PM_SPH   3  /* model/torus-sph/src/custom.f90 (radial form)  */
+#define CUMC_SRC_COLLAPSAR 4 /* model/collapsar/src/custom.f90:340-395: gravity of
+                                the potential of cumc_poisson_* plus the black
+                                hole m_bh/(r - r_sh)^2; the hole's mass grows
+                                each stage by the inner-face mass flux
+                                (custom.f90:450-478, cumc_collapsar_set)       */
 /* model boundary hooks (CUSTOM_BOUNDARY_X/Y/Z) */
 #define CUMC_BC_NONE      0
 #define CUMC_BC_TORUS_CYL 1  /* model/torus-cyn/src/custom.f90:146-208        */
@@ -304,6 +313,19 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
  * or set it (a warm start, or a restart from a checkpoint). */
 int cumc_poisson_get(cumc_handle *h, double *phi);
 int cumc_poisson_set(cumc_handle *h, const double *phi);
+
+/* The collapsar model's black hole (model/collapsar/src/custom.f90:450-485),
+ * for a spherical handle with source_kind CUMC_SRC_COLLAPSAR: its mass m_bh
+ * and the speed of light in code units c_code (clight * vel2code), so that
+ * r_sh = 2 m_bh / c_code^2.  After every RK stage the mass grows by
+ * dt * max(mdot, 0), mdot = the inner-face mass flux summed over the sphere
+ * (-flux(irho,0,k,l) xF(0)^2 dcose(k) dz(l)), combined with the stage's
+ * Shu-Osher weights.  A horizon reaching the inner face (r_sh >= xF(0)) ends
+ * the step with CUMC_ESTATE (the reference STOPs).  The sum's order is
+ * fixed (1024 strided partial sums in sequence, then a pairwise tree); the
+ * reference's OpenMP reduction leaves it unspecified. */
+int cumc_collapsar_set(cumc_handle *h, double m_bh, double c_code);
+int cumc_collapsar_get(cumc_handle *h, double *m_bh, double *r_sh);
 
 /* For inspection (no counterpart in the reference): the learned-flag state of
  * sweep dir as the last refresh left it.  flags = one byte per cell of the

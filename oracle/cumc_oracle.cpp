@@ -116,6 +116,13 @@ struct Sim {
     std::vector<R> primL, primR, uL, uR, fluxL, fluxR;  /* 8 vars */
     std::vector<R> eps, cs, dpdrho, dpdeps, epsL, epsR, csL, csR;
     std::vector<R> bcell, ecell;  /* 3 vars */
+    /* the collapsar model (CUMC_SRC_COLLAPSAR): the self-gravity potential
+     * on cells 0..n+1 (natural layout, j fastest), the black hole, and the
+     * inner-face mass flux of the x sweep (GETFLUX_X's mflux_x(k,l)) */
+    std::vector<double> phi_;
+    double m_bh = 0.0, mbh_old = 0.0, r_sh = 0.0, c_code = 1.0;
+    bool horizon_hit = false;
+    std::vector<R> mflux;
     std::vector<R> eface;         /* 6 vars */
     std::vector<R> efx, efy, efz;
 
@@ -377,6 +384,21 @@ struct Sim {
                         E(j, k, l) = factor * E(j, k, l) + (1.0 - factor) * eps_floor;
                         if (E(j, k, l) < 0.0) E(j, k, l) = eps_floor;
                     }
+        } else if (m.floor_kind == CUMC_FLOOR_COLLAPSAR) {
+            /* model/collapsar/src/custom.f90:289-304: prim(irho:ivz) blended
+             * with the atmosphere prim_a = (rho_a, 0, 0, 0), eps with eps_a */
+            const double rho_a = m.rho_floor, eps_a = m.eps_floor;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j) {
+                        R diff = P(irho, j, k, l) - rho_a;
+                        R factor = max_(sign1_(diff), R(0.0));
+                        P(irho, j, k, l) = factor * P(irho, j, k, l) + (1.0 - factor) * rho_a;
+                        for (int i = ivx; i <= ivz; ++i) P(i, j, k, l) = factor * P(i, j, k, l) + (1.0 - factor) * 0.0;
+                        E(j, k, l) = factor * E(j, k, l) + (1.0 - factor) * eps_a;
+                        if (E(j, k, l) < 0.0) E(j, k, l) = eps_a;
+                    }
         }
     }
 
@@ -429,6 +451,34 @@ struct Sim {
                         SC(ivz, j, k, l) = SC(ivz, j, k, l) + (-(factor * P(irho, j, k, l) * dphidz));
                         SC(itau, j, k, l) = SC(itau, j, k, l) +
                             (-(factor * P(irho, j, k, l) * (P(ivx, j, k, l) * dphidr + P(ivz, j, k, l) * dphidz)));
+                    }
+        } else if (m.source_kind == CUMC_SRC_COLLAPSAR) {
+            /* model/collapsar/src/custom.f90:355-385: the potential's gradient
+             * (first_derivative, custom.f90:402-409) plus the black hole */
+            const long long px = nx + 2, py = (long long)(nx + 2) * (ny + 2);
+            auto ph = [&](int j, int k, int l) { return R(phi_[j + px * k + py * l]); };
+            auto fd = [](R xm1, R xc, R xp1, R fm1, R fc, R fp1) {
+                R h2 = xp1 - xc, h1 = xc - xm1;
+                return ((fp1 - fc) * h1 * h1 + (fc - fm1) * h2 * h2) / (h1 * h2 * (h1 + h2));
+            };
+            const double mb = m_bh, rs = r_sh;
+#pragma omp parallel for collapse(2) schedule(static)
+            for (int l = 1; l <= nz; ++l)
+                for (int k = 1; k <= ny; ++k)
+                    for (int j = 1; j <= nx; ++j) {
+                        R diff = P(irho, j, k, l) - m.rho_floor;
+                        R factor = max_(sign1_(diff), R(0.0));
+                        R dphidx = fd(R(x(j - 1)), R(x(j)), R(x(j + 1)), ph(j - 1, k, l), ph(j, k, l), ph(j + 1, k, l));
+                        R dphidy = fd(R(y(k - 1)), R(y(k)), R(y(k + 1)), ph(j, k - 1, l), ph(j, k, l), ph(j, k + 1, l));
+                        R dphidz = fd(R(z(l - 1)), R(z(l)), R(z(l + 1)), ph(j, k, l - 1), ph(j, k, l), ph(j, k, l + 1));
+                        dphidx = dphidx + mb / ((x(j) - rs) * (x(j) - rs));
+                        const R rho = P(irho, j, k, l);
+                        SC(ivx, j, k, l) = SC(ivx, j, k, l) - factor * rho * dphidx;
+                        SC(ivy, j, k, l) = SC(ivy, j, k, l) - factor * rho * dphidy / x(j);
+                        SC(ivz, j, k, l) = SC(ivz, j, k, l) - factor * rho * dphidz / x(j) / sine(k);
+                        SC(itau, j, k, l) = SC(itau, j, k, l) -
+                            factor * rho * (P(ivx, j, k, l) * dphidx + P(ivy, j, k, l) * dphidy / x(j) +
+                                            P(ivz, j, k, l) * dphidz / x(j) / sine(k));
                     }
         } else if (m.source_kind == CUMC_SRC_PM_SPH) {
             /* model/torus-sph/src/custom.f90 CUSTOM_SOURCE (radial form) */
@@ -1192,6 +1242,12 @@ struct Sim {
             recon(dir);
             buildstates(dir);
             riemann(dir);
+            if (dir == 1 && cfg.model.source_kind == CUMC_SRC_COLLAPSAR) {
+                /* GETFLUX_X, model/collapsar/src/custom.f90:222-240 */
+                mflux.assign((size_t)ny * nz, R(0.0));
+                for (int l = 1; l <= nz; ++l)
+                    for (int k = 1; k <= ny; ++k) mflux[(size_t)(k - 1) + (size_t)ny * (l - 1)] = FL(irho, 0, k, l);
+            }
             flux_diff(dir);
             mhd_flux(dir);
         }
@@ -1234,7 +1290,42 @@ struct Sim {
             fromrvetou();
             boundary();
             update();
+            custom_update(stage, dt);
         }
+    }
+
+    /* CUSTOM_UPDATE of the collapsar model for p_in = stage > 0
+     * (model/collapsar/src/custom.f90:450-485): mdot from the inner-face mass
+     * flux, the black hole mass by the stage's Shu-Osher weights, r_sh.  The
+     * reference sums with an OpenMP reduction of unspecified order; this
+     * sums in the engine's fixed order: 1024 strided partial sums, each in
+     * sequence, then a pairwise tree. */
+    void custom_update(int stage, double dt) {
+        if (cfg.model.source_kind != CUMC_SRC_COLLAPSAR) return;
+        const int n = ny * nz;
+        std::vector<R> part(1024);
+        const double xf0 = xF(0);
+        for (int t = 0; t < 1024; ++t) {
+            R acc = R(0.0);
+            for (int i = t; i < n; i += 1024) {
+                const int k = i % ny + 1, l = i / ny + 1;
+                acc = acc + (-mflux[(size_t)i]) * xf0 * xf0 * dcose(k) * dz(l);
+            }
+            part[(size_t)t] = acc;
+        }
+        for (int s = 512; s > 0; s >>= 1)
+            for (int t = 0; t < s; ++t) part[(size_t)t] = part[(size_t)t] + part[(size_t)(t + s)];
+        const double mdot = dv(max_(part[0], R(0.0)));
+        if (stage == 1) {
+            mbh_old = m_bh;
+            m_bh = mbh_old + dt * mdot;
+        } else if (stage == 2) {
+            m_bh = rk20 * mbh_old + rk21 * m_bh + rk22 * dt * mdot;
+        } else {
+            m_bh = rk30 * mbh_old + rk31 * m_bh + rk32 * dt * mdot;
+        }
+        r_sh = 2.0 * m_bh / (c_code * c_code);
+        if (r_sh >= xf0) horizon_hit = true;  /* the reference STOPs */
     }
 
     /* INITIAL_UPDATE initial.f90:86-116 */
@@ -1700,6 +1791,33 @@ int orc_poisson_solve(const cumc_config *cfg, const double *rho, double rho_atm,
     if (iters) *iters = converged ? n : max_iter;
     if (err) *err = abserror;
     return converged;
+}
+
+/* the collapsar model's black hole and potential (engine: cumc_collapsar_*,
+ * cumc_poisson_*); phi: (nx+2)*(ny+2)*(nz+2), j fastest */
+void orc_collapsar_set(void *p, double m_bh, double c_code) {
+    Handle *h = (Handle *)p;
+    auto set = [&](auto *s) {
+        s->m_bh = m_bh;
+        s->mbh_old = m_bh;
+        s->c_code = c_code;
+        s->r_sh = 2.0 * m_bh / (c_code * c_code);
+    };
+    if (h->counting) set(h->c); else set(h->d);
+}
+int orc_collapsar_get(void *p, double *m_bh, double *r_sh) {
+    Handle *h = (Handle *)p;
+    auto get = [&](auto *s) {
+        *m_bh = s->m_bh;
+        *r_sh = s->r_sh;
+        return s->horizon_hit ? 1 : 0;
+    };
+    return h->counting ? get(h->c) : get(h->d);
+}
+void orc_set_phi(void *p, const double *phi) {
+    Handle *h = (Handle *)p;
+    auto set = [&](auto *s) { s->phi_.assign(phi, phi + (size_t)(s->nx + 2) * (s->ny + 2) * (s->nz + 2)); };
+    if (h->counting) set(h->c); else set(h->d);
 }
 
 void orc_reset_counts(void) { g_ops = OpCounts(); }

@@ -68,6 +68,10 @@ def lib():
         L.orc_poisson_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
                                         C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.orc_poisson_solve.restype = C.c_int
+        L.orc_collapsar_set.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.orc_collapsar_get.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_collapsar_get.restype = C.c_int
+        L.orc_set_phi.argtypes = [C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -127,6 +131,21 @@ class Oracle:
         tt = C.c_double(t)
         n = lib().orc_evolve(self.h, t_end, max_steps, C.byref(tt))
         return tt.value, n
+
+    def collapsar_set(self, m_bh, c_code):
+        lib().orc_collapsar_set(self.h, float(m_bh), float(c_code))
+
+    def collapsar_get(self):
+        """(m_bh, r_sh, horizon reached the inner face)."""
+        m, r = C.c_double(), C.c_double()
+        hit = lib().orc_collapsar_get(self.h, C.byref(m), C.byref(r))
+        return m.value, r.value, bool(hit)
+
+    def set_phi(self, phi):
+        sp = self.spec
+        P = np.ascontiguousarray(phi, dtype=np.float64)
+        assert P.shape == (sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2)
+        lib().orc_set_phi(self.h, P.ctypes.data)
 
     def max_divb(self):
         return lib().orc_max_divb(self.h)
