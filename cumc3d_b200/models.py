@@ -367,12 +367,20 @@ WORKLOADS = {
 # ---------------------------------------------------------------------------
 def smooth_state(nx, ny, nz, n_dim, coordinate_flag=0, boundary_flag=(0, 0, 0, 0, 0, 0), x_range=(0.0, 1.0),
                  y_range=(0.0, 1.0), z_range=(0.0, 1.0), seed=1, recon="weno", riemann="hlld", cfl=0.4,
-                 gamma=5.0 / 3.0, precision="fp64", model=None, **kw):
+                 gamma=5.0 / 3.0, precision="fp64", model=None, faces=None, **kw):
+    """faces: optional (xF, yF, zF) face arrays (indices -3..n+3), e.g. the
+    non-uniform grids of cumc3d_b200.grids; the ranges then follow them."""
     rng = np.random.Generator(np.random.PCG64(seed))
     spec = _base_spec(nx, ny, nz, n_dim, boundary_flag, x_range, y_range, z_range,
                       coordinate_flag=coordinate_flag, cfl=cfl, recon=recon, riemann=riemann,
                       precision=precision, model=model or dict(gamma=gamma, floor="eps"),
                       name="smooth_%dd_c%d" % (n_dim, coordinate_flag), **kw)
+    if faces is not None:
+        for key, f, n in zip(("xF", "yF", "zF"), faces, (nx, ny, nz)):
+            f = np.asarray(f, dtype=np.float64)
+            assert f.shape == (n + 7,)
+            spec[key] = f
+        x_range, y_range, z_range = ((float(f[3]), float(f[-4])) for f in faces)
     xf, yf, zf = spec["xF"], spec["yF"], spec["zF"]
     X = (centers(xf) - x_range[0]) / (x_range[1] - x_range[0])
     Y = (centers(yf) - y_range[0]) / (y_range[1] - y_range[0])

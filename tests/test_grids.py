@@ -1,0 +1,51 @@
+"""Non-uniform grid files and generators (CPU): the restated generators
+against the grid files the reference ships (model/torus-*/grid/*.dat, when
+the reference tree is present), and the CUSTOM_GRID reader's checks."""
+import os
+
+import numpy as np
+import pytest
+
+from cumc3d_b200 import grids
+
+REF = "/root/reference/model"
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+def test_generators_reproduce_the_shipped_grid_files_bitwise():
+    nx, ny, nz, r, th, ph = grids.spherical_torus_grid()
+    xF, yF, zF = grids.load_grid(os.path.join(REF, "torus-sph", "grid"), nx, ny, nz,
+                                 names=("r_grid.dat", "th_grid.dat", "phi_grid.dat"))
+    for a, b in ((r, xF), (th, yF), (ph, zF)):
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    nr, nphi, nz, r, ph, z = grids.cylindrical_torus_grid()
+    xF, yF, zF = grids.load_grid(os.path.join(REF, "torus-cyn", "grid"), nr, nphi, nz)
+    for a, b in ((r, xF), (ph, yF), (z, zF)):
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_generated_grids_have_the_expected_shape():
+    nx, ny, nz, r, th, ph = grids.spherical_torus_grid()
+    assert (nx, ny, nz) == (124, 44, 128)
+    assert r[3] == 1.5 and abs(r[-4] - 31.5) < 1e-12 and th[3] == 0.0 and th[-4] == np.pi
+    assert np.all(np.diff(r) > 0) and np.all(np.diff(th) > 0)
+    # geometric stretching away from the equator, mirrored through it
+    d = np.diff(th[3:-3])
+    assert np.allclose(d, d[::-1]) and d[0] > d[len(d) // 2]
+    nr, nphi, nz, r, ph, z = grids.cylindrical_torus_grid()
+    assert (nr, nphi, nz) == (136, 128, 136)
+    assert np.array_equal(z, -z[::-1])
+
+
+def test_unsolvable_stretching_is_refused():
+    with pytest.raises(ValueError, match="no theta stretching"):
+        grids.spherical_torus_grid(nz=64)
+
+
+def test_reader_checks_the_line_count_and_round_trips(tmp_path):
+    nx, ny, nz, r, th, ph = grids.spherical_torus_grid(nz=96)
+    p = tmp_path / "r_grid.dat"
+    grids.write_faces(p, r)
+    assert np.array_equal(grids.read_faces(p, nx), r)
+    with pytest.raises(ValueError, match="inconsistent number of r-grid faces"):
+        grids.read_faces(p, nx + 1, "r")
