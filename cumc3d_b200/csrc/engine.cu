@@ -282,6 +282,33 @@ __global__ void __launch_bounds__(1024) k_bh_update(const Dev d, int stage) {
 }
 
 // ---------------------------------------------------------------------------
+// output snapshot (print_hydroprofile, solver/mhd/dataio.f90:31-240): the
+// datasets "primitive" = prim(imin:ibx-1, 0:nx+1, 0:ny+1, 0:nz+1),
+// "epsilon" = epsilon(0:nx+1, 0:ny+1, 0:nz+1) and "bfield" =
+// prim(ibx:ibz, -1:nx+1, -1:ny+1, -1:nz+1), each in Fortran order, packed
+// into one device buffer in that order.  One thread per cell of -1..n+1.
+// ---------------------------------------------------------------------------
+__global__ void k_snapshot_pack(const Dev d, double *__restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x - 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y - 1;
+    const int l = blockIdx.z - 1;
+    if (j > d.nx + 1 || k > d.ny + 1) return;
+    const long long px = d.nx + 2, py = d.ny + 2, pz = d.nz + 2;
+    const long long n_prim = 5 * px * py * pz, n_eps = px * py * pz;
+    const int c = cidx(d, j, k, l);
+    const long long b = 3 * ((j + 1) + (long long)(d.nx + 3) * ((k + 1) + (long long)(d.ny + 3) * (l + 1)));
+    double *bf = out + n_prim + n_eps;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) bf[b + v] = d.P[5 + v][c];
+    if (j >= 0 && k >= 0 && l >= 0) {
+        const long long e = j + px * (k + py * l);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) out[5 * e + v] = d.P[v][c];
+        out[n_prim + e] = d.EPS[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // du/dt and the Shu-Osher combination over j,k,l = 0..n
 // ---------------------------------------------------------------------------
 template <class FT>  // storage type of the hydro face fluxes (double, or float in the FP32 form)
@@ -889,6 +916,11 @@ struct cumc_handle {
     double sor_rho_atm = 0.0;
     cudaGraph_t sor_graph = nullptr;
     cudaGraphExec_t sor_exec = nullptr;
+    // output snapshots (cumc_snapshot_*): device staging, copy stream, events
+    double *snap_dev = nullptr;
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_packed = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
 };
 
 static std::string g_create_err;
@@ -1450,6 +1482,12 @@ int cumc_destroy(cumc_handle *h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     if (h->sor_exec) cudaGraphExecDestroy(h->sor_exec);
     if (h->sor_graph) cudaGraphDestroy(h->sor_graph);
+    if (h->snap_stream) {  // a snapshot copy in flight reads the staging buffer
+        cudaStreamSynchronize(h->snap_stream);
+        cudaStreamDestroy(h->snap_stream);
+    }
+    if (h->snap_packed) cudaEventDestroy(h->snap_packed);
+    if (h->snap_done) cudaEventDestroy(h->snap_done);
     for (void *p : h->allocs) cudaFree(p);
     for (int i = 0; i < 2; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -1899,6 +1937,52 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
     if (iters_out) *iters_out = st[0];
     if (err_out) *err_out = e;
     if (converged_out) *converged_out = st[1] == 1 ? 1 : 0;
+    return CUMC_OK;
+}
+
+int cumc_snapshot_start(cumc_handle *h, double *primitive, double *epsilon, double *bfield) {
+    if (!h || !primitive || !epsilon || !bfield) return fail(h, CUMC_EINVAL, "null argument");
+    if (!h->have_state) return fail(h, CUMC_ENOTREADY, "no state: cumc_set_state first");
+    const Dev &d = h->d;
+    const size_t n_prim = (size_t)5 * (d.nx + 2) * (d.ny + 2) * (d.nz + 2);
+    const size_t n_eps = (size_t)(d.nx + 2) * (d.ny + 2) * (d.nz + 2);
+    const size_t n_b = (size_t)3 * (d.nx + 3) * (d.ny + 3) * (d.nz + 3);
+    if (h->snap_pending) {  // one snapshot in flight at a time
+        int rc = cumc_snapshot_wait(h);
+        if (rc) return rc;
+    }
+    if (!h->snap_dev) {
+        double *p = nullptr;
+        if (cudaMalloc(&p, (n_prim + n_eps + n_b) * sizeof(double)) != cudaSuccess)
+            return fail(h, CUMC_ENOMEM, "snapshot staging: out of device memory");
+        h->allocs.push_back(p);
+        h->snap_dev = p;
+        CK(cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->snap_packed, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+    }
+    // pack on the compute stream (after the steps issued so far), copy out on
+    // the copy stream while later steps run
+    const dim3 b(32, 8, 1), g((d.nx + 3 + 31) / 32, (d.ny + 3 + 7) / 8, d.nz + 3);
+    k_snapshot_pack<<<g, b, 0, h->stream>>>(d, h->snap_dev);
+    h->launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->snap_packed, h->stream));
+    CK(cudaStreamWaitEvent(h->snap_stream, h->snap_packed, 0));
+    CK(cudaMemcpyAsync(primitive, h->snap_dev, n_prim * sizeof(double), cudaMemcpyDeviceToHost, h->snap_stream));
+    CK(cudaMemcpyAsync(epsilon, h->snap_dev + n_prim, n_eps * sizeof(double), cudaMemcpyDeviceToHost, h->snap_stream));
+    CK(cudaMemcpyAsync(bfield, h->snap_dev + n_prim + n_eps, n_b * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->snap_stream));
+    CK(cudaEventRecord(h->snap_done, h->snap_stream));
+    h->snap_pending = true;
+    return CUMC_OK;
+}
+
+int cumc_snapshot_wait(cumc_handle *h) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->snap_pending) return CUMC_OK;
+    h->snap_pending = false;
+    CK(cudaEventSynchronize(h->snap_done));
     return CUMC_OK;
 }
 

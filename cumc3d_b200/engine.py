@@ -27,7 +27,7 @@ EXPORTS = [
     "cumc_batch_run1_noalloc",
     "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest",
     "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set",
-    "cumc_collapsar_set", "cumc_collapsar_get", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_collapsar_set", "cumc_collapsar_get", "cumc_snapshot_start", "cumc_snapshot_wait", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
@@ -94,6 +94,8 @@ def load_library(path=None):
     L.cumc_poisson_get.argtypes = [C.c_void_p, C.c_void_p]
     L.cumc_poisson_set.argtypes = [C.c_void_p, C.c_void_p]
     L.cumc_collapsar_set.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.cumc_snapshot_start.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.cumc_snapshot_wait.argtypes = [C.c_void_p]
     L.cumc_collapsar_get.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.cumc_learn_flags.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
@@ -258,6 +260,25 @@ class Solver:
         if P.shape != (sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2):
             raise ValueError("phi must be (nz+2, ny+2, nx+2)")
         self._check(self.L.cumc_poisson_set(self.h, P.ctypes.data))
+
+    # ---- output snapshots (print_hydroprofile's datasets, cumc_snapshot_*) ----
+    def snapshot_start(self, primitive, epsilon, bfield):
+        """Start copying the state into three float64 arrays (shapes of
+        cumc3d_b200.snapshot.buffers; page-locked ones make it asynchronous).
+        Keep them alive and untouched until snapshot_wait."""
+        sp = self.spec
+        shp = ((sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2, 5), (sp["nz"] + 2, sp["ny"] + 2, sp["nx"] + 2),
+               (sp["nz"] + 3, sp["ny"] + 3, sp["nx"] + 3, 3))
+        for a, s in zip((primitive, epsilon, bfield), shp):
+            if a.shape != s or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("snapshot buffer must be a contiguous float64 array of shape %s" % (s,))
+        self._snap = (primitive, epsilon, bfield)  # kept alive while the copy runs
+        self._check(self.L.cumc_snapshot_start(self.h, primitive.ctypes.data, epsilon.ctypes.data,
+                                               bfield.ctypes.data))
+
+    def snapshot_wait(self):
+        self._check(self.L.cumc_snapshot_wait(self.h))
+        self._snap = None
 
     def collapsar_set(self, m_bh, c_code):
         """The collapsar model's black hole: mass and c in code units."""

@@ -314,6 +314,22 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
 int cumc_poisson_get(cumc_handle *h, double *phi);
 int cumc_poisson_set(cumc_handle *h, const double *phi);
 
+/* Output snapshot without stalling the step loop (print_hydroprofile,
+ * solver/mhd/dataio.f90:31-240, which updates the host copy and writes HDF5).
+ * cumc_snapshot_start packs the state as the reference writes it --
+ * primitive = prim(1:5, 0:nx+1, 0:ny+1, 0:nz+1) (5*(nx+2)*(ny+2)*(nz+2)
+ * doubles), epsilon = epsilon(0:nx+1, 0:ny+1, 0:nz+1), bfield =
+ * prim(ibx:ibz, -1:nx+1, -1:ny+1, -1:nz+1) (3*(nx+3)*(ny+3)*(nz+3)), all in
+ * Fortran order -- into a device buffer, after the steps already issued, and
+ * copies it to the three host buffers on a separate stream; steps issued
+ * afterwards run meanwhile and do not change the snapshot.  The buffers may
+ * not be read or freed until cumc_snapshot_wait returns.  Page-locked
+ * buffers (cudaHostAlloc) make the copy asynchronous; with pageable ones
+ * start returns after the copy.  One snapshot in flight per handle (start
+ * waits for the previous one). */
+int cumc_snapshot_start(cumc_handle *h, double *primitive, double *epsilon, double *bfield);
+int cumc_snapshot_wait(cumc_handle *h);
+
 /* The collapsar model's black hole (model/collapsar/src/custom.f90:450-485),
  * for a spherical handle with source_kind CUMC_SRC_COLLAPSAR: its mass m_bh
  * and the speed of light in code units c_code (clight * vel2code), so that
