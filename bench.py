@@ -451,6 +451,75 @@ def bench_poisson(args, world, rank, local, dist):
     return 0
 
 
+def bench_snapshots(args, world, rank, local, dist):
+    """Output without stalling: the 3D blast at --n^3 run for --steps steps,
+    with a snapshot of the reference's output datasets every
+    --snapshot-every steps (cumc_snapshot_start into page-locked buffers, the
+    copy overlapping the next steps; wait before the next start), against the
+    same run without output and with a blocking full-state download
+    (cumc_get_state, what an UPDATE HOST + write would cost).  Metric =
+    zone-updates/s of the run with snapshots; wall clock around each run."""
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import engine, models, snapshot
+    n, every = args.n, args.snapshot_every
+    spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    zones = spec["nx"] * spec["ny"] * spec["nz"]
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.autotune()
+    s.evolve(1e30, args.warmup)
+    bufs = snapshot.buffers(spec, pinned=True)
+    host_p = np.empty_like(prim)
+    host_e = np.empty_like(eps)
+    s.snapshot_start(*bufs)  # allocate the staging buffer before timing
+    s.snapshot_wait()
+    clocks = ClockSampler(local)
+    clocks.start()
+
+    def run(mode):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done = 0
+        while done < args.steps:
+            _, k = s.evolve(1e30, every)
+            done += k
+            if mode == "async":
+                s.snapshot_start(*bufs)
+            elif mode == "blocking":
+                s.L.cumc_get_state(s.h, host_p.ctypes.data, host_e.ctypes.data)
+        if mode == "async":
+            s.snapshot_wait()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3, done
+    ms_none, k_none = run("none")
+    ms_async, k_async = run("async")
+    ms_block, k_block = run("blocking")
+    clk = clocks.stop()
+    s.close()
+    snap_bytes = sum(int(b.nbytes) for b in bufs)
+    value = zones * k_async / (ms_async * 1e-3)
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": world,
+            "steps": k_async, "warmup": args.warmup, "ms_per_step": ms_async / k_async, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "blast3d_%d^3_with_snapshots_every_%d_steps" % (n, every),
+                       "snapshot_bytes": snap_bytes, "timing": "wall clock around each run (host-driven loop)"},
+            "results": {"ms_per_step_no_output": ms_none / k_none,
+                        "ms_per_step_async_snapshots": ms_async / k_async,
+                        "ms_per_step_blocking_get_state": ms_block / k_block,
+                        "snapshots": k_async // every},
+            "e2e": None, "cpu_baseline": None, "clocks": clk,
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def _evolve_timed(engine, torch, spec, prim, eps, warmup, steps=None, t_end=None, tuning="auto", setup=None):
     """Run one handle: W warm-up steps, then time the rest (to t_end, or K
     more steps) with CUDA events on the engine stream.  Returns the handle
@@ -669,7 +738,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blast3d",
-                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "poisson"])
+                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "poisson", "snapshots"])
+    ap.add_argument("--snapshot-every", type=int, default=10, help="snapshots: steps between two snapshots")
     ap.add_argument("--sor-grid", default="384,192,192", help="poisson: nr,ntheta,nphi of the star")
     ap.add_argument("--sor-iters", type=int, default=100, help="poisson: SOR iterations per step")
     ap.add_argument("--sor-full", type=int, default=1, help="poisson: also time the full solve from phi = 0 (0: skip)")
@@ -698,7 +768,7 @@ def main():
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "poisson": 20}.get(args.workload, 0)
+        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "poisson": 20, "snapshots": 60}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -717,6 +787,8 @@ def main():
         return bench_config(args, world, rank, local, dist)
     if args.workload == "poisson":
         return bench_poisson(args, world, rank, local, dist)
+    if args.workload == "snapshots":
+        return bench_snapshots(args, world, rank, local, dist)
 
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)

@@ -171,6 +171,16 @@ INTERFACE
     TYPE(C_PTR), VALUE :: h
     REAL(C_DOUBLE), INTENT(IN) :: phi(*)
   END FUNCTION
+  ! output snapshots (the datasets of print_hydroprofile)
+  INTEGER(C_INT) FUNCTION cumc_snapshot_start(h, primitive, epsilon, bfield) BIND(C, NAME='cumc_snapshot_start')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), INTENT(OUT) :: primitive(*), epsilon(*), bfield(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_snapshot_wait(h) BIND(C, NAME='cumc_snapshot_wait')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
   ! the collapsar model's black hole
   INTEGER(C_INT) FUNCTION cumc_collapsar_set(h, m_bh, c_code) BIND(C, NAME='cumc_collapsar_set')
     IMPORT :: C_INT, C_PTR, C_DOUBLE
