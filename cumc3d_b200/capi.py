@@ -21,6 +21,7 @@ RECON = {"tvdmm": 0, "tvdvl": 1, "tvdmc": 2, "ppm": 3, "weno": 4}
 # Riemann solvers (solver/mhd/parameter.h:90-100)
 RIEMANN = {"lf": 0, "hll": 1, "hllc": 2, "hlld": 3}
 PRECISION = {"fp64": 0, "fp32": 1}
+BOUNDARY_EXCHANGE = 9  # boundary_flag of a z side shared with a neighbouring slab
 FLOOR = {"none": 0, "eps": 1, "torus": 2, "collapsar": 3}
 SOURCE = {"none": 0, "const_gy": 1, "pm_cyl": 2, "pm_sph": 3, "collapsar": 4}
 BCHOOK = {"none": 0, "torus_cyl": 1, "torus_sph": 2}

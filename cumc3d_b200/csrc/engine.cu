@@ -181,11 +181,11 @@ __global__ void k_custom_bc(const Dev d) {
         d.P[1][ci] = dmin(d.P[1][ci], 0.0);
         d.P[1][co] = dmax(d.P[1][co], 0.0);
     }
-    if (d.bc_kind == 1 && o0 < d.NX && o1 < d.NY) {  // z ghosts: (j = o0-2, k = o1-2)
+    if (d.bc_kind == 1 && o0 < d.NX && o1 < d.NY) {  // z ghosts: (j = o0-2, k = o1-2), not at cuts
         const int j = o0 - 2, k = o1 - 2;
         const int ci = cidx(d, j, k, 1 - g), co = cidx(d, j, k, d.nz + g);
-        d.P[3][ci] = dmin(d.P[3][ci], 0.0);
-        d.P[3][co] = dmax(d.P[3][co], 0.0);
+        if (d.zcut[0] != 1) d.P[3][ci] = dmin(d.P[3][ci], 0.0);
+        if (d.zcut[1] != 1) d.P[3][co] = dmax(d.P[3][co], 0.0);
     }
 }
 
@@ -638,7 +638,9 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
     if (!INIT) {
         fxm = (j > 1) ? ux_m : px_m;
         fym = (k > 1) ? uy_m : py_m;
-        fzm = (l > 1) ? uz_m : pz_m;
+        // a slab's lower cut plane is an interior face of the whole grid: its
+        // face field is this stage's constrained-transport value
+        fzm = (l > 1 || d.zcut[0] == 1) ? uz_m : pz_m;
     } else {
         fxm = px_m;
         fym = py_m;
@@ -690,8 +692,12 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
         set_error(d, CUMC_ESTATE, c, stage);
 }
 
-// FROMRVETOU on the index-0 layer: cons face fields = prim face fields
-__global__ void k_cons0(const Dev d) {
+// FROMRVETOU on the index-0 layer: cons face fields = prim face fields.  A
+// slab's lower cut plane interior to the whole grid (zcut 1) takes the prim
+// values once (INITIAL_UPDATE, as every interior cell), then evolves by
+// constrained transport; the seam of a periodic ring (zcut 2) is the whole
+// grid's boundary and keeps the rule.
+__global__ void k_cons0(const Dev d, int init) {
     if (d.S->done) return;
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     const int b = blockIdx.y;
@@ -699,7 +705,7 @@ __global__ void k_cons0(const Dev d) {
     int j, k, l;
     if (plane == 0) { if (a > d.ny || b > d.nz) return; j = 0; k = a; l = b; }
     else if (plane == 1) { if (a > d.nx || b > d.nz) return; j = a; k = 0; l = b; }
-    else { if (a > d.nx || b > d.ny) return; j = a; k = b; l = 0; }
+    else { if (a > d.nx || b > d.ny || (d.zcut[0] == 1 && !init)) return; j = a; k = b; l = 0; }
     const int c = cidx(d, j, k, l);
     d.U[5][c] = d.P[5][c];
     d.U[6][c] = d.P[6][c];
@@ -916,6 +922,9 @@ struct cumc_handle {
     double sor_rho_atm = 0.0;
     cudaGraph_t sor_graph = nullptr;
     cudaGraphExec_t sor_exec = nullptr;
+    // z-slab groups (cumc_group_*): the device, exchange events
+    int dev = 0;
+    cudaEvent_t gev_ready = nullptr, gev_copied = nullptr;
     // output snapshots (cumc_snapshot_*): device staging, copy stream, events
     double *snap_dev = nullptr;
     cudaStream_t snap_stream = nullptr;
@@ -1133,6 +1142,9 @@ static void launch_fills(cumc_handle *h, bool emf) {
     for (int axis = 0; axis < 3; ++axis) {
         FillList in = emf ? make_elist(h, axis, 0) : make_list(h, axis, 0);
         FillList out = emf ? make_elist(h, axis, 1) : make_list(h, axis, 1);
+        // a z side shared with a neighbouring slab is filled by the exchange
+        if (axis == 2 && d.zcut[0]) in.n = 0;
+        if (axis == 2 && d.zcut[1]) out.n = 0;
         int o0 = (axis == 0) ? d.NY : d.NX;
         int o1 = (axis == 2) ? d.NY : d.NZ;
         dim3 b(o0 >= 128 ? 128 : 32), g((o0 + b.x - 1) / b.x, o1, 3);
@@ -1152,13 +1164,13 @@ static void launch_fills(cumc_handle *h, bool emf) {
     }
 }
 
-static void launch_cons0(cumc_handle *h) {
+static void launch_cons0(cumc_handle *h, int init = 0) {
     const Dev &d = h->d;
     int m = d.nx + 1;
     if (d.ny + 1 > m) m = d.ny + 1;
     int mb = (d.ny + 1 > d.nz + 1) ? d.ny + 1 : d.nz + 1;
     dim3 b(32), g((m + 31) / 32, mb, 3);
-    k_cons0<<<g, b, 0, h->stream>>>(d);
+    k_cons0<<<g, b, 0, h->stream>>>(d, init);
     h->launches++;
 }
 
@@ -1177,8 +1189,17 @@ static void prof_end(cumc_handle *h, int cls) {
     h->prof_ms[cls] += ms;
 }
 
-// one RK stage (rungekutta.f90:61-100)
+// one RK stage (rungekutta.f90:61-100), in two halves: the face fluxes and
+// the cell EMFs with their ghosts (a), then the edge EMFs, the update, the
+// recovery and the state ghosts (b); a slab group exchanges ghost planes
+// after each half
+static void enqueue_stage_a(cumc_handle *h, int stage);
+static void enqueue_stage_b(cumc_handle *h, int stage);
 static void enqueue_stage(cumc_handle *h, int stage) {
+    enqueue_stage_a(h, stage);
+    enqueue_stage_b(h, stage);
+}
+static void enqueue_stage_a(cumc_handle *h, int stage) {
     const Dev &d = h->d;
     for (int dir = 0; dir < d.n_dim; ++dir) {
         prof_begin(h);
@@ -1191,6 +1212,12 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     k_ecell<<<g, b, 0, h->stream>>>(d);
     h->launches++;
     launch_fills(h, true);
+    prof_end(h, PC_EMF);
+}
+static void enqueue_stage_b(cumc_handle *h, int stage) {
+    const Dev &d = h->d;
+    dim3 g, b;
+    prof_begin(h);
     grid_dims(d, g, b, 0, d.nx, 0, d.ny, 0, d.nz);
     k_edge<<<g, b, 0, h->stream>>>(d);
     h->launches++;
@@ -1294,8 +1321,18 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     if (cfg->learned && cfg->recon != CUMC_RECON_WENO)
         return fail(nullptr, CUMC_EINVAL, "the learned smooth-face flag needs WENO reconstruction");
     const int nn[3] = {nx, ny, nz};
+    // a z side shared with a neighbouring slab (cumc_group_*): no boundary
+    // rule there; the flag pairing and parity checks see an outflow side
+    int bflag[6];
+    int zcut[2] = {0, 0};
+    for (int i = 0; i < 6; ++i) bflag[i] = cfg->boundary_flag[i];
+    for (int s = 0; s < 2; ++s)
+        if (bflag[4 + s] == CUMC_BOUNDARY_EXCHANGE) { zcut[s] = 1; bflag[4 + s] = 1; }
+    for (int i = 0; i < 4; ++i)
+        if (bflag[i] == CUMC_BOUNDARY_EXCHANGE) return fail(nullptr, CUMC_EINVAL, "slabs are cut along z only");
+    if ((zcut[0] || zcut[1]) && cfg->n_dim < 3) return fail(nullptr, CUMC_EINVAL, "z slabs need a 3D grid");
     for (int a = 0; a < 3; ++a) {
-        int fi = cfg->boundary_flag[2 * a], fo = cfg->boundary_flag[2 * a + 1];
+        int fi = bflag[2 * a], fo = bflag[2 * a + 1];
         if (fi < 0 || fi > 4 || fo < 0 || fo > 4) return fail(nullptr, CUMC_EINVAL, "boundary flag out of range");
         if ((fi == 0) != (fo == 0)) return fail(nullptr, CUMC_EINVAL, "periodic boundary flags must come in pairs");
         if ((fi >= 2 || fo >= 2) && nn[a] < 3) return fail(nullptr, CUMC_EINVAL, "parity boundaries need at least 3 zones");
@@ -1313,7 +1350,9 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     memset(&d, 0, sizeof(Dev));
     d.nx = nx; d.ny = ny; d.nz = nz; d.n_dim = cfg->n_dim; d.coord = cfg->coordinate_flag;
     d.NX = nx + 6; d.NY = ny + 6; d.NZ = nz + 6; d.N3 = (int)N3;
-    for (int i = 0; i < 6; ++i) d.bf[i] = cfg->boundary_flag[i];
+    for (int i = 0; i < 6; ++i) d.bf[i] = bflag[i];
+    d.zcut[0] = zcut[0];
+    d.zcut[1] = zcut[1];
     // epsilon y-outer rule of BOUNDARY1D_NM (boundary.f90:243-282)
     d.eps_y_out_mode = d.bf[2] == 0 ? 0 : (d.bf[3] == 1 ? 1 : (d.bf[3] >= 2 ? 2 : -1));
     d.fixn = cfg->fix_periodic_normal_faces ? 1 : 0;
@@ -1377,6 +1416,7 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
         }
     }
 
+    cudaGetDevice(&h->dev);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         g_create_err = "cudaStreamCreate failed";
         delete h;
@@ -1487,6 +1527,8 @@ int cumc_destroy(cumc_handle *h) {
         cudaStreamDestroy(h->snap_stream);
     }
     if (h->snap_packed) cudaEventDestroy(h->snap_packed);
+    if (h->gev_ready) cudaEventDestroy(h->gev_ready);
+    if (h->gev_copied) cudaEventDestroy(h->gev_copied);
     if (h->snap_done) cudaEventDestroy(h->snap_done);
     for (void *p : h->allocs) cudaFree(p);
     for (int i = 0; i < 2; ++i)
@@ -1556,16 +1598,21 @@ int cumc_get_array(cumc_handle *h, int which, double *out, size_t n_doubles) {
     return download_aos(h, src, nc, out);
 }
 
-int cumc_initial_update(cumc_handle *h) {
-    if (!h) return fail(h, CUMC_EINVAL, "null handle");
-    if (!h->have_state) return fail(h, CUMC_ENOTREADY, "set_state first");
+// INITIAL_UPDATE (initial.f90:86-116): CHECKRHO, FROMRVETOU, BOUNDARY, UPDATE
+static void enqueue_initial(cumc_handle *h) {
     const Dev &d = h->d;
     dim3 g, b;
     grid_dims(d, g, b, 1, d.nx, 1, d.ny, 1, d.nz);
     k_recover<1><<<g, b, 0, h->stream>>>(d, 0);
     h->launches++;
-    launch_cons0(h);
+    launch_cons0(h, 1);
     launch_fills(h, false);
+}
+
+int cumc_initial_update(cumc_handle *h) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (!h->have_state) return fail(h, CUMC_ENOTREADY, "set_state first");
+    enqueue_initial(h);
     CK(cudaGetLastError());
     int rc = check_scalars(h);
     if (rc) return rc;
@@ -1938,6 +1985,198 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
     if (err_out) *err_out = e;
     if (converged_out) *converged_out = st[1] == 1 ? 1 : 0;
     return CUMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// z-slab groups: one grid cut along z into slabs, one handle per slab, on
+// one or several GPUs of this process.  Each slab holds its cells and three
+// ghost planes per side; at the two ghost fills of every stage (the cell and
+// face EMFs, the state) a side marked CUMC_BOUNDARY_EXCHANGE takes the
+// neighbour's three boundary planes instead of a boundary rule -- whole
+// padded planes, so each array is one contiguous copy into the receiver's
+// own memory (cudaMemcpyPeerAsync: over NVLink between GPUs, a device copy
+// on one GPU).  The arrays are those the single grid's z fill would copy,
+// plus the normal face field (interior there); every value a slab reads in
+// its ghost planes is then the value the undivided grid holds at that
+// place, and the group's state equals the single grid's bit for bit.
+// ---------------------------------------------------------------------------
+static int group_check(cumc_handle **hs, int n, bool *ring) {
+    if (!hs || n < 2) return fail(nullptr, CUMC_EINVAL, "a group needs at least two slabs");
+    for (int i = 0; i < n; ++i)
+        if (!hs[i]) return fail(nullptr, CUMC_EINVAL, "null slab handle");
+    const Dev &a = hs[0]->d;
+    for (int i = 0; i < n; ++i) {
+        const Dev &d = hs[i]->d;
+        if (d.nx != a.nx || d.ny != a.ny || d.coord != a.coord || d.n_dim != 3 ||
+            hs[i]->cfg.precision != hs[0]->cfg.precision)
+            return fail(hs[i], CUMC_EINVAL, "slabs differ in x/y extent, geometry or precision");
+        if (d.learned || d.source_kind == CUMC_SRC_COLLAPSAR || (hs[i]->cfg.fixpole && d.coord == 2))
+            return fail(hs[i], CUMC_EINVAL, "the learned flag, the collapsar source and FIXPOLE need the whole grid");
+        if (i + 1 < n && !(d.zcut[1] && hs[i + 1]->d.zcut[0]))
+            return fail(hs[i], CUMC_EINVAL, "neighbouring slabs must mark their shared z side as exchanged");
+    }
+    *ring = hs[0]->d.zcut[0] != 0;
+    if (*ring != (hs[n - 1]->d.zcut[1] != 0))
+        return fail(hs[0], CUMC_EINVAL, "a periodic z axis needs both end sides exchanged");
+    // the seam of a ring is the whole grid's periodic boundary: its sides keep
+    // the boundary rules (index-0 layer, clamps) and take only their fill data
+    // from the neighbour
+    if (*ring) {
+        hs[0]->d.zcut[0] = 2;
+        hs[n - 1]->d.zcut[1] = 2;
+    }
+    return CUMC_OK;
+}
+
+static int group_exchange(cumc_handle **hs, int n, bool ring, bool emf) {
+    cumc_handle *h = hs[0];  // errors are reported on the first slab
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    // the arrays of the single grid's z fill; at an interior cut also the
+    // normal face field (interior there), at the seam only as that fill has
+    // it (fix_periodic_normal_faces)
+    auto lists = [&](cumc_handle *q, int side, double **a) {
+        const Dev &d = q->d;
+        int m = 0;
+        if (emf) {
+            for (int i = 0; i < 3; ++i) a[m++] = d.EC[i];
+            a[m++] = d.EF[e_xy]; a[m++] = d.EF[e_yx]; a[m++] = d.EF[e_zx]; a[m++] = d.EF[e_zy];
+        } else {
+            for (int i = 0; i < 7; ++i) a[m++] = d.P[i];
+            if (d.zcut[side] == 1 || d.fixn) a[m++] = d.P[7];
+            for (int i = 0; i < 3; ++i) a[m++] = d.BC[i];
+            a[m++] = d.CS;
+            a[m++] = d.EPS;
+        }
+        return m;
+    };
+    for (int i = 0; i < n; ++i) {
+        cumc_handle *q = hs[i];
+        CK(cudaSetDevice(q->dev));
+        if (!q->gev_ready) {
+            CK(cudaEventCreateWithFlags(&q->gev_ready, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&q->gev_copied, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(q->gev_ready, q->stream));
+    }
+    for (int i = 0; i < n; ++i) {
+        cumc_handle *r = hs[i];
+        const Dev &d = r->d;
+        const size_t plane = (size_t)d.NX * d.NY, bytes = 3 * plane * sizeof(double);
+        CK(cudaSetDevice(r->dev));
+        for (int side = 0; side < 2; ++side) {
+            if (!d.zcut[side]) continue;
+            const int j = side == 0 ? (i > 0 ? i - 1 : (ring ? n - 1 : -1)) : (i + 1 < n ? i + 1 : (ring ? 0 : -1));
+            if (j < 0) continue;
+            cumc_handle *s = hs[j];
+            CK(cudaStreamWaitEvent(r->stream, s->gev_ready, 0));
+            double *da[16], *sa[16];
+            const int m = lists(r, side, da);
+            lists(s, 1 - side, sa);
+            // lower ghosts (planes -2..0) <- the neighbour's planes nz-2..nz;
+            // upper ghosts (nz+1..nz+3) <- the neighbour's planes 1..3
+            const size_t dst_off = side == 0 ? 0 : (size_t)(d.nz + 3) * plane;
+            const size_t src_off = side == 0 ? (size_t)s->d.nz * plane : 3 * plane;
+            for (int v = 0; v < m; ++v)
+                CK(cudaMemcpyPeerAsync(da[v] + dst_off, r->dev, sa[v] + src_off, s->dev, bytes, r->stream));
+        }
+        CK(cudaEventRecord(r->gev_copied, r->stream));
+    }
+    // a slab overwrites the planes its neighbours read only after their copies
+    for (int i = 0; i < n; ++i) {
+        cumc_handle *q = hs[i];
+        CK(cudaSetDevice(q->dev));
+        for (int side = 0; side < 2; ++side) {
+            if (!q->d.zcut[side]) continue;
+            const int j = side == 0 ? (i > 0 ? i - 1 : (ring ? n - 1 : -1)) : (i + 1 < n ? i + 1 : (ring ? 0 : -1));
+            if (j >= 0) CK(cudaStreamWaitEvent(q->stream, hs[j]->gev_copied, 0));
+        }
+    }
+    cudaSetDevice(dev0);
+    return CUMC_OK;
+}
+
+static int group_finish(cumc_handle **hs, int n) {
+    int dev0 = 0, rc = CUMC_OK;
+    cudaGetDevice(&dev0);
+    for (int i = 0; i < n && rc == CUMC_OK; ++i) {
+        cudaSetDevice(hs[i]->dev);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(hs[i], CUMC_ECUDA, std::string("group launch: ") + cudaGetErrorString(e));
+        else rc = check_scalars(hs[i]);
+    }
+    cudaSetDevice(dev0);
+    return rc;
+}
+
+int cumc_group_initial_update(cumc_handle **hs, int n) {
+    bool ring = false;
+    int rc = group_check(hs, n, &ring);
+    if (rc) return rc;
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    for (int i = 0; i < n; ++i) {
+        if (!hs[i]->have_state) return fail(hs[i], CUMC_ENOTREADY, "set_state first");
+        cudaSetDevice(hs[i]->dev);
+        enqueue_initial(hs[i]);
+    }
+    cudaSetDevice(dev0);
+    rc = group_exchange(hs, n, ring, false);
+    if (rc) return rc;
+    rc = group_finish(hs, n);
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i) hs[i]->initialised = true;
+    return CUMC_OK;
+}
+
+int cumc_group_finddt(cumc_handle **hs, int n, double *dt) {
+    bool ring = false;
+    int rc = group_check(hs, n, &ring);
+    if (rc) return rc;
+    if (!dt) return fail(hs[0], CUMC_EINVAL, "null argument");
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    double m = 0.0;
+    for (int i = 0; i < n && rc == CUMC_OK; ++i) {
+        cudaSetDevice(hs[i]->dev);
+        double di = 0.0;
+        rc = cumc_finddt(hs[i], &di);
+        if (i == 0 || di < m) m = di;  // FINDDT's minimum, over the slabs
+    }
+    cudaSetDevice(dev0);
+    if (rc) return rc;
+    *dt = m;
+    return CUMC_OK;
+}
+
+int cumc_group_step(cumc_handle **hs, int n, double dt) {
+    bool ring = false;
+    int rc = group_check(hs, n, &ring);
+    if (rc) return rc;
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(hs[0], CUMC_EINVAL, "dt must be positive and finite");
+    cumc_handle *h = hs[0];  // errors are reported on the first slab
+    int dev0 = 0;
+    cudaGetDevice(&dev0);
+    for (int i = 0; i < n; ++i) {
+        if (!hs[i]->initialised) return fail(hs[i], CUMC_ENOTREADY, "initial_update first");
+        cudaSetDevice(hs[i]->dev);
+        CK(cudaMemcpyAsync(&hs[i]->d.S->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, hs[i]->stream));
+    }
+    for (int stage = 1; stage <= 3; ++stage) {
+        for (int i = 0; i < n; ++i) {
+            cudaSetDevice(hs[i]->dev);
+            enqueue_stage_a(hs[i], stage);
+        }
+        cudaSetDevice(dev0);
+        if ((rc = group_exchange(hs, n, ring, true))) return rc;
+        for (int i = 0; i < n; ++i) {
+            cudaSetDevice(hs[i]->dev);
+            enqueue_stage_b(hs[i], stage);
+        }
+        cudaSetDevice(dev0);
+        if ((rc = group_exchange(hs, n, ring, false))) return rc;
+    }
+    return group_finish(hs, n);
 }
 
 int cumc_snapshot_start(cumc_handle *h, double *primitive, double *epsilon, double *bfield) {

@@ -47,6 +47,8 @@ struct Dev {
     signed char bfac[6][12];  // parity per side (xin,xout,yin,yout,zin,zout) and variable 1..11
     double gamma, cfl;
     int floor_kind, source_kind, bc_kind;
+    int zcut[2];            // z side (lower, upper) shared with a neighbouring slab: 1 a cut
+                            // interior to the whole grid, 2 the seam of a periodic ring
     double rho_floor, eps_floor, p_floor, g_const, r_sh;
 
     double *P[8];   // prim

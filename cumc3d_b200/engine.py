@@ -27,7 +27,8 @@ EXPORTS = [
     "cumc_batch_run1_noalloc",
     "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest",
     "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set",
-    "cumc_collapsar_set", "cumc_collapsar_get", "cumc_snapshot_start", "cumc_snapshot_wait", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_collapsar_set", "cumc_collapsar_get", "cumc_snapshot_start", "cumc_snapshot_wait",
+    "cumc_group_initial_update", "cumc_group_finddt", "cumc_group_step", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
@@ -96,6 +97,9 @@ def load_library(path=None):
     L.cumc_collapsar_set.argtypes = [C.c_void_p, C.c_double, C.c_double]
     L.cumc_snapshot_start.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_snapshot_wait.argtypes = [C.c_void_p]
+    L.cumc_group_initial_update.argtypes = [C.c_void_p, C.c_int]
+    L.cumc_group_finddt.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+    L.cumc_group_step.argtypes = [C.c_void_p, C.c_int, C.c_double]
     L.cumc_collapsar_get.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.cumc_learn_flags.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
@@ -534,3 +538,72 @@ def check_div3(seed, n):
     if rc != 0:
         raise CumcError(rc, "div3 check failed to run")
     return m.value, ex.value
+
+
+class SlabGroup:
+    """One grid cut along z into slabs, one Solver per slab (cumc_group_*).
+
+    sizes: the slabs' z cell counts (summing to spec["nz"]); devices: a CUDA
+    device per slab (None: the current one).  A periodic z axis makes the
+    slabs a ring.  set_state / get_state take and give the whole grid's
+    arrays (prim (nz+6, ny+6, nx+6, 8), eps (nz+6, ny+6, nx+6)); the group's
+    state equals the undivided grid's bit for bit."""
+
+    def __init__(self, spec, sizes, devices=None):
+        if sum(sizes) != spec["nz"] or min(sizes) < 3:
+            raise ValueError("slab sizes must be >= 3 and sum to nz")
+        self.spec, self.sizes = spec, list(sizes)
+        bf = list(spec["boundary_flag"])
+        ring = bf[4] == 0
+        self.offsets = [sum(sizes[:i]) for i in range(len(sizes))]
+        self.slabs = []
+        for i, (o, m) in enumerate(zip(self.offsets, sizes)):
+            sp = dict(spec)
+            sp["nz"] = m
+            sp["zF"] = np.asarray(spec["zF"])[o:o + m + 7]   # faces -3..m+3 of the slab
+            f = list(bf)
+            f[4] = capi.BOUNDARY_EXCHANGE if (i > 0 or ring) else bf[4]
+            f[5] = capi.BOUNDARY_EXCHANGE if (i + 1 < len(sizes) or ring) else bf[5]
+            sp["boundary_flag"] = f
+            if devices is not None:
+                import torch
+                torch.cuda.set_device(devices[i])
+            self.slabs.append(Solver(sp))
+        self.L = self.slabs[0].L
+        self._arr = (C.c_void_p * len(self.slabs))(*[s.h for s in self.slabs])
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CumcError(rc, self.L.cumc_last_error(self.slabs[0].h).decode())
+
+    def set_state(self, prim, eps):
+        for s, o, m in zip(self.slabs, self.offsets, self.sizes):
+            s.set_state(np.ascontiguousarray(prim[o:o + m + 6]), np.ascontiguousarray(eps[o:o + m + 6]))
+
+    def initial_update(self):
+        self._check(self.L.cumc_group_initial_update(self._arr, len(self.slabs)))
+
+    def finddt(self):
+        dt = C.c_double()
+        self._check(self.L.cumc_group_finddt(self._arr, len(self.slabs), C.byref(dt)))
+        return dt.value
+
+    def step(self, dt):
+        self._check(self.L.cumc_group_step(self._arr, len(self.slabs), float(dt)))
+
+    def _gather(self, parts):
+        """Interior planes of every slab, in z order (axis 0 of the padded
+        arrays), as the whole grid's interior."""
+        return np.concatenate([p[3:3 + m] for p, m in zip(parts, self.sizes)], axis=0)
+
+    def get_state(self):
+        """(prim, eps) of the interior cells, (nz, ny+6, nx+6, ...)."""
+        st = [s.get_state() for s in self.slabs]
+        return self._gather([p for p, _ in st]), self._gather([e for _, e in st])
+
+    def get_array(self, which):
+        return self._gather([s.get_array(which) for s in self.slabs])
+
+    def close(self):
+        for s in self.slabs:
+            s.close()

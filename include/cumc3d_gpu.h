@@ -79,6 +79,10 @@ extern "C" {
                                 each stage by the inner-face mass flux
                                 (custom.f90:450-478, cumc_collapsar_set)       */
 /* model boundary hooks (CUSTOM_BOUNDARY_X/Y/Z) */
+/* boundary_flag value of a z side shared with a neighbouring slab (no
+ * counterpart in the reference): its ghost planes come from the neighbour
+ * (cumc_group_*) instead of a boundary rule */
+#define CUMC_BOUNDARY_EXCHANGE 9
 #define CUMC_BC_NONE      0
 #define CUMC_BC_TORUS_CYL 1  /* model/torus-cyn/src/custom.f90:146-208        */
 #define CUMC_BC_TORUS_SPH 2  /* model/torus-sph/src/custom.f90 (x clamp only) */
@@ -104,7 +108,9 @@ typedef struct cumc_config {
     int n_dim;                   /* 1, 2 or 3                                     */
     int coordinate_flag;         /* 0 Cartesian, 1 cylindrical, 2 spherical       */
     int boundary_flag[6];        /* xin xout yin yout zin zout: 0 periodic,
-                                    1 outflow, 2 reflect, 3 axis, 4 equator       */
+                                    1 outflow, 2 reflect, 3 axis, 4 equator;
+                                    zin/zout may be CUMC_BOUNDARY_EXCHANGE (a
+                                    slab of a z-decomposed grid, cumc_group_*)  */
     const double *xF;            /* face coordinates, indices -3..nx+3 (nx+7)     */
     const double *yF;            /* indices -3..ny+3 (ny+7)                       */
     const double *zF;            /* indices -3..nz+3 (nz+7)                       */
@@ -313,6 +319,25 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
  * or set it (a warm start, or a restart from a checkpoint). */
 int cumc_poisson_get(cumc_handle *h, double *phi);
 int cumc_poisson_set(cumc_handle *h, const double *phi);
+
+/* z-slab groups (the multi-GPU layout of the 3D path; no counterpart in the
+ * reference, which runs one grid on one device).  A grid cut along z into
+ * n >= 2 slabs, one handle per slab in z order, created with the slab's z
+ * faces (its cells plus three ghost faces per side) and
+ * boundary_flag[4]/[5] = CUMC_BOUNDARY_EXCHANGE on every side shared with a
+ * neighbour (both ends too for a periodic z axis: the slabs form a ring).
+ * The handles may live on different GPUs of this process (each created with
+ * its GPU current); the ghost planes travel between them as contiguous
+ * peer copies into the receiver's memory, twice per RK stage.  The group's
+ * state equals the undivided grid's bit for bit.  Steps run host-driven
+ * (no cumc_evolve); not with the learned flag, the collapsar source or
+ * FIXPOLE, which need the whole grid at once.
+ * cumc_group_initial_update: INITIAL_UPDATE on every slab, ghosts exchanged;
+ * cumc_group_finddt: FINDDT, the minimum over the slabs;
+ * cumc_group_step: one SSP-RK3 step of every slab. */
+int cumc_group_initial_update(cumc_handle **slabs, int n);
+int cumc_group_finddt(cumc_handle **slabs, int n, double *dt);
+int cumc_group_step(cumc_handle **slabs, int n, double dt);
 
 /* Output snapshot without stalling the step loop (print_hydroprofile,
  * solver/mhd/dataio.f90:31-240, which updates the host copy and writes HDF5).
