@@ -520,6 +520,69 @@ def bench_snapshots(args, world, rank, local, dist):
     return 0
 
 
+def bench_slabs(args, world, rank, local, dist):
+    """The 3D path cut along z into slabs (cumc_group_*, one process): the
+    blast at --n^3 as --slabs slabs spread round-robin over the visible GPUs,
+    against the undivided grid, both host-driven (FINDDT + RUNGEKUTTA per
+    step).  Metric = zone-updates/s of the slab group (whole grid); with one
+    GPU the slabs share it, which measures the exchange's cost."""
+    import torch
+
+    from cumc3d_b200 import engine, models
+    n, ns = args.n, args.slabs
+    spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    zones = spec["nx"] * spec["ny"] * spec["nz"]
+    ndev = torch.cuda.device_count()
+    sizes = [n // ns + (1 if i < n % ns else 0) for i in range(ns)]
+
+    def run(obj, step, finddt):
+        for _ in range(args.warmup):
+            step(finddt())
+        for d in range(ndev):
+            torch.cuda.synchronize(d)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step(finddt())
+        for d in range(ndev):
+            torch.cuda.synchronize(d)
+        return (time.perf_counter() - t0) * 1e3 / args.steps
+
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.autotune()
+    ms_single = run(s, s.rungekutta, s.finddt)
+    s.close()
+    g = engine.SlabGroup(spec, sizes, devices=[i % ndev for i in range(ns)])
+    g.set_state(prim, eps)
+    g.initial_update()
+    for sl in g.slabs:
+        sl.autotune()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_group = run(g, g.step, g.finddt)
+    clk = clocks.stop()
+    g.close()
+    plane = (spec["nx"] + 6) * (spec["ny"] + 6) * 8
+    cuts = ns  # a periodic ring
+    xbytes = cuts * 2 * 3 * 3 * plane * (13 + 7)  # per step: sides x stages x planes x arrays
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": zones / (ms_group * 1e-3), "unit": "zone-updates/s",
+            "n_gpus": ndev, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_group,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "blast3d_%d^3_as_%d_z_slabs_on_%d_gpus" % (n, ns, ndev), "slabs": sizes,
+                       "timing": "wall clock around host-driven steps, all devices synchronised"},
+            "results": {"ms_per_step_undivided": ms_single, "ms_per_step_slabs": ms_group,
+                        "ghost_bytes_per_step": xbytes},
+            "e2e": None, "cpu_baseline": None, "clocks": clk,
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def _evolve_timed(engine, torch, spec, prim, eps, warmup, steps=None, t_end=None, tuning="auto", setup=None):
     """Run one handle: W warm-up steps, then time the rest (to t_end, or K
     more steps) with CUDA events on the engine stream.  Returns the handle
@@ -738,7 +801,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blast3d",
-                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "poisson", "snapshots"])
+                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "poisson", "snapshots", "slabs"])
+    ap.add_argument("--slabs", type=int, default=2, help="slabs: number of z slabs")
     ap.add_argument("--snapshot-every", type=int, default=10, help="snapshots: steps between two snapshots")
     ap.add_argument("--sor-grid", default="384,192,192", help="poisson: nr,ntheta,nphi of the star")
     ap.add_argument("--sor-iters", type=int, default=100, help="poisson: SOR iterations per step")
@@ -768,7 +832,7 @@ def main():
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "poisson": 20, "snapshots": 60}.get(args.workload, 0)
+        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "poisson": 20, "snapshots": 60, "slabs": 30}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -789,6 +853,8 @@ def main():
         return bench_poisson(args, world, rank, local, dist)
     if args.workload == "snapshots":
         return bench_snapshots(args, world, rank, local, dist)
+    if args.workload == "slabs":
+        return bench_slabs(args, world, rank, local, dist)
 
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)

@@ -2056,6 +2056,15 @@ static int group_exchange(cumc_handle **hs, int n, bool ring, bool emf) {
         if (!q->gev_ready) {
             CK(cudaEventCreateWithFlags(&q->gev_ready, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&q->gev_copied, cudaEventDisableTiming));
+            // direct copies between neighbouring GPUs (NVLink) where the
+            // hardware allows; otherwise the driver stages them
+            for (int side = 0; side < 2; ++side) {
+                const int j = side == 0 ? (i > 0 ? i - 1 : (ring ? n - 1 : -1)) : (i + 1 < n ? i + 1 : (ring ? 0 : -1));
+                if (j < 0 || hs[j]->dev == q->dev) continue;
+                int can = 0;
+                cudaDeviceCanAccessPeer(&can, q->dev, hs[j]->dev);
+                if (can && cudaDeviceEnablePeerAccess(hs[j]->dev, 0) != cudaSuccess) cudaGetLastError();
+            }
         }
         CK(cudaEventRecord(q->gev_ready, q->stream));
     }

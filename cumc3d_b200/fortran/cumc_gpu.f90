@@ -23,6 +23,7 @@ INTEGER(C_INT), PARAMETER :: CUMC_FP64 = 0, CUMC_FP32 = 1
 INTEGER(C_INT), PARAMETER :: CUMC_FLOOR_NONE = 0, CUMC_FLOOR_EPS = 1, CUMC_FLOOR_TORUS = 2, CUMC_FLOOR_COLLAPSAR = 3
 INTEGER(C_INT), PARAMETER :: CUMC_SRC_NONE = 0, CUMC_SRC_CONST_GY = 1, CUMC_SRC_PM_CYL = 2, CUMC_SRC_PM_SPH = 3
 INTEGER(C_INT), PARAMETER :: CUMC_SRC_COLLAPSAR = 4
+INTEGER(C_INT), PARAMETER :: CUMC_BOUNDARY_EXCHANGE = 9
 
 ! cumc_model (include/cumc3d_gpu.h)
 TYPE, BIND(C) :: cumc_model
@@ -170,6 +171,24 @@ INTERFACE
     IMPORT :: C_INT, C_PTR, C_DOUBLE
     TYPE(C_PTR), VALUE :: h
     REAL(C_DOUBLE), INTENT(IN) :: phi(*)
+  END FUNCTION
+  ! z-slab groups (slabs: an array of handles in z order)
+  INTEGER(C_INT) FUNCTION cumc_group_initial_update(slabs, n) BIND(C, NAME='cumc_group_initial_update')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: slabs
+    INTEGER(C_INT), VALUE :: n
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_group_finddt(slabs, n, dt) BIND(C, NAME='cumc_group_finddt')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: slabs
+    INTEGER(C_INT), VALUE :: n
+    REAL(C_DOUBLE), INTENT(OUT) :: dt
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_group_step(slabs, n, dt) BIND(C, NAME='cumc_group_step')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: slabs
+    INTEGER(C_INT), VALUE :: n
+    REAL(C_DOUBLE), VALUE :: dt
   END FUNCTION
   ! output snapshots (the datasets of print_hydroprofile)
   INTEGER(C_INT) FUNCTION cumc_snapshot_start(h, primitive, epsilon, bfield) BIND(C, NAME='cumc_snapshot_start')
