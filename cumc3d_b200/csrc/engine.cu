@@ -2000,6 +2000,13 @@ int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out,
 // its ghost planes is then the value the undivided grid holds at that
 // place, and the group's state equals the single grid's bit for bit.
 // ---------------------------------------------------------------------------
+// restores the caller's current device when a group call returns, on every path
+struct DeviceGuard {
+    int dev = 0;
+    DeviceGuard() { cudaGetDevice(&dev); }
+    ~DeviceGuard() { cudaSetDevice(dev); }
+};
+
 static int group_check(cumc_handle **hs, int n, bool *ring) {
     if (!hs || n < 2) return fail(nullptr, CUMC_EINVAL, "a group needs at least two slabs");
     for (int i = 0; i < n; ++i)
@@ -2030,8 +2037,7 @@ static int group_check(cumc_handle **hs, int n, bool *ring) {
 
 static int group_exchange(cumc_handle **hs, int n, bool ring, bool emf) {
     cumc_handle *h = hs[0];  // errors are reported on the first slab
-    int dev0 = 0;
-    cudaGetDevice(&dev0);
+    DeviceGuard guard;
     // the arrays of the single grid's z fill; at an interior cut also the
     // normal face field (interior there), at the seam only as that fill has
     // it (fix_periodic_normal_faces)
@@ -2101,20 +2107,18 @@ static int group_exchange(cumc_handle **hs, int n, bool ring, bool emf) {
             if (j >= 0) CK(cudaStreamWaitEvent(q->stream, hs[j]->gev_copied, 0));
         }
     }
-    cudaSetDevice(dev0);
     return CUMC_OK;
 }
 
 static int group_finish(cumc_handle **hs, int n) {
-    int dev0 = 0, rc = CUMC_OK;
-    cudaGetDevice(&dev0);
+    DeviceGuard guard;
+    int rc = CUMC_OK;
     for (int i = 0; i < n && rc == CUMC_OK; ++i) {
         cudaSetDevice(hs[i]->dev);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) rc = fail(hs[i], CUMC_ECUDA, std::string("group launch: ") + cudaGetErrorString(e));
         else rc = check_scalars(hs[i]);
     }
-    cudaSetDevice(dev0);
     return rc;
 }
 
@@ -2122,14 +2126,12 @@ int cumc_group_initial_update(cumc_handle **hs, int n) {
     bool ring = false;
     int rc = group_check(hs, n, &ring);
     if (rc) return rc;
-    int dev0 = 0;
-    cudaGetDevice(&dev0);
+    DeviceGuard guard;
     for (int i = 0; i < n; ++i) {
         if (!hs[i]->have_state) return fail(hs[i], CUMC_ENOTREADY, "set_state first");
         cudaSetDevice(hs[i]->dev);
         enqueue_initial(hs[i]);
     }
-    cudaSetDevice(dev0);
     rc = group_exchange(hs, n, ring, false);
     if (rc) return rc;
     rc = group_finish(hs, n);
@@ -2143,8 +2145,7 @@ int cumc_group_finddt(cumc_handle **hs, int n, double *dt) {
     int rc = group_check(hs, n, &ring);
     if (rc) return rc;
     if (!dt) return fail(hs[0], CUMC_EINVAL, "null argument");
-    int dev0 = 0;
-    cudaGetDevice(&dev0);
+    DeviceGuard guard;
     double m = 0.0;
     for (int i = 0; i < n && rc == CUMC_OK; ++i) {
         cudaSetDevice(hs[i]->dev);
@@ -2152,7 +2153,6 @@ int cumc_group_finddt(cumc_handle **hs, int n, double *dt) {
         rc = cumc_finddt(hs[i], &di);
         if (i == 0 || di < m) m = di;  // FINDDT's minimum, over the slabs
     }
-    cudaSetDevice(dev0);
     if (rc) return rc;
     *dt = m;
     return CUMC_OK;
@@ -2164,8 +2164,7 @@ int cumc_group_step(cumc_handle **hs, int n, double dt) {
     if (rc) return rc;
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(hs[0], CUMC_EINVAL, "dt must be positive and finite");
     cumc_handle *h = hs[0];  // errors are reported on the first slab
-    int dev0 = 0;
-    cudaGetDevice(&dev0);
+    DeviceGuard guard;
     for (int i = 0; i < n; ++i) {
         if (!hs[i]->initialised) return fail(hs[i], CUMC_ENOTREADY, "initial_update first");
         cudaSetDevice(hs[i]->dev);
@@ -2176,13 +2175,11 @@ int cumc_group_step(cumc_handle **hs, int n, double dt) {
             cudaSetDevice(hs[i]->dev);
             enqueue_stage_a(hs[i], stage);
         }
-        cudaSetDevice(dev0);
         if ((rc = group_exchange(hs, n, ring, true))) return rc;
         for (int i = 0; i < n; ++i) {
             cudaSetDevice(hs[i]->dev);
             enqueue_stage_b(hs[i], stage);
         }
-        cudaSetDevice(dev0);
         if ((rc = group_exchange(hs, n, ring, false))) return rc;
     }
     return group_finish(hs, n);
