@@ -540,6 +540,29 @@ def check_div3(seed, n):
     return m.value, ex.value
 
 
+def slab_specs(spec, sizes):
+    """The per-slab specs of a z cut: each slab's z faces are its cells plus
+    three ghost faces per side, a sub-array of the whole grid's zF; a side
+    shared with a neighbour is marked BOUNDARY_EXCHANGE (both ends too when
+    z is periodic: the slabs form a ring).  Returns (specs, z offsets)."""
+    if sum(sizes) != spec["nz"] or min(sizes) < 3:
+        raise ValueError("slab sizes must be >= 3 and sum to nz")
+    bf = list(spec["boundary_flag"])
+    ring = bf[4] == 0
+    offsets = [sum(sizes[:i]) for i in range(len(sizes))]
+    out = []
+    for i, (o, m) in enumerate(zip(offsets, sizes)):
+        sp = dict(spec)
+        sp["nz"] = m
+        sp["zF"] = np.asarray(spec["zF"])[o:o + m + 7]   # faces -3..m+3 of the slab
+        f = list(bf)
+        f[4] = capi.BOUNDARY_EXCHANGE if (i > 0 or ring) else bf[4]
+        f[5] = capi.BOUNDARY_EXCHANGE if (i + 1 < len(sizes) or ring) else bf[5]
+        sp["boundary_flag"] = f
+        out.append(sp)
+    return out, offsets
+
+
 class SlabGroup:
     """One grid cut along z into slabs, one Solver per slab (cumc_group_*).
 
@@ -550,35 +573,32 @@ class SlabGroup:
     state equals the undivided grid's bit for bit."""
 
     def __init__(self, spec, sizes, devices=None):
-        if sum(sizes) != spec["nz"] or min(sizes) < 3:
-            raise ValueError("slab sizes must be >= 3 and sum to nz")
+        specs, self.offsets = slab_specs(spec, sizes)
         self.spec, self.sizes = spec, list(sizes)
-        bf = list(spec["boundary_flag"])
-        ring = bf[4] == 0
-        self.offsets = [sum(sizes[:i]) for i in range(len(sizes))]
+        self.devices = list(devices) if devices is not None else None
         self.slabs = []
-        for i, (o, m) in enumerate(zip(self.offsets, sizes)):
-            sp = dict(spec)
-            sp["nz"] = m
-            sp["zF"] = np.asarray(spec["zF"])[o:o + m + 7]   # faces -3..m+3 of the slab
-            f = list(bf)
-            f[4] = capi.BOUNDARY_EXCHANGE if (i > 0 or ring) else bf[4]
-            f[5] = capi.BOUNDARY_EXCHANGE if (i + 1 < len(sizes) or ring) else bf[5]
-            sp["boundary_flag"] = f
-            if devices is not None:
-                import torch
-                torch.cuda.set_device(devices[i])
-            self.slabs.append(Solver(sp))
+        for i, sp in enumerate(specs):
+            with self._on(i):
+                self.slabs.append(Solver(sp))
         self.L = self.slabs[0].L
         self._arr = (C.c_void_p * len(self.slabs))(*[s.h for s in self.slabs])
+
+    def _on(self, i):
+        """Context with slab i's GPU current (calls on a handle run on its GPU)."""
+        import contextlib
+        if self.devices is None:
+            return contextlib.nullcontext()
+        import torch
+        return torch.cuda.device(self.devices[i])
 
     def _check(self, rc):
         if rc != 0:
             raise CumcError(rc, self.L.cumc_last_error(self.slabs[0].h).decode())
 
     def set_state(self, prim, eps):
-        for s, o, m in zip(self.slabs, self.offsets, self.sizes):
-            s.set_state(np.ascontiguousarray(prim[o:o + m + 6]), np.ascontiguousarray(eps[o:o + m + 6]))
+        for i, (s, o, m) in enumerate(zip(self.slabs, self.offsets, self.sizes)):
+            with self._on(i):
+                s.set_state(np.ascontiguousarray(prim[o:o + m + 6]), np.ascontiguousarray(eps[o:o + m + 6]))
 
     def initial_update(self):
         self._check(self.L.cumc_group_initial_update(self._arr, len(self.slabs)))
@@ -598,12 +618,20 @@ class SlabGroup:
 
     def get_state(self):
         """(prim, eps) of the interior cells, (nz, ny+6, nx+6, ...)."""
-        st = [s.get_state() for s in self.slabs]
+        st = []
+        for i, s in enumerate(self.slabs):
+            with self._on(i):
+                st.append(s.get_state())
         return self._gather([p for p, _ in st]), self._gather([e for _, e in st])
 
     def get_array(self, which):
-        return self._gather([s.get_array(which) for s in self.slabs])
+        parts = []
+        for i, s in enumerate(self.slabs):
+            with self._on(i):
+                parts.append(s.get_array(which))
+        return self._gather(parts)
 
     def close(self):
-        for s in self.slabs:
-            s.close()
+        for i, s in enumerate(self.slabs):
+            with self._on(i):
+                s.close()
