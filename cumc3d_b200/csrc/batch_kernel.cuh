@@ -93,7 +93,7 @@ __device__ __forceinline__ void batch_floor(const BatchDev &b, double &e) {
 
 constexpr int BATCH_THREADS = 256;
 constexpr int BATCH_CLUSTER = 8;          // CTAs that share one large problem
-constexpr int BATCH_COOP_MIN_CELLS = 128; // per CTA: smaller problems run on one CTA
+constexpr int BATCH_COOP_MIN_N = 1024;    // problems of at most this many cells run on one CTA
 
 struct BatchShared {
     unsigned long long part_dt;  // this CTA's FINDDT minimum (bit pattern)
@@ -401,9 +401,9 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
 }
 
 // Persistent kernel.  Launched in clusters of `size` CTAs: while the next
-// problem (largest first) has more than BATCH_COOP_MIN_CELLS cells per CTA,
-// the whole cluster runs it; from the first smaller one on, every CTA takes
-// problems on its own.
+// problem (largest first) has more than BATCH_COOP_MIN_N cells, the whole
+// cluster runs it; from the first smaller one on, every CTA takes problems on
+// its own.
 template <class T, int REC, int RS>
 __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch(const BatchDev b) {
     __shared__ BatchShared sh;
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch(const BatchDev b) {
             pi = cluster.map_shared_rank(&sh, 0)->pick;
             cluster.sync();
             if (pi >= b.nprob) return;
-            if (b.prob[b.order[pi]].n <= BATCH_COOP_MIN_CELLS * size) {
+            if (b.prob[b.order[pi]].n <= BATCH_COOP_MIN_N) {
                 coop = false;  // from here on every CTA takes its own problems
                 if (rank != 0) continue;
             }
@@ -448,6 +448,10 @@ static cudaError_t launch_batch_one(const BatchDev &b, int clusters, int cluster
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (cluster_size > 8) {
+        cudaError_t e = cudaFuncSetAttribute(k_batch<T, REC, RS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
     if (clusters <= 0) {
         // size the persistent grid: as many clusters as can be resident
         int nc = 0;
