@@ -88,7 +88,7 @@ extern "C" {
 #define CUMC_BC_TORUS_SPH 2  /* model/torus-sph/src/custom.f90 (x clamp only) */
 
 /* Model descriptor: replaces the per-stage device hooks each reference model
- * links in (EOS, floors, sources, custom boundaries; SURVEY layer L6). */
+ * links in (EOS, floors, sources, custom boundaries). */
 typedef struct cumc_model {
     double gamma;        /* ggas: ideal-gas adiabatic index                       */
     int    floor_kind;   /* CUMC_FLOOR_*                                          */

@@ -1,6 +1,9 @@
 """Non-uniform grid files and generators (CPU): the restated generators
-against the grid files the reference ships (model/torus-*/grid/*.dat, when
-the reference tree is present), and the CUSTOM_GRID reader's checks."""
+against the grid files the reference ships (model/torus-*/grid/*.dat) --
+through digests of those files recorded in tests/golden/grid_digests.json by
+tests/golden/make_grid_digests.py, and against the files themselves when the
+reference tree is present -- and the CUSTOM_GRID reader's checks."""
+import json
 import os
 
 import numpy as np
@@ -8,7 +11,31 @@ import pytest
 
 from cumc3d_b200 import grids
 
-REF = "/root/reference/model"
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("CUMC_REFERENCE_TREE", "/root/reference") + "/model"
+
+
+def _generated():
+    nx, ny, nz, r, th, ph = grids.spherical_torus_grid()
+    nr, nphi, nzc, rc, phc, zc = grids.cylindrical_torus_grid()
+    return {"torus-sph/r_grid.dat": r, "torus-sph/th_grid.dat": th, "torus-sph/phi_grid.dat": ph,
+            "torus-cyn/r_grid.dat": rc, "torus-cyn/phi_grid.dat": phc, "torus-cyn/z_grid.dat": zc}
+
+
+def test_generators_match_the_digests_of_the_shipped_grid_files():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mgd", os.path.join(HERE, "golden", "make_grid_digests.py"))
+    mgd = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mgd)
+    with open(os.path.join(HERE, "golden", "grid_digests.json")) as f:
+        want = json.load(f)
+    got = _generated()
+    assert sorted(got) == sorted(want)
+    for name, faces in got.items():
+        w = want[name]
+        assert faces.size == w["n_faces"], name
+        assert (faces[0], faces[-1]) == (w["first"], w["last"]), name
+        assert mgd.digest(faces) == w["sha256"], name
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
