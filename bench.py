@@ -525,10 +525,13 @@ def bench_slabs(args, world, rank, local, dist):
     blast at --n^3 as --slabs slabs spread round-robin over the visible GPUs,
     against the undivided grid, both host-driven (FINDDT + RUNGEKUTTA per
     step).  Metric = zone-updates/s of the slab group (whole grid); with one
-    GPU the slabs share it, which measures the exchange's cost."""
+    GPU the slabs share it, which measures the exchange's cost.  Under
+    torchrun (N > 1) one slab per rank instead (bench_slab_ranks)."""
     import torch
 
     from cumc3d_b200 import engine, models
+    if world > 1:
+        return bench_slab_ranks(args, world, rank, local, dist)
     n, ns = args.n, args.slabs
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
     spec["positivity_fallback"] = 1
@@ -577,6 +580,60 @@ def bench_slabs(args, world, rank, local, dist):
                        "timing": "wall clock around host-driven steps, all devices synchronised"},
             "results": {"ms_per_step_undivided": ms_single, "ms_per_step_slabs": ms_group,
                         "ghost_bytes_per_step": xbytes},
+            "e2e": None, "cpu_baseline": None, "clocks": clk,
+        }
+        print(json.dumps(line))
+    return 0
+
+
+def bench_slab_ranks(args, world, rank, local, dist):
+    """One slab per rank (SlabRank): the blast at --n^3 cut into N z slabs,
+    one per GPU, a periodic ring; ghost planes by NCCL send/recv into each
+    receiver's memory, dt by an all-reduce (min), host-driven steps.  Strong
+    scaling: the grid is fixed.  Time: CUDA events on each rank's engine
+    stream around the K steps, the max over ranks."""
+    import torch
+
+    from cumc3d_b200 import engine, models
+    n = args.n
+    spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    zones = spec["nx"] * spec["ny"] * spec["nz"]
+    sizes = [n // world + (1 if i < n % world else 0) for i in range(world)]
+    r = engine.SlabRank(spec, sizes, rank)
+    r.set_state(prim, eps)
+    r.initial_update()
+    r.solver.autotune()
+    for _ in range(args.warmup):
+        r.step(r.finddt())
+    stream = torch.cuda.ExternalStream(r.solver.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0.record(stream)
+    for _ in range(args.steps):
+        r.step(r.finddt())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item()) / args.steps
+    xbytes = sum(r.send[k].numel() for k in r.send) * 3  # sent per step by this rank (3 stages)
+    r.close()
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": zones / (ms * 1e-3), "unit": "zone-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "blast3d_%d^3_as_%d_z_slabs_one_per_rank" % (n, world), "slabs": sizes,
+                       "parallelism": "z slabs, NCCL send/recv of ghost planes",
+                       "timing": "CUDA events on each rank's engine stream, max over ranks"},
+            "results": {"ghost_bytes_sent_per_step_rank0": xbytes},
             "e2e": None, "cpu_baseline": None, "clocks": clk,
         }
         print(json.dumps(line))

@@ -2035,27 +2035,30 @@ static int group_check(cumc_handle **hs, int n, bool *ring) {
     return CUMC_OK;
 }
 
+// the arrays whose ghost planes one z side takes from its neighbour: those
+// of the single grid's z fill; at an interior cut also the normal face field
+// (interior there), at the seam only as that fill has it
+// (fix_periodic_normal_faces).  emf: the EMF fill (cell and face EMFs),
+// else the state fill.
+static int halo_arrays(const cumc_handle *q, int side, bool emf, double **a) {
+    const Dev &d = q->d;
+    int m = 0;
+    if (emf) {
+        for (int i = 0; i < 3; ++i) a[m++] = d.EC[i];
+        a[m++] = d.EF[e_xy]; a[m++] = d.EF[e_yx]; a[m++] = d.EF[e_zx]; a[m++] = d.EF[e_zy];
+    } else {
+        for (int i = 0; i < 7; ++i) a[m++] = d.P[i];
+        if (d.zcut[side] == 1 || d.fixn) a[m++] = d.P[7];
+        for (int i = 0; i < 3; ++i) a[m++] = d.BC[i];
+        a[m++] = d.CS;
+        a[m++] = d.EPS;
+    }
+    return m;
+}
+
 static int group_exchange(cumc_handle **hs, int n, bool ring, bool emf) {
     cumc_handle *h = hs[0];  // errors are reported on the first slab
     DeviceGuard guard;
-    // the arrays of the single grid's z fill; at an interior cut also the
-    // normal face field (interior there), at the seam only as that fill has
-    // it (fix_periodic_normal_faces)
-    auto lists = [&](cumc_handle *q, int side, double **a) {
-        const Dev &d = q->d;
-        int m = 0;
-        if (emf) {
-            for (int i = 0; i < 3; ++i) a[m++] = d.EC[i];
-            a[m++] = d.EF[e_xy]; a[m++] = d.EF[e_yx]; a[m++] = d.EF[e_zx]; a[m++] = d.EF[e_zy];
-        } else {
-            for (int i = 0; i < 7; ++i) a[m++] = d.P[i];
-            if (d.zcut[side] == 1 || d.fixn) a[m++] = d.P[7];
-            for (int i = 0; i < 3; ++i) a[m++] = d.BC[i];
-            a[m++] = d.CS;
-            a[m++] = d.EPS;
-        }
-        return m;
-    };
     for (int i = 0; i < n; ++i) {
         cumc_handle *q = hs[i];
         CK(cudaSetDevice(q->dev));
@@ -2086,8 +2089,8 @@ static int group_exchange(cumc_handle **hs, int n, bool ring, bool emf) {
             cumc_handle *s = hs[j];
             CK(cudaStreamWaitEvent(r->stream, s->gev_ready, 0));
             double *da[16], *sa[16];
-            const int m = lists(r, side, da);
-            lists(s, 1 - side, sa);
+            const int m = halo_arrays(r, side, emf, da);
+            halo_arrays(s, 1 - side, emf, sa);
             // lower ghosts (planes -2..0) <- the neighbour's planes nz-2..nz;
             // upper ghosts (nz+1..nz+3) <- the neighbour's planes 1..3
             const size_t dst_off = side == 0 ? 0 : (size_t)(d.nz + 3) * plane;
@@ -2183,6 +2186,129 @@ int cumc_group_step(cumc_handle **hs, int n, double dt) {
         if ((rc = group_exchange(hs, n, ring, false))) return rc;
     }
     return group_finish(hs, n);
+}
+
+// ---------------------------------------------------------------------------
+// One slab per process (one rank per GPU): the same stage split and ghost
+// planes as the group above, with the planes carried by the caller.  Each
+// exchange point is pack (the three planes next to a cut side, every array
+// of the list one after another, into a contiguous device buffer) -> the
+// caller moves the buffer to the neighbour (NCCL send/recv over NVLink, or a
+// host-staged copy) -> unpack into the neighbour's three ghost planes.  All
+// of it is ordered on the handle's stream.
+// ---------------------------------------------------------------------------
+static int slab_check(cumc_handle *h) {
+    if (!h) return fail(nullptr, CUMC_EINVAL, "null handle");
+    const Dev &d = h->d;
+    if (!d.zcut[0] && !d.zcut[1]) return fail(h, CUMC_EINVAL, "not a slab: no z side is CUMC_BOUNDARY_EXCHANGE");
+    if (d.learned || d.source_kind == CUMC_SRC_COLLAPSAR || (h->cfg.fixpole && d.coord == 2))
+        return fail(h, CUMC_EINVAL, "the learned flag, the collapsar source and FIXPOLE need the whole grid");
+    return CUMC_OK;
+}
+
+static int slab_side(cumc_handle *h, int fill, int side) {
+    int rc = slab_check(h);
+    if (rc) return rc;
+    if ((fill != CUMC_FILL_STATE && fill != CUMC_FILL_EMF) || (side != 0 && side != 1))
+        return fail(h, CUMC_EINVAL, "fill must be CUMC_FILL_STATE or CUMC_FILL_EMF, side 0 (lower z) or 1 (upper z)");
+    if (!h->d.zcut[side]) return fail(h, CUMC_EINVAL, "this z side is not exchanged");
+    return CUMC_OK;
+}
+
+int cumc_slab_seam(cumc_handle *h, int side) {
+    int rc = slab_side(h, CUMC_FILL_STATE, side);
+    if (rc) return rc;
+    if (h->initialised) return fail(h, CUMC_EINVAL, "mark the seam before cumc_slab_initial_begin");
+    h->d.zcut[side] = 2;
+    return CUMC_OK;
+}
+
+int cumc_slab_halo_bytes(cumc_handle *h, int fill, int side, size_t *bytes) {
+    int rc = slab_side(h, fill, side);
+    if (rc) return rc;
+    if (!bytes) return fail(h, CUMC_EINVAL, "null argument");
+    double *a[16];
+    const int m = halo_arrays(h, side, fill == CUMC_FILL_EMF, a);
+    *bytes = (size_t)m * 3 * h->d.NX * h->d.NY * sizeof(double);
+    return CUMC_OK;
+}
+
+// planes 1..3 (side 0) or nz-2..nz (side 1) -> buf
+int cumc_slab_halo_pack(cumc_handle *h, int fill, int side, void *buf) {
+    int rc = slab_side(h, fill, side);
+    if (rc) return rc;
+    if (!buf) return fail(h, CUMC_EINVAL, "null buffer");
+    const Dev &d = h->d;
+    const size_t plane = (size_t)d.NX * d.NY, n3 = 3 * plane;
+    const size_t off = side == 0 ? 3 * plane : (size_t)d.nz * plane;
+    double *a[16];
+    const int m = halo_arrays(h, side, fill == CUMC_FILL_EMF, a);
+    for (int v = 0; v < m; ++v)
+        CK(cudaMemcpyAsync((double *)buf + v * n3, a[v] + off, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->stream));
+    return CUMC_OK;
+}
+
+// buf -> ghost planes -2..0 (side 0) or nz+1..nz+3 (side 1)
+int cumc_slab_halo_unpack(cumc_handle *h, int fill, int side, const void *buf) {
+    int rc = slab_side(h, fill, side);
+    if (rc) return rc;
+    if (!buf) return fail(h, CUMC_EINVAL, "null buffer");
+    const Dev &d = h->d;
+    const size_t plane = (size_t)d.NX * d.NY, n3 = 3 * plane;
+    const size_t off = side == 0 ? 0 : (size_t)(d.nz + 3) * plane;
+    double *a[16];
+    const int m = halo_arrays(h, side, fill == CUMC_FILL_EMF, a);
+    for (int v = 0; v < m; ++v)
+        CK(cudaMemcpyAsync(a[v] + off, (const double *)buf + v * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->stream));
+    return CUMC_OK;
+}
+
+int cumc_slab_initial_begin(cumc_handle *h) {
+    int rc = slab_check(h);
+    if (rc) return rc;
+    if (!h->have_state) return fail(h, CUMC_ENOTREADY, "set_state first");
+    enqueue_initial(h);
+    CK(cudaGetLastError());
+    return CUMC_OK;
+}
+
+int cumc_slab_initial_end(cumc_handle *h) {
+    int rc = slab_check(h);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    if ((rc = check_scalars(h))) return rc;
+    h->initialised = true;
+    return CUMC_OK;
+}
+
+int cumc_slab_step_begin(cumc_handle *h, double dt) {
+    int rc = slab_check(h);
+    if (rc) return rc;
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, CUMC_EINVAL, "dt must be positive and finite");
+    CK(cudaMemcpyAsync(&h->d.S->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    return CUMC_OK;
+}
+
+int cumc_slab_stage(cumc_handle *h, int stage, int part) {
+    int rc = slab_check(h);
+    if (rc) return rc;
+    if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
+    if (stage < 1 || stage > 3 || (part != 0 && part != 1))
+        return fail(h, CUMC_EINVAL, "stage must be 1..3 and part 0 or 1");
+    if (part == 0) enqueue_stage_a(h, stage);
+    else enqueue_stage_b(h, stage);
+    CK(cudaGetLastError());
+    return CUMC_OK;
+}
+
+int cumc_slab_step_end(cumc_handle *h) {
+    int rc = slab_check(h);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    return check_scalars(h);
 }
 
 int cumc_snapshot_start(cumc_handle *h, double *primitive, double *epsilon, double *bfield) {

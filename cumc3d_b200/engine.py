@@ -28,7 +28,10 @@ EXPORTS = [
     "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest",
     "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set",
     "cumc_collapsar_set", "cumc_collapsar_get", "cumc_snapshot_start", "cumc_snapshot_wait",
-    "cumc_group_initial_update", "cumc_group_finddt", "cumc_group_step", "cumc_mlp_grad", "cumc_mlp_train",
+    "cumc_group_initial_update", "cumc_group_finddt", "cumc_group_step",
+    "cumc_slab_seam", "cumc_slab_halo_bytes", "cumc_slab_halo_pack", "cumc_slab_halo_unpack",
+    "cumc_slab_initial_begin", "cumc_slab_initial_end", "cumc_slab_step_begin", "cumc_slab_stage",
+    "cumc_slab_step_end", "cumc_mlp_grad", "cumc_mlp_train",
     "cumc_mlp_infer", "cumc_mlp_last_error",
     "cumc_last_error",
 ]
@@ -100,6 +103,15 @@ def load_library(path=None):
     L.cumc_group_initial_update.argtypes = [C.c_void_p, C.c_int]
     L.cumc_group_finddt.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     L.cumc_group_step.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    L.cumc_slab_seam.argtypes = [C.c_void_p, C.c_int]
+    L.cumc_slab_halo_bytes.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_size_t)]
+    L.cumc_slab_halo_pack.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.cumc_slab_halo_unpack.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.cumc_slab_initial_begin.argtypes = [C.c_void_p]
+    L.cumc_slab_initial_end.argtypes = [C.c_void_p]
+    L.cumc_slab_step_begin.argtypes = [C.c_void_p, C.c_double]
+    L.cumc_slab_stage.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.cumc_slab_step_end.argtypes = [C.c_void_p]
     L.cumc_collapsar_get.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.cumc_learn_flags.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.cumc_learn_harvest.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p]
@@ -635,3 +647,193 @@ class SlabGroup:
         for i, s in enumerate(self.slabs):
             with self._on(i):
                 s.close()
+
+
+FILL_STATE, FILL_EMF = 0, 1  # the two exchange points of a stage (CUMC_FILL_*)
+
+
+def halo_peers(rank, n, ring):
+    """(lower, upper) neighbour ranks of slab `rank` of n along z; None on a
+    side that is a boundary of the whole grid."""
+    lo = rank - 1 if rank > 0 else (n - 1 if ring else None)
+    hi = rank + 1 if rank + 1 < n else (0 if ring else None)
+    return lo, hi
+
+
+def halo_p2p_ops(peers, send, recv, group=None, tags=True):
+    """torch.distributed point-to-point ops of one exchange point.  send /
+    recv: side -> buffer.  What a rank packs at side s its neighbour unpacks
+    at side 1 - s.  Sends are posted in side order 0, 1 and receives in side
+    order 1, 0: in a ring of two slabs both neighbours are the same rank and
+    the two messages between a pair are matched in posting order (NCCL), so
+    this order pairs the lower planes with the upper ghosts; the tags (the
+    sender's side) pair them the same way where tags are honoured (gloo;
+    tags=False leaves matching to the posting order alone)."""
+    import torch.distributed as dist
+    ops = [dist.P2POp(dist.isend, send[s], peers[s], group, tag=s if tags else 0)
+           for s in (0, 1) if peers[s] is not None]
+    ops += [dist.P2POp(dist.irecv, recv[s], peers[s], group, tag=(1 - s) if tags else 0)
+            for s in (1, 0) if peers[s] is not None]
+    return ops
+
+
+class SlabRank:
+    """One slab of a z-cut grid per process: the one-rank-per-GPU form of
+    SlabGroup (cumc_slab_*).  spec / sizes as for SlabGroup (the whole grid,
+    the slabs' z cell counts); this process holds slab `rank`, on the current
+    CUDA device.  The ghost planes travel by torch.distributed send/recv of
+    contiguous device buffers (NCCL over NVLink between GPUs), or through
+    pinned host buffers when the process group's backend is not NCCL (gloo,
+    e.g. several ranks on one GPU).  finddt is the minimum over the ranks
+    (an all-reduce).  The ranks' states equal the undivided grid's bit for
+    bit."""
+
+    def __init__(self, spec, sizes, rank, group=None):
+        import torch
+        specs, offsets = slab_specs(spec, sizes)
+        if len(sizes) < 2:
+            raise ValueError("a z cut needs at least two slabs")
+        self.n, self.rank, self.group = len(sizes), rank, group
+        self.offset, self.size = offsets[rank], sizes[rank]
+        ring = spec["boundary_flag"][4] == 0
+        self.peers = halo_peers(rank, self.n, ring)
+        self.solver = Solver(specs[rank])
+        self.L, self.h = self.solver.L, self.solver.h
+        if ring and rank == 0:
+            self._check(self.L.cumc_slab_seam(self.h, 0))
+        if ring and rank == self.n - 1:
+            self._check(self.L.cumc_slab_seam(self.h, 1))
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self._stream = torch.cuda.ExternalStream(self.solver.stream(), device=self.device)
+        self.send, self.recv = {}, {}
+        for fill in (FILL_STATE, FILL_EMF):
+            for side in (0, 1):
+                if self.peers[side] is None:
+                    continue
+                nb = C.c_size_t()
+                self._check(self.L.cumc_slab_halo_bytes(self.h, fill, side, C.byref(nb)))
+                self.send[fill, side] = torch.empty(nb.value, dtype=torch.uint8, device=self.device)
+                self.recv[fill, side] = torch.empty(nb.value, dtype=torch.uint8, device=self.device)
+        self._staged = None
+        self.time, self.n_step = 0.0, 0
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CumcError(rc, self.L.cumc_last_error(self.h).decode())
+
+    # -- the per-rank calls (one exchange point = pack, transport, unpack) --
+    def pack(self, fill):
+        for side in (0, 1):
+            if self.peers[side] is not None:
+                self._check(self.L.cumc_slab_halo_pack(self.h, fill, side, self.send[fill, side].data_ptr()))
+
+    def unpack(self, fill):
+        for side in (0, 1):
+            if self.peers[side] is not None:
+                self._check(self.L.cumc_slab_halo_unpack(self.h, fill, side, self.recv[fill, side].data_ptr()))
+
+    def stage(self, stage, part):
+        self._check(self.L.cumc_slab_stage(self.h, stage, part))
+
+    def initial_begin(self):
+        self._check(self.L.cumc_slab_initial_begin(self.h))
+
+    def initial_end(self):
+        self._check(self.L.cumc_slab_initial_end(self.h))
+
+    def step_begin(self, dt):
+        self._check(self.L.cumc_slab_step_begin(self.h, float(dt)))
+
+    def step_end(self):
+        self._check(self.L.cumc_slab_step_end(self.h))
+
+    # -- torch.distributed driver --
+    def _transport(self, fill):
+        import torch
+        import torch.distributed as dist
+        if self._staged is None:
+            self._staged = dist.get_backend(self.group) != "nccl"
+            if self._staged:
+                self._hsend = {k: torch.empty(v.numel(), dtype=torch.uint8, pin_memory=True) for k, v in self.send.items()}
+                self._hrecv = {k: torch.empty(v.numel(), dtype=torch.uint8, pin_memory=True) for k, v in self.recv.items()}
+        sides = [s for s in (0, 1) if self.peers[s] is not None]
+        if not self._staged:
+            # NCCL runs on its own stream, after the packs on the engine's
+            # stream; wait() orders the engine's stream after it
+            with torch.cuda.stream(self._stream):
+                works = dist.batch_isend_irecv(halo_p2p_ops(self.peers, {s: self.send[fill, s] for s in sides},
+                                                            {s: self.recv[fill, s] for s in sides}, self.group))
+                for w in works:
+                    w.wait()
+            return
+        with torch.cuda.stream(self._stream):
+            for s in sides:
+                self._hsend[fill, s].copy_(self.send[fill, s], non_blocking=True)
+        self._stream.synchronize()
+        works = dist.batch_isend_irecv(halo_p2p_ops(self.peers, {s: self._hsend[fill, s] for s in sides},
+                                                    {s: self._hrecv[fill, s] for s in sides}, self.group))
+        for w in works:
+            w.wait()
+        with torch.cuda.stream(self._stream):
+            for s in sides:
+                self.recv[fill, s].copy_(self._hrecv[fill, s], non_blocking=True)
+
+    def exchange(self, fill):
+        self.pack(fill)
+        self._transport(fill)
+        self.unpack(fill)
+
+    def set_state(self, prim, eps):
+        """The whole grid's prim (nz+6, ny+6, nx+6, 8) and eps; this rank
+        takes its planes."""
+        o, m = self.offset, self.size
+        self.solver.set_state(np.ascontiguousarray(prim[o:o + m + 6]), np.ascontiguousarray(eps[o:o + m + 6]))
+
+    def initial_update(self):
+        self.initial_begin()
+        self.exchange(FILL_STATE)
+        self.initial_end()
+
+    def finddt(self):
+        import torch
+        import torch.distributed as dist
+        dt = self.solver.finddt()
+        t = torch.tensor([dt], dtype=torch.float64, device="cpu" if self._is_staged() else self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
+        return float(t.item())
+
+    def _is_staged(self):
+        if self._staged is None:
+            import torch.distributed as dist
+            return dist.get_backend(self.group) != "nccl"
+        return self._staged
+
+    def step(self, dt):
+        self.step_begin(dt)
+        for stage in (1, 2, 3):
+            self.stage(stage, 0)
+            self.exchange(FILL_EMF)
+            self.stage(stage, 1)
+            self.exchange(FILL_STATE)
+        self.step_end()
+        self.time += dt
+        self.n_step += 1
+
+    def get_state(self):
+        """(prim, eps) of this slab's interior planes, (size, ny+6, nx+6, ...)."""
+        p, e = self.solver.get_state()
+        return p[3:3 + self.size], e[3:3 + self.size]
+
+    def get_array(self, which):
+        return self.solver.get_array(which)[3:3 + self.size]
+
+    def close(self):
+        """Release the halo buffers while the engine's stream still exists
+        (freeing a buffer that a copy used records an event on that stream),
+        then the handle."""
+        import torch
+        self._stream.synchronize()
+        self.send, self.recv = {}, {}
+        self._hsend, self._hrecv = {}, {}
+        torch.cuda.synchronize(self.device)
+        self.solver.close()

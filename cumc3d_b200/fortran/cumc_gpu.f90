@@ -24,6 +24,7 @@ INTEGER(C_INT), PARAMETER :: CUMC_FLOOR_NONE = 0, CUMC_FLOOR_EPS = 1, CUMC_FLOOR
 INTEGER(C_INT), PARAMETER :: CUMC_SRC_NONE = 0, CUMC_SRC_CONST_GY = 1, CUMC_SRC_PM_CYL = 2, CUMC_SRC_PM_SPH = 3
 INTEGER(C_INT), PARAMETER :: CUMC_SRC_COLLAPSAR = 4
 INTEGER(C_INT), PARAMETER :: CUMC_BOUNDARY_EXCHANGE = 9
+INTEGER(C_INT), PARAMETER :: CUMC_FILL_STATE = 0, CUMC_FILL_EMF = 1
 
 ! cumc_model (include/cumc3d_gpu.h)
 TYPE, BIND(C) :: cumc_model
@@ -189,6 +190,51 @@ INTERFACE
     TYPE(C_PTR), VALUE :: slabs
     INTEGER(C_INT), VALUE :: n
     REAL(C_DOUBLE), VALUE :: dt
+  END FUNCTION
+  ! one slab per MPI rank: the caller moves the packed device buffers
+  ! (CUDA-aware MPI_Sendrecv, or NCCL) between neighbouring ranks
+  INTEGER(C_INT) FUNCTION cumc_slab_seam(h, side) BIND(C, NAME='cumc_slab_seam')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: side
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_halo_bytes(h, fill, side, nbytes) BIND(C, NAME='cumc_slab_halo_bytes')
+    IMPORT :: C_INT, C_PTR, C_SIZE_T
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: fill, side
+    INTEGER(C_SIZE_T), INTENT(OUT) :: nbytes
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_halo_pack(h, fill, side, buf) BIND(C, NAME='cumc_slab_halo_pack')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h, buf
+    INTEGER(C_INT), VALUE :: fill, side
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_halo_unpack(h, fill, side, buf) BIND(C, NAME='cumc_slab_halo_unpack')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h, buf
+    INTEGER(C_INT), VALUE :: fill, side
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_initial_begin(h) BIND(C, NAME='cumc_slab_initial_begin')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_initial_end(h) BIND(C, NAME='cumc_slab_initial_end')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_step_begin(h, dt) BIND(C, NAME='cumc_slab_step_begin')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    REAL(C_DOUBLE), VALUE :: dt
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_stage(h, stage, part) BIND(C, NAME='cumc_slab_stage')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: stage, part
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_slab_step_end(h) BIND(C, NAME='cumc_slab_step_end')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
   END FUNCTION
   ! output snapshots (the datasets of print_hydroprofile)
   INTEGER(C_INT) FUNCTION cumc_snapshot_start(h, primitive, epsilon, bfield) BIND(C, NAME='cumc_snapshot_start')

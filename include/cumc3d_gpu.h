@@ -339,6 +339,41 @@ int cumc_group_initial_update(cumc_handle **slabs, int n);
 int cumc_group_finddt(cumc_handle **slabs, int n, double *dt);
 int cumc_group_step(cumc_handle **slabs, int n, double dt);
 
+/* One slab per process (one rank per GPU; no counterpart in the reference).
+ * The same slabs, stage split and ghost planes as cumc_group_*, with the
+ * planes carried by the caller: at each exchange point pack the three
+ * planes next to every exchanged z side into a contiguous device buffer,
+ * send it to that side's neighbour (NCCL send/recv, or a host-staged copy),
+ * and unpack what the neighbour sent into the side's ghost planes.  A
+ * buffer packed at side s is unpacked by the neighbour at side 1 - s; both
+ * ends of one cut agree on its size.  Everything is ordered on the handle's
+ * stream (cumc_stream): a transport that runs on another stream orders
+ * itself after the pack and before the unpack.  One step of a slab:
+ *
+ *   cumc_finddt ; the minimum over the ranks ; cumc_slab_step_begin(dt)
+ *   for stage 1..3:
+ *     cumc_slab_stage(stage, 0) ; exchange CUMC_FILL_EMF
+ *     cumc_slab_stage(stage, 1) ; exchange CUMC_FILL_STATE
+ *   cumc_slab_step_end
+ *
+ * and INITIAL_UPDATE: cumc_slab_initial_begin ; exchange CUMC_FILL_STATE ;
+ * cumc_slab_initial_end.  For a periodic z axis the two end sides of the
+ * ring are the whole grid's periodic boundary: mark them with
+ * cumc_slab_seam (the first slab's side 0, the last slab's side 1) before
+ * cumc_slab_initial_begin.  The ranks' states equal the undivided grid's bit
+ * for bit.  Not with the learned flag, the collapsar source or FIXPOLE. */
+#define CUMC_FILL_STATE 0  /* the state fill that ends a stage (BOUNDARY)         */
+#define CUMC_FILL_EMF   1  /* the EMF fill inside a stage (BOUNDARY_EFIELD)       */
+int cumc_slab_seam(cumc_handle *h, int side);
+int cumc_slab_halo_bytes(cumc_handle *h, int fill, int side, size_t *bytes);
+int cumc_slab_halo_pack(cumc_handle *h, int fill, int side, void *device_buffer);
+int cumc_slab_halo_unpack(cumc_handle *h, int fill, int side, const void *device_buffer);
+int cumc_slab_initial_begin(cumc_handle *h);
+int cumc_slab_initial_end(cumc_handle *h);
+int cumc_slab_step_begin(cumc_handle *h, double dt);
+int cumc_slab_stage(cumc_handle *h, int stage, int part);
+int cumc_slab_step_end(cumc_handle *h);
+
 /* Output snapshot without stalling the step loop (print_hydroprofile,
  * solver/mhd/dataio.f90:31-240, which updates the host copy and writes HDF5).
  * cumc_snapshot_start packs the state as the reference writes it --
