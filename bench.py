@@ -993,13 +993,34 @@ def main():
             fp64_pipe = json.load(f).get("%s/%s/fp64" % (args.recon, args.riemann))
     if fp64_pipe is not None:
         roofline["fp64_pipe_frac_ncu"] = fp64_pipe
-        roofline["note"] = ("the flux kernels are FP64-pipe bound (fp64_pipe_frac_ncu); the HBM fraction is "
-                            "reported against the algorithmic bytes of a fused pass")
+        roofline["note"] = ("the flux kernels are FP64-pipe bound (fp64_pipe_frac_ncu; roofline.fp64 counts a "
+                            "division or square root as one flop, though each is several FP64 instructions); "
+                            "the HBM fraction is reported against the algorithmic bytes of a fused pass")
     step_gbs = STEP_BYTES_PER_ZONE * value / world / 1e9
     try:
         fp64_peak = engine.fp64_peak_tflops()
     except Exception:
         fp64_peak = None
+    # the FP64 side: exact operation counts per zone of this workload (the
+    # oracle on its counting scalar type, oracle/count_ops.py)
+    step_fp64 = None
+    okey = "blast3d_%s_%s" % (args.recon, args.riemann)
+    opath = os.path.join(ROOT, "profiles", "op_counts.json")
+    ops = None
+    if args.precision == "fp64" and os.path.exists(opath):
+        with open(opath) as f:
+            ops = json.load(f).get(okey)
+    if ops is not None and fp64_peak:
+        if dominant.startswith("flux"):
+            fl = ops["flux_sweep_flops_per_zone"] * zones
+            roofline["fp64"] = {"flops_per_launch": fl, "achieved_tflops": fl / (avg_ms * 1e-3) / 1e12,
+                                "peak_tflops": fp64_peak, "frac": fl / (avg_ms * 1e-3) / 1e12 / fp64_peak,
+                                "peak_source": "cumc_fp64_peak (DFMA loop, measured in this run)",
+                                "counts": "profiles/op_counts.json %s: flux_sweep_flops_per_zone "
+                                          "(add, mul, div, sqrt one flop each)" % okey}
+        tf = ops["flops_per_zone_update"] * value / world / 1e12
+        step_fp64 = {"flops_per_zone_update": ops["flops_per_zone_update"], "achieved_tflops": tf,
+                     "frac": tf / fp64_peak}
 
     # end to end through the C-ABI with pinned host buffers
     e2e = None
@@ -1065,6 +1086,7 @@ def main():
             "roofline": roofline,
             "step_hbm": {"bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved_gbs": step_gbs,
                          "frac": step_gbs / peak_gbs},
+            "step_fp64": step_fp64,
             "fp64_peak_tflops_measured": fp64_peak,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -41,7 +41,17 @@ namespace orc {
 /* scalar types                                                        */
 /* ------------------------------------------------------------------ */
 struct OpCounts { uint64_t add = 0, mul = 0, div = 0, sqrt = 0, cmp = 0; };
-static OpCounts g_ops;
+/* counts per phase of the step: 0 the rest, 1 face reconstruction,
+ * 2 BUILDSTATES + the Riemann solver, 3 FINDDT */
+enum { PH_OTHER = 0, PH_RECON = 1, PH_RIEMANN = 2, PH_DT = 3, N_PHASES = 4 };
+static OpCounts g_ops_ph[N_PHASES];
+static int g_phase = PH_OTHER;
+#define g_ops g_ops_ph[g_phase]
+struct PhaseScope {
+    int saved;
+    explicit PhaseScope(int p) : saved(g_phase) { g_phase = p; }
+    ~PhaseScope() { g_phase = saved; }
+};
 
 struct CReal {
     double v;
@@ -1239,9 +1249,15 @@ struct Sim {
         get_source();
         custom_source();
         for (int dir = 1; dir <= n_dim; ++dir) {
-            recon(dir);
-            buildstates(dir);
-            riemann(dir);
+            {
+                PhaseScope ph(PH_RECON);
+                recon(dir);
+            }
+            {
+                PhaseScope ph(PH_RIEMANN);
+                buildstates(dir);
+                riemann(dir);
+            }
             if (dir == 1 && cfg.model.source_kind == CUMC_SRC_COLLAPSAR) {
                 /* GETFLUX_X, model/collapsar/src/custom.f90:222-240 */
                 mflux.assign((size_t)ny * nz, R(0.0));
@@ -1338,6 +1354,7 @@ struct Sim {
 
     /* FINDDT rungekutta.f90:221-332 */
     double finddt() {
+        PhaseScope ph(PH_DT);
         double dt_out2 = 1.0e5;
 #pragma omp parallel for collapse(2) schedule(static) reduction(min : dt_out2)
         for (int l = 1; l <= nz; ++l)
@@ -1820,10 +1837,20 @@ void orc_set_phi(void *p, const double *phi) {
     if (h->counting) set(h->c); else set(h->d);
 }
 
-void orc_reset_counts(void) { g_ops = OpCounts(); }
-void orc_get_counts(uint64_t *out5) {
-    out5[0] = g_ops.add; out5[1] = g_ops.mul; out5[2] = g_ops.div; out5[3] = g_ops.sqrt; out5[4] = g_ops.cmp;
+void orc_reset_counts(void) {
+    for (int p = 0; p < N_PHASES; ++p) g_ops_ph[p] = OpCounts();
 }
+/* add, mul, div, sqrt, cmp summed over the phases (phase < 0) or of one
+ * phase (0 the rest, 1 reconstruction, 2 BUILDSTATES + Riemann, 3 FINDDT) */
+void orc_get_phase_counts(int phase, uint64_t *out5) {
+    for (int i = 0; i < 5; ++i) out5[i] = 0;
+    for (int p = 0; p < N_PHASES; ++p) {
+        if (phase >= 0 && p != phase) continue;
+        const OpCounts &c = g_ops_ph[p];
+        out5[0] += c.add; out5[1] += c.mul; out5[2] += c.div; out5[3] += c.sqrt; out5[4] += c.cmp;
+    }
+}
+void orc_get_counts(uint64_t *out5) { orc_get_phase_counts(-1, out5); }
 /* OpenMP threads of the following calls (the reference hard-codes 4,
  * solver/mhd/main.f90:31; the baselines also run on every host core) */
 void orc_set_num_threads(int n) {

@@ -56,6 +56,7 @@ def lib():
         L.orc_max_divb.argtypes = [C.c_void_p]
         L.orc_max_divb.restype = C.c_double
         L.orc_get_counts.argtypes = [C.POINTER(C.c_uint64)]
+        L.orc_get_phase_counts.argtypes = [C.c_int, C.POINTER(C.c_uint64)]
         L.orc_num_threads.restype = C.c_int
         L.orc_set_num_threads.argtypes = [C.c_int]
         L.orc_recon_cell.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -155,9 +156,15 @@ def reset_counts():
     lib().orc_reset_counts()
 
 
-def get_counts():
+PHASES = {"other": 0, "recon": 1, "riemann": 2, "finddt": 3}
+
+
+def get_counts(phase=None):
+    """Operations of a counting handle since reset_counts: all phases, or
+    one of PHASES ("recon": face reconstruction; "riemann": BUILDSTATES and
+    the Riemann solver; "finddt"; "other": the rest of the step)."""
     out = (C.c_uint64 * 5)()
-    lib().orc_get_counts(out)
+    lib().orc_get_phase_counts(-1 if phase is None else PHASES[phase], out)
     return dict(add=out[0], mul=out[1], div=out[2], sqrt=out[3], cmp=out[4])
 
 
