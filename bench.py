@@ -786,6 +786,37 @@ def bench_config(args, world, rank, local, dist):
         key = args.precision
         n, ms = out[key]["steps"], out[key]["ms"]
         name = "alfven3d_%d^3_%s_%s_cfl0.4_one_period" % (n3, recon, args.riemann)
+    elif args.workload == "torus_sph":
+        # the spherical torus on the refined grid its model reads (124 x 44 x
+        # 128), PPM + HLLD at CFL 0.8 as the reference ships them, FP64 and FP32
+        recon = args.recon_c or "ppm"
+        spec, prim, eps = models.torus_sph(recon=recon, riemann=args.riemann)
+        spec["positivity_fallback"] = 1 if recon == "weno" else 0
+        # periodic phi: as for the cylindrical torus, the face-0 option keeps
+        # the wound-up B_phi divergence-free at the seam
+        spec["fix_periodic_normal_faces"] = 1
+        zones = spec["nx"] * spec["ny"] * spec["nz"]
+        out = {}
+        clocks.start()
+        for name_f, sp in (("fp64", dict(spec)), ("fp32", dict(spec, precision="fp32"))):
+            s, k, t_ms = _evolve_timed(engine, torch, sp, prim, eps, args.warmup, steps=args.steps)
+            out[name_f] = dict(cons=s.get_array(capi.ARR_CONS), divb=s.find_divb(), steps=k, ms=t_ms, t=s.time)
+            s.close()
+        clk = clocks.stop()
+        sl = (slice(3, spec["nz"] + 3), slice(3, spec["ny"] + 3), slice(3, spec["nx"] + 3))
+        a, b = out["fp32"]["cons"][sl].reshape(-1, 8), out["fp64"]["cons"][sl].reshape(-1, 8)
+        den = np.abs(b).sum(axis=0)
+        l1 = (np.abs(a - b).sum(axis=0) / np.where(den == 0, 1, den)).tolist()
+        extra.update({"l1_fp32_vs_fp64_per_var": l1, "l1_fp32_vs_fp64_max": max(l1),
+                      "max_divb": {f: out[f]["divb"] for f in out}, "time_reached": {f: out[f]["t"] for f in out},
+                      "orbital_period": spec["t_orbit"]})
+        for f in out:
+            extra["%s_zone_updates_per_s" % f] = zones * out[f]["steps"] / (out[f]["ms"] * 1e-3)
+        n, ms = out[args.precision]["steps"], out[args.precision]["ms"]
+        name = "torus_sph_%dx%dx%d_%s_%s_ct_cfl0.8" % (spec["nx"], spec["ny"], spec["nz"], recon, args.riemann)
+        if not args.no_cpu:
+            cpu = cpu_baseline_of(lambda: models.torus_sph(recon=recon, riemann=args.riemann), 2,
+                                  "CPU oracle, the same torus and grid, 2 RK3 steps")
     else:  # torus
         recon = args.recon_c or "weno"
         spec, prim, eps = models.torus_cyl(recon=recon, riemann=args.riemann, precision="fp64")
@@ -858,7 +889,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blast3d",
-                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "poisson", "snapshots", "slabs"])
+                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "torus_sph", "poisson", "snapshots",
+                             "slabs"])
     ap.add_argument("--slabs", type=int, default=2, help="slabs: number of z slabs")
     ap.add_argument("--snapshot-every", type=int, default=10, help="snapshots: steps between two snapshots")
     ap.add_argument("--sor-grid", default="384,192,192", help="poisson: nr,ntheta,nphi of the star")
@@ -889,7 +921,8 @@ def main():
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "poisson": 20, "snapshots": 60, "slabs": 30}.get(args.workload, 0)
+        args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "torus_sph": 1000, "poisson": 20, "snapshots": 60,
+                      "slabs": 30}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -904,7 +937,7 @@ def main():
     engine.load_library()
     if args.workload == "batch1d":
         return bench_batch(args, world, rank, local, dist)
-    if args.workload in ("briowu", "alfven3d", "torus"):
+    if args.workload in ("briowu", "alfven3d", "torus", "torus_sph"):
         return bench_config(args, world, rank, local, dist)
     if args.workload == "poisson":
         return bench_poisson(args, world, rank, local, dist)

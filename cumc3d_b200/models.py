@@ -287,6 +287,136 @@ def torus_cyl(nr=192, nphi=128, nz=192, r_range=(2.0, 42.0), z_range=(-20.0, 20.
     return spec, prim, np.ascontiguousarray(eps)
 
 
+def torus_sph(nr=None, ntheta=None, nphi=None, faces=None, r_range=(1.5, 31.5), recon="ppm", riemann="hlld",
+              cfl=0.8, precision="fp64", learned=0, seed=20261203, r_sh=1.0, s_in=3.0, s_max=4.7, q=2.0,
+              gamma=5.0 / 3.0, rho_max=1.0, rho_fac=1e-4, rho_cut=0.5, p_beta=350.0, noise=1e-4, fixpole=1):
+    """Torus around a pseudo-Newtonian (Paczynski-Wiita, r_sh = 1) point
+    mass on a spherical (r, theta, phi) grid: GET_MODEL of
+    model/torus-sph/src/model.f90:6-316 with the values of its param.h
+    (q = 2, s_in = 3, s_max = 4.7, gamma = 5/3, rho_fac = 1e-4, rho_cut = 0.5,
+    field scaled to the minimum plasma beta p_beta = 350, no corona).
+
+    The grid: ``faces`` (xF, yF, zF), or nr x ntheta x nphi uniform cells
+    over r_range x (0, pi) x (0, 2 pi), or by default the refined grid the
+    model reads (CUSTOM_GRID, model/torus-sph/src/custom.f90:54-145), made
+    by the restated generator (124 x 44 x 128 cells).  Boundaries: outflow
+    in r with the torus's radial-velocity clamps, the polar axis in theta
+    (with FIXPOLE), periodic in phi.  Density inside the torus
+    (model.f90:84-122): H = -Phi(r) + l_K^2 s^(2-2q)/(2-2q) + C with
+    Phi(r) = -1/(r - r_sh), s = r sin(theta); rho = (H (g-1)/g/K)^(1/(g-1))
+    where it exceeds the atmosphere and s >= s_in, else the atmosphere
+    rho_fac rho_max; p = K rho^g.  A_phi = (rho - rho_cut)/rho_max where
+    rho >= rho_cut, averaged to the cell corners; the face field is its
+    curl (model.f90:127-145, 209-226).  The density is perturbed by a
+    seeded uniform 1e-4 (model.f90:285-294; RANDOM_NUMBER there).
+    Solver defaults as the reference's solver/mhd/parameter.h ships them:
+    PPM + HLLD, CFL 0.8.  The atmosphere is cold (p = K rho_atm^gamma, about
+    1.7e-9 against 0.14 in the torus): WENO-Z reconstructs negative face
+    pressures next to the torus within a step and the sound speed becomes
+    NaN, in the reference's arithmetic as in this one, so WENO-Z needs the
+    positivity fallback here.
+    Returns (spec, prim, eps); cells outside 1..n hold the atmosphere until
+    INITIAL_UPDATE fills the ghosts."""
+    from . import grids
+    g = gamma
+    if faces is None and nr is None:
+        nr, ntheta, nphi, r, th, ph = grids.spherical_torus_grid()
+        faces = (r, th, ph)
+    spec = _base_spec(nr, ntheta, nphi, 3, (1, 1, 3, 3, 0, 0), r_range, (0.0, math.pi), (0.0, 2.0 * math.pi),
+                      coordinate_flag=2, cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      learned=learned, fixpole=fixpole, name="torus_sph_%dx%dx%d" % (nr, ntheta, nphi))
+    if faces is not None:
+        for key, f, n in zip(("xF", "yF", "zF"), faces, (nr, ntheta, nphi)):
+            f = np.asarray(f, dtype=np.float64)
+            if f.shape != (n + 7,):
+                raise ValueError("%s needs %d faces (indices -3..n+3)" % (key, n + 7))
+            spec[key] = f
+    xF, yF = spec["xF"], spec["yF"]
+    x, y = centers(xF), centers(yF)            # indices -2..n+3
+    dx = xF[1:] - xF[:-1]
+    sinf = np.sin(yF[1:])                      # indices -2..ny+3 (sinf(k) = sin(yF(k)))
+    if fixpole:  # getgrid.f90:91-98, after the other metric arrays: sin 0 on the axis
+        sinf[2], sinf[2 + ntheta] = 0.0, 0.0
+    dcose = -(np.cos(yF[1:]) - np.cos(yF[:-1]))
+    dy = yF[1:] - yF[:-1]
+    dx_cb = xF[1:] ** 3 - xF[:-1] ** 3
+
+    def schwarzschild(rr):
+        return -1.0 / (rr - r_sh)
+
+    lkep2 = s_max ** (2.0 * q - 1.0) / (s_max - r_sh) ** 2
+    c_const = schwarzschild(s_in) - lkep2 * s_in ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q)
+    h_max = -schwarzschild(s_max) + lkep2 * s_max ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q) + c_const
+    k_poly = h_max * (g - 1.0) / g / rho_max ** (g - 1.0)
+    if k_poly < 0.0:
+        raise ValueError("The polytropic constant is negative")
+    rho_a = rho_fac * rho_max
+    X, Y = np.meshgrid(x, y, indexing="xy")    # (ny+6, nx+6): [k+2, j+2]
+    s_eq = X * np.sin(Y)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        enth = -schwarzschild(X) + lkep2 * s_eq ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q) + c_const
+    enth = np.where(np.isfinite(enth) & (enth > 0.0), enth, 0.0)
+    rho_t = (enth * (g - 1.0) / g / k_poly) ** (1.0 / (g - 1.0))
+    inside = (rho_t > rho_a) & (s_eq >= s_in)
+    interior = np.zeros_like(inside)
+    interior[3:3 + ntheta, 3:3 + nr] = True      # cells 1..n, where GET_MODEL writes
+    inside &= interior
+    rho2 = np.where(inside, rho_t, rho_a)
+    with np.errstate(divide="ignore"):
+        vphi2 = np.where(inside, np.sqrt(lkep2) * np.where(inside, s_eq, 1.0) ** (-q) * s_eq, 0.0)
+    p2 = k_poly * rho2 ** g
+    eps2 = k_poly * rho2 ** (g - 1.0) / (g - 1.0)
+    a_phi = np.where(interior & (rho2 >= rho_cut), (rho2 - rho_cut) / rho_max, 0.0)
+
+    def face_b(a_ph):
+        # corners (j, k) for j, k = 1..n from the cells j..j+1, k..k+1
+        a_c = np.zeros_like(a_ph)
+        a_c[3:3 + ntheta, 3:3 + nr] = 0.25 * (a_ph[3:3 + ntheta, 3:3 + nr] + a_ph[3:3 + ntheta, 4:4 + nr]
+                                               + a_ph[4:4 + ntheta, 3:3 + nr] + a_ph[4:4 + ntheta, 4:4 + nr])
+        bx = np.zeros_like(a_ph)
+        by = np.zeros_like(a_ph)
+        kk = slice(2, 3 + ntheta)                  # k = 0..ny
+        jj = slice(2, 3 + nr)                      # j = 0..nx
+        km, jm = slice(1, 2 + ntheta), slice(1, 2 + nr)
+        xf = xF[1:]                                # xF(j) at index j+2
+        bx[kk, jj] = ((sinf[kk, None] * a_c[kk, jj] - sinf[km, None] * a_c[km, jj])
+                      / (xf[None, jj] * dcose[kk, None] + np.finfo(np.float64).tiny))
+        by[kk, jj] = -(xf[None, jj] * a_c[kk, jj] - xf[None, jm] * a_c[kk, jm]) / (x[None, jj] * dx[None, jj])
+        return bx, by
+
+    bx, by = face_b(a_phi)
+    # cell-centred field for the beta normalisation (model.f90:150-158)
+    xf = xF[1:]
+    bxc = np.zeros_like(bx)
+    byc = np.zeros_like(by)
+    ki, ji = slice(3, 3 + ntheta), slice(3, 3 + nr)
+    kim, jim = slice(2, 2 + ntheta), slice(2, 2 + nr)
+    bxc[ki, ji] = 1.5 * dx[None, ji] / dx_cb[None, ji] * (xf[None, ji] ** 2 * bx[ki, ji] + xf[None, jim] ** 2 * bx[ki, jim])
+    byc[ki, ji] = 0.5 * dy[ki, None] / dcose[ki, None] * (sinf[ki, None] * by[ki, ji] + sinf[kim, None] * by[kim, ji])
+    b2 = bxc ** 2 + byc ** 2
+    sel = interior & (b2 > 0.0)
+    beta_min = np.min(2.0 * p2[sel] / b2[sel]) if np.any(sel) else 1e30
+    b0 = math.sqrt(beta_min / p_beta)
+    bx, by = face_b(a_phi * b0)
+    prim = np.zeros((nphi + 6, ntheta + 6, nr + 6, 8), dtype=np.float64)
+    prim[..., IRHO] = rho2[None]
+    prim[..., IVZ] = vphi2[None]
+    prim[..., ITAU] = p2[None]
+    prim[..., IBX] = bx[None]
+    prim[..., IBY] = by[None]
+    eps = np.broadcast_to(eps2[None], prim.shape[:3]).copy()
+    rho_floor = rho_max * rho_fac
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pert = (rng.random(prim.shape[:3]) - 0.5) / 0.5 * noise
+    above = prim[..., IRHO] > rho_floor
+    above[:, ~interior] = False
+    prim[..., IRHO] = np.where(above, prim[..., IRHO] + prim[..., IRHO] * pert, prim[..., IRHO])
+    spec["model"] = dict(gamma=g, floor="torus", rho_floor=rho_floor, eps_floor=k_poly * rho_floor ** (g - 1.0) / (g - 1.0),
+                         p_floor=k_poly * rho_floor ** g, source="pm_sph", r_sh=r_sh, bc="torus_sph")
+    spec["t_orbit"] = 2.0 * math.pi / (math.sqrt(lkep2) * s_max ** (-q))
+    return spec, prim, np.ascontiguousarray(eps)
+
+
 # ---------------------------------------------------------------------------
 # self-gravitating star on a spherical grid: the setting of the collapsar
 # model's gravity solve (model/collapsar/src/custom.f90:489-620).  The

@@ -84,6 +84,29 @@ def test_spherical_fixpole_bitwise(oracle_mod):
     assert_bitwise(g, o, spec)
 
 
+@pytest.mark.parametrize("grid,recon", [("uniform", "ppm"), ("shipped_r_theta", "ppm"), ("uniform", "weno")])
+def test_spherical_torus_model_bitwise(oracle_mod, grid, recon):
+    """The spherical torus (model/torus-sph: pseudo-Newtonian point mass
+    with r_sh = 1, torus floors, radial clamps, polar axis with FIXPOLE) from
+    its own initial model, PPM + HLLD at CFL 0.8 as the reference ships it:
+    on a uniform grid, and on the refined r and theta faces the model reads
+    (with 8 phi cells); and WENO-Z with the positivity fallback."""
+    import math
+    from cumc3d_b200 import grids
+    if grid == "uniform":
+        spec, prim, eps = models.torus_sph(32, 20, 8, r_range=(2.0, 10.0), recon=recon)
+    else:
+        nx, ny, _, r, th, _ = grids.spherical_torus_grid()
+        ph = models.faces(0.0, 2.0 * math.pi, 8)
+        spec, prim, eps = models.torus_sph(nx, ny, 8, faces=(r, th, ph), recon=recon)
+    spec["positivity_fallback"] = 1 if recon == "weno" else 0
+    g, o, dg, do = run_pair(spec, prim, eps, 4, oracle_mod)
+    assert np.isfinite(interior(g["prim"], spec)).all()
+    assert dg == do
+    assert_bitwise(g, o, spec)
+    assert_bitwise(g, o, spec, what=("cons",))
+
+
 def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
     """The headline blast (p 10 : 0.1, beta 0.2 outside) breaks the reference's
     WENO-Z + HLLD within a few steps (negative face pressure, see
