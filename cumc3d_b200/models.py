@@ -91,6 +91,104 @@ def riemann_1d(nx, left, right, bx, gamma=5.0 / 3.0, recon="ppm", riemann="hlld"
     return spec, prim, eps
 
 
+# ---------------------------------------------------------------------------
+# 2D MHD problems of the riemann model: model/riemann/src/riemann2d.f90:441-640
+# ---------------------------------------------------------------------------
+RIEMANN_2D = {
+    # test_model: (name, gamma, boundary_flag, x range, y range, t_end)
+    13: ("current_sheet", 5.0 / 3.0, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 10.0),
+    14: ("rotor", 5.0 / 3.0, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.295),
+    15: ("orszag_tang", 5.0 / 3.0, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 1.0),
+    16: ("blast", 5.0 / 3.0, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.2),
+    17: ("kelvin_helmholtz", 1.4, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 5.0),
+    18: ("rayleigh_taylor", 1.4, (0, 0, 2, 2, 1, 1), (0.0, 1.0), (0.0, 1.0), 12.5),
+    19: ("current_loop", 5.0 / 3.0, (0, 0, 0, 0, 1, 1), (-1.0, 1.0), (-0.5, 0.5), 2.0),
+}
+
+
+def riemann_2d(test_model, nx=128, ny=None, recon="ppm", riemann="hlld", cfl=0.4, precision="fp64", seed=20261203):
+    """The MHD tests of the riemann model's 2D set, by its test_model number
+    (riemann2d.f90:441-640): 13 current sheet, 14 rotor, 15 Orszag-Tang
+    vortex, 16 blast, 17 Kelvin-Helmholtz, 18 Rayleigh-Taylor (with the
+    model's constant gravity g = 0.1 in -y, custom.f90:132-159), 19 advected
+    current loop.  Boundaries, gamma and end times as the file states them;
+    the cells 0..n are set, face fields from the cell-centre formulas as the
+    reference writes them, the loop's from a corner vector potential.  The
+    seeded uniform numbers stand in for RANDOM_NUMBER (17, 18)."""
+    name, g, bflag, xr, yr, t_end = RIEMANN_2D[test_model]
+    ny = ny or nx
+    model = dict(gamma=g, floor="eps")
+    if test_model == 18:
+        model.update(source="const_gy", g_const=0.1)
+    spec = _base_spec(nx, ny, 1, 2, bflag, xr, yr, (0.0, 1.0), cfl=cfl, recon=recon, riemann=riemann,
+                      precision=precision, model=model, t_end=t_end, name="riemann2d_%s_%dx%d" % (name, nx, ny))
+    prim, eps = _alloc(nx, ny, 1)
+    x, y = centers(spec["xF"]), centers(spec["yF"])
+    xF, yF = spec["xF"][1:], spec["yF"][1:]           # xF(j) at index j+2
+    dx, dy = spec["xF"][1:] - spec["xF"][:-1], spec["yF"][1:] - spec["yF"][:-1]
+    J, K = slice(2, nx + 3), slice(2, ny + 3)          # cells 0..n
+    X, Y = np.meshgrid(x[J], y[K], indexing="xy")      # (ny+1, nx+1): [k, j]
+    P = np.zeros(X.shape + (8,))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pi = math.pi
+    if test_model == 13:
+        P[..., IBY] = np.where((X <= 0.25) | (X >= 0.75), 1.0, -1.0) / math.sqrt(4.0 * pi)
+        P[..., IRHO] = 1.0
+        P[..., ITAU] = 0.1 * 0.5
+        P[..., IVX] = 0.1 * np.sin(2.0 * pi * (Y - 0.5))
+    elif test_model == 14:
+        r0, r1 = 0.1, 0.115
+        r = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+        fr = (r1 - r) / (r1 - r0)
+        inner, outer = r <= r0, r >= r1
+        rs = np.where(inner | outer, 1.0, r)
+        P[..., IRHO] = np.where(inner, 10.0, np.where(outer, 1.0, 1.0 + 9.0 * fr))
+        P[..., IVX] = np.where(inner, -1.0 * (Y - 0.5) / r0, np.where(outer, 0.0, -fr * 1.0 * (Y - 0.5) / rs))
+        P[..., IVY] = np.where(inner, 1.0 * (X - 0.5) / r0, np.where(outer, 0.0, fr * 1.0 * (X - 0.5) / rs))
+        P[..., ITAU] = 0.5
+        P[..., IBX] = 2.5 / math.sqrt(4.0 * pi)
+    elif test_model == 15:
+        P[..., IRHO] = 25.0 / 36.0 / pi
+        P[..., ITAU] = 5.0 / 12.0 / pi
+        P[..., IVX] = -np.sin(2.0 * pi * Y)
+        P[..., IVY] = np.sin(2.0 * pi * X)
+        P[..., IBX] = -np.sin(2.0 * pi * Y) / math.sqrt(4.0 * pi)
+        P[..., IBY] = np.sin(4.0 * pi * X) / math.sqrt(4.0 * pi)
+    elif test_model == 16:
+        d = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+        P[..., ITAU] = np.where(d <= 0.1, 10.0, 0.1)
+        P[..., IRHO] = 1.0
+        P[..., IBX] = 1.0 / math.sqrt(2)
+        P[..., IBY] = 1.0 / math.sqrt(2)
+    elif test_model == 17:
+        outer = (Y > 0.75) | (Y < 0.25)
+        d = rng.random(X.shape + (2,))                  # two draws per cell, in loop order
+        P[..., IRHO] = np.where(outer, 1.0, 2.0)
+        P[..., IVX] = np.where(outer, 0.5 + 0.01 * d[..., 0], -0.5 + 0.01 * d[..., 0])
+        P[..., ITAU] = 2.5
+        P[..., IVY] = 0.01 * d[..., 1]
+        P[..., IBX] = 0.2
+    elif test_model == 18:
+        P[..., IRHO] = np.where(Y <= 0.5, 1.0, 2.0)
+        P[..., ITAU] = 2.5 - 0.1 * P[..., IRHO] * (Y - 0.5)
+        d = rng.random(X.shape)
+        P[..., IVY] = 0.01 * d * (1.0 + np.cos(8.0 * pi * (Y - 0.5) / 3.0)) / 2.0
+        P[..., IBX] = 0.0125
+    else:  # 19: face field from the corner vector potential (cells 0..n)
+        P[..., IRHO] = 1.0
+        P[..., ITAU] = 1.0
+        P[..., IVX] = 2.0
+        P[..., IVY] = 1.0
+        XF, YF = np.meshgrid(xF[J], yF[K], indexing="xy")
+        a = np.zeros((ny + 2, nx + 2))                  # corners -1..n, zero at -1
+        a[1:, 1:] = 0.001 * np.maximum(0.0, 0.3 - np.sqrt(XF ** 2 + YF ** 2))
+        P[..., IBX] = (a[1:, 1:] - a[:-1, 1:]) / dy[K][:, None]
+        P[..., IBY] = -(a[1:, 1:] - a[1:, :-1]) / dx[J][None, :]
+    prim[:, K, J, :] = P[None]
+    eps[:, K, J] = (P[..., ITAU] / P[..., IRHO] / (g - 1.0))[None]
+    return spec, prim, eps
+
+
 def batch_problems(n_problems=512, seed=20261203, nmin=128, nmax=4096):
     """Seeded parameters of the batched workload (one 1D Riemann problem each)."""
     rng = np.random.Generator(np.random.PCG64(seed))

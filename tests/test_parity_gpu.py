@@ -107,6 +107,22 @@ def test_spherical_torus_model_bitwise(oracle_mod, grid, recon):
     assert_bitwise(g, o, spec, what=("cons",))
 
 
+@pytest.mark.parametrize("tm,recon,riemann", [(13, "ppm", "hlld"), (14, "weno", "hlld"), (15, "ppm", "hlld"),
+                                              (15, "weno", "hllc"), (16, "ppm", "hlld"), (17, "weno", "hlld"),
+                                              (18, "ppm", "hlld"), (19, "tvdmc", "hll")])
+def test_riemann_model_2d_mhd_problems_bitwise(oracle_mod, tm, recon, riemann):
+    """The riemann model's 2D MHD tests (riemann2d.f90:441-640): current
+    sheet, rotor (outflow), Orszag-Tang, blast, Kelvin-Helmholtz,
+    Rayleigh-Taylor (the model's constant-gravity source, reflecting y) and
+    the advected current loop; ten steps, every bit."""
+    spec, prim, eps = models.riemann_2d(tm, 40, 40 if tm != 19 else 20, recon=recon, riemann=riemann)
+    g, o, dg, do = run_pair(spec, prim, eps, 10, oracle_mod)
+    assert dg == do
+    assert_bitwise(g, o, spec)
+    assert_bitwise(g, o, spec, what=("cons",))
+    assert g["divb"] == o["divb"]
+
+
 def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
     """The headline blast (p 10 : 0.1, beta 0.2 outside) breaks the reference's
     WENO-Z + HLLD within a few steps (negative face pressure, see
