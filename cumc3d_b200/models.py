@@ -92,6 +92,76 @@ def riemann_1d(nx, left, right, bx, gamma=5.0 / 3.0, recon="ppm", riemann="hlld"
 
 
 # ---------------------------------------------------------------------------
+# the riemann model's 1D set: model/riemann/src/riemann1d.f90:28-330
+# ---------------------------------------------------------------------------
+_S4PI = 1.0 / math.sqrt(4.0 * math.pi)
+RIEMANN_1D = {
+    # test_model: (name, gamma, boundary_flag, t_end, left, right); a state
+    # is {var: value}, split at x = 0.5 unless the test says otherwise
+    1: ("toro1", 1.4, (1, 1, 1, 1, 1, 1), 0.25, {IRHO: 1.0, ITAU: 1.0}, {IRHO: 0.125, ITAU: 0.1}),
+    2: ("toro2", 1.4, (1, 1, 1, 1, 1, 1), 0.15, {IVX: -2.0, IRHO: 1.0, ITAU: 0.4}, {IVX: 2.0, IRHO: 1.0, ITAU: 0.4}),
+    3: ("toro3", 1.4, (1, 1, 1, 1, 1, 1), 0.012, {ITAU: 1000.0, IRHO: 1.0}, {ITAU: 0.01, IRHO: 1.0}),
+    4: ("toro4", 1.4, (1, 1, 1, 1, 1, 1), 0.035, {ITAU: 0.01, IRHO: 1.0}, {ITAU: 100.0, IRHO: 1.0}),
+    5: ("toro5", 1.4, (1, 1, 1, 1, 1, 1), 0.035, {IVX: 19.5975, ITAU: 460.894, IRHO: 5.99924},
+        {IVX: -6.19633, ITAU: 46.0950, IRHO: 5.99924}),
+    6: ("interacting_shocks", 1.4, (2, 2, 1, 1, 1, 1), 0.038, None, None),
+    7: ("shu_osher", 1.4, (1, 1, 1, 1, 1, 1), 0.178, None, None),
+    8: ("sedov", 1.4, (2, 1, 1, 1, 1, 1), 0.47, None, None),
+    9: ("dai_woodward", 5.0 / 3.0, (1, 1, 1, 1, 1, 1), 0.15, {IRHO: 1.0, ITAU: 1.0, IBY: 1.0, IBX: 1.0},
+        {IRHO: 0.2, ITAU: 0.1, IBY: 0.0, IBX: 1.0}),
+    10: ("brio_wu", 2.0, (1, 1, 1, 1, 1, 1), 0.1, {IRHO: 1.0, ITAU: 1.0, IBY: 1.0, IBX: 0.75},
+         {IRHO: 0.125, ITAU: 0.1, IBY: -1.0, IBX: 0.75}),
+    11: ("seven_discontinuities", 5.0 / 3.0, (1, 1, 1, 1, 1, 1), 0.2,
+         {IRHO: 1.08, ITAU: 0.95, IVX: 1.2, IVY: 0.01, IVZ: 0.5, IBY: 3.6 * _S4PI, IBX: 2.0 * _S4PI, IBZ: 2.0 * _S4PI},
+         {IRHO: 1.0, ITAU: 1.0, IVX: 0.0, IVY: 0.0, IVZ: 0.0, IBY: 4.0 * _S4PI, IBX: 2.0 * _S4PI, IBZ: 2.0 * _S4PI}),
+    12: ("magnetosonic_rarefactions", 5.0 / 3.0, (1, 1, 1, 1, 1, 1), 0.1,
+         {IVX: -1.0, IRHO: 1.0, ITAU: 1.0, IBY: 1.0}, {IVX: 1.0, IRHO: 1.0, ITAU: 1.0, IBY: 1.0}),
+    13: ("two_fast_shocks", 5.0 / 3.0, (1, 1, 1, 1, 1, 1), 0.03,
+         {IVX: 36.87, IVY: -0.155, IVZ: -0.0386, IRHO: 1.0, ITAU: 1.0, IBX: 4.0 * _S4PI, IBY: 4.0 * _S4PI,
+          IBZ: 1.0 * _S4PI},
+         {IVX: -36.87, IVY: 0.0, IVZ: 0.0, IRHO: 1.0, ITAU: 1.0, IBX: 4.0 * _S4PI, IBY: 4.0 * _S4PI,
+          IBZ: 1.0 * _S4PI}),
+}
+
+
+def riemann_1d_test(test_model, nx=800, recon="ppm", riemann="hlld", cfl=0.8, precision="fp64"):
+    """The riemann model's 1D tests by test_model number (riemann1d.f90:
+    1-5 Toro's tests, 6 two interacting blast waves (reflecting), 7
+    Shu-Osher, 8 Sedov (reflecting inner side, Cartesian: mu = 1), 9 Dai &
+    Woodward, 10 Brio-Wu, 11 seven discontinuities, 12 magnetosonic
+    rarefactions, 13 two fast shocks) on [0, 1].  As the reference: the
+    hydrodynamic tests (1-8) set cells 1..n, the MHD ones (9-13) cells 0..n;
+    the rest stays as INITIAL_UPDATE finds it (prim 0, epsilon undefined)."""
+    name, g, bflag, t_end, left, right = RIEMANN_1D[test_model]
+    spec = _base_spec(nx, 1, 1, 1, bflag, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0), cfl=cfl, recon=recon,
+                      riemann=riemann, precision=precision, model=dict(gamma=g, floor="eps"), t_end=t_end,
+                      name="riemann1d_%s_%d" % (name, nx))
+    prim, eps = _alloc(nx, 1, 1)
+    x = centers(spec["xF"])                       # index j+2
+    j0 = 0 if test_model >= 9 else 1
+    for j in range(j0, nx + 1):
+        c = prim[:, :, j + 2]
+        xj = x[j + 2]
+        if left is not None:
+            for v, val in (left if xj <= 0.5 else right).items():
+                c[..., v] = val
+        elif test_model == 6:
+            c[..., ITAU] = 1.0e3 if xj <= 0.1 else (1.0e2 if xj >= 0.9 else 1.0e-2)
+            c[..., IRHO] = 1.0
+        elif test_model == 7:
+            if xj <= 0.1:
+                c[..., IRHO], c[..., IVX], c[..., ITAU] = 3.857143, 2.629369, 10.3333
+            else:
+                c[..., IRHO], c[..., IVX], c[..., ITAU] = 1.0 + 0.2 * math.sin(5.0e1 * xj), 0.0, 1.0
+        else:  # 8, Sedov: the blast energy in the first four cells
+            mu = 1.0  # coordinate_flag + 1, Cartesian
+            c[..., ITAU] = (3.0 * (g - 1.0) * 1.0) / ((1.0 + mu) * math.pi * x[4 + 2] ** mu) if j <= 4 else 1.0e-5
+            c[..., IRHO] = 1.0
+        eps[:, :, j + 2] = c[..., ITAU] / c[..., IRHO] / (g - 1.0)
+    return spec, prim, eps
+
+
+# ---------------------------------------------------------------------------
 # 2D MHD problems of the riemann model: model/riemann/src/riemann2d.f90:441-640
 # ---------------------------------------------------------------------------
 RIEMANN_2D = {

@@ -107,6 +107,19 @@ def test_spherical_torus_model_bitwise(oracle_mod, grid, recon):
     assert_bitwise(g, o, spec, what=("cons",))
 
 
+@pytest.mark.parametrize("tm", range(1, 14))
+def test_riemann_model_1d_set_to_end_time_bitwise(oracle_mod, tm):
+    """The riemann model's 1D tests (riemann1d.f90: Toro 1-5, interacting
+    blast waves, Shu-Osher, Sedov, Dai-Woodward, Brio-Wu, seven
+    discontinuities, magnetosonic rarefactions, two fast shocks), PPM + HLLD
+    at CFL 0.8, each to its end time in one device time loop."""
+    spec, prim, eps = models.riemann_1d_test(tm, 200)
+    g, o, dg, do = run_pair(spec, prim, eps, 100000, oracle_mod, use_evolve=True, t_end=spec["t_end"])
+    assert dg == do and dg[0][0] == spec["t_end"]
+    assert_bitwise(g, o, spec)
+    assert_bitwise(g, o, spec, what=("cons",))
+
+
 @pytest.mark.parametrize("tm,recon,riemann", [(13, "ppm", "hlld"), (14, "weno", "hlld"), (15, "ppm", "hlld"),
                                               (15, "weno", "hllc"), (16, "ppm", "hlld"), (17, "weno", "hlld"),
                                               (18, "ppm", "hlld"), (19, "tvdmc", "hll")])
