@@ -166,6 +166,18 @@ def riemann_1d_test(test_model, nx=800, recon="ppm", riemann="hlld", cfl=0.8, pr
 # ---------------------------------------------------------------------------
 RIEMANN_2D = {
     # test_model: (name, gamma, boundary_flag, x range, y range, t_end)
+    1: ("gresho", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 3.0),
+    2: ("toro_blast", 1.4, (2, 2, 2, 2, 1, 1), (0.0, 1.0), (0.0, 1.5), 1.0),
+    3: ("toro_explosion", 1.4, (2, 1, 2, 1, 1, 1), (0.0, 1.5), (0.0, 1.5), 2.667),
+    4: ("implosion", 1.4, (2, 2, 2, 2, 1, 1), (0.0, 0.3), (0.0, 0.3), 2.5),
+    5: ("kelvin_helmholtz_hydro", 1.4, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 5.0),
+    6: ("rayleigh_taylor_hydro", 1.4, (0, 0, 2, 2, 1, 1), (0.0, 0.5), (0.0, 1.5), 12.75),
+    7: ("quadrants_3", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.3),
+    8: ("quadrants_4", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.25),
+    9: ("quadrants_6", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.3),
+    10: ("quadrants_12", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.25),
+    11: ("quadrants_15", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.2),
+    12: ("quadrants_17", 1.4, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.3),
     13: ("current_sheet", 5.0 / 3.0, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 10.0),
     14: ("rotor", 5.0 / 3.0, (1, 1, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), 0.295),
     15: ("orszag_tang", 5.0 / 3.0, (0, 0, 0, 0, 1, 1), (0.0, 1.0), (0.0, 1.0), 1.0),
@@ -176,19 +188,36 @@ RIEMANN_2D = {
 }
 
 
+# the four-quadrant problems (tests 7-12): (rho, p, vx, vy) in the quadrants
+# (x < 0.5, y < 0.5), (x > 0.5, y < 0.5), (x < 0.5, y > 0.5), (x > 0.5, y > 0.5)
+_QUADRANTS = {
+    7: ((0.138, 0.0290, 1.2060, 1.2060), (0.5323, 0.3, 0.0, 1.2060), (0.5323, 0.3, 1.2060, 0.0), (1.5, 1.5, 0.0, 0.0)),
+    8: ((1.1, 1.1, 0.8939, 0.8939), (0.5065, 0.35, 0.0, 0.8939), (0.5065, 0.35, 0.8939, 0.0), (1.1, 1.1, 0.0, 0.0)),
+    9: ((1.0, 1.0, -0.75, 0.5), (3.0, 1.0, -0.75, -0.5), (2.0, 1.0, 0.75, 0.5), (1.0, 1.0, 0.75, -0.5)),
+    10: ((0.8, 1.0, 0.0, 0.0), (1.0, 1.0, 0.0, 0.7276), (1.0, 1.0, 0.7276, 0.5), (0.5313, 0.4, 0.0, 0.0)),
+    11: ((0.8, 0.4, 0.1, -0.3), (0.5313, 0.4, 0.1, 0.4276), (0.5197, 0.4, -0.6259, -0.3), (1.0, 1.0, 0.1, -0.3)),
+    12: ((1.0625, 0.4, 0.0, 0.2145), (0.5197, 0.4, 0.0, -1.1259), (2.0, 1.0, 0.0, -0.3), (1.0, 1.0, 0.0, -0.4)),
+}
+
+
 def riemann_2d(test_model, nx=128, ny=None, recon="ppm", riemann="hlld", cfl=0.4, precision="fp64", seed=20261203):
-    """The MHD tests of the riemann model's 2D set, by its test_model number
-    (riemann2d.f90:441-640): 13 current sheet, 14 rotor, 15 Orszag-Tang
-    vortex, 16 blast, 17 Kelvin-Helmholtz, 18 Rayleigh-Taylor (with the
-    model's constant gravity g = 0.1 in -y, custom.f90:132-159), 19 advected
-    current loop.  Boundaries, gamma and end times as the file states them;
-    the cells 0..n are set, face fields from the cell-centre formulas as the
-    reference writes them, the loop's from a corner vector potential.  The
-    seeded uniform numbers stand in for RANDOM_NUMBER (17, 18)."""
+    """The riemann model's 2D set by its test_model number (riemann2d.f90):
+    hydrodynamics -- 1 Gresho vortex, 2 Toro's blast, 3 Toro's explosion
+    (Cartesian), 4 implosion, 5 Kelvin-Helmholtz, 6 Rayleigh-Taylor, 7-12
+    the four-quadrant Riemann problems (configurations 3, 4, 6, 12, 15, 17);
+    MHD (riemann2d.f90:441-640) -- 13 current sheet, 14 rotor, 15
+    Orszag-Tang vortex, 16 blast, 17 Kelvin-Helmholtz, 18 Rayleigh-Taylor, 19
+    advected current loop.  Both Rayleigh-Taylor tests feel the model's
+    constant gravity g = 0.1 in -y (custom.f90:132-159).  Boundaries, boxes,
+    gamma and end times as the file states them; as the reference, the
+    hydrodynamic tests set cells 1..n and the MHD ones 0..n, face fields from
+    the cell-centre formulas as the reference writes them, the loop's from a
+    corner vector potential.  The seeded uniform numbers stand in for
+    RANDOM_NUMBER (5, 17, 18)."""
     name, g, bflag, xr, yr, t_end = RIEMANN_2D[test_model]
     ny = ny or nx
     model = dict(gamma=g, floor="eps")
-    if test_model == 18:
+    if test_model in (6, 18):
         model.update(source="const_gy", g_const=0.1)
     spec = _base_spec(nx, ny, 1, 2, bflag, xr, yr, (0.0, 1.0), cfl=cfl, recon=recon, riemann=riemann,
                       precision=precision, model=model, t_end=t_end, name="riemann2d_%s_%dx%d" % (name, nx, ny))
@@ -196,12 +225,52 @@ def riemann_2d(test_model, nx=128, ny=None, recon="ppm", riemann="hlld", cfl=0.4
     x, y = centers(spec["xF"]), centers(spec["yF"])
     xF, yF = spec["xF"][1:], spec["yF"][1:]           # xF(j) at index j+2
     dx, dy = spec["xF"][1:] - spec["xF"][:-1], spec["yF"][1:] - spec["yF"][:-1]
-    J, K = slice(2, nx + 3), slice(2, ny + 3)          # cells 0..n
-    X, Y = np.meshgrid(x[J], y[K], indexing="xy")      # (ny+1, nx+1): [k, j]
+    lo = 2 if test_model >= 13 else 3                   # first cell set: 0 (MHD) or 1
+    J, K = slice(lo, nx + 3), slice(lo, ny + 3)
+    X, Y = np.meshgrid(x[J], y[K], indexing="xy")      # [k, j]
     P = np.zeros(X.shape + (8,))
     rng = np.random.Generator(np.random.PCG64(seed))
     pi = math.pi
-    if test_model == 13:
+    if test_model == 1:
+        d = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+        ds = np.where(d > 0.0, d, 1.0)
+        inner, ring = d <= 0.2, (d > 0.2) & (d <= 0.4)
+        P[..., ITAU] = np.where(inner, 5.0 + 12.5 * d ** 2,
+                                np.where(ring, 9.0 - 4.0 * math.log(0.2) + 12.5 * d ** 2 - 20.0 * d
+                                         + 4.0 * np.log(np.where(ring, d, 1.0)), 3.0 + 4.0 * math.log(2.0)))
+        P[..., IVX] = np.where(inner, -5.0 * (Y - 0.5), np.where(ring, -(2.0 - 5.0 * d) * (Y - 0.5) / ds, 0.0))
+        P[..., IVY] = np.where(inner, 5.0 * (X - 0.5), np.where(ring, (2.0 - 5.0 * d) * (X - 0.5) / ds, 0.0))
+        P[..., IRHO] = 1.0
+    elif test_model == 2:
+        d = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+        P[..., ITAU] = np.where(d <= 0.1, 10.0, 1.0)
+        P[..., IRHO] = 1.0
+    elif test_model == 3:
+        inside = np.sqrt(X ** 2 + Y ** 2) < 0.4
+        P[..., IRHO] = np.where(inside, 1.0, 0.125)
+        P[..., ITAU] = np.where(inside, 1.0, 0.1)
+    elif test_model == 4:
+        outer = X + Y > 0.15
+        P[..., IRHO] = np.where(outer, 1.0, 0.125)
+        P[..., ITAU] = np.where(outer, 1.0, 0.14)
+    elif test_model == 5:
+        outer = (Y > 0.75) | (Y < 0.25)
+        d = rng.random(X.shape + (2,))                  # two draws per cell, in loop order
+        P[..., IRHO] = np.where(outer, 1.0, 2.0)
+        P[..., IVX] = np.where(outer, -0.5 + 0.01 * (d[..., 0] - 0.5), 0.5 + 0.01 * (d[..., 0] - 0.5))
+        P[..., IVY] = 0.01 * (d[..., 1] - 0.5)
+        P[..., ITAU] = 2.5
+    elif test_model == 6:
+        P[..., IRHO] = np.where(Y < 0.75, 1.0, 2.0)
+        P[..., ITAU] = 2.5 - 0.1 * P[..., IRHO] * Y
+        P[..., IVY] = 0.025 * (1.0 + np.cos(4.0 * pi * (X - 0.25))) * (1.0 + np.cos(3.0 * pi * (Y - 0.75)))
+    elif test_model <= 12:
+        xl, xh = (X > 0.0) & (X < 0.5), (X > 0.5) & (X < 1.0)
+        yl, yh = (Y > 0.0) & (Y < 0.5), (Y > 0.5) & (Y < 1.0)
+        for q, m in zip(_QUADRANTS[test_model], (xl & yl, xh & yl, xl & yh, xh & yh)):
+            for v, val in zip((IRHO, ITAU, IVX, IVY), q):
+                P[..., v] = np.where(m, val, P[..., v])
+    elif test_model == 13:
         P[..., IBY] = np.where((X <= 0.25) | (X >= 0.75), 1.0, -1.0) / math.sqrt(4.0 * pi)
         P[..., IRHO] = 1.0
         P[..., ITAU] = 0.1 * 0.5
@@ -255,7 +324,41 @@ def riemann_2d(test_model, nx=128, ny=None, recon="ppm", riemann="hlld", cfl=0.4
         P[..., IBX] = (a[1:, 1:] - a[:-1, 1:]) / dy[K][:, None]
         P[..., IBY] = -(a[1:, 1:] - a[1:, :-1]) / dx[J][None, :]
     prim[:, K, J, :] = P[None]
-    eps[:, K, J] = (P[..., ITAU] / P[..., IRHO] / (g - 1.0))[None]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        eps[:, K, J] = (P[..., ITAU] / P[..., IRHO] / (g - 1.0))[None]
+    return spec, prim, eps
+
+
+def riemann_3d(test_model, n=64, recon="ppm", riemann="hlld", cfl=0.4, precision="fp64"):
+    """The riemann model's 3D set (model/riemann/src/riemann3d.f90): 1 the
+    spherical explosion in the unit cube (rho, p = 1 inside r < 0.4 of the
+    origin corner, 0.125, 0.1 outside; gamma 1.4; the boundary flags its
+    comment gives, (1,2,1,2,1,2)), 2 the oblique Sod tube (bands of x+y+z
+    at 0.5, 1, 1.5; gamma 5/3; outflow).  Cells 1..n set, as the reference."""
+    if test_model == 1:
+        g, bflag, name = 1.4, (1, 2, 1, 2, 1, 2), "explosion"
+    elif test_model == 2:
+        g, bflag, name = 5.0 / 3.0, (1, 1, 1, 1, 1, 1), "oblique_sod"
+    else:
+        raise ValueError("no such test model")
+    spec = _base_spec(n, n, n, 3, bflag, (0.0, 1.0), (0.0, 1.0), (0.0, 1.0), cfl=cfl, recon=recon,
+                      riemann=riemann, precision=precision, model=dict(gamma=g, floor="eps"),
+                      name="riemann3d_%s_%d" % (name, n))
+    prim, eps = _alloc(n, n, n)
+    c = centers(spec["xF"])[3:n + 3]
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    P = np.zeros(X.shape + (8,))
+    if test_model == 1:
+        inside = np.sqrt(X ** 2 + Y ** 2 + Z ** 2) < 0.4
+        P[..., IRHO] = np.where(inside, 1.0, 0.125)
+        P[..., ITAU] = np.where(inside, 1.0, 0.1)
+    else:
+        s = X + Y + Z
+        band = (s < 0.5) | ((s > 1.0) & (s < 1.5))
+        P[..., IRHO] = np.where(band, 4.0, 1.0)
+        P[..., ITAU] = np.where(band, 1.0, 0.1795)
+    prim[3:n + 3, 3:n + 3, 3:n + 3] = P
+    eps[3:n + 3, 3:n + 3, 3:n + 3] = P[..., ITAU] / P[..., IRHO] / (g - 1.0)
     return spec, prim, eps
 
 

@@ -120,6 +120,27 @@ def test_riemann_model_1d_set_to_end_time_bitwise(oracle_mod, tm):
     assert_bitwise(g, o, spec, what=("cons",))
 
 
+@pytest.mark.parametrize("tm", range(1, 13))
+def test_riemann_model_2d_hydro_problems_bitwise(oracle_mod, tm):
+    """The riemann model's 2D hydrodynamic tests (riemann2d.f90: Gresho,
+    Toro's blast and explosion, implosion, Kelvin-Helmholtz,
+    Rayleigh-Taylor with gravity, the four-quadrant problems); ten steps."""
+    recon, riemann = ("weno", "hllc") if tm % 3 == 0 else ("ppm", "hlld")
+    spec, prim, eps = models.riemann_2d(tm, 40, recon=recon, riemann=riemann)
+    g, o, dg, do = run_pair(spec, prim, eps, 10, oracle_mod)
+    assert dg == do
+    assert_bitwise(g, o, spec)
+    assert_bitwise(g, o, spec, what=("cons",))
+
+
+@pytest.mark.parametrize("tm", [1, 2])
+def test_riemann_model_3d_problems_bitwise(oracle_mod, tm):
+    spec, prim, eps = models.riemann_3d(tm, 20)
+    g, o, dg, do = run_pair(spec, prim, eps, 5, oracle_mod)
+    assert dg == do
+    assert_bitwise(g, o, spec)
+
+
 @pytest.mark.parametrize("tm,recon,riemann", [(13, "ppm", "hlld"), (14, "weno", "hlld"), (15, "ppm", "hlld"),
                                               (15, "weno", "hllc"), (16, "ppm", "hlld"), (17, "weno", "hlld"),
                                               (18, "ppm", "hlld"), (19, "tvdmc", "hll")])

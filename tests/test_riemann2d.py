@@ -69,3 +69,41 @@ def test_divergence_stays_at_roundoff_or_at_the_seam(tm):
         out[fix] = (_div2d(spec, p) * (spec["xF"][4] - spec["xF"][3]) / b)
     assert out[1].max() < 1e-12
     assert out[0][1:, 1:].max() < 1e-12           # away from the first row and column
+
+
+def _run(spec, prim, eps, steps):
+    o = O.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    p0, _ = o.get_state()
+    for _ in range(steps):
+        o.rk3_step(o.finddt())
+    p, _ = o.get_state()
+    o.close()
+    return p0, p
+
+
+def test_gresho_vortex_stays_steady():
+    """Test 1 is a steady rotating equilibrium: pressure gradient against
+    the centrifugal term."""
+    p0, p = _run(*models.riemann_2d(1, 48), 20)
+    a, b = p[3, 3:-3, 3:-3, IVX], p0[3, 3:-3, 3:-3, IVX]
+    assert np.abs(a - b).sum() / np.abs(b).sum() < 0.02
+
+
+def test_quadrant_configuration_4_keeps_its_mirror_symmetry():
+    """Test 8 (configuration 4) is symmetric about the diagonal x = y; the
+    x and y sweeps keep it bit for bit."""
+    _, p = _run(*models.riemann_2d(8, 48), 20)
+    c = p[3, 3:-3, 3:-3]
+    assert np.array_equal(c[..., IRHO], c[..., IRHO].T)
+    assert np.array_equal(c[..., IVX], c[..., IVY].T)
+
+
+def test_oblique_sod_is_symmetric_under_axis_permutations():
+    """riemann3d test 2 depends on x + y + z only; after a few steps the
+    state is invariant under exchanging the axes."""
+    _, p = _run(*models.riemann_3d(2, 16), 4)
+    r = p[3:-3, 3:-3, 3:-3, IRHO]
+    for perm in ((0, 2, 1), (1, 0, 2), (2, 1, 0)):
+        assert np.allclose(r, r.transpose(perm), rtol=1e-12, atol=0)
