@@ -59,6 +59,14 @@ END TYPE
 
 INTEGER(C_INT), PARAMETER :: CUMC_LEARN_NP = 2657
 
+! cumc_train_config (include/cumc3d_gpu.h): Adam training of the flag network
+TYPE, BIND(C) :: cumc_train_config
+  INTEGER(C_INT) :: steps, batch
+  REAL(C_FLOAT) :: lr, delta
+  REAL(C_FLOAT) :: beta1, beta2, eps
+  INTEGER(C_LONG_LONG) :: seed
+END TYPE
+
 INTERFACE
   INTEGER(C_INT) FUNCTION cumc_create(cfg, h) BIND(C, NAME='cumc_create')
     IMPORT :: C_INT, C_PTR, cumc_config
@@ -256,6 +264,132 @@ INTERFACE
     IMPORT :: C_INT, C_PTR, C_DOUBLE
     TYPE(C_PTR), VALUE :: h
     REAL(C_DOUBLE), INTENT(OUT) :: m_bh, r_sh
+  END FUNCTION
+  ! arrays, synchronisation, stream, counters
+  INTEGER(C_INT) FUNCTION cumc_get_array(h, which, out, n_doubles) BIND(C, NAME='cumc_get_array')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE, C_SIZE_T
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: which
+    REAL(C_DOUBLE), INTENT(OUT) :: out(*)
+    INTEGER(C_SIZE_T), VALUE :: n_doubles
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_sync(h) BIND(C, NAME='cumc_sync')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  INTEGER(C_INT64_T) FUNCTION cumc_launch_count(h) BIND(C, NAME='cumc_launch_count')
+    IMPORT :: C_INT64_T, C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  TYPE(C_PTR) FUNCTION cumc_stream(h) BIND(C, NAME='cumc_stream')
+    IMPORT :: C_PTR
+    TYPE(C_PTR), VALUE :: h
+  END FUNCTION
+  ! diagnostics, autotuner, numerics self-checks
+  INTEGER(C_INT) FUNCTION cumc_profile_step(h, nsteps, ms_out, n_out) BIND(C, NAME='cumc_profile_step')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: nsteps, n_out
+    REAL(C_DOUBLE), INTENT(OUT) :: ms_out(*)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_autotune(h, choice_out, best_ms_out) BIND(C, NAME='cumc_autotune')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), INTENT(OUT) :: choice_out(5)
+    REAL(C_DOUBLE), INTENT(OUT) :: best_ms_out
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_set_tuning(h, choice) BIND(C, NAME='cumc_set_tuning')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), INTENT(IN) :: choice(5)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_check_div3(seed, n, mismatches, example) BIND(C, NAME='cumc_check_div3')
+    IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
+    INTEGER(C_LONG_LONG), VALUE :: seed, n
+    INTEGER(C_LONG_LONG), INTENT(OUT) :: mismatches
+    REAL(C_DOUBLE), INTENT(OUT) :: example
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_fp64_peak(tflops) BIND(C, NAME='cumc_fp64_peak')
+    IMPORT :: C_INT, C_DOUBLE
+    REAL(C_DOUBLE), INTENT(OUT) :: tflops
+  END FUNCTION
+  ! batched 1D problems: synchronisation, stream, counter
+  INTEGER(C_INT) FUNCTION cumc_batch_sync(b) BIND(C, NAME='cumc_batch_sync')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: b
+  END FUNCTION
+  TYPE(C_PTR) FUNCTION cumc_batch_last_error(b) BIND(C, NAME='cumc_batch_last_error')
+    IMPORT :: C_PTR
+    TYPE(C_PTR), VALUE :: b
+  END FUNCTION
+  TYPE(C_PTR) FUNCTION cumc_batch_stream(b) BIND(C, NAME='cumc_batch_stream')
+    IMPORT :: C_PTR
+    TYPE(C_PTR), VALUE :: b
+  END FUNCTION
+  INTEGER(C_INT64_T) FUNCTION cumc_batch_launch_count(b) BIND(C, NAME='cumc_batch_launch_count')
+    IMPORT :: C_INT64_T, C_PTR
+    TYPE(C_PTR), VALUE :: b
+  END FUNCTION
+  ! one 1D problem with no device allocation (hosts that own all device
+  ! memory, e.g. an OpenACC code whose arrays are mapped once); err holds
+  ! the message of a failed call
+  INTEGER(C_INT) FUNCTION cumc_batch_run1_noalloc(cfg, prim, eps, max_steps, stream, prim_row, eps_row, &
+      t_out, steps_out, status_out, err, err_len) BIND(C, NAME='cumc_batch_run1_noalloc')
+    IMPORT :: C_INT, C_PTR, C_DOUBLE, C_CHAR, C_SIZE_T, cumc_batch_config
+    TYPE(cumc_batch_config), INTENT(IN) :: cfg
+    REAL(C_DOUBLE), INTENT(IN) :: prim(*), eps(*)
+    INTEGER(C_INT), VALUE :: max_steps
+    TYPE(C_PTR), VALUE :: stream
+    REAL(C_DOUBLE), INTENT(OUT) :: prim_row(*), eps_row(*)
+    REAL(C_DOUBLE), INTENT(OUT) :: t_out
+    INTEGER(C_INT), INTENT(OUT) :: steps_out, status_out
+    CHARACTER(KIND=C_CHAR), INTENT(OUT) :: err(*)
+    INTEGER(C_SIZE_T), VALUE :: err_len
+  END FUNCTION
+  ! learned flag: counters, flag maps, sample harvest, network kernels
+  INTEGER(C_INT) FUNCTION cumc_learn_stats(h, out4) BIND(C, NAME='cumc_learn_stats')
+    IMPORT :: C_INT, C_PTR, C_LONG_LONG
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_LONG_LONG), INTENT(OUT) :: out4(4)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_learn_flags(h, dir, flags, warps, tiles, sizes_out) BIND(C, NAME='cumc_learn_flags')
+    IMPORT :: C_INT, C_PTR, C_LONG_LONG
+    TYPE(C_PTR), VALUE :: h, flags, warps, tiles
+    INTEGER(C_INT), VALUE :: dir
+    INTEGER(C_LONG_LONG), INTENT(OUT) :: sizes_out(3)
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_learn_harvest(h, dir, stride, out, cap, rows_out) BIND(C, NAME='cumc_learn_harvest')
+    IMPORT :: C_INT, C_PTR, C_LONG_LONG, C_FLOAT
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: dir
+    INTEGER(C_LONG_LONG), VALUE :: stride, cap
+    REAL(C_FLOAT), INTENT(OUT) :: out(*)
+    INTEGER(C_LONG_LONG), INTENT(OUT) :: rows_out
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_mlp_grad(params, samples, n, delta, grad_out, loss_out) BIND(C, NAME='cumc_mlp_grad')
+    IMPORT :: C_INT, C_LONG_LONG, C_FLOAT
+    REAL(C_FLOAT), INTENT(IN) :: params(*), samples(*)
+    INTEGER(C_LONG_LONG), VALUE :: n
+    REAL(C_FLOAT), VALUE :: delta
+    REAL(C_FLOAT), INTENT(OUT) :: grad_out(*), loss_out
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_mlp_train(samples, n, tc, params_inout, loss_curve) BIND(C, NAME='cumc_mlp_train')
+    IMPORT :: C_INT, C_LONG_LONG, C_FLOAT, C_PTR, cumc_train_config
+    REAL(C_FLOAT), INTENT(IN) :: samples(*)
+    INTEGER(C_LONG_LONG), VALUE :: n
+    TYPE(cumc_train_config), INTENT(IN) :: tc
+    REAL(C_FLOAT), INTENT(INOUT) :: params_inout(*)
+    TYPE(C_PTR), VALUE :: loss_curve      ! REAL(C_FLOAT) per step, or C_NULL_PTR
+  END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_mlp_infer(params, features, ld, n, logits) BIND(C, NAME='cumc_mlp_infer')
+    IMPORT :: C_INT, C_LONG_LONG, C_FLOAT
+    REAL(C_FLOAT), INTENT(IN) :: params(*), features(*)
+    INTEGER(C_INT), VALUE :: ld
+    INTEGER(C_LONG_LONG), VALUE :: n
+    REAL(C_FLOAT), INTENT(OUT) :: logits(*)
+  END FUNCTION
+  TYPE(C_PTR) FUNCTION cumc_mlp_last_error() BIND(C, NAME='cumc_mlp_last_error')
+    IMPORT :: C_PTR
   END FUNCTION
 END INTERFACE
 
