@@ -558,6 +558,101 @@ def torus_cyl(nr=192, nphi=128, nz=192, r_range=(2.0, 42.0), z_range=(-20.0, 20.
     return spec, prim, np.ascontiguousarray(eps)
 
 
+def torus_cyn(nr=128, nphi=128, nz=128, faces=None, r_range=(1.5, 21.5), z_range=(-10.0, 10.0), recon="ppm",
+              riemann="hlld", cfl=0.8, precision="fp64", learned=0, seed=20261203, r_sh=1.0, s_in=3.0, s_max=4.7,
+              q=2.0, gamma=5.0 / 3.0, rho_max=1.0, rho_fac=1e-4, rho_cut=0.5, p_beta=350.0, noise=1e-4):
+    """The reference's own cylindrical torus: GET_MODEL of
+    model/torus-cyn/src/model.f90:6-316 with the values of its param.h
+    (Paczynski-Wiita potential r_sh = 1, q = 2, s_in = 3, s_max = 4.7, gamma =
+    5/3, atmosphere rho_fac rho_max at p = K rho^gamma, rho_cut = 0.5, minimum
+    plasma beta 350, no corona) on the uniform grid of its parameter.h (r in
+    [1.5, 21.5], phi in [0, 2 pi), z in [-10, 10], 128^3, boundaries
+    (1,1,0,0,1,1), PPM + HLLD, CFL 0.8); ``faces`` takes a refined grid
+    (CUSTOM_GRID with refine_grid).  The C5 benchmark torus (`torus_cyl`)
+    is a different, Newtonian setup.
+
+    As the reference: the field's beta normalisation averages only the
+    radial face field to the cell centres (bcell(ibz) is not filled there,
+    model.f90:137-145, and B_phi is zero), and the density is perturbed by
+    a seeded uniform 1e-4 (model.f90:285-294)."""
+    g = gamma
+    spec = _base_spec(nr, nphi, nz, 3, (1, 1, 0, 0, 1, 1), r_range, (0.0, 2.0 * math.pi), z_range,
+                      coordinate_flag=1, cfl=cfl, recon=recon, riemann=riemann, precision=precision,
+                      learned=learned, name="torus_cyn_%dx%dx%d" % (nr, nphi, nz))
+    if faces is not None:
+        for key, f, n in zip(("xF", "yF", "zF"), faces, (nr, nphi, nz)):
+            f = np.asarray(f, dtype=np.float64)
+            if f.shape != (n + 7,):
+                raise ValueError("%s needs %d faces (indices -3..n+3)" % (key, n + 7))
+            spec[key] = f
+    xF, zF = spec["xF"], spec["zF"]
+    x, z = centers(xF), centers(zF)
+    dx, dz = xF[1:] - xF[:-1], zF[1:] - zF[:-1]
+
+    def schwarzschild(r, zz):
+        return -1.0 / (np.sqrt(r ** 2 + zz ** 2) - r_sh)
+
+    lkep2 = s_max ** (2.0 * q - 1.0) / (s_max - r_sh) ** 2
+    c_const = schwarzschild(s_in, 0.0) - lkep2 * s_in ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q)
+    h_max = -schwarzschild(s_max, 0.0) + lkep2 * s_max ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q) + c_const
+    k_poly = h_max * (g - 1.0) / g / rho_max ** (g - 1.0)
+    if k_poly < 0.0:
+        raise ValueError("The polytropic constant is negative")
+    rho_a = rho_fac * rho_max
+    R, Z = np.meshgrid(x, z, indexing="xy")      # (nz+6, nr+6): [l+2, j+2]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        enth = -schwarzschild(R, Z) + lkep2 * R ** (2.0 - 2.0 * q) / (2.0 - 2.0 * q) + c_const
+    enth = np.where(np.isfinite(enth) & (enth > 0.0), enth, 0.0)
+    rho_t = (enth * (g - 1.0) / g / k_poly) ** (1.0 / (g - 1.0))
+    interior = np.zeros(R.shape, dtype=bool)
+    interior[3:3 + nz, 3:3 + nr] = True
+    inside = (rho_t > rho_a) & (R >= s_in) & interior
+    rho2 = np.where(inside, rho_t, rho_a)
+    vphi2 = np.where(inside, np.sqrt(lkep2) * np.where(inside, R, 1.0) ** (-q) * R, 0.0)
+    p2 = k_poly * rho2 ** g
+    eps2 = k_poly * rho2 ** (g - 1.0) / (g - 1.0)
+    a_phi = np.where(interior & (rho2 >= rho_cut), (rho2 - rho_cut) / rho_max, 0.0)
+    xf = xF[1:]                                   # xF(j) at index j+2
+
+    def face_b(a_ph):
+        a_c = np.zeros_like(a_ph)                 # corners j, l = 1..n from cells j..j+1, l..l+1
+        a_c[3:3 + nz, 3:3 + nr] = 0.25 * (a_ph[3:3 + nz, 3:3 + nr] + a_ph[3:3 + nz, 4:4 + nr]
+                                           + a_ph[4:4 + nz, 3:3 + nr] + a_ph[4:4 + nz, 4:4 + nr])
+        bx, bz = np.zeros_like(a_ph), np.zeros_like(a_ph)
+        ll, jj = slice(2, 3 + nz), slice(2, 3 + nr)          # l, j = 0..n
+        lm, jm = slice(1, 2 + nz), slice(1, 2 + nr)
+        bx[ll, jj] = -(a_c[ll, jj] - a_c[lm, jj]) / dz[ll, None]
+        bz[ll, jj] = (xf[None, jj] * a_c[ll, jj] - xf[None, jm] * a_c[ll, jm]) / (x[None, jj] * dx[None, jj])
+        return bx, bz
+
+    bx, bz = face_b(a_phi)
+    li, ji, jim = slice(3, 3 + nz), slice(3, 3 + nr), slice(2, 2 + nr)
+    bxc = np.zeros_like(bx)
+    bxc[li, ji] = (xf[None, ji] * bx[li, ji] + xf[None, jim] * bx[li, jim]) / (xf[None, ji] + xf[None, jim])
+    b2 = bxc ** 2
+    sel = interior & (b2 > 0.0)
+    beta_min = np.min(2.0 * p2[sel] / b2[sel]) if np.any(sel) else 1e30
+    bx, bz = face_b(a_phi * math.sqrt(beta_min / p_beta))
+    prim = np.zeros((nz + 6, nphi + 6, nr + 6, 8), dtype=np.float64)
+    prim[..., IRHO] = rho2[:, None, :]
+    prim[..., IVY] = vphi2[:, None, :]
+    prim[..., ITAU] = p2[:, None, :]
+    prim[..., IBX] = bx[:, None, :]
+    prim[..., IBZ] = bz[:, None, :]
+    eps = np.broadcast_to(eps2[:, None, :], prim.shape[:3]).copy()
+    rho_floor = rho_max * rho_fac
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pert = (rng.random(prim.shape[:3]) - 0.5) / 0.5 * noise
+    above = (prim[..., IRHO] > rho_floor) & interior[:, None, :]
+    above[:, :3, :] = False
+    above[:, 3 + nphi:, :] = False
+    prim[..., IRHO] = np.where(above, prim[..., IRHO] + prim[..., IRHO] * pert, prim[..., IRHO])
+    spec["model"] = dict(gamma=g, floor="torus", rho_floor=rho_floor, eps_floor=k_poly * rho_floor ** (g - 1.0) / (g - 1.0),
+                         p_floor=k_poly * rho_floor ** g, source="pm_cyl", r_sh=r_sh, bc="torus_cyl")
+    spec["t_orbit"] = 2.0 * math.pi / (math.sqrt(lkep2) * s_max ** (-q))
+    return spec, prim, np.ascontiguousarray(eps)
+
+
 def torus_sph(nr=None, ntheta=None, nphi=None, faces=None, r_range=(1.5, 31.5), recon="ppm", riemann="hlld",
               cfl=0.8, precision="fp64", learned=0, seed=20261203, r_sh=1.0, s_in=3.0, s_max=4.7, q=2.0,
               gamma=5.0 / 3.0, rho_max=1.0, rho_fac=1e-4, rho_cut=0.5, p_beta=350.0, noise=1e-4, fixpole=1):

@@ -107,6 +107,16 @@ def test_spherical_torus_model_bitwise(oracle_mod, grid, recon):
     assert_bitwise(g, o, spec, what=("cons",))
 
 
+def test_reference_cylindrical_torus_model_bitwise(oracle_mod):
+    """The reference's own torus-cyn setup (pseudo-Newtonian r_sh = 1,
+    PPM + HLLD at CFL 0.8), from its initial model."""
+    spec, prim, eps = models.torus_cyn(40, 8, 40, r_range=(1.5, 9.5), z_range=(-4.0, 4.0))
+    g, o, dg, do = run_pair(spec, prim, eps, 6, oracle_mod)
+    assert dg == do
+    assert_bitwise(g, o, spec)
+    assert_bitwise(g, o, spec, what=("cons",))
+
+
 @pytest.mark.parametrize("tm", range(1, 14))
 def test_riemann_model_1d_set_to_end_time_bitwise(oracle_mod, tm):
     """The riemann model's 1D tests (riemann1d.f90: Toro 1-5, interacting
