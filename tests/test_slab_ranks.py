@@ -99,3 +99,41 @@ def test_ghost_planes_hold_the_neighbours_cells(tmp_path, world, ring, tags):
                 k = 8 if seam else 9
                 want = g + 0.01 * np.arange(k)[:, None] + 1e-4 * np.arange(NV)[None, :]
                 assert np.array_equal(a[l + 2, :k], want), (r, side, l)
+
+
+def _leaving_rank_main(rank, world, port, out_dir):
+    import datetime
+    import time
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    try:
+        s = FakeSlab(rank, world, False)
+        dist.barrier()                      # one step together
+        if rank == 1:
+            return                          # leaves between steps, nothing in flight
+        sides = [d for d in (0, 1) if s.peers[d] is not None]
+        send = {d: s.pack(engine.FILL_STATE, d) for d in sides}
+        recv = {d: torch.empty_like(send[d]) for d in sides}
+        t0 = time.time()
+        try:
+            for w in dist.batch_isend_irecv(engine.halo_p2p_ops(s.peers, send, recv)):
+                w.wait()
+            outcome = "completed"
+        except RuntimeError:
+            outcome = "error"
+        with open(os.path.join(out_dir, "r0.txt"), "w") as f:
+            f.write("%s %.1f" % (outcome, time.time() - t0))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_a_rank_that_leaves_ends_its_neighbours_exchange_with_an_error(tmp_path):
+    """Failure detection on the host: rank 1 leaves between steps; rank 0's
+    next halo exchange ends with an error (the peer's connection closes, or
+    the process group's 5 s timeout runs out) instead of waiting for good."""
+    mp.start_processes(_leaving_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    outcome, secs = (tmp_path / "r0.txt").read_text().split()
+    assert outcome == "error" and float(secs) < 60
