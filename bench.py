@@ -916,6 +916,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--concurrent-sweeps", type=int, default=0,
+                    help="1: each stage's three flux sweeps as concurrent graph branches (same bits)")
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (the engine's autotuner) or split,tpb_recon,tpb_riemann,min_blocks[,recon_tile] "
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
@@ -964,6 +966,9 @@ def main():
         s.set_tuning(bool(sp), tr, tm, mb, rt)
         tuning = dict(split=bool(sp), tpb_recon=tr, tpb_riemann=tm, riemann_min_blocks=mb, recon_tile=rt,
                       pinned=True)
+    if args.concurrent_sweeps:
+        s.set_concurrent_sweeps(True)
+    tuning["concurrent_sweeps"] = bool(args.concurrent_sweeps)
     s.evolve(1e30, args.warmup)
     s.sync()
     stream = torch.cuda.ExternalStream(s.stream())
@@ -1070,6 +1075,8 @@ def main():
         else:
             s2.set_tuning(tuning["split"], tuning["tpb_recon"], tuning["tpb_riemann"], tuning["riemann_min_blocks"],
                           tuning["recon_tile"])
+        if args.concurrent_sweeps:
+            s2.set_concurrent_sweeps(True)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()

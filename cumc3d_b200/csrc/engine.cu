@@ -903,6 +903,13 @@ struct cumc_handle {
     // flux tiles (autotuned or default): block dims per direction
     dim3 fblk[3];
     int flux_mode = 1;  // 0 fused recon+Riemann kernel, 1 split kernels
+    // the three sweeps' face fluxes as concurrent graph branches (each sweep
+    // reads the primitives and writes its own fluxes and face EMFs); sweeps 1
+    // and 2 run on their own streams with their own face-state buffers
+    bool sweeps_concurrent = false;
+    cudaStream_t fstream[2] = {nullptr, nullptr};
+    cudaEvent_t fev[3] = {nullptr, nullptr, nullptr};
+    void *qsets[2][14] = {};   // QL[0..6], QR[0..6] of sweeps 1 and 2
     // captured step graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -1075,18 +1082,26 @@ static void default_flux_blocks(cumc_handle *h) {
     h->fblk[2] = dim3(32, 8, 1);
 }
 
-static void launch_flux(cumc_handle *h, int dir, int stage = 1) {
-    const Dev &d = h->d;
+static void launch_flux(cumc_handle *h, int dir, int stage = 1, cudaStream_t st = nullptr) {
+    if (!st) st = h->stream;
+    Dev dq = h->d;
+    if (st != h->stream && dir > 0) {  // a concurrent sweep: its own face states
+        for (int i = 0; i < 7; ++i) {
+            dq.QL[i] = h->qsets[dir - 1][i];
+            dq.QR[i] = h->qsets[dir - 1][7 + i];
+        }
+    }
+    const Dev &d = dq;
     if (d.learned) {  // WENO with the learned smooth-face flag (split kernels)
-        if (h->cfg.precision == CUMC_FP32) launch_split_learned_fp32(d, dir, h->cfg.riemann, stage, h->stream);
-        else launch_split_learned_fp64(d, dir, h->cfg.riemann, stage, h->stream);
+        if (h->cfg.precision == CUMC_FP32) launch_split_learned_fp32(d, dir, h->cfg.riemann, stage, st);
+        else launch_split_learned_fp64(d, dir, h->cfg.riemann, stage, st);
         // stage 1: network + per-warp decisions + staged reconstruction + Riemann
         h->launches += (stage == 1) ? 4 : 2;
         return;
     }
     if (h->flux_mode == 1) {
-        if (h->cfg.precision == CUMC_FP32) launch_split_fp32(d, dir, h->cfg.recon, h->cfg.riemann, h->stream);
-        else launch_split_fp64(d, dir, h->cfg.recon, h->cfg.riemann, h->stream);
+        if (h->cfg.precision == CUMC_FP32) launch_split_fp32(d, dir, h->cfg.recon, h->cfg.riemann, st);
+        else launch_split_fp64(d, dir, h->cfg.recon, h->cfg.riemann, st);
         h->launches += 2;
         return;
     }
@@ -1100,8 +1115,8 @@ static void launch_flux(cumc_handle *h, int dir, int stage = 1) {
     // face states of the tile + its staged stencils (2-cell halo along the sweep)
     const size_t staged = 7 * (size_t)(dir == 0 ? (b.x + 4) * b.y : b.x * (b.y + 4));
     const size_t smem = (2 * 7 * (size_t)b.x * b.y + staged) * (f32 ? sizeof(float) : sizeof(double));
-    if (f32) launch_flux_fp32(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, h->stream);
-    else launch_flux_fp64(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, h->stream);
+    if (f32) launch_flux_fp32(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, st);
+    else launch_flux_fp64(d, dir, h->cfg.recon, h->cfg.riemann, g, b, smem, st);
     h->launches++;
 }
 
@@ -1201,10 +1216,22 @@ static void enqueue_stage(cumc_handle *h, int stage) {
 }
 static void enqueue_stage_a(cumc_handle *h, int stage) {
     const Dev &d = h->d;
-    for (int dir = 0; dir < d.n_dim; ++dir) {
-        prof_begin(h);
-        launch_flux(h, dir, stage);
-        prof_end(h, PC_FLUX_X + dir);
+    if (h->sweeps_concurrent && h->prof_class < 0 && !d.learned && d.n_dim > 1) {
+        // fork: the sweeps after the previous stage's last kernel; join: the
+        // EMFs after all three (events record into a captured graph as edges)
+        cudaEventRecord(h->fev[0], h->stream);
+        for (int dir = 1; dir < d.n_dim; ++dir) cudaStreamWaitEvent(h->fstream[dir - 1], h->fev[0], 0);
+        for (int dir = 0; dir < d.n_dim; ++dir) launch_flux(h, dir, stage, dir == 0 ? h->stream : h->fstream[dir - 1]);
+        for (int dir = 1; dir < d.n_dim; ++dir) {
+            cudaEventRecord(h->fev[dir], h->fstream[dir - 1]);
+            cudaStreamWaitEvent(h->stream, h->fev[dir], 0);
+        }
+    } else {
+        for (int dir = 0; dir < d.n_dim; ++dir) {
+            prof_begin(h);
+            launch_flux(h, dir, stage);
+            prof_end(h, PC_FLUX_X + dir);
+        }
     }
     dim3 g, b;
     prof_begin(h);
@@ -1526,6 +1553,10 @@ int cumc_destroy(cumc_handle *h) {
         cudaStreamSynchronize(h->snap_stream);
         cudaStreamDestroy(h->snap_stream);
     }
+    for (int i = 0; i < 2; ++i)
+        if (h->fstream[i]) cudaStreamDestroy(h->fstream[i]);
+    for (int i = 0; i < 3; ++i)
+        if (h->fev[i]) cudaEventDestroy(h->fev[i]);
     if (h->snap_packed) cudaEventDestroy(h->snap_packed);
     if (h->gev_ready) cudaEventDestroy(h->gev_ready);
     if (h->gev_copied) cudaEventDestroy(h->gev_copied);
@@ -1811,6 +1842,26 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     h->d.tpb_recon = choice[1];
     h->d.tpb_riemann = choice[2];
     h->d.riemann_minb = choice[3];
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return CUMC_OK;
+}
+
+int cumc_set_concurrent_sweeps(cumc_handle *h, int on) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (on && !h->fstream[0]) {
+        const size_t n3 = (size_t)h->d.N3;
+        for (int q = 0; q < 2; ++q)
+            for (int i = 0; i < 14; ++i) {
+                double *p = dalloc(h, n3);
+                if (!p) return fail(h, CUMC_ENOMEM, "out of device memory for the concurrent sweeps' face states");
+                h->qsets[q][i] = p;
+            }
+        for (int i = 0; i < 2; ++i) CK(cudaStreamCreateWithFlags(&h->fstream[i], cudaStreamNonBlocking));
+        for (int i = 0; i < 3; ++i) CK(cudaEventCreateWithFlags(&h->fev[i], cudaEventDisableTiming));
+    }
+    h->sweeps_concurrent = on != 0;
+    // a captured step graph holds the old launch order
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
     return CUMC_OK;

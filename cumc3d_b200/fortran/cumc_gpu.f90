@@ -303,6 +303,11 @@ INTERFACE
     TYPE(C_PTR), VALUE :: h
     INTEGER(C_INT), INTENT(IN) :: choice(5)
   END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_set_concurrent_sweeps(h, on) BIND(C, NAME='cumc_set_concurrent_sweeps')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: on
+  END FUNCTION
   INTEGER(C_INT) FUNCTION cumc_check_div3(seed, n, mismatches, example) BIND(C, NAME='cumc_check_div3')
     IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
     INTEGER(C_LONG_LONG), VALUE :: seed, n

@@ -209,6 +209,13 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out);
 /* Set the launch shape by hand, same five integers as choice_out above. */
 int cumc_set_tuning(cumc_handle *h, const int *choice);
 
+/* on = 1: each stage's three face-flux sweeps (reconstruction + Riemann
+ * per direction) run as concurrent branches -- sweeps y and z on streams of
+ * their own with their own face-state buffers (14 more arrays of the padded
+ * grid each), joined before the EMFs; results are bit-identical either way.
+ * Not used with the learned flag or while cumc_profile_step records. */
+int cumc_set_concurrent_sweeps(cumc_handle *h, int on);
+
 /* Numerics self-check (no counterpart in the reference): compares the FP64
  * engine's FMA-corrected division by 3 with the IEEE quotient on n generated
  * normal inputs; *mismatches counts differing bit patterns. */

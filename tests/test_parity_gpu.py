@@ -212,3 +212,40 @@ def test_every_launch_shape_is_bitwise_identical(oracle_mod, tuning, recon):
     po, eo = o.get_state()
     assert np.array_equal(interior(pg, spec), interior(po, spec))
     assert np.array_equal(interior(eg, spec), interior(eo, spec))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_concurrent_sweeps_are_bitwise_identical(oracle_mod, precision):
+    """The three flux sweeps as concurrent branches (their own streams and
+    face-state buffers, joined before the EMFs): the same bits as the
+    sequential sweeps, eager and in the captured step graph; FP64 also
+    against the oracle."""
+    from cumc3d_b200.engine import Solver
+    spec, prim, eps = models.blast_3d(24, recon="weno", riemann="hlld", radius=0.25, p_in=1.0, precision=precision)
+    runs = []
+    for conc, graph in ((False, False), (True, False), (True, True)):
+        g = Solver(spec)
+        g.set_state(prim, eps)
+        g.initial_update()
+        g.set_tuning(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=1)
+        g.set_concurrent_sweeps(conc)
+        if graph:
+            g.evolve(1e30, 4)
+        else:
+            for _ in range(4):
+                g.rungekutta(g.finddt())
+        p, e = g.get_state()
+        runs.append((interior(p, spec), interior(e, spec)))
+        g.close()
+    for p, e in runs[1:]:
+        assert np.array_equal(p.view(np.uint64), runs[0][0].view(np.uint64))
+        assert np.array_equal(e.view(np.uint64), runs[0][1].view(np.uint64))
+    if precision == "fp64":
+        o = oracle_mod.Oracle(spec)
+        o.set_state(prim, eps)
+        o.initial_update()
+        for _ in range(4):
+            o.rk3_step(o.finddt())
+        po, eo = o.get_state()
+        o.close()
+        assert np.array_equal(runs[2][0].view(np.uint64), interior(po, spec).view(np.uint64))
