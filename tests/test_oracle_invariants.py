@@ -166,3 +166,32 @@ def test_brio_wu_structure(oracle_mod):
     assert 0.6 < rho[(x > 0.5) & (x < 0.54)].mean() < 0.75  # post compound-wave plateau
     assert by.min() > -1.05 and by.max() < 1.05  # small PPM overshoot at the fast rarefaction
     assert o.max_divb() >= 0.0
+
+
+def _alfven_error(oracle_mod, n, recon):
+    """Relative L1 of B_y after one period of the 3D CP Alfven wave, whose
+    exact solution then equals the initial state."""
+    from cumc3d_b200 import capi
+    spec, prim, eps = models.alfven_3d(n, recon=recon)
+    o = oracle_mod.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    c0 = o.get_array(capi.ARR_CONS)
+    t, _ = o.evolve(spec["t_end"], 100000)
+    c = o.get_array(capi.ARR_CONS)
+    o.close()
+    assert t == spec["t_end"]
+    sl = (slice(3, n + 3),) * 3
+    a, b = c[sl][..., 6], c0[sl][..., 6]
+    return np.abs(a - b).sum() / np.abs(b).sum()
+
+
+@pytest.mark.parametrize("recon", ["weno", "tvdmc"])
+def test_alfven_wave_converges_at_second_order(oracle_mod, recon):
+    """Known answer for smooth MHD: after one period the wave is back where
+    it started, and the error falls at least at second order (the
+    dimension-by-dimension flux and the CT average bound the order)."""
+    e = [_alfven_error(oracle_mod, n, recon) for n in (8, 16, 32)]
+    orders = np.log2(np.array(e[:-1]) / np.array(e[1:]))
+    assert np.all(orders > 1.8), (e, orders)
+    assert e[-1] < 3e-3
