@@ -12,7 +12,10 @@
  * therefore follows the Fortran routine by routine, loop by loop, in the same
  * floating-point operation order (Fortran left-to-right evaluation, x**2 as
  * x*x), and is checked by invariants instead of reference outputs
- * (tests/test_oracle_invariants.py).
+ * (tests/test_oracle_invariants.py) and by known answers: the exact
+ * ideal-gas Riemann solution on the riemann model's Toro tubes
+ * (tests/test_riemann1d.py) and the CP Alfven wave, exact after one period,
+ * converging at second order.
  *
  * Layout mirrors the reference: prim(imin:imax,-2:nx+3,-2:ny+3,-2:nz+3) with
  * the variable index fastest.  All arrays start as NaN so that any read of a

@@ -5,7 +5,9 @@ CPU-baseline / reference legs of bench.py, never by the product package.
 
 PARITY UNPINNED: the reference is Fortran and cannot be built here (no
 Fortran compiler); it ships no golden vectors.  The oracle is a line-by-line
-restatement checked by invariants (tests/test_oracle_invariants.py).
+restatement checked by invariants (tests/test_oracle_invariants.py) and by
+known answers (the exact Riemann solution on the Toro tubes,
+tests/test_riemann1d.py; the CP Alfven wave after one period).
 """
 import ctypes as C
 import os
