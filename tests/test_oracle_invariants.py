@@ -195,3 +195,28 @@ def test_alfven_wave_converges_at_second_order(oracle_mod, recon):
     orders = np.log2(np.array(e[:-1]) / np.array(e[1:]))
     assert np.all(orders > 1.8), (e, orders)
     assert e[-1] < 3e-3
+
+
+@pytest.mark.parametrize("riemann", ["hlld", "hllc", "hll", "lf"])
+def test_stationary_contact_is_exact_for_the_contact_resolving_solvers(oracle_mod, riemann):
+    """An isolated stationary contact (density jump at equal pressure, at
+    rest, normal field only) is a fixed point of HLLD and HLLC -- their
+    middle wave sits on it with zero mass flux (Miyoshi & Kusano 2005) --
+    bit for bit; HLL and LF smear it."""
+    left = dict(rho=1.0, p=1.0, vx=0.0, vy=0.0, vz=0.0, by=0.0, bz=0.0)
+    right = dict(rho=0.3, p=1.0, vx=0.0, vy=0.0, vz=0.0, by=0.0, bz=0.0)
+    for recon in ("ppm", "weno", "tvdmc"):
+        spec, prim, eps = models.riemann_1d(100, left, right, 0.8, recon=recon, riemann=riemann)
+        o = oracle_mod.Oracle(spec)
+        o.set_state(prim, eps)
+        o.initial_update()
+        p0, _ = o.get_state()
+        for _ in range(30):
+            o.rk3_step(o.finddt())
+        p, _ = o.get_state()
+        o.close()
+        d = np.abs(p[3, 3, 3:-3, 0] - p0[3, 3, 3:-3, 0]).max()
+        if riemann in ("hlld", "hllc"):
+            assert d == 0.0, (recon, d)
+        else:
+            assert d > 0.05, (recon, d)
