@@ -83,3 +83,41 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(engine.CumcError) as e:
         engine.Solver(spec)
     assert e.value.code == capi.CUMC_ECUDA
+
+
+def test_header_is_strict_c99_and_links_every_function():
+    """A C host: the header compiles as ISO C99 with every warning an error,
+    and a program that takes the address of every declared function links
+    against the engine library (nothing is run: no device is needed)."""
+    import tempfile
+    funcs = declared_functions()
+    body = "\n".join("    (void)&%s;" % f for f in funcs)
+    src = '#include "cumc3d_gpu.h"\nint main(void) {\n%s\n    return 0;\n}\n' % body
+    lib = engine.LIB_PATH
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "all.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "all")
+        r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                            os.path.join(ROOT, "include"), c, lib, "-Wl,--allow-shlib-undefined", "-o", exe],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    assert len(funcs) > 50
+
+
+def test_train_config_layout_matches_header():
+    import tempfile
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "cumc3d_gpu.h"
+int main(void){printf("%zu %zu %zu\n", sizeof(cumc_train_config), offsetof(cumc_train_config, lr),
+ offsetof(cumc_train_config, seed));return 0;}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        vals = list(map(int, subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()))
+    assert vals == [C.sizeof(capi.CumcTrainConfig), capi.CumcTrainConfig.lr.offset, capi.CumcTrainConfig.seed.offset]
