@@ -28,6 +28,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/cumc3d_gpu.h"
 #include "engine.cuh"
 #include "learned.cuh"
@@ -890,6 +892,13 @@ __global__ void k_dfma_probe(double *out, int iters) {
 // ===========================================================================
 using namespace cumc;
 
+// NVTX range over the host code that enqueues one part of the update (a
+// profiler's timeline shows the solver's structure; free without a tool)
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
+
 struct cumc_handle {
     cumc_config cfg;
     Dev d;
@@ -1215,6 +1224,7 @@ static void enqueue_stage(cumc_handle *h, int stage) {
     enqueue_stage_b(h, stage);
 }
 static void enqueue_stage_a(cumc_handle *h, int stage) {
+    Range r("cumc stage: face fluxes + cell EMFs");
     const Dev &d = h->d;
     if (h->sweeps_concurrent && h->prof_class < 0 && !d.learned && d.n_dim > 1) {
         // fork: the sweeps after the previous stage's last kernel; join: the
@@ -1242,6 +1252,7 @@ static void enqueue_stage_a(cumc_handle *h, int stage) {
     prof_end(h, PC_EMF);
 }
 static void enqueue_stage_b(cumc_handle *h, int stage) {
+    Range r("cumc stage: edge EMFs + update + recovery + ghosts");
     const Dev &d = h->d;
     dim3 g, b;
     prof_begin(h);
@@ -1641,6 +1652,7 @@ static void enqueue_initial(cumc_handle *h) {
 }
 
 int cumc_initial_update(cumc_handle *h) {
+    Range r("cumc INITIAL_UPDATE");
     if (!h) return fail(h, CUMC_EINVAL, "null handle");
     if (!h->have_state) return fail(h, CUMC_ENOTREADY, "set_state first");
     enqueue_initial(h);
@@ -1652,6 +1664,7 @@ int cumc_initial_update(cumc_handle *h) {
 }
 
 int cumc_finddt(cumc_handle *h, double *dt) {
+    Range r("cumc FINDDT");
     if (!h || !dt) return fail(h, CUMC_EINVAL, "null argument");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
     enqueue_finddt(h, 0);
@@ -1663,6 +1676,7 @@ int cumc_finddt(cumc_handle *h, double *dt) {
 }
 
 int cumc_rk3_step(cumc_handle *h, double dt) {
+    Range r("cumc RUNGEKUTTA");
     if (!h) return fail(h, CUMC_EINVAL, "null handle");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(h, CUMC_EINVAL, "dt must be positive and finite");
@@ -1675,6 +1689,7 @@ int cumc_rk3_step(cumc_handle *h, double dt) {
 }
 
 int cumc_evolve(cumc_handle *h, double t_end, int max_steps, double *t_inout, int *steps_out) {
+    Range r("cumc evolve");
     if (!h || !t_inout) return fail(h, CUMC_EINVAL, "null argument");
     if (!h->initialised) return fail(h, CUMC_ENOTREADY, "initial_update first");
     if (steps_out) *steps_out = 0;
@@ -2000,6 +2015,7 @@ int cumc_poisson_setup(cumc_handle *h, double rho_atm, double omega) {
 
 int cumc_poisson_solve(cumc_handle *h, int max_iter, double tol, int *iters_out, double *err_out,
                        int *converged_out) {
+    Range r("cumc Poisson solve");
     if (!h) return fail(h, CUMC_EINVAL, "null handle");
     if (!h->sor_ready) return fail(h, CUMC_ENOTREADY, "cumc_poisson_setup first");
     if (max_iter < 1 || !(tol >= 0.0)) return fail(h, CUMC_EINVAL, "bad iteration limit or tolerance");
@@ -2363,6 +2379,7 @@ int cumc_slab_step_end(cumc_handle *h) {
 }
 
 int cumc_snapshot_start(cumc_handle *h, double *primitive, double *epsilon, double *bfield) {
+    Range r("cumc snapshot");
     if (!h || !primitive || !epsilon || !bfield) return fail(h, CUMC_EINVAL, "null argument");
     if (!h->have_state) return fail(h, CUMC_ENOTREADY, "no state: cumc_set_state first");
     const Dev &d = h->d;
