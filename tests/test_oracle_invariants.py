@@ -220,3 +220,39 @@ def test_stationary_contact_is_exact_for_the_contact_resolving_solvers(oracle_mo
             assert d == 0.0, (recon, d)
         else:
             assert d > 0.05, (recon, d)
+
+
+def _entropy_wave_error(oracle_mod, n, recon):
+    """Mean |rho - rho_exact| after one period of a density wave carried at
+    v = 1, p = 1 through a periodic 1D tube (exact: the initial state)."""
+    import math
+    from cumc3d_b200.capi import IRHO, ITAU, IVX
+    spec = models._base_spec(n, 1, 1, 1, (0, 0, 1, 1, 1, 1), (0.0, 1.0), (0.0, 1.0), (0.0, 1.0), cfl=0.4,
+                             recon=recon, riemann="hlld", precision="fp64", model=dict(gamma=1.4, floor="eps"),
+                             name="entropy_wave_%d" % n)
+    prim, eps = models._alloc(n, 1, 1)
+    x = models.centers(spec["xF"])
+    prim[..., IRHO] = (1.0 + 0.2 * np.sin(2.0 * math.pi * x))[None, None, :]
+    prim[..., IVX] = 1.0
+    prim[..., ITAU] = 1.0
+    eps[...] = prim[..., ITAU] / prim[..., IRHO] / 0.4
+    o = oracle_mod.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    p0, _ = o.get_state()
+    t, _ = o.evolve(1.0, 1000000)
+    p, _ = o.get_state()
+    o.close()
+    assert t == 1.0
+    return np.abs(p[3, 3, 3:-3, IRHO] - p0[3, 3, 3:-3, IRHO]).mean()
+
+
+@pytest.mark.parametrize("recon,order", [("weno", 3.3), ("ppm", 1.8), ("tvdmc", 1.6), ("tvdvl", 1.7),
+                                         ("tvdmm", 1.5)])
+def test_1d_entropy_wave_converges_at_the_scheme_order(oracle_mod, recon, order):
+    """Known answer for a smooth 1D flow: WENO-Z beyond third order at
+    these resolutions (fifth in space, SSP-RK3 in time), PPM second, the TVD
+    limiters between first and second (they clip the smooth extrema)."""
+    e = [_entropy_wave_error(oracle_mod, n, recon) for n in (32, 64, 128)]
+    orders = np.log2(np.array(e[:-1]) / np.array(e[1:]))
+    assert np.all(orders > order), (e, orders)
