@@ -98,6 +98,10 @@ def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+# the keys of a spec's "model" dict (the fields of cumc_model)
+MODEL_KEYS = {"gamma", "floor", "rho_floor", "eps_floor", "p_floor", "source", "g_const", "r_sh", "bc"}
+
+
 def make_config(spec):
     """Build a ``CumcConfig`` from a plain dict (see :mod:`cumc3d_b200.models`).
 
@@ -111,6 +115,9 @@ def make_config(spec):
     if xF.size != nx + 7 or yF.size != ny + 7 or zF.size != nz + 7:
         raise ValueError("face arrays must hold indices -3..n+3")
     m = spec.get("model", {})
+    unknown = sorted(set(m) - MODEL_KEYS)
+    if unknown:
+        raise ValueError("unknown model descriptor keys: %s" % ", ".join(unknown))
     model = CumcModel(
         gamma=float(m.get("gamma", 5.0 / 3.0)),
         floor_kind=FLOOR[m.get("floor", "none")],
