@@ -86,7 +86,7 @@ __device__ __forceinline__ double bmin_block(double v, double *red) {
     return r;
 }
 
-// floors of model/riemann/src/custom.f90:260-284 (eps >= 0)
+// floors of model/riemann/src/custom.f90:103-127 (eps >= 0)
 __device__ __forceinline__ void batch_floor(const BatchDev &b, double &e) {
     if (b.floor_kind == 1) e = dmax(e, 0.0);
 }

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
                     sc[3] = sc[3] - (rho * vx * vz - bx * bz) * G - (rho * vy * vz - by * bz) * G * tf;
                 }
             }
-            if (d.source_kind == 1) {  // model/riemann/src/custom.f90:299-312
+            if (d.source_kind == 1) {  // model/riemann/src/custom.f90:143-155
                 sc[2] = sc[2] - d.g_const * rho;
             } else if (d.source_kind == 2) {  // model/torus-cyn/src/custom.f90:298-314
                 const double diff = rho - d.rho_floor;
@@ -572,7 +572,7 @@ __device__ __forceinline__ void cell_b(const Dev &d, int j, int k, int l, double
 }
 
 __device__ __forceinline__ void apply_floor(const Dev &d, double &rho, double &vx, double &vy, double &vz, double &e) {
-    if (d.floor_kind == 1) {  // model/riemann/src/custom.f90:272-278
+    if (d.floor_kind == 1) {  // model/riemann/src/custom.f90:115-121
         e = dmax(e, 0.0);
     } else if (d.floor_kind == 2) {  // model/torus-cyn/src/custom.f90:253-269
         const double diff = rho - d.rho_floor;
@@ -661,7 +661,8 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
         d.U[6][c] = bfy;
         d.U[7][c] = bfz;
     }
-    // FINDPRESSURE (model/riemann/src/findpressure.f90:88-97, torus floor branch)
+    // FINDPRESSURE (model/riemann/src/findpressure.f90:7-51; the torus floor branch of
+    // model/torus-cyn/src/findpressure.f90:7-58)
     const double g1 = d.gamma - 1.0;
     double p, dpdrho, dpdeps;
     if (d.floor_kind != 2 || rho > d.rho_floor) {

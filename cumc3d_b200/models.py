@@ -9,7 +9,7 @@ Each builder returns ``(spec, prim, eps)``:
 * ``eps``  -- float64 array of shape (nz+6, ny+6, nx+6).
 
 Cells the reference's GET_MODEL leaves unset hold NaN in ``eps`` (its
-``epsilon`` array is never zeroed, solver/mhd/initial.f90:239-240 only zeroes
+``epsilon`` array is never zeroed, solver/mhd/initial.f90:68-70 only zeroes
 ``prim`` and ``cons``), so any read of an undefined value becomes visible.
 """
 import math

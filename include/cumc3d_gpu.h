@@ -61,7 +61,7 @@ extern "C" {
 #define CUMC_FP32 1   /* FP32 reconstruction + Riemann flux, FP64 elsewhere      */
 /* per-stage floors (CUSTOM_CHECKRHO + FINDPRESSURE of the model) */
 #define CUMC_FLOOR_NONE  0
-#define CUMC_FLOOR_EPS   1   /* model/riemann/src/custom.f90:260-284          */
+#define CUMC_FLOOR_EPS   1   /* model/riemann/src/custom.f90:103-127          */
 #define CUMC_FLOOR_TORUS 2   /* model/torus-cyn/src/custom.f90:240-275,
                                 model/torus-cyn/src/findpressure.f90:7-37    */
 #define CUMC_FLOOR_COLLAPSAR 3 /* model/collapsar/src/custom.f90:269-330: the
@@ -70,7 +70,7 @@ extern "C" {
                                 (model/collapsar/src/findpressure.f90)         */
 /* model source terms (CUSTOM_SOURCE) */
 #define CUMC_SRC_NONE     0
-#define CUMC_SRC_CONST_GY 1  /* model/riemann/src/custom.f90:289-316          */
+#define CUMC_SRC_CONST_GY 1  /* model/riemann/src/custom.f90:132-159          */
 #define CUMC_SRC_PM_CYL   2  /* model/torus-cyn/src/custom.f90:280-320        */
 #define CUMC_SRC_PM_SPH   3  /* model/torus-sph/src/custom.f90 (radial form)  */
 #define CUMC_SRC_COLLAPSAR 4 /* model/collapsar/src/custom.f90:340-395: gravity of

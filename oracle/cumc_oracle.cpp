@@ -378,7 +378,7 @@ struct Sim {
     void custom_checkrho() {
         const cumc_model &m = cfg.model;
         if (m.floor_kind == CUMC_FLOOR_EPS) {
-            /* model/riemann/src/custom.f90:260-284 */
+            /* model/riemann/src/custom.f90:103-127 */
 #pragma omp parallel for collapse(2) schedule(static)
             for (int l = 1; l <= nz; ++l)
                 for (int k = 1; k <= ny; ++k)
@@ -415,7 +415,7 @@ struct Sim {
         }
     }
 
-    /* FINDPRESSURE: model/riemann/src/findpressure.f90:76-99 and
+    /* FINDPRESSURE: model/riemann/src/findpressure.f90:7-51 and
      * model/torus-cyn/src/findpressure.f90:7-37 (the floor branch) */
     void findpressure() {
         const cumc_model &m = cfg.model;
@@ -442,7 +442,7 @@ struct Sim {
     void custom_source() {
         const cumc_model &m = cfg.model;
         if (m.source_kind == CUMC_SRC_CONST_GY) {
-            /* model/riemann/src/custom.f90:299-312 */
+            /* model/riemann/src/custom.f90:143-155 */
 #pragma omp parallel for collapse(2) schedule(static)
             for (int l = 1; l <= nz; ++l)
                 for (int k = 1; k <= ny; ++k)
