@@ -33,3 +33,11 @@ def test_engine_reproduces_golden(name):
     out = make_golden.run_case(name, Solver)
     for k in ("prim", "eps", "bcell", "steps"):
         assert np.array_equal(out[k], ref[k]), k
+
+
+@pytest.mark.parametrize("name", sorted(make_golden.ORACLE_CASES))
+def test_oracle_reproduces_golden_models(oracle_mod, name):
+    ref = load(name)
+    out = make_golden.run_case(name, oracle_mod.Oracle)
+    for k in ("prim", "eps", "bcell", "steps"):
+        assert np.array_equal(out[k], ref[k]), k
