@@ -11,14 +11,21 @@ step (FINDDT + 3 stages) over all 256^3 zones; the workload is 200 steps.
   e2e     the same metric through the C-ABI with host buffers: pinned-host
           upload of the Fortran-layout state, INITIAL_UPDATE, the K steps and
           the download of the result, all inside the wall-clock window;
-  roofline the dominant kernel's algorithmic HBM bytes per launch over its
-          CUDA-event duration, against the measured copy bandwidth;
+  roofline the dominant kernel (a flux sweep: reconstruction + Riemann)
+          against the FP64 roofline: max(algorithmic bytes / measured copy
+          bandwidth, exact FP64 operation count / measured DFMA peak) over
+          its CUDA-event duration; the HBM side alongside;
+  parity_sample  the engine and the CPU oracle on the same 256x256x64 slab
+          of the blast for 2 steps, compared bit for bit;
   cpu_baseline  the CPU oracle (a restatement of the reference's Fortran,
-          OpenMP on all host cores) on a bounded slab of the same workload.
+          -march=native, OpenMP on all host cores) on that slab.
 
 `--impl reference` times that CPU oracle alone (the reference itself is
-Fortran and cannot be built on this image).  For N > 1 each rank runs an
-independent replica (weak scaling); time is the max over ranks.
+Fortran and cannot be built on this image) on the same workload, each step a
+256x256x64 slab of it.  For N > 1 (torchrun, or `--gpus N`, which launches
+torchrun itself) the grid is cut into N z slabs, one per rank, with ghost
+planes exchanged over NCCL (strong scaling); `--replicas` runs N independent
+copies instead.  Time is the max over ranks.
 """
 import argparse
 import json
@@ -101,7 +108,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(args):
+    """Rank, world and process group from the torchrun environment.  NCCL
+    (one rank per GPU) unless --dry-run, which uses gloo on the CPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -111,38 +120,102 @@ def dist_setup(n_gpus):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if args.dry_run:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        else:
+            # NCCL's init log (communicator, ranks, transports) on stderr
+            os.environ.setdefault("NCCL_DEBUG", "INFO")
+            os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                    device_id=torch.device("cuda", local))
     return world, rank, local, dist
 
 
-def cpu_baseline_of(build, steps, sample):
+def ranks_info(dist):
+    """What the process group is: its backend, size and (NCCL) version."""
+    if not dist:
+        return {"world_size": 1, "backend": None}
+    info = {"world_size": dist.get_world_size(), "backend": dist.get_backend()}
+    if info["backend"] == "nccl":
+        import torch
+        v = torch.cuda.nccl.version()
+        info["nccl_version"] = ".".join(str(x) for x in v) if isinstance(v, tuple) else v
+    return info
+
+
+def self_spawn(n):
+    """`bench.py --gpus N` outside torchrun: launch N ranks through
+    torch.distributed.run on this node and return its exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def oracle_recipe():
+    """Switch the oracle to its -march=native build (compiled on this host)
+    for timing; returns the recipe's description."""
+    from oracle import oracle as O
+    return O.use_native()
+
+
+def cpu_baseline_of(build, steps, sample, keep=False):
     """The CPU oracle (a restatement of the reference's Fortran, OpenMP) on a
     bounded sample of a workload, on all host cores and on the reference's
-    hard-coded 4 threads (solver/mhd/main.f90:31)."""
+    hard-coded 4 threads (solver/mhd/main.f90:31).  keep: also return the
+    all-cores run's final state, time reached and fallback count (the
+    parity sample's oracle side)."""
     from oracle import oracle as O
-    out = {"unit": "zone-updates/s", "kind": "port", "sample": sample}
+    recipe = oracle_recipe()
+    out = {"unit": "zone-updates/s", "kind": "port", "sample": sample, "build": recipe}
+    kept = None
     try:
-        allc = os.cpu_count() or 1
+        allc = len(os.sched_getaffinity(0))
         for threads, key in ((allc, "value"), (4, "value_4_threads")):
             O.set_num_threads(threads)
             spec, prim, eps = build()
             o = O.Oracle(spec)
             o.set_state(prim, eps)
             o.initial_update()
+            t = 0.0
             t0 = time.perf_counter()
             for _ in range(steps):
-                o.rk3_step(o.finddt())
+                dt = o.finddt()
+                o.rk3_step(dt)
+                t += dt
             el = time.perf_counter() - t0
             out[key] = spec["nx"] * spec["ny"] * spec["nz"] * steps / el
             if key == "value":
                 out["cores"] = O.num_threads()
                 out["seconds"] = el
+                if keep:
+                    from cumc3d_b200 import capi
+                    p, e = o.get_state()
+                    kept = dict(prim=p, eps=e, bcell=o.get_array(capi.ARR_BCELL), cs=o.get_array(capi.ARR_CS),
+                                t=t, fallback=o.fallback_count(), spec=spec, init=(prim, eps))
             o.close()
         O.set_num_threads(allc)
     except Exception as ex:  # the baseline must not hide the GPU number
         out.update({"value": None, "cores": None, "sample": "failed: %s" % ex})
-    return out
+    return (out, kept) if keep else out
+
+
+def blast_slab(n, nz, recon, riemann):
+    """The headline blast as an n x n x nz periodic z slab (same cross-section,
+    same scheme and flags), the CPU-sized sample of the workload."""
+    from cumc3d_b200 import models
+    sp, pr, ep = models.blast_3d(n, nz=nz, recon=recon, riemann=riemann)
+    sp["positivity_fallback"] = 1
+    sp["fix_periodic_normal_faces"] = 1
+    return sp, pr, ep
+
+
+def blast_workload(n, recon, riemann):
+    return "blast3d_%d^3_%s_%s_ct_rk3_cfl0.4" % (n, recon, riemann)
 
 
 def reference_arm(args):
@@ -150,15 +223,15 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from cumc3d_b200 import models
     from oracle import oracle as O
     O.build()
     if args.workload == "batch1d":
         return reference_batch(args, world)
-    n = 48
-    spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
-    spec["positivity_fallback"] = 1
-    spec["fix_periodic_normal_faces"] = 1
+    recipe = oracle_recipe()
+    # every host thread this process may use (torchrun sets OMP_NUM_THREADS=1)
+    O.set_num_threads(len(os.sched_getaffinity(0)))
+    n, nz = args.n, 64
+    spec, prim, eps = blast_slab(n, nz, args.recon, args.riemann)
     o = O.Oracle(spec)
     o.set_state(prim, eps)
     o.initial_update()
@@ -168,15 +241,18 @@ def reference_arm(args):
     for _ in range(args.steps):
         o.rk3_step(o.finddt())
     el = time.perf_counter() - t0
-    zones = n ** 3
+    zones = n * n * nz
     value = zones * args.steps / el
-    sample = "blast3d at %d^3 (same domain, same scheme), %d timed steps after %d warm-up" % (n, args.steps, args.warmup)
+    sample = ("each step one RK3 step of a %dx%dx%d periodic z slab of the %d^3 blast (same cross-section, "
+              "scheme and flags; a quarter of the zones), %d timed steps after %d warm-up; %s" % (
+                  n, n, nz, n, args.steps, args.warmup, recipe))
     line = {
         "impl": "reference", "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "blast3d_256^3_weno_hlld_ct_rk3_cfl0.4 (reference arm: CPU oracle on a %d^3 sample)" % n,
-                   "recon": args.recon, "riemann": args.riemann},
+        "config": {"workload": blast_workload(n, args.recon, args.riemann), "grid": [n, n, n], "recon": args.recon,
+                   "riemann": args.riemann, "precision": "fp64", "boundary": "periodic",
+                   "positivity_fallback": 1, "fix_periodic_normal_faces": 1},
         "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": O.num_threads(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -591,10 +667,12 @@ def bench_slab_ranks(args, world, rank, local, dist):
     one per GPU, a periodic ring; ghost planes by NCCL send/recv into each
     receiver's memory, dt by an all-reduce (min), host-driven steps.  Strong
     scaling: the grid is fixed.  Time: CUDA events on each rank's engine
-    stream around the K steps, the max over ranks."""
+    stream around the K steps, the max over ranks.  e2e: each rank's slab
+    uploaded from pinned host memory, INITIAL_UPDATE, the K steps and the
+    slab's download, wall clock, max over ranks."""
     import torch
 
-    from cumc3d_b200 import engine, models
+    from cumc3d_b200 import engine, models, shard
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann)
     spec["positivity_fallback"] = 1
@@ -604,7 +682,7 @@ def bench_slab_ranks(args, world, rank, local, dist):
     r = engine.SlabRank(spec, sizes, rank)
     r.set_state(prim, eps)
     r.initial_update()
-    r.solver.autotune()
+    tuning = r.solver.autotune()
     for _ in range(args.warmup):
         r.step(r.finddt())
     stream = torch.cuda.ExternalStream(r.solver.stream())
@@ -614,29 +692,71 @@ def bench_slab_ranks(args, world, rank, local, dist):
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
+    l0 = r.solver.launch_count()
     e0.record(stream)
     for _ in range(args.steps):
         r.step(r.finddt())
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item()) / args.steps
+    launches = int(shard.sum_over_ranks(r.solver.launch_count() - l0, dist, "cuda"))
+    ms = shard.max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / args.steps
     xbytes = sum(r.send[k].numel() for k in r.send) * 3  # sent per step by this rank (3 stages)
+    # this rank's flux sweeps against the FP64 roofline (its slab's zones)
+    prof = r.solver.profile_step(args.profile_steps)
+    try:
+        fp64_peak = engine.fp64_peak_tflops()
+    except Exception:
+        fp64_peak = None
+    roofline, _, _ = flux_roofline(args, prof, args.profile_steps, spec["nx"] * spec["ny"] * sizes[rank],
+                                   tuning, fp64_peak)
+    roofline["note"] = "rank 0's slab (%d z planes)" % sizes[0]
     r.close()
+    # end to end: host slab in, K steps, slab out
+    e2e = None
+    if not args.no_e2e:
+        o = sum(sizes[:rank])
+        hp = torch.from_numpy(prim[o:o + sizes[rank] + 6].copy()).pin_memory()
+        he = torch.from_numpy(eps[o:o + sizes[rank] + 6].copy()).pin_memory()
+        r2 = engine.SlabRank(spec, sizes, rank)
+        r2.set_state(prim, eps)  # untimed: the tuner needs a live state
+        r2.initial_update()
+        r2.solver.autotune()
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r2.solver.set_state_ptr(hp.data_ptr(), he.data_ptr())
+        r2.initial_update()
+        for _ in range(args.steps):
+            r2.step(r2.finddt())
+        out_p, out_e = r2.get_state()
+        torch.cuda.synchronize()
+        el = shard.max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        nbytes = shard.sum_over_ranks(int(hp.numel() * 8 + he.numel() * 8), dist, "cuda")
+        r2.close()
+        e2e = {"value": zones * args.steps / el, "unit": "zone-updates/s",
+               "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+               "wall_s": el, "steps": args.steps,
+               "note": "each rank's slab uploaded and downloaded once per run of %d steps, amortised" % args.steps}
     if rank == 0:
         line = {
             "metric": "zone-updates/s", "value": zones / (ms * 1e-3), "unit": "zone-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "blast3d_%d^3_as_%d_z_slabs_one_per_rank" % (n, world), "slabs": sizes,
-                       "parallelism": "z slabs, NCCL send/recv of ghost planes",
-                       "timing": "CUDA events on each rank's engine stream, max over ranks"},
+            "config": {"workload": blast_workload(n, args.recon, args.riemann), "grid": [n, n, n],
+                       "recon": args.recon, "riemann": args.riemann, "precision": "fp64", "boundary": "periodic",
+                       "positivity_fallback": 1, "fix_periodic_normal_faces": 1, "slabs": sizes,
+                       "parallelism": parallelism_of(args, world),
+                       "l2": "state %.1f GB per rank, >> 126 MB L2 (no flush needed)" % (
+                           7.0 * sizes[0] / n),
+                       "timing": "CUDA events on each rank's engine stream, max over ranks", "autotuned": tuning},
+            "roofline": roofline,
             "results": {"ghost_bytes_sent_per_step_rank0": xbytes},
-            "e2e": None, "cpu_baseline": None, "clocks": clk,
+            "e2e": e2e, "cpu_baseline": None, "gpu_launches": launches, "ranks": ranks_info(dist), "clocks": clk,
         }
         print(json.dumps(line))
+    dist.barrier()
+    dist.destroy_process_group()
     return 0
 
 
@@ -921,20 +1041,29 @@ def main():
     ap.add_argument("--tuning", default="auto",
                     help="'auto' (the engine's autotuner) or split,tpb_recon,tpb_riemann,min_blocks[,recon_tile] "
                          "(pinned launch shape, e.g. for profiler runs where timing is distorted)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="N > 1: independent copies of the workload per rank instead of z slabs of one grid")
+    ap.add_argument("--parity-sample", type=int, default=1,
+                    help="1: check the engine bit for bit against the CPU oracle on the CPU baseline's slab")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="set up the ranks and the process group (gloo) and print the line's layout; no kernels")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "torus_sph": 1000, "poisson": 20, "snapshots": 60,
                       "slabs": 30}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return self_spawn(args.gpus)
     if args.impl == "reference":
         return reference_arm(args)
 
-    world, rank, local, dist = dist_setup(args.gpus)
-    import numpy as np
+    world, rank, local, dist = dist_setup(args)
+    if args.dry_run:
+        return dry_run(args, world, rank, dist)
     import torch
 
-    from cumc3d_b200 import engine, models
+    from cumc3d_b200 import engine
     torch.cuda.set_device(local)
     engine.load_library()
     if args.workload == "batch1d":
@@ -947,7 +1076,141 @@ def main():
         return bench_snapshots(args, world, rank, local, dist)
     if args.workload == "slabs":
         return bench_slabs(args, world, rank, local, dist)
+    if world > 1 and not args.replicas:
+        return bench_slab_ranks(args, world, rank, local, dist)
+    return bench_blast(args, world, rank, local, dist)
 
+
+def parallelism_of(args, world):
+    if world == 1:
+        return "single"
+    if args.workload in ("blast3d", "slabs") and not args.replicas:
+        return "z-slabs x %d (one per rank, NCCL send/recv of ghost planes, all-reduce min of dt)" % world
+    if args.workload == "batch1d":
+        return "problems sharded over %d ranks" % world
+    return "replicas"
+
+
+def dry_run(args, world, rank, dist):
+    """The launch layout without a GPU: ranks, process group, parallelism."""
+    info = ranks_info(dist)
+    if dist:
+        dist.barrier()
+    if rank == 0:
+        print(json.dumps({"metric": "zone-updates/s", "value": None, "unit": "zone-updates/s", "n_gpus": world,
+                          "dry_run": True, "ranks": info,
+                          "config": {"workload": blast_workload(args.n, args.recon, args.riemann),
+                                     "parallelism": parallelism_of(args, world)},
+                          "scaling": "strong" if world > 1 and not args.replicas else "weak"}))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def flux_roofline(args, prof, profile_steps, zones, tuning, fp64_peak):
+    """Roofline of the dominant kernel class (a flux sweep on the FP64 path):
+    bytes = 120 B/zone (the fused pass minimum), flops = the oracle's exact
+    count per zone of a sweep; achieved = flops / launch time against the
+    measured DFMA peak; frac = max(bytes / BW, flops / FP64 peak) / time, the
+    FP64 roofline of the scope table; the HBM side and the measured traffic
+    (ncu, profiles/traffic.json) alongside."""
+    per_stage = {k: v for k, v in prof.items() if k != "dt"}
+    dominant = max(per_stage, key=per_stage.get)
+    avg_ms = prof[dominant] / (profile_steps * 3)
+    peak_gbs, peak_kind = load_peaks()
+    if dominant.startswith("flux"):
+        bytes_launch = FLUX_BYTES_PER_ZONE * zones
+        if tuning.get("split", True):
+            kname = "%s + k_riemann, %s sweep (%s, %s)" % ("k_recon_tile" if tuning.get("recon_tile") else "k_recon",
+                                                           dominant[-1], args.recon, args.riemann)
+        else:
+            kname = "k_flux<%s,%s,%s>" % (dominant[-1], args.recon, args.riemann)
+    else:
+        bytes_launch = None
+        kname = dominant
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tdat = json.load(f)
+        key = "%s/%s/%s/%s" % (dominant, args.recon, args.riemann, args.precision)
+        if key in tdat:
+            traffic = tdat[key]["bytes_per_zone"] * zones
+    gbs = (bytes_launch / (avg_ms * 1e-3) / 1e9) if bytes_launch else None
+    hbm = {"achieved": gbs, "peak": peak_gbs, "unit": "GB/s", "frac": (gbs / peak_gbs) if gbs else None,
+           "bytes_per_launch": bytes_launch, "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peak_kind,
+           "traffic_over_algorithmic": (traffic / bytes_launch) if traffic and bytes_launch else None}
+    ops = None
+    okey = "blast3d_%s_%s" % (args.recon, args.riemann)
+    opath = os.path.join(ROOT, "profiles", "op_counts.json")
+    if args.precision == "fp64" and os.path.exists(opath):
+        with open(opath) as f:
+            ops = json.load(f).get(okey)
+    roof = {"kernel": kname, "avg_launch_ms": avg_ms, "traffic": traffic, "hbm": hbm,
+            "class_ms_per_step": {k: v / profile_steps for k, v in prof.items()}}
+    if ops is not None and fp64_peak and dominant.startswith("flux"):
+        fl = ops["flux_sweep_flops_per_zone"] * zones
+        tf = fl / (avg_ms * 1e-3) / 1e12
+        t_bound = max(bytes_launch / (peak_gbs * 1e9), fl / (fp64_peak * 1e12))
+        roof.update({"bound": "fp64", "achieved": tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": t_bound / (avg_ms * 1e-3), "flops_per_launch": fl,
+                     "peak_source": "cumc_fp64_peak (DFMA loop, measured in this run)",
+                     "counts": "profiles/op_counts.json %s: flux_sweep_flops_per_zone (add, mul, div, sqrt one "
+                               "flop each; a division or square root is several FP64 instructions)" % okey})
+    else:
+        roof.update({"bound": "hbm", "achieved": gbs, "peak": peak_gbs, "unit": "GB/s", "frac": hbm["frac"]})
+    fpath = os.path.join(ROOT, "profiles", "fp64_pipe.json")
+    if os.path.exists(fpath) and args.precision == "fp64":
+        with open(fpath) as f:
+            pipe = json.load(f).get("%s/%s/fp64" % (args.recon, args.riemann))
+        if pipe is not None:
+            roof["fp64_pipe_frac_ncu"] = pipe
+    return roof, ops, peak_gbs
+
+
+def parity_sample_check(args, kept, tuning):
+    """The engine on the CPU baseline's slab, the same steps through the same
+    captured step graph as the timed run, compared bit for bit with the
+    oracle's state (prim incl. face B, epsilon, cell B, sound speed on the
+    interior; the time reached)."""
+    import numpy as np
+
+    from cumc3d_b200 import capi, engine
+    spec = kept["spec"]
+    prim, eps = kept["init"]
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.initial_update()
+    # the launch shapes the timed run was tuned to
+    s.set_tuning(tuning["split"], tuning["tpb_recon"], tuning["tpb_riemann"], tuning["riemann_min_blocks"],
+                 tuning["recon_tile"])
+    s.fallback_count(1)
+    t, k = s.evolve(1e30, 2)
+    p, e = s.get_state()
+    got = dict(prim=p, eps=e, bcell=s.get_array(capi.ARR_BCELL), cs=s.get_array(capi.ARR_CS))
+    fb = s.fallback_count()
+    s.close()
+    nx, ny, nz = spec["nx"], spec["ny"], spec["nz"]
+    sl = (slice(3, nz + 3), slice(3, ny + 3), slice(3, nx + 3))
+    mism = {}
+    for key in ("prim", "eps", "bcell", "cs"):
+        a, b = got[key][sl], kept[key][sl]
+        mism[key] = int(np.count_nonzero(~((a == b) | (np.isnan(a) & np.isnan(b)))))
+    ok = all(v == 0 for v in mism.values()) and t == kept["t"] and fb == kept["fallback"]
+    return {"bitwise": bool(ok), "cells": nx * ny * nz, "grid": [nx, ny, nz], "steps": k,
+            "time_equal": t == kept["t"], "mismatched_values": mism,
+            "fallback_cells_gpu": fb, "fallback_cells_oracle": kept["fallback"],
+            "what": "prim (incl. face B), epsilon, cell B, c_s on the interior after 2 RK3 steps of the "
+                    "captured step graph, the tuned launch shapes of the timed run"}
+
+
+def bench_blast(args, world, rank, local, dist):
+    """The headline workload on one GPU (or N replicas with --replicas)."""
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import engine, models
     n = args.n
     spec, prim, eps = models.blast_3d(n, recon=args.recon, riemann=args.riemann, precision=args.precision)
     # the reference's WENO-Z + HLLD produces negative face pressure on this
@@ -996,72 +1259,21 @@ def main():
 
     # per-kernel-class timing (CUDA events on the engine stream, eager launches)
     prof = s.profile_step(args.profile_steps)
-    per_stage = {k: v for k, v in prof.items() if k != "dt"}
-    dominant = max(per_stage, key=per_stage.get)
-    launches_of = args.profile_steps * 3
-    avg_ms = prof[dominant] / launches_of
-    peak_gbs, peak_kind = load_peaks()
-    if dominant.startswith("flux"):
-        bytes_launch = FLUX_BYTES_PER_ZONE * zones
-        if tuning.get("split", True):
-            kname = "%s + k_riemann, %s sweep (%s, %s)" % ("k_recon_tile" if tuning.get("recon_tile") else "k_recon",
-                                                           dominant[-1], args.recon, args.riemann)
-        else:
-            kname = "k_flux<%s,%s,%s>" % (dominant[-1], args.recon, args.riemann)
-    else:
-        bytes_launch = None
-        kname = dominant
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            tdat = json.load(f)
-        key = "%s/%s/%s/%s" % (dominant, args.recon, args.riemann, args.precision)
-        if key in tdat:
-            traffic = tdat[key]["bytes_per_zone"] * zones
-    achieved = (bytes_launch / (avg_ms * 1e-3) / 1e9) if bytes_launch else None
-    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
-                "frac": (achieved / peak_gbs) if achieved else None, "traffic": traffic,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peak_kind,
-                "avg_launch_ms": avg_ms, "class_ms_per_step": {k: v / args.profile_steps for k, v in prof.items()}}
-    fp64_pipe = None
-    fpath = os.path.join(ROOT, "profiles", "fp64_pipe.json")
-    if os.path.exists(fpath) and args.precision == "fp64":
-        with open(fpath) as f:
-            fp64_pipe = json.load(f).get("%s/%s/fp64" % (args.recon, args.riemann))
-    if fp64_pipe is not None:
-        roofline["fp64_pipe_frac_ncu"] = fp64_pipe
-        roofline["note"] = ("the flux kernels are FP64-pipe bound (fp64_pipe_frac_ncu; roofline.fp64 counts a "
-                            "division or square root as one flop, though each is several FP64 instructions); "
-                            "the HBM fraction is reported against the algorithmic bytes of a fused pass")
-    step_gbs = STEP_BYTES_PER_ZONE * value / world / 1e9
     try:
         fp64_peak = engine.fp64_peak_tflops()
     except Exception:
         fp64_peak = None
-    # the FP64 side: exact operation counts per zone of this workload (the
-    # oracle on its counting scalar type, oracle/count_ops.py)
+    roofline, ops, peak_gbs = flux_roofline(args, prof, args.profile_steps, zones, tuning, fp64_peak)
+    step_gbs = STEP_BYTES_PER_ZONE * value / world / 1e9
     step_fp64 = None
-    okey = "blast3d_%s_%s" % (args.recon, args.riemann)
-    opath = os.path.join(ROOT, "profiles", "op_counts.json")
-    ops = None
-    if args.precision == "fp64" and os.path.exists(opath):
-        with open(opath) as f:
-            ops = json.load(f).get(okey)
     if ops is not None and fp64_peak:
-        if dominant.startswith("flux"):
-            fl = ops["flux_sweep_flops_per_zone"] * zones
-            roofline["fp64"] = {"flops_per_launch": fl, "achieved_tflops": fl / (avg_ms * 1e-3) / 1e12,
-                                "peak_tflops": fp64_peak, "frac": fl / (avg_ms * 1e-3) / 1e12 / fp64_peak,
-                                "peak_source": "cumc_fp64_peak (DFMA loop, measured in this run)",
-                                "counts": "profiles/op_counts.json %s: flux_sweep_flops_per_zone "
-                                          "(add, mul, div, sqrt one flop each)" % okey}
         tf = ops["flops_per_zone_update"] * value / world / 1e12
         step_fp64 = {"flops_per_zone_update": ops["flops_per_zone_update"], "achieved_tflops": tf,
                      "frac": tf / fp64_peak}
 
-    # end to end through the C-ABI with pinned host buffers
-    e2e = None
+    # end to end through the C-ABI with pinned host buffers; the same handle
+    # counts the cells that took the positivity fallback
+    e2e, fallback = None, None
     if not args.no_e2e:
         hp = torch.from_numpy(prim).pin_memory()
         he = torch.from_numpy(eps).pin_memory()
@@ -1077,6 +1289,7 @@ def main():
                           tuning["recon_tile"])
         if args.concurrent_sweeps:
             s2.set_concurrent_sweeps(True)
+        s2.fallback_count(1)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -1091,24 +1304,26 @@ def main():
             t = torch.tensor([el], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = float(t.item())
+        fb = s2.fallback_count()
         s2.close()
         nbytes_in = hp.numel() * 8 + he.numel() * 8
         e2e = {"value": world * zones * n2 / el, "unit": "zone-updates/s",
                "h2d_bytes_per_step": nbytes_in / max(n2, 1), "d2h_bytes_per_step": nbytes_in / max(n2, 1),
                "wall_s": el, "steps": n2,
                "note": "state upload and result download once per run of %d steps, amortised per step" % n2}
+        fallback = {"cells_per_step": fb / max(n2, 1), "steps": n2,
+                    "fraction_of_reconstructions": fb / max(1, n2 * 9 * zones),
+                    "what": "cells whose reconstruction took the first-order positivity fallback, per RK3 step "
+                            "(3 stages x 3 sweeps reconstruct every zone 9 times a step), from t = 0"}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         nz_slab = 64
-
-        def slab():
-            sp, pr, ep = models.blast_3d(n, nz=nz_slab, recon=args.recon, riemann=args.riemann)
-            sp["positivity_fallback"] = 1
-            sp["fix_periodic_normal_faces"] = 1
-            return sp, pr, ep
-        cpu = cpu_baseline_of(slab, 2, "CPU oracle, %dx%dx%d periodic slab of the blast, 2 RK3 steps" % (
-            n, n, nz_slab))
+        cpu, kept = cpu_baseline_of(lambda: blast_slab(n, nz_slab, args.recon, args.riemann), 2,
+                                    "CPU oracle, %dx%dx%d periodic slab of the blast, 2 RK3 steps" % (n, n, nz_slab),
+                                    keep=True)
+        if kept is not None and args.parity_sample and args.precision == "fp64":
+            parity = parity_sample_check(args, kept, tuning)
 
     s.close()
     if rank == 0:
@@ -1117,20 +1332,23 @@ def main():
             "steps": nsteps, "warmup": args.warmup, "ms_per_step": ms / nsteps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "blast3d_%d^3_%s_%s_ct_rk3_cfl0.4" % (n, args.recon, args.riemann),
+            "config": {"workload": blast_workload(n, args.recon, args.riemann),
                        "grid": [n, n, n], "recon": args.recon, "riemann": args.riemann,
                        "precision": args.precision, "boundary": "periodic", "steps_in_workload": 200,
                        "positivity_fallback": 1, "fix_periodic_normal_faces": 1,
                        "l2": "state 7 GB resident in HBM, >> 126 MB L2 (no flush needed)",
-                       "parallelism": "replicas" if world > 1 else "single", "autotuned": tuning},
+                       "parallelism": parallelism_of(args, world), "autotuned": tuning},
             "roofline": roofline,
             "step_hbm": {"bytes_per_zone_update": STEP_BYTES_PER_ZONE, "achieved_gbs": step_gbs,
                          "frac": step_gbs / peak_gbs},
             "step_fp64": step_fp64,
             "fp64_peak_tflops_measured": fp64_peak,
+            "parity_sample": parity,
+            "positivity_fallback": fallback,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
+            "ranks": ranks_info(dist),
             "clocks": clk,
         }
         print(json.dumps(line))

@@ -9,6 +9,7 @@
 
 #include "../../include/cumc3d_gpu.h"
 #include "batch_kernel.cuh"
+#include "weights1d.cuh"
 
 using namespace cumc;
 
@@ -33,41 +34,13 @@ static int bfail(cumc_batch *b, int code, const std::string &m) {
     return code;
 }
 
-// PPM/WENO/TVD weights of one axis (same formulas as the 3D handle)
+// PPM/WENO/TVD weights of one axis (same formulas as the 3D handle; the
+// per-cell routine is shared with the allocation-free entry point)
 static void axis_weights(int rec, int n, const double *xF, double *dx_out, double *w_out) {
-    std::vector<double> dx(n + 6);
-    for (int j = -2; j <= n + 3; ++j) dx[j + 2] = xF[j + 3] - xF[j + 2];
-    for (int j = 0; j < n + 6; ++j) dx_out[j] = dx[j];
-    auto D = [&](int j) { return dx[j + 2]; };
+    for (int j = -2; j <= n + 3; ++j) dx_out[j + 2] = xF[j + 3] - xF[j + 2];
     for (int j = 0; j < (n + 6) * 14; ++j) w_out[j] = 0.0;
-    if (rec == 3 || rec == 4) {
-        for (int j = 0; j <= n + 1; ++j) {
-            double *w = w_out + (size_t)(j + 2) * 14;
-            const double dm2 = D(j - 2), dm1 = D(j - 1), dc = D(j), dp1 = D(j + 1), dp2 = D(j + 2);
-            if (rec == 4) {
-                double a12 = dp2 / (dp1 + dp2), a01 = dp1 / (dc + dp1), a10 = dc / (dm1 + dc), a21 = dm1 / (dm2 + dm1);
-                w[0] = (1.0 - a01); w[1] = a01; w[2] = (1.0 - a12); w[3] = a12; w[4] = (1.0 - a10);
-                w[5] = a10; w[6] = (1.0 - a21); w[7] = a21; w[8] = (1.0 - a21); w[9] = a12;
-            } else {
-                double a1R = dc / (dc + dp1), a1L = dm1 / (dm1 + dc);
-                double aR = 2.0 * dp1 * dc / (dp1 + dc), aL = 2.0 * dc * dm1 / (dc + dm1);
-                double deltaXR = dm1 + dc + dp1 + dp2, deltaXL = dm2 + dm1 + dc + dp1;
-                double z1R = (dm1 + dc) / (2.0 * dc + dp1), z1L = (dm2 + dm1) / (2.0 * dm1 + dc);
-                double zR = (dp2 + dp1) / (2.0 * dp1 + dc), zL = (dp1 + dc) / (2.0 * dc + dm1);
-                double cc1 = dc / (dm1 + dc + dp1), cp1 = dp1 / (dc + dp1 + dp2), cm1 = dm1 / (dm2 + dm1 + dc);
-                double cc2 = (2.0 * dm1 + dc) / (dp1 + dc), cp2 = (2.0 * dc + dp1) / (dp2 + dp1), cm2 = (2.0 * dm2 + dm1) / (dc + dm1);
-                double cc3 = (dc + 2.0 * dp1) / (dm1 + dc), cp3 = (dp1 + 2.0 * dp2) / (dc + dp1), cm3 = (dm1 + 2.0 * dc) / (dm2 + dm1);
-                w[0] = a1L; w[1] = aL * (z1L - zL) / deltaXL; w[2] = (-dm1 * z1L) / deltaXL; w[3] = dc * zL / deltaXL;
-                w[4] = a1R; w[5] = aR * (z1R - zR) / deltaXR; w[6] = (-dc * z1R) / deltaXR; w[7] = dp1 * zR / deltaXR;
-                w[8] = cm1 * cm2; w[9] = cm1 * cm3; w[10] = cc1 * cc2; w[11] = cc1 * cc3; w[12] = cp1 * cp2; w[13] = cp1 * cp3;
-            }
-        }
-    } else {
-        for (int j = -1; j <= n + 2; ++j) {
-            w_out[(size_t)(j + 2) * 14 + 0] = (D(j) + D(j + 1)) / D(j);
-            w_out[(size_t)(j + 2) * 14 + 1] = (D(j) + D(j - 1)) / D(j);
-        }
-    }
+    const int jlo = (rec == 3 || rec == 4) ? 0 : -1, jhi = (rec == 3 || rec == 4) ? n + 1 : n + 2;
+    for (int j = jlo; j <= jhi; ++j) batch_cell_weights(rec, dx_out, j, w_out + (size_t)(j + 2) * 14);
 }
 
 extern "C" {

@@ -947,6 +947,9 @@ struct cumc_handle {
     cudaStream_t snap_stream = nullptr;
     cudaEvent_t snap_packed = nullptr, snap_done = nullptr;
     bool snap_pending = false;
+    // positivity-fallback counter (cumc_fallback_count)
+    unsigned long long *fb_dev = nullptr;
+    unsigned long long fb_host[1] = {0};
 };
 
 static std::string g_create_err;
@@ -1860,6 +1863,34 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     h->d.riemann_minb = choice[3];
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    return CUMC_OK;
+}
+
+int cumc_fallback_count(cumc_handle *h, int enable, unsigned long long *count_out) {
+    if (!h) return fail(h, CUMC_EINVAL, "null handle");
+    if (enable < -1 || enable > 1) return fail(h, CUMC_EINVAL, "enable must be -1, 0 or 1");
+    if (enable == 1) {
+        if (!h->fb_dev) {
+            CK(cudaMalloc((void **)&h->fb_dev, sizeof(unsigned long long)));
+            h->allocs.push_back(h->fb_dev);  // freed with the handle
+        }
+        CK(cudaMemsetAsync(h->fb_dev, 0, sizeof(unsigned long long), h->stream));
+    }
+    unsigned long long *want = (enable == 1) ? h->fb_dev : (enable == 0) ? nullptr : h->d.fb_count;
+    if (want != h->d.fb_count) {
+        h->d.fb_count = want;
+        // the captured step holds the kernels' parameters: capture it again
+        if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+        if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    }
+    if (count_out) {
+        *count_out = 0;
+        if (h->fb_dev) {
+            CK(cudaMemcpyAsync(h->fb_host, h->fb_dev, sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            *count_out = *h->fb_host;
+        }
+    }
     return CUMC_OK;
 }
 

@@ -87,6 +87,9 @@ struct Dev {
     int phx;
     double c_code;
     unsigned long long *lstats;  // audit counters (LEARN_STAT_SLOTS x LEARN_STAT_FIELDS)
+    // cells whose reconstruction took the positivity fallback, summed over
+    // sweeps and stages (null: not counted; cumc_fallback_count)
+    unsigned long long *fb_count;
 };
 
 __device__ __forceinline__ int cidx(const Dev &d, int j, int k, int l) {

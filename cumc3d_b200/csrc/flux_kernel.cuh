@@ -142,6 +142,8 @@ __global__ void __launch_bounds__(256) k_flux(const Dev d) {
                 // first-order fallback when an edge density or pressure is not
                 // positive (optional; the reference has no such guard)
                 fallback = !(sVM[0 * nthr + tid] > T(0) && sVP[0 * nthr + tid] > T(0) && vm > T(0) && vp > T(0));
+                // a cell shared by two tiles (ls = TS - 1 and 0 of the next) counts once
+                if (fallback && d.fb_count && (ls < TS - 1 || c == ns + 1)) atomicAdd(d.fb_count, 1ull);
                 if (fallback) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
@@ -266,6 +268,7 @@ __global__ void __launch_bounds__(256) k_recon(const Dev d) {
         if (v == 0) { vm_rho = vm; vp_rho = vp; }
         if (v == 4 && d.pos_fallback) {
             fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
+            if (fallback && d.fb_count) atomicAdd(d.fb_count, 1ull);
             if (fallback) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {

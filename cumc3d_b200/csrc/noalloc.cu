@@ -12,20 +12,25 @@
 //  * at most NOALLOC_MAX_CELLS (4096) zones; larger problems are rejected with
 //    CUMC_EINVAL before any device work;
 //  * the scratch is one static array per device (NOALLOC_SCRATCH_BYTES, about
-//    3.5 MB); the first call on a device, with that device current, looks up
-//    its address (cudaGetSymbolAddress) and keeps it: make that first call
-//    before any stream capture;
-//  * every call clears the work counter and the per-cell arrays it uses
-//    (cudaMemsetAsync) before filling them, so no state survives between calls;
+//    3.5 MB), held by every device that loads the library until exit; each
+//    call, with the device current, looks up its address in the current
+//    context (cudaGetSymbolAddress).  The first call on a device (and the
+//    first after a cudaDeviceReset) loads the module: make it before any
+//    stream capture;
+//  * a CUDA error left pending by the caller's earlier work is reported as
+//    such (CUMC_ECUDA) before any device work, so the launch checks below
+//    only ever see this call's own launches;
+//  * every call clears the whole scratch array (one cudaMemsetAsync of about
+//    3.5 MB) before filling it, so no state survives between calls;
 //  * calls that overlap in time on the same device (other threads, other
 //    streams) share the one scratch array and race: serialise them.
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "../../include/cumc3d_gpu.h"
 #include "batch_kernel.cuh"
+#include "weights1d.cuh"
 
 using namespace cumc;
 
@@ -42,10 +47,6 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_HEAD + (size_t)NOALLOC_PER_CELL
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::mutex g_setup_mutex;
-void *g_scratch_ptr[NOALLOC_MAX_DEVICES] = {};
-
 // the message goes to the caller's buffer (no library-held string)
 struct ErrBuf {
     char *p;
@@ -59,51 +60,19 @@ struct ErrBuf {
     }
 };
 
-// the static array's device address on the current device (set-up once)
+// the static array's device address in the current device's context.  Looked
+// up on every call rather than cached: a cudaDeviceReset (or another context
+// made current) reloads the module and may move the array, and an address
+// kept from before would then point at freed or foreign memory.  Once the
+// module is loaded the lookup is a host-side table read and allocates nothing.
 int scratch_base(void **out, const ErrBuf &eb) {
-    auto nfail = [&](int code, const char *msg) { return eb.fail(code, msg); };
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return nfail(CUMC_ECUDA, "no current CUDA device");
-    if (dev >= NOALLOC_MAX_DEVICES) return nfail(CUMC_EINVAL, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return nfail(CUMC_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return eb.fail(CUMC_ECUDA, "no current CUDA device");
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return eb.fail(CUMC_ECUDA, "cudaGetSymbolAddress of the static scratch failed");
+    *out = p;
     return CUMC_OK;
-}
-
-// reconstruction weights of one padded cell (the same expressions, in the same
-// order, as the handle-based set-up of the 1D batch)
-__device__ void cell_weights(int rec, const double *dxr, int j, double *w) {
-    auto D = [&](int i) { return dxr[i + 2]; };
-    for (int m = 0; m < 14; ++m) w[m] = 0.0;
-    if (rec == 3 || rec == 4) {
-        const double dm2 = D(j - 2), dm1 = D(j - 1), dc = D(j), dp1 = D(j + 1), dp2 = D(j + 2);
-        if (rec == 4) {
-            double a12 = dp2 / (dp1 + dp2), a01 = dp1 / (dc + dp1), a10 = dc / (dm1 + dc), a21 = dm1 / (dm2 + dm1);
-            w[0] = (1.0 - a01); w[1] = a01; w[2] = (1.0 - a12); w[3] = a12; w[4] = (1.0 - a10);
-            w[5] = a10; w[6] = (1.0 - a21); w[7] = a21; w[8] = (1.0 - a21); w[9] = a12;
-        } else {
-            double a1R = dc / (dc + dp1), a1L = dm1 / (dm1 + dc);
-            double aR = 2.0 * dp1 * dc / (dp1 + dc), aL = 2.0 * dc * dm1 / (dc + dm1);
-            double deltaXR = dm1 + dc + dp1 + dp2, deltaXL = dm2 + dm1 + dc + dp1;
-            double z1R = (dm1 + dc) / (2.0 * dc + dp1), z1L = (dm2 + dm1) / (2.0 * dm1 + dc);
-            double zR = (dp2 + dp1) / (2.0 * dp1 + dc), zL = (dp1 + dc) / (2.0 * dc + dm1);
-            double cc1 = dc / (dm1 + dc + dp1), cp1 = dp1 / (dc + dp1 + dp2), cm1 = dm1 / (dm2 + dm1 + dc);
-            double cc2 = (2.0 * dm1 + dc) / (dp1 + dc), cp2 = (2.0 * dc + dp1) / (dp2 + dp1), cm2 = (2.0 * dm2 + dm1) / (dc + dm1);
-            double cc3 = (dc + 2.0 * dp1) / (dm1 + dc), cp3 = (dp1 + 2.0 * dp2) / (dc + dp1), cm3 = (dm1 + 2.0 * dc) / (dm2 + dm1);
-            w[0] = a1L; w[1] = aL * (z1L - zL) / deltaXL; w[2] = (-dm1 * z1L) / deltaXL; w[3] = dc * zL / deltaXL;
-            w[4] = a1R; w[5] = aR * (z1R - zR) / deltaXR; w[6] = (-dc * z1R) / deltaXR; w[7] = dp1 * zR / deltaXR;
-            w[8] = cm1 * cm2; w[9] = cm1 * cm3; w[10] = cc1 * cc2; w[11] = cc1 * cc3; w[12] = cp1 * cp2; w[13] = cp1 * cp3;
-        }
-    } else {
-        w[0] = (D(j) + D(j + 1)) / D(j);
-        w[1] = (D(j) + D(j - 1)) / D(j);
-    }
 }
 
 struct Staging {
@@ -125,7 +94,7 @@ __global__ void k_noalloc_setup(const BatchDev b, const Staging st, int n, int r
     for (int i = threadIdx.x; i < NX; i += blockDim.x) {
         const int j = i - 2;
         double wl[14];
-        if (j >= jlo && j <= jhi) cell_weights(rec, dx, j, wl);
+        if (j >= jlo && j <= jhi) batch_cell_weights(rec, dx, j, wl);
         else for (int m = 0; m < 14; ++m) wl[m] = 0.0;
         for (int m = 0; m < 14; ++m) {
             w[(size_t)i * 14 + m] = wl[m];
@@ -180,6 +149,8 @@ int cumc_batch_run1_noalloc(const cumc_batch_config *cfg, const double *prim, co
     if (cfg->gamma <= 1.0 || !(cfg->cfl > 0.0)) return nfail(CUMC_EINVAL, "bad gamma or cfl");
     if (cfg->floor_kind != CUMC_FLOOR_NONE && cfg->floor_kind != CUMC_FLOOR_EPS)
         return nfail(CUMC_EINVAL, "batched problems support the none/eps floors");
+    if (cudaPeekAtLastError() != cudaSuccess)
+        return nfail(CUMC_ECUDA, "a CUDA error is pending from earlier work on this thread (not from this call)");
     void *base = nullptr;
     int rc = scratch_base(&base, eb);
     if (rc != CUMC_OK) return rc;
@@ -233,8 +204,9 @@ int cumc_batch_run1_noalloc(const cumc_batch_config *cfg, const double *prim, co
     st.xF = xf;
     st.out = stage;
 
-    // clear what is read before written: the head (work counter, problem
-    // record) and the per-cell rows used by this problem size
+    // clear the whole array: the head (work counter, problem record) and every
+    // per-cell row, whatever the problem size (about 3.5 MB, well under a
+    // microsecond of HBM time)
     bool ok = cudaMemsetAsync(head, 0, NOALLOC_HEAD, s) == cudaSuccess;
     ok = ok && cudaMemsetAsync(cells, 0, (size_t)NOALLOC_PER_CELL * NOALLOC_ROW * sizeof(double), s) == cudaSuccess;
     // inputs: the three prim rows the 1D kernel reads, the eps row and the faces

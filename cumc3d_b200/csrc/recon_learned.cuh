@@ -105,6 +105,7 @@ __device__ __forceinline__ void learned_reconstruct(const Dev &d, const LearnedC
         if (v == 0) { vm_rho = vm; vp_rho = vp; }
         if (v == 4 && d.pos_fallback) {
             fallback = !(vm_rho > 0.0f && vp_rho > 0.0f && vm > 0.0f && vp > 0.0f);
+            if (fallback && q.valid && d.fb_count) atomicAdd(d.fb_count, 1ull);
             if (fallback && q.valid) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {

@@ -190,6 +190,7 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) 
             if (v == 0) { vm_rho = vm; vp_rho = vp; }
             if (v == 4 && d.pos_fallback) {
                 fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
+                if (fallback && d.fb_count) atomicAdd(d.fb_count, 1ull);
                 if (fallback) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {

@@ -21,7 +21,7 @@ EXPORTS = [
     "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
-    "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_check_div3",
+    "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_fallback_count", "cumc_check_div3",
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
@@ -76,6 +76,7 @@ def load_library(path=None):
     L.cumc_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.cumc_set_tuning.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     L.cumc_set_concurrent_sweeps.argtypes = [C.c_void_p, C.c_int]
+    L.cumc_fallback_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)]
     L.cumc_check_div3.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
@@ -235,6 +236,13 @@ class Solver:
     def set_concurrent_sweeps(self, on=True):
         """Run each stage's three flux sweeps as concurrent branches (same bits)."""
         self._check(self.L.cumc_set_concurrent_sweeps(self.h, 1 if on else 0))
+
+    def fallback_count(self, enable=-1):
+        """Cells reconstructed with the positivity fallback since counting was
+        enabled (enable=1 restarts from zero, 0 stops, -1 only reads)."""
+        n = C.c_ulonglong()
+        self._check(self.L.cumc_fallback_count(self.h, int(enable), C.byref(n)))
+        return int(n.value)
 
     # ---- learned smooth-face flag (FP32 WENO form, handle created with learned=1) ----
     def learn_set(self, params, threshold=0.0, audit_interval=10, audit_tol=1e-6, flag_interval=1):

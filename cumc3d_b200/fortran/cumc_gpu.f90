@@ -308,6 +308,12 @@ INTERFACE
     TYPE(C_PTR), VALUE :: h
     INTEGER(C_INT), VALUE :: on
   END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_fallback_count(h, enable, count_out) BIND(C, NAME='cumc_fallback_count')
+    IMPORT :: C_INT, C_PTR, C_LONG_LONG
+    TYPE(C_PTR), VALUE :: h
+    INTEGER(C_INT), VALUE :: enable
+    INTEGER(C_LONG_LONG), INTENT(OUT) :: count_out
+  END FUNCTION
   INTEGER(C_INT) FUNCTION cumc_check_div3(seed, n, mismatches, example) BIND(C, NAME='cumc_check_div3')
     IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
     INTEGER(C_LONG_LONG), VALUE :: seed, n

@@ -216,6 +216,15 @@ int cumc_set_tuning(cumc_handle *h, const int *choice);
  * Not used with the learned flag or while cumc_profile_step records. */
 int cumc_set_concurrent_sweeps(cumc_handle *h, int on);
 
+/* Positivity-fallback counter (no counterpart in the reference, which has no
+ * fallback): enable = 1 starts counting from zero the cells whose
+ * reconstruction took the optional first-order fallback (one count per cell
+ * per sweep and stage); enable = 0 stops counting; enable = -1 leaves the
+ * state as it is.  count_out (may be NULL) receives the count so far (the
+ * call synchronises the handle's stream).  Counting costs one atomic per
+ * fallback cell and nothing otherwise. */
+int cumc_fallback_count(cumc_handle *h, int enable, unsigned long long *count_out);
+
 /* Numerics self-check (no counterpart in the reference): compares the FP64
  * engine's FMA-corrected division by 3 with the IEEE quotient on n generated
  * normal inputs; *mismatches counts differing bit patterns. */
@@ -448,12 +457,15 @@ const char *cumc_mlp_last_error(void);
  *   prim_row, eps_row  host outputs as for cumc_batch_get_state;
  *   t_out, steps_out, status_out  as for cumc_batch_run (may be NULL);
  *   err, err_len  optional buffer for the failure message.
- * The first call on each device, with that device current, does the set-up
- * (looks up the static array's address); make it before any stream capture.
- * Each call clears the work counter and the scratch rows before use.  Calls
- * that overlap in time on one device share the static array and race:
- * serialise them.  Results equal cumc_batch_create/_set_state/_run/_get_state
- * on the same single problem. */
+ * Every call looks up the static array's address in the current context
+ * (cudaGetSymbolAddress), so an address never goes stale after a
+ * cudaDeviceReset; the first call on each device, with that device current,
+ * (and the first after a reset) loads the module: make it before any stream
+ * capture.  A CUDA error already pending on the calling thread is returned
+ * as CUMC_ECUDA before any device work.  Each call clears the whole static
+ * array before use.  Calls that overlap in time on one device share the
+ * static array and race: serialise them.  Results equal
+ * cumc_batch_create/_set_state/_run/_get_state on the same single problem. */
 int cumc_batch_run1_noalloc(const cumc_batch_config *cfg, const double *prim, const double *eps, int max_steps,
                             void *stream, double *prim_row, double *eps_row, double *t_out, int *steps_out,
                             int *status_out, char *err, size_t err_len);

@@ -117,6 +117,8 @@ struct Sim {
     int NX, NY, NZ; /* padded extents n+6 */
     double ggas, cfl;
     std::string err;
+    /* cells reconstructed with the positivity fallback (all sweeps, stages) */
+    unsigned long long fb_count = 0;
 
     /* grid (1D), index offset 3 for the -3..n+3 face arrays, 2 for cells */
     std::vector<double> xF_, yF_, zF_;
@@ -826,8 +828,11 @@ struct Sim {
                     bool fallback = cfg.positivity_fallback &&
                         !(PR(irho, jm, km, lm) > 0.0 && PL(irho, j, k, l) > 0.0 &&
                           PR(itau, jm, km, lm) > 0.0 && PL(itau, j, k, l) > 0.0);
-                    if (fallback)
+                    if (fallback) {
+#pragma omp atomic
+                        fb_count++;
                         for (int i = imin; i <= itau; ++i) { PR(i, jm, km, lm) = P(i, j, k, l); PL(i, j, k, l) = P(i, j, k, l); }
+                    }
                     epsR[c3(jm, km, lm)] = eos_eps(PR(irho, jm, km, lm), PR(itau, jm, km, lm));
                     epsL[c3(j, k, l)] = eos_eps(PL(irho, j, k, l), PL(itau, j, k, l));
                     csR[c3(jm, km, lm)] = eos_cs(PR(itau, jm, km, lm), PR(irho, jm, km, lm), epsR[c3(jm, km, lm)]);
@@ -1502,6 +1507,10 @@ void orc_get_array(void *p, int which, double *out) {
         else if (which == 2) for (size_t i = 0; i < n3; ++i) out[i] = dv(s->cs[i]);
     };
     if (h->counting) grab(h->c); else grab(h->d);
+}
+unsigned long long orc_fallback_count(void *p) {
+    Handle *h = (Handle *)p;
+    return h->counting ? h->c->fb_count : h->d->fb_count;
 }
 void orc_initial_update(void *p) {
     SerialScope serial_(((Handle *)p)->counting != 0);

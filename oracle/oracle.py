@@ -20,17 +20,59 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "liboracle.so")
 SRC = os.path.join(HERE, "cumc_oracle.cpp")
 
-# one recipe for parity and timing: no FP contraction (bitwise order is kept),
-# OpenMP loops as in the reference's CPU build, generic x86-64 code.
+# parity recipe: no FP contraction (bitwise order is kept), OpenMP loops as in
+# the reference's CPU build, generic x86-64 code (the library travels).
 CXXFLAGS = ["-std=c++17", "-O3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared"]
+# timed recipe of the CPU baseline: the same plus -march=native, compiled on
+# the host that runs it (the code it emits may not run on another CPU); the
+# arithmetic is the same (no contraction, no fast-math), only vectorised
+NATIVE_DIR = os.path.join(BUILD, "native")
+NATIVE_LIB = os.path.join(NATIVE_DIR, "liboracle.so")
+
+
+def _deps_mtime():
+    return max(os.path.getmtime(SRC), os.path.getmtime(os.path.join(HERE, "..", "include", "cumc3d_gpu.h")))
 
 
 def build(force=False):
     os.makedirs(BUILD, exist_ok=True)
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
-            os.path.getmtime(SRC), os.path.getmtime(os.path.join(HERE, "..", "include", "cumc3d_gpu.h"))):
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < _deps_mtime():
         subprocess.check_call(["g++"] + CXXFLAGS + ["-o", LIB, SRC])
     return LIB
+
+
+def _cpu_key():
+    """Model name and flags of this host's CPU (the native build's target)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            txt = f.read()
+    except OSError:
+        return "unknown"
+    keep = [ln for ln in txt.splitlines() if ln.startswith(("model name", "flags"))][:2]
+    return "\n".join(keep)
+
+
+def use_native():
+    """Switch this process to the -march=native build (compiled here on first
+    use, again when the host CPU differs from the one it was built for).
+    Must be called before the first Oracle is made.  Returns a description of
+    the recipe in use; on a compiler failure the generic build stays."""
+    global LIB
+    if _lib is not None:
+        return "generic (-O3, the library was already loaded)"
+    os.makedirs(NATIVE_DIR, exist_ok=True)
+    stamp = os.path.join(NATIVE_DIR, "cpu.txt")
+    key = _cpu_key()
+    old = open(stamp).read() if os.path.exists(stamp) else None
+    if old != key or not os.path.exists(NATIVE_LIB) or os.path.getmtime(NATIVE_LIB) < _deps_mtime():
+        try:
+            subprocess.check_call(["g++"] + CXXFLAGS + ["-march=native", "-o", NATIVE_LIB, SRC])
+        except (OSError, subprocess.CalledProcessError) as ex:
+            return "generic (-O3; the -march=native build failed: %s)" % ex
+        with open(stamp, "w") as f:
+            f.write(key)
+    LIB = NATIVE_LIB
+    return "g++ -O3 -march=native -ffp-contract=off -fno-fast-math -fopenmp"
 
 
 _lib = None
@@ -42,6 +84,8 @@ def lib():
         if not os.path.exists(LIB):
             build()
         L = C.CDLL(LIB)
+        L.orc_fallback_count.argtypes = [C.c_void_p]
+        L.orc_fallback_count.restype = C.c_ulonglong
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_void_p, C.c_int]
         L.orc_last_error.restype = C.c_char_p
@@ -108,6 +152,10 @@ class Oracle:
         eps = np.ascontiguousarray(eps, dtype=np.float64)
         assert prim.shape == self.shape + (8,) and eps.shape == self.shape
         lib().orc_set_state(self.h, prim.ctypes.data, eps.ctypes.data)
+
+    def fallback_count(self):
+        """Cells reconstructed with the positivity fallback so far."""
+        return int(lib().orc_fallback_count(self.h))
 
     def get_state(self):
         prim = np.empty(self.shape + (8,))

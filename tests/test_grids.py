@@ -12,7 +12,10 @@ import pytest
 from cumc3d_b200 import grids
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("CUMC_REFERENCE_TREE", "/root/reference") + "/model"
+# the reference tree, when a user points CUMC_REFERENCE_TREE at it; without it
+# the direct comparison is skipped and the digests above carry the check
+_TREE = os.environ.get("CUMC_REFERENCE_TREE", "")
+REF = os.path.join(_TREE, "model") if _TREE else ""
 
 
 def _generated():
@@ -38,7 +41,7 @@ def test_generators_match_the_digests_of_the_shipped_grid_files():
         assert mgd.digest(faces) == w["sha256"], name
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="CUMC_REFERENCE_TREE not set to the reference tree")
 def test_generators_reproduce_the_shipped_grid_files_bitwise():
     nx, ny, nz, r, th, ph = grids.spherical_torus_grid()
     xF, yF, zF = grids.load_grid(os.path.join(REF, "torus-sph", "grid"), nx, ny, nz,

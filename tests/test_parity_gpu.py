@@ -249,3 +249,52 @@ def test_concurrent_sweeps_are_bitwise_identical(oracle_mod, precision):
         po, eo = o.get_state()
         o.close()
         assert np.array_equal(runs[2][0].view(np.uint64), interior(po, spec).view(np.uint64))
+
+
+@pytest.mark.parametrize("n,nz", [(96, 96), (128, 40)])
+def test_headline_blast_parameters_at_size_bitwise(oracle_mod, n, nz):
+    """The bench's own blast (radius 0.1, p 10 : 0.1, B = (1, 1, 0)/sqrt 2,
+    WENO-Z + HLLD + CT, CFL 0.4, positivity fallback and the periodic-face
+    option) at 96^3 and on a 128 x 128 x 40 slab, through the captured step
+    graph with the autotuned launch shapes, against the oracle bit for bit;
+    the fallback counters of the two agree."""
+    from cumc3d_b200.engine import Solver
+    spec, prim, eps = models.blast_3d(n, nz=nz, recon="weno", riemann="hlld")
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    g = Solver(spec)
+    g.set_state(prim, eps)
+    g.initial_update()
+    g.autotune()
+    g.fallback_count(1)
+    tg, kg = g.evolve(1e30, 6)
+    o = oracle_mod.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    to = 0.0
+    for _ in range(6):
+        dt = o.finddt()
+        o.rk3_step(dt)
+        to += dt
+    assert kg == 6 and tg == to
+    pg, eg = g.get_state()
+    po, eo = o.get_state()
+    assert np.array_equal(interior(pg, spec), interior(po, spec))
+    assert np.array_equal(interior(eg, spec), interior(eo, spec))
+    assert g.fallback_count() == o.fallback_count()
+    g.close()
+    o.close()
+
+
+def test_torus_benchmark_config_at_96x64x96_bitwise(oracle_mod):
+    """The cylindrical torus workload (GM = 1 point mass, constant-l
+    polytrope, A_phi field loops at min beta 100, 1% seeded pressure noise,
+    r in [2, 42], z in [-20, 20], WENO-Z + HLLD + CT, positivity fallback and
+    the periodic-face option) at 96 x 64 x 96, three steps, bit for bit."""
+    spec, prim, eps = models.torus_cyl(nr=96, nphi=64, nz=96, recon="weno", riemann="hlld")
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    g, o, dg, do = run_pair(spec, prim, eps, 3, oracle_mod)
+    assert dg == do
+    assert_bitwise(g, o, spec)
+    assert_bitwise(g, o, spec, what=("cons",))
