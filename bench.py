@@ -1045,6 +1045,8 @@ def main():
                     help="N > 1: independent copies of the workload per rank instead of z slabs of one grid")
     ap.add_argument("--parity-sample", type=int, default=1,
                     help="1: check the engine bit for bit against the CPU oracle on the CPU baseline's slab")
+    ap.add_argument("--precision-forms", type=int, default=1,
+                    help="1: also time the FP64 / FP32 / FP32+learned forms on the 256^3 CP Alfven wave")
     ap.add_argument("--dry-run", action="store_true",
                     help="set up the ranks and the process group (gloo) and print the line's layout; no kernels")
     args = ap.parse_args()
@@ -1205,6 +1207,64 @@ def parity_sample_check(args, kept, tuning):
                     "captured step graph, the tuned launch shapes of the timed run"}
 
 
+def precision_forms(args, learned_params):
+    """The precision forms on the CP Alfven wave at 256^3 (WENO-Z + HLLD + CT,
+    CFL 0.4): plain FP64, FP32 bulk, FP32 bulk + learned smooth-face flag
+    (the bench's flag settings), each from the same initial state: 8 warm-up
+    steps, then 24 timed steps (one audit cycle) with CUDA events on the
+    engine stream; relative L1 per conserved variable of each form against
+    the FP64 form after those 32 steps."""
+    import numpy as np
+    import torch
+
+    from cumc3d_b200 import capi, engine, models
+    from cumc3d_b200.accuracy import rel_l1
+    n, warm, steps = 256, 8, 24
+    spec, prim, eps = models.alfven_3d(n, recon="weno")
+    forms = [("fp64", dict(spec, precision="fp64"), None), ("fp32", dict(spec, precision="fp32"), None)]
+    if learned_params and os.path.exists(learned_params):
+        P = np.load(learned_params)
+
+        def setup(s, P=P):
+            s.learn_set(P, threshold=args.learn_threshold, audit_interval=args.audit_interval, audit_tol=1e-5,
+                        flag_interval=args.flag_interval)
+        forms.append(("fp32+learned", dict(spec, precision="fp32", learned=1), setup))
+    out, cons = {}, {}
+    for name, sp, setup in forms:
+        s = engine.Solver(sp)
+        s.set_state(prim, eps)
+        s.initial_update()
+        if setup is not None:
+            setup(s)
+        s.autotune()
+        s.evolve(1e30, warm)
+        s.sync()
+        stream = torch.cuda.ExternalStream(s.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _, k = s.evolve(1e30, steps)
+        e1.record(stream)
+        s.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / k
+        cons[name] = s.get_array(capi.ARR_CONS)[3:n + 3, 3:n + 3, 3:n + 3]
+        out[name] = {"zone_updates_per_s": n ** 3 / (ms * 1e-3), "ms_per_step": ms}
+        if setup is not None:
+            st = s.learn_stats()
+            out[name]["flagged_fraction_at_audits"] = st["flagged"] / max(1, st["audited"])
+        s.close()
+    for name in out:
+        if name != "fp64":
+            l1 = rel_l1(cons[name], cons["fp64"])
+            out[name]["l1_vs_fp64_max"] = float(l1.max())
+            out[name]["l1_vs_fp64_per_var"] = l1.tolist()
+            out[name]["speedup_vs_fp64"] = out[name]["zone_updates_per_s"] / out["fp64"]["zone_updates_per_s"]
+    out["workload"] = "alfven3d_256^3_weno_hlld_ct_cfl0.4, %d warm-up + %d timed steps per form" % (warm, steps)
+    return out
+
+
 def bench_blast(args, world, rank, local, dist):
     """The headline workload on one GPU (or N replicas with --replicas)."""
     import numpy as np
@@ -1316,6 +1376,10 @@ def bench_blast(args, world, rank, local, dist):
                     "what": "cells whose reconstruction took the first-order positivity fallback, per RK3 step "
                             "(3 stages x 3 sweeps reconstruct every zone 9 times a step), from t = 0"}
 
+    forms = None
+    if rank == 0 and world == 1 and args.precision_forms:
+        forms = precision_forms(args, args.learned_params)
+
     cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         nz_slab = 64
@@ -1344,6 +1408,7 @@ def bench_blast(args, world, rank, local, dist):
             "step_fp64": step_fp64,
             "fp64_peak_tflops_measured": fp64_peak,
             "parity_sample": parity,
+            "precision_forms": forms,
             "positivity_fallback": fallback,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -313,18 +313,41 @@ __global__ void k_snapshot_pack(const Dev d, double *__restrict__ out) {
 // ---------------------------------------------------------------------------
 // du/dt and the Shu-Osher combination over j,k,l = 0..n
 // ---------------------------------------------------------------------------
-template <class FT>  // storage type of the hydro face fluxes (double, or float in the FP32 form)
-__global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
-    if (d.S->done) return;
-    // flat index over j,k,l = 0..n (x fastest)
-    const int ex = d.nx + 1, ey = d.ny + 1, ez = d.nz + 1;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)ex * ey * ez) return;
-    const int j = (int)(t % ex);
-    const long long r = t / ex;
-    const int k = (int)(r % ey);
-    const int l = (int)(r / ey);
-    const int c = cidx(d, j, k, l);
+// l_operator face-B induction of one face component, spatial.f90:639-702
+// (x: from the z edges at k, k-1 and the y edges at l, l-1; y and z alike)
+__device__ __forceinline__ double lr_face_x(const Dev &d, int j, int k, int l, double ez0, double ezy, double ey0,
+                                           double eyz) {
+    if (d.coord == 0) return -(dv(ez0 - ezy, DY(k)) - dv(ey0 - eyz, DZ(l)));
+    if (d.coord == 1) return dv(-(ez0 - ezy), XF(j) * DY(k)) + dv(ey0 - eyz, DZ(l));
+    return (-(SINF(k) * ez0 - SINF(k - 1) * ezy) + (ey0 - eyz) * (DY(k) / DZ(l))) / (XF(j) * DCOSE(k) + small_num);
+}
+__device__ __forceinline__ double lr_face_y(const Dev &d, int j, int k, int l, double ex0, double exz, double ez0,
+                                           double ezx) {
+    if (d.coord == 0) return -(dv(ex0 - exz, DZ(l)) - dv(ez0 - ezx, DX(j)));
+    if (d.coord == 1) return dv(-(ex0 - exz), DZ(l)) + dv(ez0 - ezx, DX(j));
+    return (-(ex0 - exz) / (XBAR(j) * SINF(k) * DZ(l) + small_num) + (XF(j) * ez0 - XF(j - 1) * ezx) / (XC(j) * DX(j)));
+}
+__device__ __forceinline__ double lr_face_z(const Dev &d, int j, int k, int l, double ey0, double eyx, double ex0,
+                                           double exy) {
+    if (d.coord == 0) return -(dv(ey0 - eyx, DX(j)) - dv(ex0 - exy, DY(k)));
+    if (d.coord == 1) return dv(-(XF(j) * ey0 - XF(j - 1) * eyx), XC(j) * DX(j)) + dv(ex0 - exy, XC(j) * DY(k));
+    return (-(XF(j) * ey0 - XF(j - 1) * eyx) / (XC(j) * DX(j)) + (ex0 - exy) / (XBAR(j) * DY(k)));
+}
+
+// the Shu-Osher combination of one variable, rungekutta.f90:61-167
+__device__ __forceinline__ double rk_combine(int stage, double u, double u0, double dt, double lr) {
+    if (stage == 1) return u + dt * lr;
+    if (stage == 2) return rk20 * u0 + rk21 * u + rk22 * dt * lr;
+    return rk30 * u0 + rk31 * u + rk32 * dt * lr;
+}
+
+// FLUX_DIFF + sources + the face-B induction + the Shu-Osher combination of
+// one cell (j,k,l in 0..n): un = the cell's new conserved state; in stage 1
+// the old state is saved to u_old.  (Hydro components of the index-0 layers
+// are combined with a zero operator, as the reference leaves them undefined
+// and never reads them back.)
+template <class FT>
+__device__ __forceinline__ void rk_cell(const Dev &d, int stage, int j, int k, int l, int c, double *un) {
     const int sy = d.NX, sz = d.NX * d.NY;
     const bool interior = (j >= 1 && k >= 1 && l >= 1);
     // issue every independent load first: this kernel is bound by memory-level
@@ -444,33 +467,33 @@ __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
         for (int i = 0; i < 5; ++i) lr[i] = 0.0;  // undefined in the reference, never read back
     }
     // l_operator face-B induction, spatial.f90:639-702
-    if (d.coord == 0) {
-        lr[5] = -(dv(ez0 - ezy, DY(k)) - dv(ey0 - eyz, DZ(l)));
-        lr[6] = -(dv(ex0 - exz, DZ(l)) - dv(ez0 - ezx, DX(j)));
-        lr[7] = -(dv(ey0 - eyx, DX(j)) - dv(ex0 - exy, DY(k)));
-    } else if (d.coord == 1) {
-        lr[5] = dv(-(ez0 - ezy), XF(j) * DY(k)) + dv(ey0 - eyz, DZ(l));
-        lr[6] = dv(-(ex0 - exz), DZ(l)) + dv(ez0 - ezx, DX(j));
-        lr[7] = dv(-(XF(j) * ey0 - XF(j - 1) * eyx), XC(j) * DX(j)) + dv(ex0 - exy, XC(j) * DY(k));
-    } else {
-        lr[5] = (-(SINF(k) * ez0 - SINF(k - 1) * ezy) + (ey0 - eyz) * (DY(k) / DZ(l))) / (XF(j) * DCOSE(k) + small_num);
-        lr[6] = (-(ex0 - exz) / (XBAR(j) * SINF(k) * DZ(l) + small_num) + (XF(j) * ez0 - XF(j - 1) * ezx) / (XC(j) * DX(j)));
-        lr[7] = (-(XF(j) * ey0 - XF(j - 1) * eyx) / (XC(j) * DX(j)) + (ex0 - exy) / (XBAR(j) * DY(k)));
-    }
+    lr[5] = lr_face_x(d, j, k, l, ez0, ezy, ey0, eyz);
+    lr[6] = lr_face_y(d, j, k, l, ex0, exz, ez0, ezx);
+    lr[7] = lr_face_z(d, j, k, l, ey0, eyx, ex0, exy);
     // rungekutta.f90:61-167
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        double un;
-        if (stage == 1) {
-            d.U0[i][c] = u[i];
-            un = u[i] + dt * lr[i];
-        } else if (stage == 2) {
-            un = rk20 * u0[i] + rk21 * u[i] + rk22 * dt * lr[i];
-        } else {
-            un = rk30 * u0[i] + rk31 * u[i] + rk32 * dt * lr[i];
-        }
-        d.U[i][c] = un;
+        if (stage == 1) d.U0[i][c] = u[i];
+        un[i] = rk_combine(stage, u[i], u0[i], dt, lr[i]);
     }
+}
+
+template <class FT>  // storage type of the hydro face fluxes (double, or float in the FP32 form)
+__global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
+    if (d.S->done) return;
+    // flat index over j,k,l = 0..n (x fastest)
+    const int ex = d.nx + 1, ey = d.ny + 1, ez = d.nz + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ex * ey * ez) return;
+    const int j = (int)(t % ex);
+    const long long r = t / ex;
+    const int k = (int)(r % ey);
+    const int l = (int)(r / ey);
+    const int c = cidx(d, j, k, l);
+    double un[8];
+    rk_cell<FT>(d, stage, j, k, l, c, un);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) d.U[i][c] = un[i];
 }
 
 // k_rk of the FP32 form on Cartesian grids without sources (GET_SOURCE and
@@ -596,27 +619,15 @@ __device__ __forceinline__ void apply_floor(const Dev &d, double &rho, double &v
     }
 }
 
+// One interior cell (j,k,l >= 1).  !INIT: from its new conserved state --
+// u_c the hydro part, bfx..bfz its own new face fields, ux_m..uz_m the new
+// fields of its lower faces; px_m..pz_m the lower faces' primitive fields
+// (used on the index-1 layers, whose lower face FROMUTORVE leaves alone).
 template <int INIT>
-__global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
-    if (d.S->done) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int l = blockIdx.z + 1;
-    if (j > d.nx || k > d.ny || l > d.nz) return;
-    const int c = cidx(d, j, k, l);
-    const int sy = d.NX, sz = d.NX * d.NY;
-    double rho, vx, vy, vz, e, bfx, bfy, bfz, bc[3];
-    // every load of the cell issued before any arithmetic (the kernel waits on
-    // memory, not on its few flops); the lower-face operands of FROMRVETOU are
-    // selected afterwards from loads of both candidates
-    double ux_m = 0.0, uy_m = 0.0, uz_m = 0.0, u_c[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const double px_m = d.P[5][c - 1], py_m = d.P[6][c - sy], pz_m = d.P[7][c - sz];
-    if (!INIT) {
-        bfx = d.U[5][c]; bfy = d.U[6][c]; bfz = d.U[7][c];
-        ux_m = d.U[5][c - 1]; uy_m = d.U[6][c - sy]; uz_m = d.U[7][c - sz];
-#pragma unroll
-        for (int i = 0; i < 5; ++i) u_c[i] = d.U[i][c];
-    }
+__device__ __forceinline__ void recover_cell(const Dev &d, int stage, int j, int k, int l, int c, const double *u_c,
+                                             double bfx, double bfy, double bfz, double ux_m, double uy_m,
+                                             double uz_m, double px_m, double py_m, double pz_m) {
+    double rho, vx, vy, vz, e, bc[3];
     if (!INIT) {
         cell_b(d, j, k, l, bfx, ux_m, bfy, uy_m, bfz, uz_m, bc);
         const double u0 = u_c[0];
@@ -693,6 +704,30 @@ __global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
     // guard: a state no later stage can recover from
     if (!(rho > 0.0) || !isfinite(e) || !isfinite(p) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz) || !isfinite(cs))
         set_error(d, CUMC_ESTATE, c, stage);
+}
+
+template <int INIT>
+__global__ void __launch_bounds__(256) k_recover(const Dev d, int stage) {
+    if (d.S->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int l = blockIdx.z + 1;
+    if (j > d.nx || k > d.ny || l > d.nz) return;
+    const int c = cidx(d, j, k, l);
+    const int sy = d.NX, sz = d.NX * d.NY;
+    double bfx = 0.0, bfy = 0.0, bfz = 0.0;
+    // every load of the cell issued before any arithmetic (the kernel waits on
+    // memory, not on its few flops); the lower-face operands of FROMRVETOU are
+    // selected afterwards from loads of both candidates
+    double ux_m = 0.0, uy_m = 0.0, uz_m = 0.0, u_c[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double px_m = d.P[5][c - 1], py_m = d.P[6][c - sy], pz_m = d.P[7][c - sz];
+    if (!INIT) {
+        bfx = d.U[5][c]; bfy = d.U[6][c]; bfz = d.U[7][c];
+        ux_m = d.U[5][c - 1]; uy_m = d.U[6][c - sy]; uz_m = d.U[7][c - sz];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) u_c[i] = d.U[i][c];
+    }
+    recover_cell<INIT>(d, stage, j, k, l, c, u_c, bfx, bfy, bfz, ux_m, uy_m, uz_m, px_m, py_m, pz_m);
 }
 
 // FROMRVETOU on the index-0 layer: cons face fields = prim face fields.  A

@@ -798,10 +798,14 @@ def star_sph(nr=96, ntheta=48, nphi=48, r_range=(2.0, 40.0), theta_range=(0.1 * 
     1 + asym * sin(theta) cos(phi) + 1% seeded noise), rho_atm outside;
     p = K rho^(5/3) with K = 1; v = 0, B = 0.  Returns (spec, prim, eps).
 
-    The default theta range keeps clear of the axis: with cells next to the
-    poles, whose phi-coefficients grow as 1/sin^2(theta), the reference's
-    over-relaxation factor 1.9 makes the red-black iteration diverge on
-    these grids (1.7 converges)."""
+    The default theta range keeps clear of the axis.  Pole to pole, the
+    rows of the cells next to the axis are strongly non-symmetric (the
+    cot(theta) d/dtheta term gives the outer theta neighbour a weight
+    2 / (r dtheta)^2 and the inner one about none) unless the phi coupling,
+    1 / (r sin(theta) dphi)^2, dominates them; with few phi cells it does
+    not, the Jacobi eigenvalues of the red-black splitting turn complex and
+    over-relaxation by 1.9 diverges (48 phi cells: diverges, 1.7 converges;
+    128 phi cells, the collapsar model's grid: 1.9 converges)."""
     g = 5.0 / 3.0
     full = theta_range[0] == 0.0 and theta_range[1] == math.pi
     spec = _base_spec(nr, ntheta, nphi, 3, (1, 1, 3 if full else 1, 3 if full else 1, 0, 0), r_range, theta_range,
@@ -844,6 +848,167 @@ def collapsar_sph(nr=96, ntheta=48, nphi=48, m_bh=0.2, c_code=20.0, v_in=0.02, r
     spec["m_bh"] = m_bh
     spec["c_code"] = c_code
     spec["name"] = "collapsar_sph_%dx%dx%d" % (nr, ntheta, nphi)
+    return spec, prim, np.ascontiguousarray(eps)
+
+
+# ---------------------------------------------------------------------------
+# the collapsar model from the progenitor files it ships
+# (model/collapsar/profile/: par.dat, hydro.dat, r_grid.dat, th_grid.dat,
+# phi_grid.dat)
+# ---------------------------------------------------------------------------
+COLLAPSAR_GRID = (156, 44, 128)   # the shipped grid files' cell counts (nx, ny, nz)
+
+
+def read_collapsar_profile(directory):
+    """The collapsar model's input files as GET_MODEL and CUSTOM_GRID read
+    them (model/collapsar/src/model.f90:44-90, custom.f90:78-150): par.dat's
+    five numbers (gamma, the black hole mass, the mass, length and time
+    conversions from cgs), hydro.dat's density and pressure for cells
+    -2..nx+3, and the r, theta, phi faces -3..n+3.  The cell counts follow
+    from the files (the reference checks them against its compiled nx, ny,
+    nz).  Returns a dict of numpy arrays."""
+    import os
+
+    from . import grids
+
+    def numbers(name):
+        with open(os.path.join(directory, name)) as f:
+            return [[float(t) for t in ln.split()] for ln in f.read().splitlines() if ln.strip()]
+    par = numbers("par.dat")[0]
+    hydro = np.array(numbers("hydro.dat"), dtype=np.float64)
+    n_r = len(numbers("r_grid.dat")) - 7
+    n_th = len(numbers("th_grid.dat")) - 7
+    n_ph = len(numbers("phi_grid.dat")) - 7
+    if hydro.shape != (n_r + 6, 2):
+        raise ValueError("inconsistent number of simulation grids: hydro.dat has %d lines, the r grid %d cells"
+                         % (hydro.shape[0], n_r))
+    xF, yF, zF = grids.load_grid(directory, n_r, n_th, n_ph, names=("r_grid.dat", "th_grid.dat", "phi_grid.dat"))
+    return dict(par=np.array(par[:5], dtype=np.float64), rho=hydro[:, 0].copy(), p=hydro[:, 1].copy(),
+                xF=xF, yF=yF, zF=zF)
+
+
+def collapsar_model(profile, recon="ppm", riemann="hlld", cfl=0.8, precision="fp64", seed=20261203,
+                    rotation_rule=2, w_0=10.0, b_0=1.0e10, v_crit=0.01, fixpole=1):
+    """GET_MODEL of the collapsar (model/collapsar/src/model.f90:6-253) with
+    the values of its param.h, from its shipped progenitor (profile = the
+    dict of read_collapsar_profile, or a directory holding the files).
+
+    Steps, in the reference's order:
+      * units from par.dat: vel2code = length / time, gauss2code =
+        (mass / length)^(1/2) / time; w_0 = 10 / time, b_0 = 1e10 gauss,
+        v_crit = 0.01 c (model.f90:44-65, param.h);
+      * rho and p of hydro.dat on every row of cells -2..nx+3, epsilon =
+        p / rho / (gamma - 1) over the whole padded grid (model.f90:86-99);
+      * the core radius s_core: the first cell centre j = 1..nx where the
+        density rises above that of cell nx (model.f90:106-112);
+      * differential rotation (rotation_rule 2, model.f90:145-167): v_phi =
+        w_0 s_core^2 / (s_core^2 + s^2) s, s = x(j) sin(y(k)), where the
+        density exceeds that of cell nx (rigid rotation, rule 1: v_crit / max
+        x times s);
+      * the field of A_phi = xF(j) sinf(k) / 2 on j, k, l = 0..n, curled onto
+        the faces 0..n (model.f90:176-194) and scaled by b_0 -- a uniform
+        field along the axis;
+      * the density of cells 1..n above that of cell nx perturbed by a
+        relative 1e-4 uniform noise, after epsilon was set (model.f90:
+        220-229; the reference's RANDOM_NUMBER stream is unseeded, this one
+        is PCG64(seed), drawn in the reference's loop order, l, k, j);
+      * the atmosphere prim_a = (rho, 0, 0, 0, p) of cell nx and its epsilon
+        (model.f90:239-242) set the floors.
+    A_phi outside 0..n (read by the curl at j = 0 and k = 0) is never set by
+    the reference; it is taken as zero here.
+    The run configuration is not shipped for this model (the solver's
+    parameter.h is set up for another one); the grid files fix a spherical
+    (r, theta, phi) grid of 156 x 44 x 128 cells over the whole sphere, so
+    the boundaries are outflow in r (with the model's radial-velocity clamps,
+    custom.f90:178-190), the polar axis in theta (with FIXPOLE, as make.inc
+    sets it) and periodic in phi; PPM + HLLD at CFL 0.8 as parameter.h ships
+    them.  Self-gravity (the Poisson solve) and the black hole (mass from
+    par.dat, r_sh = 2 m_bh / c^2) are the engine's collapsar source; the run
+    ends at 15 s (total_time = 15 tcgs2code).  Returns (spec, prim, eps)."""
+    if isinstance(profile, str):
+        if profile.endswith(".npz"):  # a recorded copy of the files (tests/golden/make_collapsar_profile.py)
+            with np.load(profile) as z:
+                profile = {k: z[k] for k in ("par", "rho", "p", "xF", "yF", "zF")}
+        else:
+            profile = read_collapsar_profile(profile)
+    ggas, m_bh, mass2code, length2code, t2code = (float(v) for v in profile["par"])
+    xF, yF, zF = (np.asarray(profile[k], dtype=np.float64) for k in ("xF", "yF", "zF"))
+    nx, ny, nz = xF.size - 7, yF.size - 7, zF.size - 7
+    clight = 2.99792458e10
+    vel2code = length2code / t2code
+    gauss2code = (mass2code / length2code) ** 0.5 / t2code
+    w0 = w_0 / t2code
+    b0 = b_0 * gauss2code
+    vcrit = v_crit * clight * vel2code
+    spec = _base_spec(nx, ny, nz, 3, (1, 1, 3, 3, 0, 0), (float(xF[3]), float(xF[-4])), (float(yF[3]), float(yF[-4])),
+                      (float(zF[3]), float(zF[-4])), coordinate_flag=2, cfl=cfl, recon=recon, riemann=riemann,
+                      precision=precision, fixpole=fixpole, name="collapsar_%dx%dx%d" % (nx, ny, nz))
+    spec["xF"], spec["yF"], spec["zF"] = xF.copy(), yF.copy(), zF.copy()
+    x, y = centers(xF), centers(yF)            # cells -2..n+3 at index j+2
+    dx = xF[1:] - xF[:-1]
+    sinf = np.sin(yF)                          # faces -3..n+3 at index k+3
+    if fixpole:  # getgrid.f90:91-98
+        sinf[3], sinf[3 + ny] = 0.0, 0.0
+    dcose = np.full(ny + 7, np.nan)
+    dcose[1:] = -(np.cos(yF[1:]) - np.cos(yF[:-1]))   # k = -2..ny+3 at index k+3 (k = -1.. used)
+    sine = np.sin(y)
+    rho_row, p_row = np.asarray(profile["rho"], dtype=np.float64), np.asarray(profile["p"], dtype=np.float64)
+    prim = np.zeros((nz + 6, ny + 6, nx + 6, 8), dtype=np.float64)
+    prim[..., IRHO] = rho_row[None, None, :]
+    prim[..., ITAU] = p_row[None, None, :]
+    eps = prim[..., ITAU] / prim[..., IRHO] / (ggas - 1.0)
+    rho_nx = rho_row[nx + 2]                  # prim(irho, nx, 1, 1)
+    s_core = None
+    for j in range(1, nx + 1):
+        if rho_row[j - 1 + 2] <= rho_nx and rho_row[j + 2] > rho_nx:
+            s_core = x[j + 2]
+            break
+    if s_core is None:
+        raise ValueError("the progenitor's density never rises above the atmosphere's")
+    inside = np.zeros((ny + 6, nx + 6), dtype=bool)
+    inside[3:ny + 3, 3:nx + 3] = rho_row[None, 3:nx + 3] > rho_nx
+    s_eq = x[None, :] * sine[:, None]
+    if rotation_rule == 1:
+        omega = vcrit / float(np.max(x))
+        vphi = omega * s_eq
+    else:
+        sc2 = s_core * s_core
+        vphi = w0 * sc2 / (sc2 + s_eq * s_eq) * s_eq
+    prim[3:nz + 3, :, :, IVZ] = np.where(inside, vphi, 0.0)[None]      # l = 1..nz
+    # A_phi on j, k = 0..n (zero elsewhere), the curl onto faces 0..n
+    a_phi = np.zeros((ny + 6, nx + 6))
+    a_phi[2:ny + 3, 2:nx + 3] = xF[None, 3:nx + 4] * sinf[3:ny + 4, None] * 0.5
+    tiny = np.finfo(np.float64).tiny
+    kk, jj = slice(2, ny + 3), slice(2, nx + 3)            # k, j = 0..n
+    km, jm = slice(1, ny + 2), slice(1, nx + 2)            # k-1, j-1
+    xf_j, xf_jm = xF[3:nx + 4], xF[2:nx + 3]               # xF(j), xF(j-1) for j = 0..nx
+    sinf_k, sinf_km = sinf[3:ny + 4], sinf[2:ny + 3]       # sinf(k), sinf(k-1)
+    bx = np.zeros((ny + 6, nx + 6))
+    by = np.zeros((ny + 6, nx + 6))
+    bx[kk, jj] = ((sinf_k[:, None] * a_phi[kk, jj] - sinf_km[:, None] * a_phi[km, jj])
+                  / (xf_j[None, :] * dcose[3:ny + 4, None] + tiny))
+    by[kk, jj] = -(xf_j[None, :] * a_phi[kk, jj] - xf_jm[None, :] * a_phi[kk, jm]) / (x[None, jj] * dx[None, jj])
+    prim[2:nz + 3, :, :, IBX] = (bx * b0)[None]                         # l = 0..nz
+    prim[2:nz + 3, :, :, IBY] = (by * b0)[None]
+    # the density perturbation, in the reference's loop order
+    rng = np.random.Generator(np.random.PCG64(seed))
+    for l in range(1, nz + 1):
+        for k in range(1, ny + 1):
+            row = prim[l + 2, k + 2, 3:nx + 3, IRHO]
+            sel = np.nonzero(row > rho_nx)[0]
+            if sel.size:
+                r = rng.random(sel.size)
+                row[sel] = row[sel] * (1.0 + 1.0e-4 * (r - 0.5) / 0.5)
+    p_a = p_row[nx + 2]
+    eps_a = p_a / rho_nx / (ggas - 1.0)
+    spec["model"] = dict(gamma=ggas, floor="collapsar", rho_floor=rho_nx, eps_floor=eps_a, source="collapsar",
+                         bc="torus_sph")
+    spec["rho_atm"] = rho_nx
+    spec["m_bh"] = m_bh
+    spec["c_code"] = clight * vel2code
+    spec["t_end"] = 15.0 * t2code
+    spec["s_core"] = s_core
+    spec["n_pot"] = 10
     return spec, prim, np.ascontiguousarray(eps)
 
 

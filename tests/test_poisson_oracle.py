@@ -84,9 +84,11 @@ def test_first_iteration_from_zero_is_not_converged():
 
 
 def test_cells_next_to_the_poles_need_less_over_relaxation():
-    """With theta running pole to pole, the reference's omega = 1.9 makes
-    the iteration diverge on this grid and 1.7 converges; clear of the axis
-    1.9 converges (recorded because the collapsar model uses 1.9)."""
+    """With theta running pole to pole on a grid with few phi cells, the
+    reference's omega = 1.9 makes the iteration diverge and 1.7 converges;
+    clear of the axis 1.9 converges, and so it does pole to pole once the
+    phi coupling dominates the axis cells' non-symmetric theta rows (the
+    collapsar model's 128 phi cells, test_collapsar_model)."""
     spec, prim, _ = models.star_sph(24, 16, 12, theta_range=(0.0, math.pi))
     rho = prim[3:-3, 3:-3, 3:-3, 0]
     _, _, _, c19 = O.poisson_solve(spec, rho, spec["rho_atm"], omega=1.9, tol=1e-12, max_iter=3000)
@@ -95,3 +97,11 @@ def test_cells_next_to_the_poles_need_less_over_relaxation():
     spec, rho = star()
     _, _, _, c = O.poisson_solve(spec, rho, spec["rho_atm"], omega=1.9, tol=1e-12, max_iter=3000)
     assert c
+    # pole to pole, 1.9 contracts once the phi cells are fine (96 x 44 x 128)
+    spec, prim, _ = models.star_sph(96, 44, 128, theta_range=(0.0, math.pi))
+    rho = prim[3:-3, 3:-3, 3:-3, 0]
+    phi, errs = None, []
+    for _ in range(3):
+        phi, _, err, _ = O.poisson_solve(spec, rho, spec["rho_atm"], omega=1.9, tol=1e-12, max_iter=100, phi=phi)
+        errs.append(err)
+    assert errs[0] > errs[1] > errs[2]
