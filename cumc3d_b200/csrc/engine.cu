@@ -982,6 +982,9 @@ struct cumc_handle {
     cudaStream_t snap_stream = nullptr;
     cudaEvent_t snap_packed = nullptr, snap_done = nullptr;
     bool snap_pending = false;
+    // tensor maps of the TMA-staged reconstruction, per sweep direction
+    TmaMaps tma[3];
+    bool tma_ok = false;
     // positivity-fallback counter (cumc_fallback_count)
     unsigned long long *fb_dev = nullptr;
     unsigned long long fb_host[1] = {0};
@@ -1119,6 +1122,45 @@ static void grid_dims(const Dev &d, dim3 &g, dim3 &b, int j0, int jn, int k0, in
     g = dim3((nj + b.x - 1) / b.x, (nk + b.y - 1) / b.y, nl);
 }
 
+// Tensor maps of the TMA-staged reconstruction (k_recon_tma): for each sweep
+// direction the seven staged arrays as 3D FP64 tensors over the padded grid
+// (x fastest), box 36 x 8 x 1 (x sweep), 34 x 12 x 1 (y) or 34 x 1 x 12 (z),
+// no swizzle, zeros outside.  The encoder comes from the driver at run time
+// (cudaGetDriverEntryPoint), so the library does not link libcuda.  Needs the
+// row pitch NX * 8 bytes to be a multiple of 16 (NX even); otherwise, or if
+// the encoder is missing, the TMA candidate stays unavailable.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static void setup_tma(cumc_handle *h) {
+    h->tma_ok = false;
+    const Dev &d = h->d;
+    if ((d.NX & 1) || d.n_dim < 1) return;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        return;
+    }
+    EncodeTiledFn enc = (EncodeTiledFn)fn;
+    const cuuint64_t dims[3] = {(cuuint64_t)d.NX, (cuuint64_t)d.NY, (cuuint64_t)d.NZ};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.NX * 8, (cuuint64_t)d.NX * d.NY * 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    for (int dir = 0; dir < 3; ++dir) {
+        const cuuint32_t box[3] = {dir == 0 ? 36u : 34u, dir == 0 ? 8u : (dir == 1 ? 12u : 1u), dir == 2 ? 12u : 1u};
+        const int tb1 = (dir == 0) ? 1 : 0, tb2 = (dir == 2) ? 1 : 2;
+        for (int v = 0; v < 7; ++v) {
+            double *base = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
+            if (enc(&h->tma[dir].m[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return;
+        }
+    }
+    h->tma_ok = true;
+}
+
 static void default_flux_blocks(cumc_handle *h) {
     const Dev &d = h->d;
     // x: TS cells along x per tile, rows of k per block
@@ -1149,7 +1191,7 @@ static void launch_flux(cumc_handle *h, int dir, int stage = 1, cudaStream_t st 
     }
     if (h->flux_mode == 1) {
         if (h->cfg.precision == CUMC_FP32) launch_split_fp32(d, dir, h->cfg.recon, h->cfg.riemann, st);
-        else launch_split_fp64(d, dir, h->cfg.recon, h->cfg.riemann, st);
+        else launch_split_fp64(d, dir, h->cfg.recon, h->cfg.riemann, st, h->tma_ok ? h->tma : nullptr);
         h->launches += 2;
         return;
     }
@@ -1546,6 +1588,13 @@ int cumc_create(const cumc_config *cfg, cumc_handle **out) {
     if (dv) h->allocs.push_back(dv);
     h->divb_dev = (unsigned long long *)dv;
     ok = ok && cudaMallocHost((void **)&h->S_host, sizeof(Scalars)) == cudaSuccess;
+    {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        d.num_sms = nsm;
+    }
+    if (ok) setup_tma(h);
     if (cfg->learned) {
         // parameters, per-tile fallback flags, audit counters (the path stays
         // off until cumc_learn_set supplies parameters)
@@ -1838,18 +1887,23 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
         {1, 256, 128, 1, 1}, {1, 256, 128, 4, 1}, {1, 256, 128, 1, 2}, {1, 256, 128, 4, 2},
         {1, 256, 128, 5, 1}, {1, 256, 128, 6, 1}, {1, 256, 128, 5, 2}, {1, 256, 128, 6, 2},
     };
-    const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
+    static const Cand tma_cands[] = {{1, 256, 128, 1, 3}, {1, 256, 128, 4, 3}, {1, 256, 128, 5, 3}, {1, 256, 128, 6, 3}};
+    std::vector<Cand> all(cands, cands + sizeof(cands) / sizeof(cands[0]));
+    // the TMA-staged reconstruction: FP64 plain form, even padded x extent
+    if (h->tma_ok && h->cfg.precision == CUMC_FP64 && !h->d.learned)
+        all.insert(all.end(), tma_cands, tma_cands + sizeof(tma_cands) / sizeof(tma_cands[0]));
+    const int nc = (int)all.size();
     double best = 1e300;
     int bi = 0;
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     for (int i = 0; i < nc; ++i) {
-        h->flux_mode = cands[i].mode;
-        h->d.tpb_recon = cands[i].tpb_recon;
-        h->d.tpb_riemann = cands[i].tpb_riemann;
-        h->d.riemann_minb = cands[i].minb;
-        h->d.recon_tile = cands[i].tile;
+        h->flux_mode = all[i].mode;
+        h->d.tpb_recon = all[i].tpb_recon;
+        h->d.tpb_riemann = all[i].tpb_riemann;
+        h->d.riemann_minb = all[i].minb;
+        h->d.recon_tile = all[i].tile;
         // with the learned flag, stage 1 of a refresh step also runs the flag
         // network, the same work for every candidate; stage 2 times the
         // kernels the candidates differ in, as every non-refresh stage runs them
@@ -1868,18 +1922,18 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    h->flux_mode = cands[bi].mode;
-    h->d.tpb_recon = cands[bi].tpb_recon;
-    h->d.tpb_riemann = cands[bi].tpb_riemann;
-    h->d.riemann_minb = cands[bi].minb;
-    h->d.recon_tile = cands[bi].tile;
+    h->flux_mode = all[bi].mode;
+    h->d.tpb_recon = all[bi].tpb_recon;
+    h->d.tpb_riemann = all[bi].tpb_riemann;
+    h->d.riemann_minb = all[bi].minb;
+    h->d.recon_tile = all[bi].tile;
     // a captured step holds the old launch shapes
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
     if (choice_out) {
-        choice_out[0] = cands[bi].mode; choice_out[1] = cands[bi].tpb_recon;
-        choice_out[2] = cands[bi].tpb_riemann; choice_out[3] = cands[bi].minb;
-        choice_out[4] = cands[bi].tile;
+        choice_out[0] = all[bi].mode; choice_out[1] = all[bi].tpb_recon;
+        choice_out[2] = all[bi].tpb_riemann; choice_out[3] = all[bi].minb;
+        choice_out[4] = all[bi].tile;
     }
     if (best_ms_out) *best_ms_out = best;
     return CUMC_OK;
@@ -1889,8 +1943,11 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
     if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 256 || (choice[1] & 31) ||
         choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4 && choice[3] != 5 && choice[3] != 6) ||
-        choice[4] < 0 || choice[4] > 2)
+        choice[4] < 0 || choice[4] > 3)
         return fail(h, CUMC_EINVAL, "tuning out of range");
+    if (choice[4] == 3 && !(h->tma_ok && h->cfg.precision == CUMC_FP64 && !h->d.learned && choice[0] == 1))
+        return fail(h, CUMC_EINVAL,
+                    "TMA-staged reconstruction (recon_tile 3) needs the split FP64 plain form and an even padded x extent");
     h->d.recon_tile = choice[4];
     h->flux_mode = choice[0];
     h->d.tpb_recon = choice[1];

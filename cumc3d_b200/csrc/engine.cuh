@@ -7,10 +7,18 @@
 // (j+2) + NX*((k+2) + NY*(l+2)), the padded extents of the reference's
 // arrays (solver/mhd/setup.f90:348-375).
 #pragma once
+#include <cuda.h>  // CUtensorMap (the type only; the encoder is fetched at run time)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace cumc {
+
+// tensor maps of the seven arrays the reconstruction of one sweep stages (the
+// five hydro primitives, the two transverse cell fields), for the TMA-staged
+// reconstruction (recon_tile.cuh, k_recon_tma)
+struct TmaMaps {
+    CUtensorMap m[7];
+};
 
 // device-resident scalars of the time loop (solver/mhd/main.f90:98-116)
 struct Scalars {
@@ -99,7 +107,7 @@ __device__ __forceinline__ int cidx(const Dev &d, int j, int k, int l) {
 // host-side launchers of the face-flux kernels (one per precision unit)
 void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
 void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
-void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
+void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s, const TmaMaps *tma = nullptr);
 void launch_split_fp32(const Dev &d, int dir, int rec, int rs, cudaStream_t s);
 void launch_split_learned_fp32(const Dev &d, int dir, int rs, int stage, cudaStream_t s);
 void launch_split_learned_fp64(const Dev &d, int dir, int rs, int stage, cudaStream_t s);

@@ -7,8 +7,8 @@ namespace cumc {
 void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s) {
     launch_flux_t<double>(d, dir, rec, rs, grid, block, smem, s);
 }
-void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s) {
-    launch_split_t<double>(d, dir, rec, rs, s);
+void launch_split_fp64(const Dev &d, int dir, int rec, int rs, cudaStream_t s, const TmaMaps *tma) {
+    launch_split_t<double>(d, dir, rec, rs, s, tma);
 }
 
 // FP64 WENO with the learned flag: the network (FP32 unit) sets the flags on

@@ -402,12 +402,48 @@ static void launch_riemann_m(const Dev &d, int rs, dim3 g, dim3 b, cudaStream_t 
         default: k_riemann<T, DIR, RS_HLLD, MINB><<<g, b, 0, s>>>(d); break;
     }
 }
+// the TMA-staged reconstruction: persistent CTAs, as many as fit on the GPU
+template <int DIR, int REC, int UNI>
+static void launch_recon_tma_r(const Dev &d, const TmaMaps &tm, cudaStream_t s) {
+    static int per_sm = 0;  // resident CTAs per SM of this instantiation
+    if (per_sm == 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_recon_tma<DIR, REC, UNI>, 256, TmaBox<DIR>::SMEM) !=
+                cudaSuccess || n < 1)
+            n = 1;
+        per_sm = n;
+    }
+    const dim3 tg = recon_tile_grid(d, DIR, 1);
+    const long long ntiles = (long long)tg.x * tg.y * tg.z;
+    long long nblk = (long long)d.num_sms * per_sm;
+    if (nblk > ntiles) nblk = ntiles;
+    k_recon_tma<DIR, REC, UNI><<<(unsigned)nblk, dim3(32, 8, 1), TmaBox<DIR>::SMEM, s>>>(d, tm);
+}
+template <int DIR, int UNI>
+static void launch_recon_tma(const Dev &d, int rec, const TmaMaps &tm, cudaStream_t s) {
+    switch (rec) {
+        case REC_TVD_MM: launch_recon_tma_r<DIR, REC_TVD_MM, UNI>(d, tm, s); break;
+        case REC_TVD_VL: launch_recon_tma_r<DIR, REC_TVD_VL, UNI>(d, tm, s); break;
+        case REC_TVD_MC: launch_recon_tma_r<DIR, REC_TVD_MC, UNI>(d, tm, s); break;
+        case REC_PPM: launch_recon_tma_r<DIR, REC_PPM, UNI>(d, tm, s); break;
+        default: launch_recon_tma_r<DIR, REC_WENO, UNI>(d, tm, s); break;
+    }
+}
+
 template <class T, int DIR>
-static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s) {
+static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s, const TmaMaps *tma = nullptr) {
     dim3 g, b;
     split_dims(d, DIR, true, g, b);
-    if (d.wuni[DIR]) launch_recon_u<T, DIR, 1>(d, rec, g, b, s);
-    else launch_recon_u<T, DIR, 0>(d, rec, g, b, s);
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (d.recon_tile == 3 && tma) {
+            if (d.wuni[DIR]) launch_recon_tma<DIR, 1>(d, rec, *tma, s);
+            else launch_recon_tma<DIR, 0>(d, rec, *tma, s);
+        } else if (d.wuni[DIR]) launch_recon_u<T, DIR, 1>(d, rec, g, b, s);
+        else launch_recon_u<T, DIR, 0>(d, rec, g, b, s);
+    } else {
+        if (d.wuni[DIR]) launch_recon_u<T, DIR, 1>(d, rec, g, b, s);
+        else launch_recon_u<T, DIR, 0>(d, rec, g, b, s);
+    }
     split_dims(d, DIR, false, g, b);
     switch (d.riemann_minb) {
         case 4: launch_riemann_m<T, DIR, 4>(d, rs, g, b, s); break;
@@ -417,10 +453,10 @@ static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s) {
     }
 }
 template <class T>
-static void launch_split_t(const Dev &d, int dir, int rec, int rs, cudaStream_t s) {
-    if (dir == 0) launch_split_dir<T, 0>(d, rec, rs, s);
-    else if (dir == 1) launch_split_dir<T, 1>(d, rec, rs, s);
-    else launch_split_dir<T, 2>(d, rec, rs, s);
+static void launch_split_t(const Dev &d, int dir, int rec, int rs, cudaStream_t s, const TmaMaps *tma = nullptr) {
+    if (dir == 0) launch_split_dir<T, 0>(d, rec, rs, s, tma ? tma + 0 : nullptr);
+    else if (dir == 1) launch_split_dir<T, 1>(d, rec, rs, s, tma ? tma + 1 : nullptr);
+    else launch_split_dir<T, 2>(d, rec, rs, s, tma ? tma + 2 : nullptr);
 }
 
 template <class T, int DIR, int REC, int RS>

@@ -10,6 +10,7 @@
 // H = 2 for the 5-point stencils (PPM, WENO), 1 for TVD.  CPT (cells per
 // thread, 1 or 2) trades halo overhead for registers; the autotuner picks.
 #pragma once
+#include "../../include/cumc3d_gpu.h"
 #include "engine.cuh"
 #include "mhd_device.cuh"
 
@@ -94,6 +95,90 @@ __global__ void __launch_bounds__(256) k_learned_warps(const Dev d, int stage) {
     }
 }
 
+// The reconstruction of the cells of one staged tile (block coordinates bx,
+// by, bz of recon_tile_grid).  The tile lies in shared memory as 7 slots of
+// SLOT elements, each SR rows of SX values; the stencil of the cell in row r,
+// lane tx sits at column tx + HO + m (x sweep) or row r + HO + m, column
+// tx + XO (y, z sweeps), m = -H..H.
+template <class T, int DIR, int REC, int UNI, int CPT, int LRN, int SX, int SLOT, int HO, int XO>
+__device__ __forceinline__ void recon_tile_cells(const Dev &d, const T *__restrict__ s, int bx, int by, int bz, int tx,
+                                                 int ty) {
+    constexpr int TX = 32, TY = 8;
+    constexpr int H = (REC == REC_PPM || REC == REC_WENO) ? 2 : 1;
+    constexpr int NR = TY * CPT;
+    const int c0 = (DIR == 0) ? bx * TX : by * NR;  // first reconstructed cell
+    T *const *QL = reinterpret_cast<T *const *>(d.QL);
+    T *const *QR = reinterpret_cast<T *const *>(d.QR);
+    const int st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+        const int r = ty + TY * i;  // row within the tile
+        int c, j, k, l, ns;
+        bool valid;
+        if (DIR == 0) {
+            c = c0 + tx; j = c; k = by * NR + r + 1; l = bz + 1; ns = d.nx;
+            valid = c <= d.nx + 1 && k <= d.ny;
+        } else if (DIR == 1) {
+            c = c0 + r; k = c; j = bx * TX + tx + 1; l = bz + 1; ns = d.ny;
+            valid = j <= d.nx && c <= d.ny + 1;
+        } else {
+            c = c0 + r; l = c; j = bx * TX + tx + 1; k = bz + 1; ns = d.nz;
+            valid = j <= d.nx && c <= d.nz + 1;
+        }
+        bool linear = false;
+        if (LRN) {
+            // the warp's decision, made once per refresh by k_learned_warps;
+            // audit steps reconstruct with WENO-Z everywhere
+            const bool row = (DIR == 0) ? k <= d.ny : (DIR == 1) ? c <= d.ny + 1 : c <= d.nz + 1;
+            const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
+            if (row && !audit) linear = d.lwarp[DIR][learned_warp<DIR>(d, bx, DIR == 0 ? k : c, DIR == 2 ? k : l)] != 0;
+        }
+        if (!valid) continue;
+        const int ci = cidx(d, j, k, l);
+        T w[14];
+        constexpr int NW = (REC == REC_PPM) ? 14 : (REC == REC_WENO) ? 10 : 2;
+        if (UNI) {
+#pragma unroll
+            for (int m = 0; m < NW; ++m) w[m] = uni_w<T>(d, DIR, m);
+        } else {
+            const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
+#pragma unroll
+            for (int m = 0; m < NW; ++m) w[m] = wp[m];
+        }
+        T vm_rho = T(0), vp_rho = T(0);
+        bool fallback = false;
+#pragma unroll
+        for (int v = 0; v < 7; ++v) {
+            // the stencil c-H .. c+H of variable v
+            auto at = [&](int m) -> T {
+                return (DIR == 0) ? s[v * SLOT + r * SX + tx + HO + m] : s[v * SLOT + (r + HO + m) * SX + tx + XO];
+            };
+            T a0 = T(0), a4 = T(0);
+            if (H == 2) { a0 = at(-2); a4 = at(2); }
+            const T a1 = at(-1), a2 = at(0), a3 = at(1);
+            T vm, vp;
+            if (LRN && linear) weno_linear<T>(w, a0, a1, a2, a3, a4, vm, vp);
+            else recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
+            if (v == 0) { vm_rho = vm; vp_rho = vp; }
+            if (v == 4 && d.pos_fallback) {
+                fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
+                if (fallback && d.fb_count) atomicAdd(d.fb_count, 1ull);
+                if (fallback) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const T cv = (DIR == 0) ? s[u * SLOT + r * SX + tx + HO] : s[u * SLOT + (r + HO) * SX + tx + XO];
+                        if (c <= ns) QL[u][ci] = cv;
+                        if (c >= 1) QR[u][ci - st] = cv;
+                    }
+                }
+            }
+            if (fallback) vm = vp = a2;
+            if (c <= ns) QL[v][ci] = vp;      // left state of face c
+            if (c >= 1) QR[v][ci - st] = vm;  // right state of face c-1
+        }
+    }
+}
+
 template <class T, int DIR, int REC, int UNI, int CPT, int LRN = 0>
 __global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) {
     if (d.S->done) return;
@@ -103,7 +188,7 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) 
     constexpr int NR = TY * CPT;                    // rows of reconstructed cells
     constexpr int SX = (DIR == 0) ? TX + 2 * H : TX;  // staged row length
     constexpr int SR = (DIR == 0) ? NR : NR + 2 * H;  // staged rows
-    __shared__ T s[7][SR][SX];
+    __shared__ T s[7 * SR * SX];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * TX + tx;
     constexpr int tb1 = (DIR == 0) ? 1 : 0;
@@ -130,80 +215,134 @@ __global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) 
 #pragma unroll
             for (int v = 0; v < 7; ++v) {
                 const double *src = (v < 5) ? d.P[v] : d.BC[v == 5 ? tb1 : tb2];
-                s[v][sr][sx] = (T)__ldg(src + ci);
+                s[v * SR * SX + sr * SX + sx] = (T)__ldg(src + ci);
             }
         }
     }
     __syncthreads();
+    recon_tile_cells<T, DIR, REC, UNI, CPT, LRN, SX, SR * SX, H, 0>(d, s, blockIdx.x, blockIdx.y, blockIdx.z, tx, ty);
+}
 
-    // ---- reconstruct CPT cells per thread ----
-    T *const *QL = reinterpret_cast<T *const *>(d.QL);
-    T *const *QR = reinterpret_cast<T *const *>(d.QR);
-    const int st = (DIR == 0) ? 1 : (DIR == 1) ? d.NX : d.NX * d.NY;
+// ---------------------------------------------------------------------------
+// The same reconstruction with the tiles staged by the tensor memory
+// accelerator (FP64 form, one cell per thread): persistent CTAs walk the
+// tiles of recon_tile_grid; while a CTA reconstructs one tile from shared
+// memory, TMA loads the next into the other buffer (cp.async.bulk.tensor,
+// one 3D box per staged array, completion on an mbarrier).  The tensor maps
+// (TmaMaps, one per staged array: the five hydro primitives and the two
+// transverse cell fields of the sweep) cover this GPU's own state arrays;
+// no multicast.  Boxes start on even x (16-byte aligned): the x sweep loads
+// cells c0-2 .. c0+33 whatever the stencil's halo, the y and z sweeps cells
+// 32 bx .. 32 bx + 33 (one column before the tile's first).  Cells outside
+// the padded grid come back as zeros and are never used.  A wait that does
+// not complete within a bound sets the device error word and the CTA skips
+// the tile, then waits (bounded) for its copies still in flight before
+// exiting.
+// ---------------------------------------------------------------------------
+template <int DIR>
+struct TmaBox {
+    static constexpr int SX = (DIR == 0) ? 36 : 34;          // box x extent
+    static constexpr int SR = (DIR == 0) ? 8 : 12;           // box rows (y for DIR 0, 1; z for DIR 2)
+    static constexpr int BYTES = SX * SR * 8;                // one array's box
+    static constexpr int SLOT = ((BYTES + 127) / 128) * 128 / 8;  // doubles per 128-byte aligned slot
+    static constexpr int SMEM = 2 * 7 * SLOT * 8 + 128;      // two buffers of seven slots, 128-byte aligned
+};
+
+__device__ __forceinline__ unsigned tma_smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned phase) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(bar), "r"(phase)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int DIR>
+__device__ __forceinline__ void tma_issue(const TmaMaps &maps, double *buf, unsigned bar, int bx, int by, int bz) {
+    using B = TmaBox<DIR>;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(7 * B::BYTES) : "memory");
+    int x, y, z;  // padded indices of the box's first element
+    if (DIR == 0) { x = bx * 32; y = by * 8 + 3; z = bz + 3; }
+    else if (DIR == 1) { x = bx * 32 + 2; y = by * 8; z = bz + 3; }
+    else { x = bx * 32 + 2; y = bz + 3; z = by * 8; }
 #pragma unroll
-    for (int i = 0; i < CPT; ++i) {
-        const int r = ty + TY * i;  // row within the tile
-        int c, j, k, l, ns;
-        bool valid;
-        if (DIR == 0) {
-            c = c0 + tx; j = c; k = blockIdx.y * NR + r + 1; l = blockIdx.z + 1; ns = d.nx;
-            valid = c <= d.nx + 1 && k <= d.ny;
-        } else if (DIR == 1) {
-            c = c0 + r; k = c; j = blockIdx.x * TX + tx + 1; l = blockIdx.z + 1; ns = d.ny;
-            valid = j <= d.nx && c <= d.ny + 1;
-        } else {
-            c = c0 + r; l = c; j = blockIdx.x * TX + tx + 1; k = blockIdx.z + 1; ns = d.nz;
-            valid = j <= d.nx && c <= d.nz + 1;
+    for (int v = 0; v < 7; ++v) {
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+                tma_smem_addr(buf + v * B::SLOT)),
+            "l"(reinterpret_cast<unsigned long long>(&maps.m[v])), "r"(x), "r"(y), "r"(z), "r"(bar)
+            : "memory");
+    }
+}
+
+template <int DIR, int REC, int UNI>
+__global__ void __launch_bounds__(256) k_recon_tma(const Dev d, const __grid_constant__ TmaMaps maps) {
+    if (d.S->done) return;
+    using B = TmaBox<DIR>;
+    extern __shared__ __align__(16) unsigned char tma_raw[];
+    // TMA destinations must start on 128-byte boundaries
+    double *const tma_smem = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(tma_raw) + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) unsigned long long bar[2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const dim3 tg = recon_tile_grid(d, DIR, 1);
+    const long long ntiles = (long long)tg.x * tg.y * tg.z;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tma_smem_addr(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tma_smem_addr(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    auto coords = [&](long long t, int &bx, int &by, int &bz) {
+        bx = (int)(t % tg.x);
+        const long long rest = t / tg.x;
+        by = (int)(rest % tg.y);
+        bz = (int)(rest / tg.y);
+    };
+    unsigned phase[2] = {0u, 0u};
+    int issued[2] = {0, 0};  // copies issued into each buffer and not yet waited for (thread 0)
+    long long t = blockIdx.x;
+    if (t < ntiles && tid == 0) {
+        int bx, by, bz;
+        coords(t, bx, by, bz);
+        tma_issue<DIR>(maps, tma_smem, tma_smem_addr(&bar[0]), bx, by, bz);
+        issued[0] = 1;
+    }
+    bool failed = false;
+    for (int i = 0; t < ntiles; ++i, t += gridDim.x) {
+        const int b = i & 1;
+        const long long tn = t + gridDim.x;
+        if (tn < ntiles && tid == 0 && !failed) {  // the next tile into the other buffer
+            int bx, by, bz;
+            coords(tn, bx, by, bz);
+            tma_issue<DIR>(maps, tma_smem + (b ^ 1) * 7 * B::SLOT, tma_smem_addr(&bar[b ^ 1]), bx, by, bz);
+            issued[b ^ 1] = 1;
         }
-        bool linear = false;
-        if (LRN) {
-            // the warp's decision, made once per refresh by k_learned_warps;
-            // audit steps reconstruct with WENO-Z everywhere
-            const bool row = (DIR == 0) ? k <= d.ny : (DIR == 1) ? c <= d.ny + 1 : c <= d.nz + 1;
-            const bool audit = d.audit_interval > 0 && (d.S->steps % d.audit_interval) == 0;
-            if (row && !audit) linear = d.lwarp[DIR][learned_warp<DIR>(d, blockIdx.x, DIR == 0 ? k : c, DIR == 2 ? k : l)] != 0;
+        const bool ok = !failed && mbar_wait_bounded(tma_smem_addr(&bar[b]), phase[b]);
+        if (ok) {
+            phase[b] ^= 1u;
+            if (tid == 0) issued[b] = 0;
+        } else if (!failed) {
+            failed = true;
+            if (atomicCAS(&d.S->err_code, 0, CUMC_ECUDA) == 0) d.S->err_stage = 100 + DIR;
         }
-        if (!valid) continue;
-        const int ci = cidx(d, j, k, l);
-        T w[14];
-        constexpr int NW = (REC == REC_PPM) ? 14 : (REC == REC_WENO) ? 10 : 2;
-        if (UNI) {
-#pragma unroll
-            for (int m = 0; m < NW; ++m) w[m] = uni_w<T>(d, DIR, m);
-        } else {
-            const T *wp = weights<T>(d, DIR) + (size_t)(c + 2) * 14;
-#pragma unroll
-            for (int m = 0; m < NW; ++m) w[m] = wp[m];
+        if (ok) {
+            int bx, by, bz;
+            coords(t, bx, by, bz);
+            recon_tile_cells<double, DIR, REC, UNI, 1, 0, B::SX, B::SLOT, 2, (DIR == 0) ? 0 : 1>(
+                d, tma_smem + b * 7 * B::SLOT, bx, by, bz, tx, ty);
         }
-        T vm_rho = T(0), vp_rho = T(0);
-        bool fallback = false;
-#pragma unroll
-        for (int v = 0; v < 7; ++v) {
-            // the stencil c-H .. c+H of variable v
-            auto at = [&](int m) -> T { return (DIR == 0) ? s[v][r][tx + H + m] : s[v][r + H + m][tx]; };
-            T a0 = T(0), a4 = T(0);
-            if (H == 2) { a0 = at(-2); a4 = at(2); }
-            const T a1 = at(-1), a2 = at(0), a3 = at(1);
-            T vm, vp;
-            if (LRN && linear) weno_linear<T>(w, a0, a1, a2, a3, a4, vm, vp);
-            else recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
-            if (v == 0) { vm_rho = vm; vp_rho = vp; }
-            if (v == 4 && d.pos_fallback) {
-                fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
-                if (fallback && d.fb_count) atomicAdd(d.fb_count, 1ull);
-                if (fallback) {
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const T cv = (DIR == 0) ? s[u][r][tx + H] : s[u][r + H][tx];
-                        if (c <= ns) QL[u][ci] = cv;
-                        if (c >= 1) QR[u][ci - st] = cv;
-                    }
-                }
-            }
-            if (fallback) vm = vp = a2;
-            if (c <= ns) QL[v][ci] = vp;      // left state of face c
-            if (c >= 1) QR[v][ci - st] = vm;  // right state of face c-1
-        }
+        __syncthreads();  // every thread is done with buffer b before it is refilled
+    }
+    // copies still in flight after a failed wait: wait for them (bounded)
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b)
+            if (issued[b]) mbar_wait_bounded(tma_smem_addr(&bar[b]), phase[b]);
     }
 }
 

@@ -920,7 +920,7 @@ def collapsar_model(profile, recon="ppm", riemann="hlld", cfl=0.8, precision="fp
     parameter.h is set up for another one); the grid files fix a spherical
     (r, theta, phi) grid of 156 x 44 x 128 cells over the whole sphere, so
     the boundaries are outflow in r (with the model's radial-velocity clamps,
-    custom.f90:178-190), the polar axis in theta (with FIXPOLE, as make.inc
+    custom.f90:160-190), the polar axis in theta (with FIXPOLE, as make.inc
     sets it) and periodic in phi; PPM + HLLD at CFL 0.8 as parameter.h ships
     them.  Self-gravity (the Poisson solve) and the black hole (mass from
     par.dat, r_sh = 2 m_bh / c^2) are the engine's collapsar source; the run

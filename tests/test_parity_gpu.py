@@ -188,6 +188,7 @@ def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=1, recon_tile=1),
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=2),
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=6, recon_tile=1),
+    dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=3),
 ])
 @pytest.mark.parametrize("recon", ["weno", "ppm", "tvdmc"])
 def test_every_launch_shape_is_bitwise_identical(oracle_mod, tuning, recon):
@@ -298,3 +299,41 @@ def test_torus_benchmark_config_at_96x64x96_bitwise(oracle_mod):
     assert dg == do
     assert_bitwise(g, o, spec)
     assert_bitwise(g, o, spec, what=("cons",))
+
+
+def test_tma_staged_reconstruction_on_the_headline_blast(oracle_mod):
+    """The TMA-staged, persistent reconstruction (recon_tile 3) on the bench's
+    blast at 64^3 (tiles that wrap the persistent grid several times, boxes
+    that reach past the padded grid): bit for bit the oracle's; and refused
+    where the padded x extent is odd (its rows are not 16-byte multiples)."""
+    from cumc3d_b200.engine import CumcError, Solver
+    spec, prim, eps = models.blast_3d(64)
+    spec["positivity_fallback"] = 1
+    spec["fix_periodic_normal_faces"] = 1
+    g = Solver(spec)
+    g.set_state(prim, eps)
+    g.initial_update()
+    g.set_tuning(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=3)
+    tg, kg = g.evolve(1e30, 4)
+    o = oracle_mod.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    to = 0.0
+    for _ in range(4):
+        dt = o.finddt()
+        o.rk3_step(dt)
+        to += dt
+    assert tg == to
+    pg, eg = g.get_state()
+    po, eo = o.get_state()
+    assert np.array_equal(interior(pg, spec), interior(po, spec))
+    assert np.array_equal(interior(eg, spec), interior(eo, spec))
+    g.close()
+    o.close()
+    spec, prim, eps = models.smooth_state(21, 12, 10, 3, recon="weno", riemann="hlld", seed=2)
+    g = Solver(spec)
+    g.set_state(prim, eps)
+    g.initial_update()
+    with pytest.raises(CumcError):
+        g.set_tuning(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=3)
+    g.close()
