@@ -230,6 +230,14 @@ int cumc_fallback_count(cumc_handle *h, int enable, unsigned long long *count_ou
  * normal inputs; *mismatches counts differing bit patterns. */
 int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example);
 
+/* Numerics self-check (no counterpart in the reference): compares the
+ * shared-divisor quotient of the Riemann solver (one reciprocal per divisor,
+ * two FMA corrections per quotient) with the IEEE FP64 division on n seeded
+ * random pairs over the whole exponent range, zeros, infinities and NaNs
+ * included; mismatches = pairs whose bits differ, example2 = the first such
+ * (numerator, divisor). */
+int cumc_check_shared_div(unsigned long long seed, long long n, unsigned long long *mismatches, double *example2);
+
 /* Measured FP64 fused-multiply-add throughput of the current device in
  * TFLOP/s (the denominator of the FP64-pipe roofline). */
 int cumc_fp64_peak(double *tflops);
