@@ -1927,6 +1927,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
         {1, 256, 64, 1, 0},  {1, 128, 64, 4, 0},  {0, 256, 128, 1, 0},
         {1, 256, 128, 1, 1}, {1, 256, 128, 4, 1}, {1, 256, 128, 1, 2}, {1, 256, 128, 4, 2},
         {1, 256, 128, 5, 1}, {1, 256, 128, 6, 1}, {1, 256, 128, 5, 2}, {1, 256, 128, 6, 2},
+        {1, 256, 128, 4, 4}, {1, 256, 128, 5, 4}, {1, 256, 128, 6, 4},
     };
     static const Cand tma_cands[] = {{1, 256, 128, 1, 3}, {1, 256, 128, 4, 3}, {1, 256, 128, 5, 3}, {1, 256, 128, 6, 3}};
     std::vector<Cand> all(cands, cands + sizeof(cands) / sizeof(cands[0]));
@@ -1984,7 +1985,7 @@ int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
     if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 256 || (choice[1] & 31) ||
         choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4 && choice[3] != 5 && choice[3] != 6) ||
-        choice[4] < 0 || choice[4] > 3)
+        choice[4] < 0 || choice[4] > 4)
         return fail(h, CUMC_EINVAL, "tuning out of range");
     if (choice[4] == 3 && !(h->tma_ok && h->cfg.precision == CUMC_FP64 && !h->d.learned && choice[0] == 1))
         return fail(h, CUMC_EINVAL,

@@ -362,20 +362,24 @@ static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &
 #include "recon_tile.cuh"
 namespace cumc {
 
-template <class T, int DIR, int UNI, int CPT>
+template <class T, int DIR, int UNI, int CPT, int MINB = 1>
 static void launch_recon_tile_c(const Dev &d, int rec, cudaStream_t s) {
     const dim3 g = recon_tile_grid(d, DIR, CPT), b(32, 8, 1);
     switch (rec) {
-        case REC_TVD_MM: k_recon_tile<T, DIR, REC_TVD_MM, UNI, CPT><<<g, b, 0, s>>>(d); break;
-        case REC_TVD_VL: k_recon_tile<T, DIR, REC_TVD_VL, UNI, CPT><<<g, b, 0, s>>>(d); break;
-        case REC_TVD_MC: k_recon_tile<T, DIR, REC_TVD_MC, UNI, CPT><<<g, b, 0, s>>>(d); break;
-        case REC_PPM: k_recon_tile<T, DIR, REC_PPM, UNI, CPT><<<g, b, 0, s>>>(d); break;
-        default: k_recon_tile<T, DIR, REC_WENO, UNI, CPT><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_MM: k_recon_tile<T, DIR, REC_TVD_MM, UNI, CPT, 0, MINB><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_VL: k_recon_tile<T, DIR, REC_TVD_VL, UNI, CPT, 0, MINB><<<g, b, 0, s>>>(d); break;
+        case REC_TVD_MC: k_recon_tile<T, DIR, REC_TVD_MC, UNI, CPT, 0, MINB><<<g, b, 0, s>>>(d); break;
+        case REC_PPM: k_recon_tile<T, DIR, REC_PPM, UNI, CPT, 0, MINB><<<g, b, 0, s>>>(d); break;
+        default: k_recon_tile<T, DIR, REC_WENO, UNI, CPT, 0, MINB><<<g, b, 0, s>>>(d); break;
     }
 }
+// recon_tile: 1, 2 staged tiles with 1 or 2 cells per thread; 4 one cell per
+// thread at 64 registers (4 blocks per SM); 3 (TMA-staged) falls back to 1
+// where no tensor maps are given
 template <class T, int DIR, int UNI>
 static void launch_recon_tile(const Dev &d, int rec, cudaStream_t s) {
     if (d.recon_tile == 2) launch_recon_tile_c<T, DIR, UNI, 2>(d, rec, s);
+    else if (d.recon_tile == 4) launch_recon_tile_c<T, DIR, UNI, 1, 4>(d, rec, s);
     else launch_recon_tile_c<T, DIR, UNI, 1>(d, rec, s);
 }
 

@@ -179,8 +179,11 @@ __device__ __forceinline__ void recon_tile_cells(const Dev &d, const T *__restri
     }
 }
 
-template <class T, int DIR, int REC, int UNI, int CPT, int LRN = 0>
-__global__ void __launch_bounds__(256) k_recon_tile(const Dev d, int stage = 0) {
+// MINB: blocks per SM the register budget is sized for (1: the compiler's
+// choice, about 76 registers for FP64 WENO-Z; 4: 64 registers, a third more
+// resident warps)
+template <class T, int DIR, int REC, int UNI, int CPT, int LRN = 0, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_recon_tile(const Dev d, int stage = 0) {
     if (d.S->done) return;
     if (LRN == 1 && learned_refresh_stage(d, stage)) return;  // the network kernel reconstructs this stage
     constexpr int TX = 32, TY = 8;

@@ -202,8 +202,10 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
  * keeps the fastest for all later steps.  choice_out[0..4] = (split?, recon
  * threads/block, Riemann threads/block, Riemann min blocks/SM (1, 4, 5, 6), staged
  * reconstruction: 0 = per-cell loads, 1 or 2 = stencils staged in shared
- * memory with that many cells per thread); best_ms_out = the flux time of
- * one stage with that choice.  Either pointer may be NULL. */
+ * memory with that many cells per thread, 3 = tiles staged by TMA
+ * (persistent, double-buffered; FP64 plain form with an even padded x
+ * extent), 4 = as 1 at 64 registers per thread); best_ms_out = the flux time
+ * of one stage with that choice.  Either pointer may be NULL. */
 int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out);
 
 /* Set the launch shape by hand, same five integers as choice_out above. */
