@@ -905,47 +905,6 @@ __global__ void k_div3_check(unsigned long long seed, long long n, unsigned long
     if (bad) atomicAdd(mismatch, bad);
 }
 
-// Self-check of the shared-divisor quotient (dvs) against the IEEE division:
-// random numerators and divisors over the whole exponent range -- normal,
-// subnormal, zero, infinite and NaN ones among them -- every bit compared
-// (two NaNs count as equal).
-__global__ void k_shared_div_check(unsigned long long seed, long long n, unsigned long long *mismatch, double *example) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    unsigned long long bad = 0;
-    auto mix = [](unsigned long long z) {
-        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-        return z ^ (z >> 31);
-    };
-    auto pick = [](unsigned long long z) {
-        // one in 16: a special value; else any biased exponent 0..2047
-        const unsigned sel = (unsigned)(z & 15u);
-        unsigned long long bits = z & 0x800FFFFFFFFFFFFFull;
-        if (sel == 0) bits &= 0x8000000000000000ull;                      // +-0
-        else if (sel == 1) bits |= 0x7FF0000000000000ull & ~0ull;          // inf or NaN
-        else bits |= ((z >> 4) % 2048ull) << 52;
-        return __longlong_as_double((long long)bits);
-    };
-    for (; i < n; i += stride) {
-        const unsigned long long z1 = mix(seed + (unsigned long long)i * 0x9E3779B97F4A7C15ull);
-        const unsigned long long z2 = mix(z1 ^ 0xD1B54A32D192ED03ull);
-        const double x = pick(z1);
-        // divisors mostly near the numerator's scale (the solver's case), some anywhere
-        double b = pick(z2);
-        if ((z2 >> 60) < 12) b = __longlong_as_double((long long)(((unsigned long long)__double_as_longlong(x) &
-                                                                   0x7FF0000000000000ull) ^ (z2 & 0x800FFFFFFFFFFFFFull)));
-        const double ref = x / b;
-        const double got = dvs<double>(x, divisor<double>(b));
-        const bool same = __double_as_longlong(ref) == __double_as_longlong(got) || (isnan(ref) && isnan(got));
-        if (!same) {
-            if (bad == 0) { example[0] = x; example[1] = b; }
-            ++bad;
-        }
-    }
-    if (bad) atomicAdd(mismatch, bad);
-}
-
 // FP64 pipe probe: independent DFMA chains, 8 per thread, no memory traffic
 __global__ void k_dfma_probe(double *out, int iters) {
     double a[8];
@@ -1928,6 +1887,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
         {1, 256, 128, 1, 1}, {1, 256, 128, 4, 1}, {1, 256, 128, 1, 2}, {1, 256, 128, 4, 2},
         {1, 256, 128, 5, 1}, {1, 256, 128, 6, 1}, {1, 256, 128, 5, 2}, {1, 256, 128, 6, 2},
         {1, 256, 128, 4, 4}, {1, 256, 128, 5, 4}, {1, 256, 128, 6, 4},
+        {1, 256, 128, 14, 1}, {1, 256, 128, 15, 1}, {1, 256, 128, 16, 1}, {1, 256, 128, 15, 4},
     };
     static const Cand tma_cands[] = {{1, 256, 128, 1, 3}, {1, 256, 128, 4, 3}, {1, 256, 128, 5, 3}, {1, 256, 128, 6, 3}};
     std::vector<Cand> all(cands, cands + sizeof(cands) / sizeof(cands[0]));
@@ -1984,7 +1944,7 @@ int cumc_autotune(cumc_handle *h, int *choice_out, double *best_ms_out) {
 int cumc_set_tuning(cumc_handle *h, const int *choice) {
     if (!h || !choice) return fail(h, CUMC_EINVAL, "null argument");
     if (choice[0] < 0 || choice[0] > 1 || choice[1] < 32 || choice[1] > 256 || (choice[1] & 31) ||
-        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4 && choice[3] != 5 && choice[3] != 6) ||
+        choice[2] < 32 || choice[2] > 128 || (choice[2] & 31) || (choice[3] != 1 && choice[3] != 4 && choice[3] != 5 && choice[3] != 6 && (choice[3] < 14 || choice[3] > 16)) ||
         choice[4] < 0 || choice[4] > 4)
         return fail(h, CUMC_EINVAL, "tuning out of range");
     if (choice[4] == 3 && !(h->tma_ok && h->cfg.precision == CUMC_FP64 && !h->d.learned && choice[0] == 1))
@@ -2699,22 +2659,6 @@ int cumc_learn_harvest(cumc_handle *h, int dir, long long stride, float *out, lo
     cudaFree(dbuf);
     if (e != cudaSuccess) return fail(h, CUMC_ECUDA, std::string("harvest: ") + cudaGetErrorString(e));
     return CUMC_OK;
-}
-
-int cumc_check_shared_div(unsigned long long seed, long long n, unsigned long long *mismatches, double *example2) {
-    if (!mismatches || !example2) return CUMC_EINVAL;
-    unsigned long long *m = nullptr;
-    double *ex = nullptr;
-    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, 2 * sizeof(*ex)) != cudaSuccess) return CUMC_ECUDA;
-    cudaMemset(m, 0, sizeof(*m));
-    cudaMemset(ex, 0, 2 * sizeof(*ex));
-    k_shared_div_check<<<148 * 16, 256>>>(seed, n, m, ex);
-    cudaError_t e = cudaDeviceSynchronize();
-    cudaMemcpy(mismatches, m, sizeof(*m), cudaMemcpyDeviceToHost);
-    cudaMemcpy(example2, ex, 2 * sizeof(*ex), cudaMemcpyDeviceToHost);
-    cudaFree(m);
-    cudaFree(ex);
-    return e == cudaSuccess ? CUMC_OK : CUMC_ECUDA;
 }
 
 int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example) {

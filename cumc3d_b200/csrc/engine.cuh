@@ -47,7 +47,8 @@ struct Dev {
     int fixn;               // carry periodic normal faces
     int pos_fallback;       // first-order fallback for non-positive edge rho/p
     int tpb_recon, tpb_riemann;  // threads per block of the split flux kernels (autotuned)
-    int riemann_minb;            // blocks/SM the Riemann kernel is compiled for (1, 4, 5, 6; autotuned)
+    int riemann_minb;            // blocks/SM the Riemann kernel is compiled for (1, 4, 5, 6; 14, 15, 16:
+                                 // the prefetching kernel at 4, 5, 6; autotuned)
     int recon_tile;              // 0: per-cell stencil loads; 1, 2: staged tiles, cells per thread (autotuned)
     int wuni[3];                 // 1: the axis's reconstruction weights are identical in every cell
     double wu[3][14];            // those weights (FP64 form)

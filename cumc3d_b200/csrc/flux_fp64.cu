@@ -32,6 +32,9 @@ static void launch_learned64_dir(const Dev &d, int rs, int stage, cudaStream_t s
         case 4: launch_riemann_m<double, DIR, 4>(d, rs, g, b, s); break;
         case 5: launch_riemann_m<double, DIR, 5>(d, rs, g, b, s); break;
         case 6: launch_riemann_m<double, DIR, 6>(d, rs, g, b, s); break;
+        case 14: launch_riemann_pf<double, DIR, 4>(d, rs, s); break;
+        case 15: launch_riemann_pf<double, DIR, 5>(d, rs, s); break;
+        case 16: launch_riemann_pf<double, DIR, 6>(d, rs, s); break;
         default: launch_riemann_m<double, DIR, 1>(d, rs, g, b, s); break;
     }
 }

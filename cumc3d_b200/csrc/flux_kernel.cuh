@@ -344,6 +344,99 @@ __global__ void __launch_bounds__(128, MINB) k_riemann(const Dev d) {
     }
 }
 
+// The Riemann kernel with its loads taken off the critical path: CTAs of 128
+// threads walk the faces of the sweep with a grid stride, and while a thread
+// solves one face, asynchronous copies (cp.async, no registers held) bring
+// the fourteen face states and the normal field of its next face into its
+// own shared-memory slots; the solve then reads them from shared memory.
+// Same faces, same arithmetic as k_riemann: the same bits.
+__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, int bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+template <class T, int DIR, int RS, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_riemann_pf(const Dev d) {
+    if (d.S->done) return;
+    __shared__ T qb[2][14][128];
+    __shared__ double bb[2][128];
+    const int tid = threadIdx.x;
+    const int ex = (DIR == 0) ? d.nx + 1 : d.nx;
+    const int ey = (DIR == 1) ? d.ny + 1 : d.ny;
+    const int ez = (DIR == 2) ? d.nz + 1 : d.nz;
+    const long long total = (long long)ex * ey * ez;
+    const long long stride = (long long)gridDim.x * 128;
+    using F = Frame<DIR>;
+    constexpr int tb1 = (DIR == 0) ? 1 : 0;
+    constexpr int tb2 = (DIR == 2) ? 1 : 2;
+    const T *const *QL = reinterpret_cast<const T *const *>(d.QL);
+    const T *const *QR = reinterpret_cast<const T *const *>(d.QR);
+    auto face_index = [&](long long t) {
+        const int a = (int)(t % ex);
+        const long long r = t / ex;
+        const int b = (int)(r % ey);
+        const int e = (int)(r / ey);
+        if (DIR == 0) return cidx(d, a, b + 1, e + 1);
+        if (DIR == 1) return cidx(d, a + 1, b, e + 1);
+        return cidx(d, a + 1, b + 1, e);
+    };
+    auto issue = [&](long long t, int buf) {
+        if (t < total) {
+            const int ci = face_index(t);
+#pragma unroll
+            for (int v = 0; v < 7; ++v) {
+                cp_async_elem(&qb[buf][v][tid], QL[v] + ci, (int)sizeof(T));
+                cp_async_elem(&qb[buf][7 + v][tid], QR[v] + ci, (int)sizeof(T));
+            }
+            cp_async_elem(&bb[buf][tid], d.P[F::ibn - 1] + ci, 8);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    long long t = (long long)blockIdx.x * 128 + tid;
+    issue(t, 0);
+    for (int i = 0; t < total; ++i, t += stride) {
+        issue(t + stride, (i + 1) & 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        const int b = i & 1;
+        const int ci = face_index(t);
+        T pl[9], pr[9];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            pl[1 + v] = qb[b][v][tid];
+            pr[1 + v] = qb[b][7 + v][tid];
+        }
+        pl[ibx + tb1] = qb[b][5][tid];
+        pr[ibx + tb1] = qb[b][12][tid];
+        pl[ibx + tb2] = qb[b][6][tid];
+        pr[ibx + tb2] = qb[b][13][tid];
+        const T bn = (T)bb[b][tid];
+        pl[F::ibn] = bn;
+        pr[F::ibn] = bn;
+        const T g = (T)d.gamma;
+        const T epsL = eos_eps(pl[irho], pl[itau], g);
+        const T epsR = eos_eps(pr[irho], pr[itau], g);
+        const T csL = eos_cs(pl[itau], pl[irho], epsL, g);
+        const T csR = eos_cs(pr[itau], pr[irho], epsR, g);
+        T fo[9];
+        riemann_face<T, DIR, RS>(pl, pr, epsL, epsR, csL, csR, fo);
+        double *const *FO = (DIR == 0) ? d.FX : (DIR == 1) ? d.FY : d.FZ;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) store_flux<T>(FO[v], ci, fo[1 + v]);
+        if (DIR == 0) {
+            d.EF[e_yx][ci] = (double)fo[ibz];
+            d.EF[e_zx][ci] = -(double)fo[iby];
+        } else if (DIR == 1) {
+            d.EF[e_xy][ci] = -(double)fo[ibz];
+            d.EF[e_zy][ci] = (double)fo[ibx];
+        } else {
+            d.EF[e_xz][ci] = (double)fo[iby];
+            d.EF[e_yz][ci] = -(double)fo[ibx];
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // launch geometry of the split kernels: a flat 1D grid over the cells (or
 // faces) of one sweep
 static inline void split_dims(const Dev &d, int dir, bool recon, dim3 &g, dim3 &b) {
@@ -395,6 +488,22 @@ static void launch_recon_u(const Dev &d, int rec, dim3 g, dim3 b, cudaStream_t s
         case REC_TVD_MC: k_recon<T, DIR, REC_TVD_MC, UNI><<<g, b, 0, s>>>(d); break;
         case REC_PPM: k_recon<T, DIR, REC_PPM, UNI><<<g, b, 0, s>>>(d); break;
         default: k_recon<T, DIR, REC_WENO, UNI><<<g, b, 0, s>>>(d); break;
+    }
+}
+// riemann_minb 14, 15, 16: the prefetching kernel at 4, 5, 6 blocks per SM
+template <class T, int DIR, int MINB>
+static void launch_riemann_pf(const Dev &d, int rs, cudaStream_t s) {
+    const long long total = (long long)((DIR == 0) ? d.nx + 1 : d.nx) * ((DIR == 1) ? d.ny + 1 : d.ny) *
+                            ((DIR == 2) ? d.nz + 1 : d.nz);
+    long long nblk = (long long)d.num_sms * MINB * 2;
+    const long long need = (total + 127) / 128;
+    if (nblk > need) nblk = need;
+    const dim3 g((unsigned)nblk), b(128);
+    switch (rs) {
+        case RS_LF: k_riemann_pf<T, DIR, RS_LF, MINB><<<g, b, 0, s>>>(d); break;
+        case RS_HLL: k_riemann_pf<T, DIR, RS_HLL, MINB><<<g, b, 0, s>>>(d); break;
+        case RS_HLLC: k_riemann_pf<T, DIR, RS_HLLC, MINB><<<g, b, 0, s>>>(d); break;
+        default: k_riemann_pf<T, DIR, RS_HLLD, MINB><<<g, b, 0, s>>>(d); break;
     }
 }
 template <class T, int DIR, int MINB>
@@ -453,6 +562,9 @@ static void launch_split_dir(const Dev &d, int rec, int rs, cudaStream_t s, cons
         case 4: launch_riemann_m<T, DIR, 4>(d, rs, g, b, s); break;
         case 5: launch_riemann_m<T, DIR, 5>(d, rs, g, b, s); break;
         case 6: launch_riemann_m<T, DIR, 6>(d, rs, g, b, s); break;
+        case 14: launch_riemann_pf<T, DIR, 4>(d, rs, s); break;
+        case 15: launch_riemann_pf<T, DIR, 5>(d, rs, s); break;
+        case 16: launch_riemann_pf<T, DIR, 6>(d, rs, s); break;
         default: launch_riemann_m<T, DIR, 1>(d, rs, g, b, s); break;
     }
 }

@@ -48,39 +48,6 @@ template <> __device__ __forceinline__ double dv<double>(double x, double y) {
     return z ? __longlong_as_double((long long)zb) : q;
 }
 
-// Quotients that share a divisor b, each equal to the IEEE quotient x / b bit
-// for bit.  The reciprocal y = RN(1/b) costs one IEEE division for the whole
-// group; each quotient is then q0 = RN(x y) refined twice by Markstein's
-// correction q' = RN(q + r y) with the residual r = x - b q exact through one
-// FMA.  q0 is within a few ulps of x / b, so q1 = RN(q0 + r0 y) is within one
-// ulp of it, and for y within half an ulp of 1/b and q within one ulp,
-// RN(q + r y) is the correctly rounded quotient (Markstein 1990; Muller et
-// al., Handbook of Floating-Point Arithmetic, section on Newton-Raphson-based
-// division with an FMA).  The theorem needs no overflow or underflow: the
-// fast path takes x and b with exponents within 2^-500 .. 2^500 (so x / b,
-// the products and the residuals stay normal) and a zero x (the signed zero
-// sign(x) sign(b)); anything else goes through dv.  Five FP64 operations per
-// quotient instead of a division's sequence, and a shorter dependency chain.
-// FP32 divides directly.
-template <class T> struct Divisor { T b, y; };
-template <class T> __device__ __forceinline__ Divisor<T> divisor(T b) { return Divisor<T>{b, T(0)}; }
-template <> __device__ __forceinline__ Divisor<double> divisor<double>(double b) { return Divisor<double>{b, 1.0 / b}; }
-template <class T> __device__ __forceinline__ T dvs(T x, const Divisor<T> &D) { return x / D.b; }
-template <> __device__ __forceinline__ double dvs<double>(double x, const Divisor<double> &D) {
-    const unsigned long long xb = (unsigned long long)__double_as_longlong(x);
-    const unsigned long long bb = (unsigned long long)__double_as_longlong(D.b);
-    const unsigned ex = (unsigned)(xb >> 52) & 0x7FFu, eb = (unsigned)(bb >> 52) & 0x7FFu;
-    const bool b_ok = (eb - 523u) <= 1000u;  // biased exponents 523..1523: |b| in 2^-500 .. 2^501
-    const bool x_zero = (xb << 1) == 0ull;
-    if (b_ok && x_zero) return __longlong_as_double((long long)((xb ^ bb) & 0x8000000000000000ull));
-    if (b_ok && (ex - 523u) <= 1000u) {
-        const double q0 = __dmul_rn(x, D.y);
-        const double q1 = __fma_rn(__fma_rn(-D.b, q0, x), D.y, q0);
-        return __fma_rn(__fma_rn(-D.b, q1, x), D.y, q1);
-    }
-    return dv(x, D.b);
-}
-
 // Fortran SIGN(1, x)
 template <class T> __device__ __forceinline__ T sign1(T x);
 template <> __device__ __forceinline__ double sign1<double>(double x) { return copysign(1.0, x); }
@@ -532,16 +499,14 @@ __device__ __forceinline__ void hlld_lean(const T *pl, const T *pr, T epsL, T ep
     constexpr int ivn = F::ivn, ivt1 = F::ivt1, ivt2 = F::ivt2, ibn = F::ibn, ibt1 = F::ibt1, ibt2 = F::ibt2;
     T usL[9], usR[9], pstL[9], pstR[9];
     T sM = sstar_hllc(pLt, pRt, pl[irho], pr[irho], pl[ivn], pr[ivn], sL, sR, pl[ibn], pr[ibn]);
-    // the star states' eight quotients by sL - sM (and by sR - sM) share a divisor
-    const Divisor<T> DL = divisor(sL - sM), DR = divisor(sR - sM);
     {
         T ul[9], ur[9];
         cons_state<T>(pl, epsL, ul);
         cons_state<T>(pr, epsR, ur);
 #pragma unroll
-        for (int i = irho; i <= itau; ++i) usL[i] = dvs(ul[i] * (sL - pl[ivn]), DL);
+        for (int i = irho; i <= itau; ++i) usL[i] = dv(ul[i] * (sL - pl[ivn]), sL - sM);
 #pragma unroll
-        for (int i = irho; i <= itau; ++i) usR[i] = dvs(ur[i] * (sR - pr[ivn]), DR);
+        for (int i = irho; i <= itau; ++i) usR[i] = dv(ur[i] * (sR - pr[ivn]), sR - sM);
     }
     T sstarL = sM - dv(dabs(pl[ibn]), dsqrt(usL[irho]));
     T sstarR = sM + dv(dabs(pr[ibn]), dsqrt(usR[irho]));
@@ -567,11 +532,11 @@ __device__ __forceinline__ void hlld_lean(const T *pl, const T *pr, T epsL, T ep
         usR[ibt2] = dv(pr[ibt2] * (pr[irho] * (sR - pr[ivn]) * (sR - pr[ivn]) - pr[ibn] * pr[ibn]), fac_1);
     }
     usL[ivn] = usL[irho] * sM;
-    usL[ivt1] = usL[ivt1] - dvs(usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1], DL);
-    usL[ivt2] = usL[ivt2] - dvs(usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2], DL);
+    usL[ivt1] = usL[ivt1] - dv(usL[ibn] * usL[ibt1] - pl[ibn] * pl[ibt1], sL - sM);
+    usL[ivt2] = usL[ivt2] - dv(usL[ibn] * usL[ibt2] - pl[ibn] * pl[ibt2], sL - sM);
     usR[ivn] = usR[irho] * sM;
-    usR[ivt1] = usR[ivt1] - dvs(usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1], DR);
-    usR[ivt2] = usR[ivt2] - dvs(usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2], DR);
+    usR[ivt1] = usR[ivt1] - dv(usR[ibn] * usR[ibt1] - pr[ibn] * pr[ibt1], sR - sM);
+    usR[ivt2] = usR[ivt2] - dv(usR[ibn] * usR[ibt2] - pr[ibn] * pr[ibt2], sR - sM);
     pstL[ivn] = sM;
     pstL[ivt1] = dv(usL[ivt1], usL[irho]);
     pstL[ivt2] = dv(usL[ivt2], usL[irho]);
@@ -582,10 +547,10 @@ __device__ __forceinline__ void hlld_lean(const T *pl, const T *pr, T epsL, T ep
     T pRs = pr[irho] * (sR - pr[ivn]) * (sM - pr[ivn]) + pRt;
     T bdotu = pl[ibx] * pl[ivx] + pl[iby] * pl[ivy] + pl[ibz] * pl[ivz];
     T bdotus = usL[ibx] * pstL[ivx] + usL[iby] * pstL[ivy] + usL[ibz] * pstL[ivz];
-    usL[itau] = usL[itau] + dvs((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn], DL);
+    usL[itau] = usL[itau] + dv((pLs * sM - pLt * pl[ivn]) - (bdotus - bdotu) * pl[ibn], sL - sM);
     bdotu = pr[ibx] * pr[ivx] + pr[iby] * pr[ivy] + pr[ibz] * pr[ivz];
     bdotus = usR[ibx] * pstR[ivx] + usR[iby] * pstR[ivy] + usR[ibz] * pstR[ivz];
-    usR[itau] = usR[itau] + dvs((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn], DR);
+    usR[itau] = usR[itau] + dv((pRs * sM - pRt * pr[ivn]) - (bdotus - bdotu) * pr[ibn], sR - sM);
     // the side whose fan the face lies in; its flux and state are rebuilt here
     const bool left = (sstarL >= T(0)) || !(sstarR <= T(0)) && (sM >= T(0));
     const T *pS = left ? pl : pr;

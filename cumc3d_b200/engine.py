@@ -21,7 +21,7 @@ EXPORTS = [
     "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
-    "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_fallback_count", "cumc_check_div3", "cumc_check_shared_div",
+    "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_fallback_count", "cumc_check_div3",
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_run1_noalloc",
@@ -78,7 +78,6 @@ def load_library(path=None):
     L.cumc_set_concurrent_sweeps.argtypes = [C.c_void_p, C.c_int]
     L.cumc_fallback_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)]
     L.cumc_check_div3.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
-    L.cumc_check_shared_div.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
     L.cumc_batch_create.argtypes = [C.POINTER(capi.CumcBatchConfig), C.POINTER(C.c_void_p)]
@@ -554,17 +553,6 @@ def fp64_peak_tflops():
     if rc != 0:
         raise CumcError(rc, "fp64 peak probe failed")
     return v.value
-
-
-def check_shared_div(seed, n):
-    """(mismatches, (numerator, divisor) of the first) of the shared-divisor
-    quotient against the IEEE division over n seeded random pairs."""
-    m = C.c_ulonglong()
-    ex = (C.c_double * 2)()
-    rc = load_library().cumc_check_shared_div(seed, n, C.byref(m), ex)
-    if rc != 0:
-        raise CumcError(rc, "cumc_check_shared_div failed")
-    return m.value, (ex[0], ex[1])
 
 
 def check_div3(seed, n):

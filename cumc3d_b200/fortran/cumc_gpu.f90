@@ -314,12 +314,6 @@ INTERFACE
     INTEGER(C_INT), VALUE :: enable
     INTEGER(C_LONG_LONG), INTENT(OUT) :: count_out
   END FUNCTION
-  INTEGER(C_INT) FUNCTION cumc_check_shared_div(seed, n, mismatches, example2) BIND(C, NAME='cumc_check_shared_div')
-    IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
-    INTEGER(C_LONG_LONG), VALUE :: seed, n
-    INTEGER(C_LONG_LONG), INTENT(OUT) :: mismatches
-    REAL(C_DOUBLE), INTENT(OUT) :: example2(2)
-  END FUNCTION
   INTEGER(C_INT) FUNCTION cumc_check_div3(seed, n, mismatches, example) BIND(C, NAME='cumc_check_div3')
     IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
     INTEGER(C_LONG_LONG), VALUE :: seed, n

@@ -200,7 +200,9 @@ int cumc_profile_step(cumc_handle *h, int nsteps, double *ms_out, int n_out);
  * shapes of the face-flux kernels (fused or split recon/Riemann, threads per
  * block, register budget of the Riemann kernel) on the handle's live state and
  * keeps the fastest for all later steps.  choice_out[0..4] = (split?, recon
- * threads/block, Riemann threads/block, Riemann min blocks/SM (1, 4, 5, 6), staged
+ * threads/block, Riemann threads/block, Riemann min blocks/SM (1, 4, 5, 6; 14,
+ * 15, 16 = the kernel that prefetches its next face's states into shared
+ * memory with asynchronous copies, at 4, 5, 6 blocks/SM), staged
  * reconstruction: 0 = per-cell loads, 1 or 2 = stencils staged in shared
  * memory with that many cells per thread, 3 = tiles staged by TMA
  * (persistent, double-buffered; FP64 plain form with an even padded x
@@ -231,14 +233,6 @@ int cumc_fallback_count(cumc_handle *h, int enable, unsigned long long *count_ou
  * engine's FMA-corrected division by 3 with the IEEE quotient on n generated
  * normal inputs; *mismatches counts differing bit patterns. */
 int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example);
-
-/* Numerics self-check (no counterpart in the reference): compares the
- * shared-divisor quotient of the Riemann solver (one reciprocal per divisor,
- * two FMA corrections per quotient) with the IEEE FP64 division on n seeded
- * random pairs over the whole exponent range, zeros, infinities and NaNs
- * included; mismatches = pairs whose bits differ, example2 = the first such
- * (numerator, divisor). */
-int cumc_check_shared_div(unsigned long long seed, long long n, unsigned long long *mismatches, double *example2);
 
 /* Measured FP64 fused-multiply-add throughput of the current device in
  * TFLOP/s (the denominator of the FP64-pipe roofline). */

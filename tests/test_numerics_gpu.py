@@ -16,13 +16,3 @@ def test_fma_corrected_div3_equals_ieee_division():
         total += 1 << 30
     assert total == 1 << 32
 
-
-def test_shared_divisor_quotient_equals_ieee_division():
-    """The HLLD star states' quotients by sL - sM and sR - sM
-    (rsolver_module.f90:628-633, 676-690, 699-703) share one reciprocal per
-    divisor and refine x * RN(1/b) twice with FMA residuals; every quotient
-    must equal x / b bit for bit, over the whole exponent range with zeros,
-    subnormals, infinities and NaNs among the operands."""
-    for seed in (11, 12, 13, 14):
-        bad, ex = engine.check_shared_div(seed * 0x9E3779B1, 1 << 28)
-        assert bad == 0, "shared-divisor quotient differs from x / b for (x, b) = %r" % (ex,)

@@ -190,6 +190,8 @@ def test_blast_100to1_with_positivity_fallback_bitwise(oracle_mod):
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=6, recon_tile=1),
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=4, recon_tile=3),
     dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=5, recon_tile=4),
+    dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=15, recon_tile=1),
+    dict(split=True, tpb_recon=256, tpb_riemann=128, riemann_min_blocks=14, recon_tile=4),
 ])
 @pytest.mark.parametrize("recon", ["weno", "ppm", "tvdmc"])
 def test_every_launch_shape_is_bitwise_identical(oracle_mod, tuning, recon):
