@@ -527,6 +527,83 @@ def bench_poisson(args, world, rank, local, dist):
     return 0
 
 
+def bench_collapsar(args, world, rank, local, dist):
+    """The collapsar model from its shipped progenitor (156 x 44 x 128,
+    spherical, PPM + HLLD, CFL 0.8; tests/golden/collapsar_profile.npz holds
+    the files' values): INITIAL_UPDATE, the initial potential (red-black SOR
+    from phi = 0 to 1e-10 at omega 1.9), then K host-driven steps (FINDDT,
+    RUNGEKUTTA with the floors, the self-gravity + black hole source and the
+    hole's growth) with the potential re-solved every n_pot = 10 steps from
+    the last one, as main.f90 and CUSTOM_UPDATE do.  Metric: zone-updates/s
+    of the run with its re-solves; device time (CUDA events on the engine
+    stream) around the K steps."""
+    import torch
+
+    from cumc3d_b200 import engine, models
+    spec, prim, eps = models.collapsar_model(os.path.join(ROOT, "tests", "golden", "collapsar_profile.npz"))
+    zones = spec["nx"] * spec["ny"] * spec["nz"]
+    s = engine.Solver(spec)
+    s.set_state(prim, eps)
+    s.initial_update()
+    s.autotune()
+    s.poisson_setup(spec["rho_atm"], 1.9)
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    it0, err0, conv0 = s.poisson_solve(100000, 1e-10)
+    e1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    initial = {"iterations": it0, "final_error": err0, "converged": conv0, "ms": e0.elapsed_time(e1)}
+    s.collapsar_set(spec["m_bh"], spec["c_code"])
+    n_pot = spec["n_pot"]
+    n_step = 0
+
+    def step():
+        nonlocal n_step
+        s.rungekutta(s.finddt())
+        resolves = 0
+        if n_step % n_pot == 0:  # CUSTOM_UPDATE at p_in = 3
+            s.poisson_solve(100000, 1e-10)
+            resolves = 1
+        n_step += 1
+        return resolves
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = s.launch_count()
+    e0.record(stream)
+    resolves = sum(step() for _ in range(args.steps))
+    e1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = s.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    m_bh, r_sh = s.collapsar_get()
+    divb = s.find_divb()
+    s.close()
+    if rank == 0:
+        line = {
+            "metric": "zone-updates/s", "value": zones * args.steps / (ms * 1e-3), "unit": "zone-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data":
+                "the reference's shipped collapsar progenitor (model/collapsar/profile)",
+            "config": {"workload": "collapsar_156x44x128_shipped_progenitor_ppm_hlld_ct_cfl0.8",
+                       "n_pot": n_pot, "omega": 1.9, "tolerance": 1e-10,
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "results": {"initial_potential_solve": initial, "potential_resolves_timed": resolves,
+                        "m_bh": m_bh, "r_sh": r_sh, "max_divb": divb},
+            "e2e": None, "cpu_baseline": None, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def bench_snapshots(args, world, rank, local, dist):
     """Output without stalling: the 3D blast at --n^3 run for --steps steps,
     with a snapshot of the reference's output datasets every
@@ -1009,7 +1086,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="blast3d",
-                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "torus_sph", "poisson", "snapshots",
+                    choices=["blast3d", "batch1d", "briowu", "alfven3d", "torus", "torus_sph", "poisson", "collapsar",
+                             "snapshots",
                              "slabs"])
     ap.add_argument("--slabs", type=int, default=2, help="slabs: number of z slabs")
     ap.add_argument("--snapshot-every", type=int, default=10, help="snapshots: steps between two snapshots")
@@ -1052,7 +1130,7 @@ def main():
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"blast3d": 200, "batch1d": 5, "torus": 2000, "torus_sph": 1000, "poisson": 20, "snapshots": 60,
-                      "slabs": 30}.get(args.workload, 0)
+                      "slabs": 30, "collapsar": 200}.get(args.workload, 0)
     if args.warmup < 3:
         args.warmup = 3
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
@@ -1074,6 +1152,8 @@ def main():
         return bench_config(args, world, rank, local, dist)
     if args.workload == "poisson":
         return bench_poisson(args, world, rank, local, dist)
+    if args.workload == "collapsar":
+        return bench_collapsar(args, world, rank, local, dist)
     if args.workload == "snapshots":
         return bench_snapshots(args, world, rank, local, dist)
     if args.workload == "slabs":

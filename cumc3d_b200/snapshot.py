@@ -12,6 +12,8 @@ image, so ``write`` stores the same datasets, under the same names, in an
 which is also what an HDF5 reader shows for the reference's files, so a
 converter only has to copy arrays across.
 """
+import json
+
 import numpy as np
 
 
@@ -44,3 +46,59 @@ def read(path):
     """dict of the datasets of a snapshot file."""
     with np.load(path) as f:
         return {k: f[k] for k in f.files}
+
+
+DATASETS = ("time", "dimension", "coordinate", "x-interface", "y-interface", "z-interface", "primitive", "epsilon",
+            "bfield")
+
+
+def write_raw(prefix, spec, time, primitive, epsilon, bfield):
+    """The same datasets as raw little-endian FP64 files ``<prefix>.<name>.bin``
+    plus ``<prefix>.json`` (each dataset's Fortran shape and byte order).  A C
+    array whose shape is the Fortran shape reversed has the Fortran array's
+    memory layout, so each file is also the bytes of the reference's array
+    in its own order (dataio.f90 passes prim(imin:ibx-1,0:nx+1,...) etc.)."""
+    data = dict(np.load(_npz_bytes(spec, time, primitive, epsilon, bfield)))
+    manifest = {}
+    for name in DATASETS:
+        a = np.ascontiguousarray(data[name], dtype="<f8")
+        with open("%s.%s.bin" % (prefix, name), "wb") as f:
+            f.write(a.tobytes())
+        manifest[name] = {"fortran_shape": list(a.shape[::-1]), "c_shape": list(a.shape), "dtype": "<f8"}
+    with open(prefix + ".json", "w") as f:
+        json.dump(manifest, f, indent=1)
+    return manifest
+
+
+def _npz_bytes(spec, time, primitive, epsilon, bfield):
+    import io
+    buf = io.BytesIO()
+    write(buf, spec, time, primitive, epsilon, bfield)
+    buf.seek(0)
+    return buf
+
+
+def read_raw(prefix):
+    """dict of the datasets of a raw snapshot (C-order arrays)."""
+    with open(prefix + ".json") as f:
+        manifest = json.load(f)
+    return {name: np.fromfile("%s.%s.bin" % (prefix, name), dtype=m["dtype"]).reshape(m["c_shape"])
+            for name, m in manifest.items()}
+
+
+def to_hdf5(source, h5path):
+    """Convert a snapshot (an ``.npz`` from ``write`` or the prefix of a raw
+    snapshot) to an HDF5 file with the reference's dataset names and shapes
+    (``rkiter-<n>-nm.hdf5`` of dataio.f90:31-240).  Needs h5py, which this
+    image does not have; the datasets are written as they are (their C
+    shapes are what an HDF5 reader shows for the reference's own files)."""
+    try:
+        import h5py
+    except ImportError as ex:
+        raise RuntimeError("to_hdf5 needs h5py (not installed here); the .npz and raw snapshots carry the same "
+                           "datasets") from ex
+    data = read(source) if str(source).endswith(".npz") else read_raw(source)
+    with h5py.File(h5path, "w") as f:
+        for name in DATASETS:
+            f.create_dataset(name, data=np.asarray(data[name], dtype=np.float64))
+    return h5path
