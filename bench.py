@@ -557,6 +557,7 @@ def bench_collapsar(args, world, rank, local, dist):
     s.sync()
     torch.cuda.synchronize()
     initial = {"iterations": it0, "final_error": err0, "converged": conv0, "ms": e0.elapsed_time(e1)}
+    phi0 = s.poisson_get()
     s.collapsar_set(spec["m_bh"], spec["c_code"])
     n_pot = spec["n_pot"]
     n_step = 0
@@ -587,6 +588,23 @@ def bench_collapsar(args, world, rank, local, dist):
     m_bh, r_sh = s.collapsar_get()
     divb = s.find_divb()
     s.close()
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        # the oracle on the same model from the same initial potential: 2 steps
+        # (FINDDT + RUNGEKUTTA with the collapsar hooks), no re-solve
+        from oracle import oracle as O
+        o = O.Oracle(spec)
+        o.set_state(prim, eps)
+        o.initial_update()
+        o.set_phi(phi0)
+        o.collapsar_set(spec["m_bh"], spec["c_code"])
+        t0 = time.perf_counter()
+        for _ in range(2):
+            o.rk3_step(o.finddt())
+        el = time.perf_counter() - t0
+        o.close()
+        cpu = {"value": zones * 2 / el, "unit": "zone-updates/s", "cores": O.num_threads(), "kind": "port",
+               "sample": "2 steps of the same model from the same initial potential, no potential re-solve"}
     if rank == 0:
         line = {
             "metric": "zone-updates/s", "value": zones * args.steps / (ms * 1e-3), "unit": "zone-updates/s",
@@ -598,7 +616,7 @@ def bench_collapsar(args, world, rank, local, dist):
                        "parallelism": "replicas" if world > 1 else "single"},
             "results": {"initial_potential_solve": initial, "potential_resolves_timed": resolves,
                         "m_bh": m_bh, "r_sh": r_sh, "max_divb": divb},
-            "e2e": None, "cpu_baseline": None, "gpu_launches": launches, "clocks": clk,
+            "e2e": None, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk,
         }
         print(json.dumps(line))
     return 0
