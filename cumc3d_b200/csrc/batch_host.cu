@@ -24,6 +24,7 @@ struct cumc_batch {
     std::vector<void *> allocs;
     std::string err;
     int sm_count = 148;
+    int cluster_size = BATCH_CLUSTER;  // CTAs that share one large problem
     int64_t launches = 0;
 };
 
@@ -93,6 +94,7 @@ int cumc_batch_create(const cumc_batch_config *cfg, cumc_batch **out) {
     d.cfl = cfg->cfl;
     d.floor_kind = cfg->floor_kind;
     d.pos_fallback = cfg->positivity_fallback ? 1 : 0;
+    d.coop_min_n = BATCH_COOP_MIN_N;
     bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
     auto A = [&](size_t bytes) -> void * {
         void *p = nullptr;
@@ -186,8 +188,8 @@ int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, 
     b->d.max_steps = max_steps > 0 ? max_steps : 0x7fffffff;
     if (cudaMemsetAsync(b->d.next, 0, sizeof(int), b->stream) != cudaSuccess) return bfail(b, CUMC_ECUDA, "memset failed");
     cudaError_t e = b->precision == CUMC_FP32
-                        ? launch_batch_fp32(b->d, b->recon, b->riemann, 0, BATCH_CLUSTER, b->stream)
-                        : launch_batch_fp64(b->d, b->recon, b->riemann, 0, BATCH_CLUSTER, b->stream);
+                        ? launch_batch_fp32(b->d, b->recon, b->riemann, 0, b->cluster_size, b->stream)
+                        : launch_batch_fp64(b->d, b->recon, b->riemann, 0, b->cluster_size, b->stream);
     if (e == cudaErrorInvalidConfiguration || e == cudaErrorInvalidValue) {
         cudaGetLastError();  // no room for a cluster: one CTA per problem
         e = b->precision == CUMC_FP32 ? launch_batch_fp32(b->d, b->recon, b->riemann, 0, 1, b->stream)
@@ -207,6 +209,16 @@ int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, 
         if (prob[p].status) bad++;
     }
     if (bad) return bfail(b, CUMC_ESTATE, std::to_string(bad) + " problem(s) reached a non-finite or non-positive state");
+    return CUMC_OK;
+}
+
+int cumc_batch_set_cluster(cumc_batch *b, int cluster_size, int coop_min_n) {
+    if (!b) return bfail(b, CUMC_EINVAL, "null batch");
+    if ((cluster_size != 1 && cluster_size != 2 && cluster_size != 4 && cluster_size != 8 && cluster_size != 16) ||
+        coop_min_n < 1)
+        return bfail(b, CUMC_EINVAL, "cluster size must be 1, 2, 4, 8 or 16 and coop_min_n >= 1");
+    b->cluster_size = cluster_size;
+    b->d.coop_min_n = coop_min_n;
     return CUMC_OK;
 }
 

@@ -44,6 +44,7 @@ struct BatchDev {
     double gamma, cfl;
     int floor_kind;
     int pos_fallback;
+    int coop_min_n;        // problems of at most this many cells run on one CTA
     int *next;             // work counter
     const int *order;      // problem ids, largest first
     BatchProblem *prob;
@@ -93,7 +94,7 @@ __device__ __forceinline__ void batch_floor(const BatchDev &b, double &e) {
 
 constexpr int BATCH_THREADS = 256;
 constexpr int BATCH_CLUSTER = 8;          // CTAs that share one large problem
-constexpr int BATCH_COOP_MIN_N = 1024;    // problems of at most this many cells run on one CTA
+constexpr int BATCH_COOP_MIN_N = 1024;    // default: problems of at most this many cells run on one CTA
 
 struct BatchShared {
     unsigned long long part_dt;  // this CTA's FINDDT minimum (bit pattern)
@@ -401,7 +402,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
 }
 
 // Persistent kernel.  Launched in clusters of `size` CTAs: while the next
-// problem (largest first) has more than BATCH_COOP_MIN_N cells, the whole
+// problem (largest first) has more than b.coop_min_n cells, the whole
 // cluster runs it; from the first smaller one on, every CTA takes problems on
 // its own.
 template <class T, int REC, int RS>
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch(const BatchDev b) {
             pi = cluster.map_shared_rank(&sh, 0)->pick;
             cluster.sync();
             if (pi >= b.nprob) return;
-            if (b.prob[b.order[pi]].n <= BATCH_COOP_MIN_N) {
+            if (b.prob[b.order[pi]].n <= b.coop_min_n) {
                 coop = false;  // from here on every CTA takes its own problems
                 if (rank != 0) continue;
             }

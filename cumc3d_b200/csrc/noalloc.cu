@@ -170,6 +170,7 @@ int cumc_batch_run1_noalloc(const cumc_batch_config *cfg, const double *prim, co
     d.cfl = cfg->cfl;
     d.floor_kind = cfg->floor_kind;
     d.pos_fallback = cfg->positivity_fallback ? 1 : 0;
+    d.coop_min_n = BATCH_COOP_MIN_N;
     d.next = (int *)head;
     d.order = (const int *)(head + 16);
     d.prob = (BatchProblem *)(head + 64);

@@ -24,6 +24,7 @@ EXPORTS = [
     "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_fallback_count", "cumc_check_div3",
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
+    "cumc_batch_set_cluster",
     "cumc_batch_run1_noalloc",
     "cumc_learn_set", "cumc_learn_stats", "cumc_learn_flags", "cumc_learn_harvest",
     "cumc_poisson_setup", "cumc_poisson_solve", "cumc_poisson_get", "cumc_poisson_set",
@@ -89,6 +90,7 @@ def load_library(path=None):
     L.cumc_batch_stream.argtypes = [C.c_void_p]
     L.cumc_batch_stream.restype = C.c_void_p
     L.cumc_batch_launch_count.argtypes = [C.c_void_p]
+    L.cumc_batch_set_cluster.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.cumc_batch_launch_count.restype = C.c_int64
     L.cumc_batch_last_error.argtypes = [C.c_void_p]
     L.cumc_batch_last_error.restype = C.c_char_p
@@ -442,6 +444,11 @@ class BatchSolver:
         if rc != 0 and (check or rc != capi.CUMC_ESTATE):
             self._check(rc)
         return t, steps, status
+
+    def set_cluster(self, cluster_size=8, coop_min_n=1024):
+        """CTAs per cluster for problems of more than coop_min_n cells
+        (smaller ones run one per CTA); results do not depend on it."""
+        self._check(self.L.cumc_batch_set_cluster(self.h, int(cluster_size), int(coop_min_n)))
 
     def sync(self):
         self._check(self.L.cumc_batch_sync(self.h))

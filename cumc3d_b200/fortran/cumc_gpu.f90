@@ -337,6 +337,11 @@ INTERFACE
     IMPORT :: C_PTR
     TYPE(C_PTR), VALUE :: b
   END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_batch_set_cluster(b, cluster_size, coop_min_n) BIND(C, NAME='cumc_batch_set_cluster')
+    IMPORT :: C_INT, C_PTR
+    TYPE(C_PTR), VALUE :: b
+    INTEGER(C_INT), VALUE :: cluster_size, coop_min_n
+  END FUNCTION
   INTEGER(C_INT64_T) FUNCTION cumc_batch_launch_count(b) BIND(C, NAME='cumc_batch_launch_count')
     IMPORT :: C_INT64_T, C_PTR
     TYPE(C_PTR), VALUE :: b

@@ -268,6 +268,12 @@ int cumc_batch_get_state(cumc_batch *b, int p, double *prim_row, double *eps_row
 /* INITIAL_UPDATE + the time loop of every problem, one launch.  Per problem:
  * t_out = time reached, steps_out = steps taken, status_out = 0 or CUMC_ESTATE. */
 int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, int *status_out);
+/* Launch shape of the next runs (no reference counterpart): problems of more
+ * than coop_min_n cells are shared by a thread-block cluster of cluster_size
+ * CTAs (1, 2, 4, 8 or 16; 16 is a non-portable size and falls back to one
+ * CTA per problem where the device cannot place it), smaller ones run one
+ * per CTA.  Defaults 8 and 1024.  Results do not depend on it. */
+int cumc_batch_set_cluster(cumc_batch *b, int cluster_size, int coop_min_n);
 int cumc_batch_sync(cumc_batch *b);
 void *cumc_batch_stream(cumc_batch *b);
 /* Number of kernel launches the batch issued since creation (one per

@@ -108,6 +108,37 @@ def test_batch_uneven_sizes_and_edges():
         assert_row_equal(rows[i][0], rows[i][1], pa, ea, spec["nx"], "n=%d" % spec["nx"])
 
 
+@pytest.mark.parametrize("cluster_size,coop_min_n", [(2, 40), (4, 64), (16, 100), (1, 1 << 30)])
+def test_batch_cluster_shapes_are_bitwise_identical(cluster_size, coop_min_n):
+    """The launch shape (CTAs per shared problem, the size above which a
+    problem is shared) changes the split of the cells, not a bit of the
+    results: against the default shape, uneven sizes around the thresholds."""
+    base = small_params(7, seed=13, nmin=30, nmax=300)
+    for prm, n in zip(base, [257, 41, 64, 65, 3, 101, 300]):
+        prm["n"] = n
+    probs = problem_specs(base, 0.03)
+    ref, t0, s0, _ = run_batch(probs)
+    b = BatchSolver([sp for sp, _, _ in probs])
+    b.set_cluster(cluster_size, coop_min_n)
+    for i, (_, prim, eps) in enumerate(probs):
+        b.set_state(i, prim, eps)
+    t, steps, _ = b.run()
+    rows = [b.get_state(i) for i in range(len(probs))]
+    b.close()
+    assert np.array_equal(t, t0) and np.array_equal(steps, s0)
+    for i, (spec, _, _) in enumerate(probs):
+        assert_row_equal(rows[i][0], rows[i][1], ref[i][0], ref[i][1], spec["nx"], "cluster %d" % i)
+
+
+def test_batch_cluster_shape_is_checked():
+    probs = problem_specs(small_params(1, seed=2), 0.01)
+    b = BatchSolver([sp for sp, _, _ in probs])
+    for cs, mn in ((3, 100), (32, 100), (8, 0)):
+        with pytest.raises(CumcError):
+            b.set_cluster(cs, mn)
+    b.close()
+
+
 def test_batch_max_steps_and_rerun():
     params = small_params(3, seed=7, nmin=64, nmax=200)
     probs = problem_specs(params, 0.5)
