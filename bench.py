@@ -230,7 +230,11 @@ def reference_arm(args):
     recipe = oracle_recipe()
     # every host thread this process may use (torchrun sets OMP_NUM_THREADS=1)
     O.set_num_threads(len(os.sched_getaffinity(0)))
-    n, nz = args.n, 64
+    # the sample shrinks with the step count so that the whole run stays
+    # within a couple of minutes: a 64-plane slab for 20 steps, down to 8
+    # planes (the same cross-section and scheme) for the full 200
+    n = args.n
+    nz = int(max(8, min(64, 8 * round(64 * 25 / max(1, args.steps + args.warmup) / 8))))
     spec, prim, eps = blast_slab(n, nz, args.recon, args.riemann)
     o = O.Oracle(spec)
     o.set_state(prim, eps)
@@ -244,8 +248,8 @@ def reference_arm(args):
     zones = n * n * nz
     value = zones * args.steps / el
     sample = ("each step one RK3 step of a %dx%dx%d periodic z slab of the %d^3 blast (same cross-section, "
-              "scheme and flags; a quarter of the zones), %d timed steps after %d warm-up; %s" % (
-                  n, n, nz, n, args.steps, args.warmup, recipe))
+              "scheme and flags; %d of %d z planes), %d timed steps after %d warm-up; %s" % (
+                  n, n, nz, n, nz, n, args.steps, args.warmup, recipe))
     line = {
         "impl": "reference", "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,

@@ -30,6 +30,15 @@ def test_reference_arm_prints_one_contract_line():
     assert "96x96x64" in cb["sample"]
 
 
+def test_reference_arm_sample_shrinks_with_the_step_count():
+    """Every step is timed, each on a thinner slab, so long runs stay short."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "200",
+                        "--warmup", "3", "--n", "24"], capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads([ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")][0])
+    assert d["steps"] == 200 and "24x24x8" in d["cpu_baseline"]["sample"]
+
+
 def test_gpus_n_spawns_n_ranks_dry_run():
     env = dict(os.environ)
     env.pop("WORLD_SIZE", None)
