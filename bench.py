@@ -231,10 +231,11 @@ def reference_arm(args):
     # every host thread this process may use (torchrun sets OMP_NUM_THREADS=1)
     O.set_num_threads(len(os.sched_getaffinity(0)))
     # the sample shrinks with the step count so that the whole run stays
-    # within a couple of minutes: a 64-plane slab for 20 steps, down to 8
-    # planes (the same cross-section and scheme) for the full 200
+    # within a few minutes: a 64-plane slab up to 25 steps with warm-up, down
+    # to 32 planes (the same cross-section and scheme; thinner slabs would
+    # spend a larger share of the work on z ghosts) for the full 200
     n = args.n
-    nz = int(max(8, min(64, 8 * round(64 * 25 / max(1, args.steps + args.warmup) / 8))))
+    nz = int(max(32, min(64, 8 * round(64 * 25 / max(1, args.steps + args.warmup) / 8))))
     spec, prim, eps = blast_slab(n, nz, args.recon, args.riemann)
     o = O.Oracle(spec)
     o.set_state(prim, eps)

@@ -36,7 +36,7 @@ def test_reference_arm_sample_shrinks_with_the_step_count():
                         "--warmup", "3", "--n", "24"], capture_output=True, text=True, cwd=ROOT, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     d = json.loads([ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")][0])
-    assert d["steps"] == 200 and "24x24x8" in d["cpu_baseline"]["sample"]
+    assert d["steps"] == 200 and "24x24x32" in d["cpu_baseline"]["sample"]
 
 
 def test_gpus_n_spawns_n_ranks_dry_run():
