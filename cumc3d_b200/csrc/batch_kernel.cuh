@@ -92,11 +92,7 @@ __device__ __forceinline__ void batch_floor(const BatchDev &b, double &e) {
     if (b.floor_kind == 1) e = dmax(e, 0.0);
 }
 
-#ifndef CUMC_BATCH_THREADS
-#define CUMC_BATCH_THREADS 256
-#endif
-constexpr int BATCH_THREADS = CUMC_BATCH_THREADS;
-constexpr int BATCH_MINB = 512 / BATCH_THREADS;  // resident CTAs per SM at 128 registers
+constexpr int BATCH_THREADS = 256;
 constexpr int BATCH_CLUSTER = 8;          // CTAs that share one large problem
 constexpr int BATCH_COOP_MIN_N = 1024;    // default: problems of at most this many cells run on one CTA
 
@@ -410,7 +406,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
 // cluster runs it; from the first smaller one on, every CTA takes problems on
 // its own.
 template <class T, int REC, int RS>
-__global__ void __launch_bounds__(BATCH_THREADS, BATCH_MINB) k_batch(const BatchDev b) {
+__global__ void __launch_bounds__(BATCH_THREADS, 2) k_batch(const BatchDev b) {
     __shared__ BatchShared sh;
     cg::cluster_group cluster = cg::this_cluster();
     const int size = (int)cluster.num_blocks();
