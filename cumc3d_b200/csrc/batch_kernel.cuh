@@ -134,12 +134,14 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
     __syncthreads();
 
     // FROMRVETOU + FINDPRESSURE of cell j; bxm = the recovered face j-1
-    auto fromrvetou = [&](int j, double bxm) {
-        const long long c = off + j;
-        const double bx = 0.5 * (b.BX[c] + bxm);
-        const double by = 0.5 * (b.BY1[c] + b.BY0[c]);
-        const double bz = 0.5 * (b.BZ1[c] + b.BZ0[c]);
-        const double rho = b.P[0][c], vx = b.P[1][c], vy = b.P[2][c], vz = b.P[3][c], e = b.EPS[c];
+    // (the values as stored: face fields bxf = BX[c], by1/by0, bz1/bz0 and the
+    // primitives of cell c, passed in so that a caller that has just stored
+    // them does not read them back)
+    auto fromrvetou_v = [&](long long c, double bxf, double bxm, double by1, double by0, double bz1, double bz0,
+                            double rho, double vx, double vy, double vz, double e) {
+        const double bx = 0.5 * (bxf + bxm);
+        const double by = 0.5 * (by1 + by0);
+        const double bz = 0.5 * (bz1 + bz0);
         const double vsquare = vx * vx + vy * vy + vz * vz;
         const double bsquare = bx * bx + by * by + bz * bz;
         b.U[0][c] = rho;
@@ -155,6 +157,11 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
         b.CS[c] = sqrt(e * g1 + rho * g1 * p / (rho * rho));
         if (!(rho > 0.0) || !isfinite(e) || !isfinite(p) || !isfinite(vx) || !isfinite(vy) || !isfinite(vz))
             sh.bad = 1;
+    };
+    auto fromrvetou = [&](int j, double bxm) {
+        const long long c = off + j;
+        fromrvetou_v(c, b.BX[c], bxm, b.BY1[c], b.BY0[c], b.BZ1[c], b.BZ0[c], b.P[0][c], b.P[1][c], b.P[2][c],
+                     b.P[3][c], b.EPS[c]);
     };
 
     // -------- INITIAL_UPDATE (initial.f90:86-116) --------
@@ -234,14 +241,24 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
 #pragma unroll
                 for (int m = 0; m < NW; ++m) w[m] = wp[m];
                 const long long i0 = cl(c0 - 2), i1 = cl(c0 - 1), i2 = cl(c0), i3 = cl(c0 + 1), i4 = cl(c0 + 2);
+                // every stencil value first: the face-state stores below may
+                // alias the primitive arrays as far as the compiler knows, so
+                // loads left between them would each wait a round trip
+                T sv[7][5];
+#pragma unroll
+                for (int v = 0; v < 7; ++v) {
+                    const double *src = (v < 5) ? b.P[v] : b.BC[v == 5 ? 1 : 2];
+                    sv[v][0] = sv[v][4] = T(0);
+                    if (REC == REC_PPM || REC == REC_WENO) { sv[v][0] = (T)src[i0]; sv[v][4] = (T)src[i4]; }
+                    sv[v][1] = (T)src[i1];
+                    sv[v][2] = (T)src[i2];
+                    sv[v][3] = (T)src[i3];
+                }
                 bool fallback = false;
                 T vm_rho = T(0), vp_rho = T(0);
 #pragma unroll
                 for (int v = 0; v < 7; ++v) {
-                    const double *src = (v < 5) ? b.P[v] : b.BC[v == 5 ? 1 : 2];
-                    T a0 = T(0), a4 = T(0);
-                    if (REC == REC_PPM || REC == REC_WENO) { a0 = (T)src[i0]; a4 = (T)src[i4]; }
-                    const T a1 = (T)src[i1], a2 = (T)src[i2], a3 = (T)src[i3];
+                    const T a0 = sv[v][0], a1 = sv[v][1], a2 = sv[v][2], a3 = sv[v][3], a4 = sv[v][4];
                     T vm, vp;
                     recon_cell<T, REC>(w, a0, a1, a2, a3, a4, vm, vp);
                     if (v == 0) { vm_rho = vm; vp_rho = vp; }
@@ -249,7 +266,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                         fallback = !(vm_rho > T(0) && vp_rho > T(0) && vm > T(0) && vp > T(0));
                         if (fallback) {
                             for (int u = 0; u < 4; ++u) {
-                                const T cv = (T)b.P[u][i2];
+                                const T cv = sv[u][2];  // (T)P[u][i2]
                                 if (c0 <= n) QL[u][c] = cv;
                                 if (c0 >= 1) QR[u][c - 1] = cv;
                             }
@@ -316,22 +333,30 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 const double eyd = (j >= 1) ? (b.EY[c] - b.EY[c - 1]) : 0.0;
                 const double lby = -((zero) / 1.0 - dv(ezd, dxj));
                 const double lbz = -(dv(eyd, dxj) - (zero) / 1.0);
-                auto combo = [&](double *Uarr, double *Oarr, double lrv) {
-                    const double u = Uarr[c];
-                    double un;
-                    if (stage == 1) { Oarr[c] = u; un = u + dt * lrv; }
-                    else if (stage == 2) un = rk20 * Oarr[c] + rk21 * u + rk22 * dt * lrv;
-                    else un = rk30 * Oarr[c] + rk31 * u + rk32 * dt * lrv;
-                    Uarr[c] = un;
-                };
+                // the ten u (and u_old) values first, then the stores
+                double *const Ua[10] = {b.U[0], b.U[1], b.U[2], b.U[3], b.U[4], b.UBX, b.UBY1, b.UBZ1, b.UBY0, b.UBZ0};
+                double *const Oa[10] = {b.O[0], b.O[1], b.O[2], b.O[3], b.O[4], b.OBX, b.OBY1, b.OBZ1, b.OBY0, b.OBZ0};
+                const double lv[10] = {lr[0], lr[1], lr[2], lr[3], lr[4], lbx, lby, lbz, lby, lbz};
+                const int nv = (j >= 1) ? 10 : 6;
+                double uu[10], oo[10];
 #pragma unroll
-                for (int i = 0; i < 5; ++i) combo(b.U[i], b.O[i], lr[i]);
-                combo(b.UBX, b.OBX, lbx);
-                if (j >= 1) {
-                    combo(b.UBY1, b.OBY1, lby);
-                    combo(b.UBZ1, b.OBZ1, lbz);
-                    combo(b.UBY0, b.OBY0, lby);
-                    combo(b.UBZ0, b.OBZ0, lbz);
+                for (int i = 0; i < 10; ++i) {
+                    uu[i] = 0.0;
+                    oo[i] = 0.0;
+                    if (i < nv) {
+                        uu[i] = Ua[i][c];
+                        if (stage != 1) oo[i] = Oa[i][c];
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 10; ++i) {
+                    if (i >= nv) continue;
+                    const double u = uu[i], lrv = lv[i];
+                    double un;
+                    if (stage == 1) { Oa[i][c] = u; un = u + dt * lrv; }
+                    else if (stage == 2) un = rk20 * oo[i] + rk21 * u + rk22 * dt * lrv;
+                    else un = rk30 * oo[i] + rk31 * u + rk32 * dt * lrv;
+                    Ua[i][c] = un;
                 }
             }
             gsync(coop);
@@ -339,36 +364,40 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
             // index-0 layer of cons (cells 1..n) ----
             for (int j = max(lo, 1) + threadIdx.x; j < min(hi, n + 1); j += blockDim.x) {
                 const long long c = off + j;
-                const double ubxm = b.UBX[c - 1];
-                const double bxu = 0.5 * (b.UBX[c] + ubxm);
-                const double byu = 0.5 * (b.UBY1[c] + b.UBY0[c]);
-                const double bzu = 0.5 * (b.UBZ1[c] + b.UBZ0[c]);
-                const double u0 = b.U[0][c];
-                const double vx = dv(b.U[1][c], u0), vy = dv(b.U[2][c], u0), vz = dv(b.U[3][c], u0);
+                // every load first (the stores below may alias them as far as
+                // the compiler knows), then the recovery on the loaded values
+                const double ubxm = b.UBX[c - 1], ubx = b.UBX[c];
+                const double uby1 = b.UBY1[c], uby0 = b.UBY0[c], ubz1 = b.UBZ1[c], ubz0 = b.UBZ0[c];
+                const double u0 = b.U[0][c], u1 = b.U[1][c], u2 = b.U[2][c], u3 = b.U[3][c], u4 = b.U[4][c];
+                const double by0 = b.BY0[c], bz0 = b.BZ0[c];
+                double by1_old = 0.0, bz1_old = 0.0, bx0 = 0.0;
+                if (j == 1) { by1_old = b.BY1[c]; bz1_old = b.BZ1[c]; bx0 = b.BX[off]; }
+                const double bxu = 0.5 * (ubx + ubxm);
+                const double byu = 0.5 * (uby1 + uby0);
+                const double bzu = 0.5 * (ubz1 + ubz0);
+                const double vx = dv(u1, u0), vy = dv(u2, u0), vz = dv(u3, u0);
                 const double bsquare = bxu * bxu + byu * byu + bzu * bzu;
                 const double vsquare = vx * vx + vy * vy + vz * vz;
-                double e = (b.U[4][c] - 0.5 * bsquare) / u0 - 0.5 * vsquare;
+                double e = (u4 - 0.5 * bsquare) / u0 - 0.5 * vsquare;
                 batch_floor(b, e);
                 if (stage == 3) batch_floor(b, e);
-                double by1_old = 0.0, bz1_old = 0.0;
-                if (j == 1) { by1_old = b.BY1[c]; bz1_old = b.BZ1[c]; }
                 b.P[0][c] = u0;
                 b.P[1][c] = vx;
                 b.P[2][c] = vy;
                 b.P[3][c] = vz;
                 b.EPS[c] = e;
-                b.BX[c] = b.UBX[c];
-                b.BY1[c] = b.UBY1[c];
-                b.BZ1[c] = b.UBZ1[c];
+                b.BX[c] = ubx;
+                b.BY1[c] = uby1;
+                b.BZ1[c] = ubz1;
                 // face j-1 after recovery: the recovered cons face, or the
                 // never-recovered face 0
-                fromrvetou(j, j == 1 ? b.BX[off] : ubxm);
-                b.UBY0[c] = b.BY0[c];
-                b.UBZ0[c] = b.BZ0[c];
+                fromrvetou_v(c, ubx, j == 1 ? bx0 : ubxm, uby1, by0, ubz1, bz0, u0, vx, vy, vz, e);
+                b.UBY0[c] = by0;
+                b.UBZ0[c] = bz0;
                 if (j == 1) {
                     // cons layer 0 takes the prim faces of j = 0 as they stood
                     // before this recovery (the j = 0 ghosts of By, Bz copy cell 1)
-                    b.UBX[off] = b.BX[off];
+                    b.UBX[off] = bx0;
                     b.UBY1[off] = by1_old;
                     b.UBZ1[off] = bz1_old;
                 }
