@@ -108,10 +108,10 @@ int cumc_batch_create(const cumc_batch_config *cfg, cumc_batch **out) {
     d.EPS = (double *)A(nb); d.CS = (double *)A(nb);
     for (int i = 0; i < 3; ++i) d.BC[i] = (double *)A(nb);
     d.BX = (double *)A(nb); d.BY1 = (double *)A(nb); d.BZ1 = (double *)A(nb); d.BY0 = (double *)A(nb); d.BZ0 = (double *)A(nb);
-    d.UBX = (double *)A(nb); d.UBY1 = (double *)A(nb); d.UBZ1 = (double *)A(nb); d.UBY0 = (double *)A(nb); d.UBZ0 = (double *)A(nb);
+    d.UBX = (double *)A(nb); d.UBXb = (double *)A(nb); d.UBY1 = (double *)A(nb); d.UBZ1 = (double *)A(nb); d.UBY0 = (double *)A(nb); d.UBZ0 = (double *)A(nb);
     d.OBX = (double *)A(nb); d.OBY1 = (double *)A(nb); d.OBZ1 = (double *)A(nb); d.OBY0 = (double *)A(nb); d.OBZ0 = (double *)A(nb);
     for (int i = 0; i < 7; ++i) { d.QL[i] = A(nb); d.QR[i] = A(nb); }
-    d.FBY = (double *)A(nb); d.FBZ = (double *)A(nb); d.EY = (double *)A(nb); d.EZ = (double *)A(nb);
+    d.EY = (double *)A(nb); d.EZ = (double *)A(nb);
     d.next = (int *)A(sizeof(int));
     int *ord = (int *)A(sizeof(int) * b->nprob);
     d.order = ord;

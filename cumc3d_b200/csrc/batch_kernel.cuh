@@ -54,9 +54,10 @@ struct BatchDev {
     double *EPS, *CS, *BC[3];
     double *BX, *BY1, *BZ1, *BY0, *BZ0;          // prim face fields
     double *U[5], *UBX, *UBY1, *UBZ1, *UBY0, *UBZ0;  // cons
+    double *UBXb;          // second buffer of the cons x faces (stages alternate)
     double *O[5], *OBX, *OBY1, *OBZ1, *OBY0, *OBZ0;  // u_old
     void *QL[7], *QR[7];   // face states (T)
-    double *F[5], *FBY, *FBZ;  // x-face fluxes: hydro + flux(iby), flux(ibz)
+    double *F[5];          // x-face fluxes (hydro)
     double *EY, *EZ;       // edge EMFs per x-face
 };
 
@@ -186,6 +187,7 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
 
     double t = 0.0;
     int steps = 0;
+    int ubp = 0;  // which buffer holds the cons x faces (INITIAL_UPDATE fills UBX)
     bool bad = false;
     while (true) {
         // -------- FINDDT (rungekutta.f90:221-332), 1D Cartesian --------
@@ -309,7 +311,16 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 b.EZ[c] = 0.50 * (fzx + fzx + ez_a + ez_b) - 0.25 * (ez_a + ez_a + ez_b + ez_b);
             }
             gsync(coop);
-            // ---- C: du/dt + Shu-Osher combination (j = 0..n) ----
+            // ---- C + D: du/dt + Shu-Osher combination (j = 0..n), then on the
+            // new values FROMUTORVE + floor, FROMRVETOU + FINDPRESSURE and the
+            // index-0 layer of cons (j = 1..n), one phase.  The only operand a
+            // cell takes from its neighbour is the updated x face below it; the
+            // thread recomputes it (the same expression on the same values the
+            // neighbour uses), reading the previous stage's faces from one
+            // buffer while the new ones go to the other, so no barrier is needed
+            // between the update and the recovery. ----
+            double *const UBXo = ubp ? b.UBXb : b.UBX;  // this stage's input x faces
+            double *const UBXn = ubp ? b.UBX : b.UBXb;  // its output
             for (int j = lo + threadIdx.x; j < min(hi, n + 1); j += blockDim.x) {
                 const long long c = off + j;
                 const double dxj = b.dx[c];
@@ -333,12 +344,23 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 const double eyd = (j >= 1) ? (b.EY[c] - b.EY[c - 1]) : 0.0;
                 const double lby = -((zero) / 1.0 - dv(ezd, dxj));
                 const double lbz = -(dv(eyd, dxj) - (zero) / 1.0);
-                // the ten u (and u_old) values first, then the stores
-                double *const Ua[10] = {b.U[0], b.U[1], b.U[2], b.U[3], b.U[4], b.UBX, b.UBY1, b.UBZ1, b.UBY0, b.UBZ0};
+                // written with round-to-nearest intrinsics so that no build
+                // (the FP32 form compiles with contraction) fuses it: the
+                // recomputed face below must equal the one its owner stores
+                auto combo = [&](double u, double o, double lrv) {
+                    if (stage == 1) return __dadd_rn(u, __dmul_rn(dt, lrv));
+                    if (stage == 2)
+                        return __dadd_rn(__dadd_rn(__dmul_rn(rk20, o), __dmul_rn(rk21, u)), __dmul_rn(__dmul_rn(rk22, dt), lrv));
+                    return __dadd_rn(__dadd_rn(__dmul_rn(rk30, o), __dmul_rn(rk31, u)), __dmul_rn(__dmul_rn(rk32, dt), lrv));
+                };
+                // every load first (a load after a store would wait its own
+                // round trip: the compiler cannot tell that the arrays do not
+                // alias), then the update and the recovery on the loaded values
+                double *const Ua[10] = {b.U[0], b.U[1], b.U[2], b.U[3], b.U[4], UBXo, b.UBY1, b.UBZ1, b.UBY0, b.UBZ0};
                 double *const Oa[10] = {b.O[0], b.O[1], b.O[2], b.O[3], b.O[4], b.OBX, b.OBY1, b.OBZ1, b.OBY0, b.OBZ0};
                 const double lv[10] = {lr[0], lr[1], lr[2], lr[3], lr[4], lbx, lby, lbz, lby, lbz};
                 const int nv = (j >= 1) ? 10 : 6;
-                double uu[10], oo[10];
+                double uu[10], oo[10], un[10];
 #pragma unroll
                 for (int i = 0; i < 10; ++i) {
                     uu[i] = 0.0;
@@ -348,30 +370,36 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                         if (stage != 1) oo[i] = Oa[i][c];
                     }
                 }
+                double um = 0.0, om = 0.0, by0 = 0.0, bz0 = 0.0, by1_old = 0.0, bz1_old = 0.0, bx0 = 0.0;
+                if (j >= 1) {
+                    um = UBXo[c - 1];  // the face below, as the stage found it
+                    if (stage != 1) om = b.OBX[c - 1];
+                    by0 = b.BY0[c];
+                    bz0 = b.BZ0[c];
+                    if (j == 1) { by1_old = b.BY1[c]; bz1_old = b.BZ1[c]; bx0 = b.BX[off]; }
+                }
 #pragma unroll
                 for (int i = 0; i < 10; ++i) {
+                    un[i] = 0.0;
                     if (i >= nv) continue;
-                    const double u = uu[i], lrv = lv[i];
-                    double un;
-                    if (stage == 1) { Oa[i][c] = u; un = u + dt * lrv; }
-                    else if (stage == 2) un = rk20 * oo[i] + rk21 * u + rk22 * dt * lrv;
-                    else un = rk30 * oo[i] + rk31 * u + rk32 * dt * lrv;
-                    Ua[i][c] = un;
+                    if (stage == 1) Oa[i][c] = uu[i];
+                    un[i] = combo(uu[i], oo[i], lv[i]);
                 }
-            }
-            gsync(coop);
-            // ---- D: FROMUTORVE + floor, FROMRVETOU + FINDPRESSURE, and the
-            // index-0 layer of cons (cells 1..n) ----
-            for (int j = max(lo, 1) + threadIdx.x; j < min(hi, n + 1); j += blockDim.x) {
-                const long long c = off + j;
-                // every load first (the stores below may alias them as far as
-                // the compiler knows), then the recovery on the loaded values
-                const double ubxm = b.UBX[c - 1], ubx = b.UBX[c];
-                const double uby1 = b.UBY1[c], uby0 = b.UBY0[c], ubz1 = b.UBZ1[c], ubz0 = b.UBZ0[c];
-                const double u0 = b.U[0][c], u1 = b.U[1][c], u2 = b.U[2][c], u3 = b.U[3][c], u4 = b.U[4][c];
-                const double by0 = b.BY0[c], bz0 = b.BZ0[c];
-                double by1_old = 0.0, bz1_old = 0.0, bx0 = 0.0;
-                if (j == 1) { by1_old = b.BY1[c]; bz1_old = b.BZ1[c]; bx0 = b.BX[off]; }
+                if (j == 0) {
+                    // cell 0: the update only (its x face's final value is the
+                    // prim face 0, written by the thread of cell 1)
+#pragma unroll
+                    for (int i = 0; i < 5; ++i) b.U[i][c] = un[i];
+                    continue;
+                }
+                UBXn[c] = un[5];
+                b.UBY1[c] = un[6];
+                b.UBZ1[c] = un[7];
+                // the recovery of cell j from its updated values (U, the y/z
+                // faces) and the updated x face below (recomputed)
+                const double ubxm = combo(um, om, lbx);
+                const double ubx = un[5], uby1 = un[6], ubz1 = un[7], uby0 = un[8], ubz0 = un[9];
+                const double u0 = un[0], u1 = un[1], u2 = un[2], u3 = un[3], u4 = un[4];
                 const double bxu = 0.5 * (ubx + ubxm);
                 const double byu = 0.5 * (uby1 + uby0);
                 const double bzu = 0.5 * (ubz1 + ubz0);
@@ -390,18 +418,19 @@ __device__ __forceinline__ void batch_problem(const BatchDev &b, BatchShared &sh
                 b.BY1[c] = uby1;
                 b.BZ1[c] = ubz1;
                 // face j-1 after recovery: the recovered cons face, or the
-                // never-recovered face 0
+                // never-recovered face 0; FROMRVETOU also rewrites U of the cell
                 fromrvetou_v(c, ubx, j == 1 ? bx0 : ubxm, uby1, by0, ubz1, bz0, u0, vx, vy, vz, e);
                 b.UBY0[c] = by0;
                 b.UBZ0[c] = bz0;
                 if (j == 1) {
                     // cons layer 0 takes the prim faces of j = 0 as they stood
                     // before this recovery (the j = 0 ghosts of By, Bz copy cell 1)
-                    b.UBX[off] = bx0;
+                    UBXn[off] = bx0;
                     b.UBY1[off] = by1_old;
                     b.UBZ1[off] = bz1_old;
                 }
             }
+            ubp ^= 1;
             gsync(coop);
         }
         t = t + dt;

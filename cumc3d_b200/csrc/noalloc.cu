@@ -38,10 +38,10 @@ namespace {
 
 constexpr int NOALLOC_MAX_CELLS = 4096;
 constexpr int NOALLOC_ROW = NOALLOC_MAX_CELLS + 8;  // padded cells -2..n+3, or faces -3..n+3
-// per padded cell, in doubles: P 5, EPS, CS, BC 3, prim faces 5, cons 5+5,
-// u_old 5+5, QL 7, QR 7, F 5 + 2, EY, EZ, dx, w 14, wf 7 (14 floats),
-// staging 3 x 8 + 1, faces 1
-constexpr int NOALLOC_PER_CELL = 10 + 5 + 10 + 10 + 14 + 7 + 2 + 1 + 14 + 7 + 25 + 1;
+// per padded cell, in doubles: P 5, EPS, CS, BC 3, prim faces 5, cons 5+5
+// plus the second x-face buffer, u_old 5+5, QL 7, QR 7, F 5, EY, EZ, dx,
+// w 14, wf 7 (14 floats), staging 3 x 8 + 1, faces 1
+constexpr int NOALLOC_PER_CELL = 10 + 5 + 11 + 10 + 14 + 5 + 2 + 1 + 14 + 7 + 25 + 1;
 constexpr size_t NOALLOC_HEAD = 256;  // work counter, order, problem record
 constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_HEAD + (size_t)NOALLOC_PER_CELL * NOALLOC_ROW * sizeof(double);
 
@@ -179,13 +179,13 @@ int cumc_batch_run1_noalloc(const cumc_batch_config *cfg, const double *prim, co
     for (int i = 0; i < 3; ++i) d.BC[i] = row();
     d.BX = row(); d.BY1 = row(); d.BZ1 = row(); d.BY0 = row(); d.BZ0 = row();
     for (int i = 0; i < 5; ++i) d.U[i] = row();
-    d.UBX = row(); d.UBY1 = row(); d.UBZ1 = row(); d.UBY0 = row(); d.UBZ0 = row();
+    d.UBX = row(); d.UBXb = row(); d.UBY1 = row(); d.UBZ1 = row(); d.UBY0 = row(); d.UBZ0 = row();
     for (int i = 0; i < 5; ++i) d.O[i] = row();
     d.OBX = row(); d.OBY1 = row(); d.OBZ1 = row(); d.OBY0 = row(); d.OBZ0 = row();
     for (int i = 0; i < 7; ++i) d.QL[i] = row();
     for (int i = 0; i < 7; ++i) d.QR[i] = row();
     for (int i = 0; i < 5; ++i) d.F[i] = row();
-    d.FBY = row(); d.FBZ = row(); d.EY = row(); d.EZ = row();
+    d.EY = row(); d.EZ = row();
     d.dx = row();
     double *w = row();
     slot += 13;  // 14 weights per cell
