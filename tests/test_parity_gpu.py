@@ -290,6 +290,38 @@ def test_headline_blast_parameters_at_size_bitwise(oracle_mod, n, nz):
     o.close()
 
 
+@pytest.mark.parametrize("recon", ["ppm", "weno"])
+def test_alfven_benchmark_config_bitwise(oracle_mod, recon):
+    """The circularly polarised Alfven wave workload (k = 2 pi (1, 1, 1),
+    amplitude 0.1, face B from an edge vector potential, periodic, HLLD, CFL
+    0.4) at 40^3 with the workload's PPM and WENO-Z, through the captured
+    step graph with the autotuned launch shapes: 8 steps bit for bit, and
+    div B equal."""
+    from cumc3d_b200.engine import Solver
+    spec, prim, eps = models.alfven_3d(40, recon=recon)
+    g = Solver(spec)
+    g.set_state(prim, eps)
+    g.initial_update()
+    g.autotune()
+    tg, kg = g.evolve(1e30, 8)
+    o = oracle_mod.Oracle(spec)
+    o.set_state(prim, eps)
+    o.initial_update()
+    to = 0.0
+    for _ in range(8):
+        dt = o.finddt()
+        o.rk3_step(dt)
+        to += dt
+    assert kg == 8 and tg == to
+    pg, eg = g.get_state()
+    po, eo = o.get_state()
+    assert np.array_equal(interior(pg, spec).view(np.uint64), interior(po, spec).view(np.uint64))
+    assert np.array_equal(interior(eg, spec).view(np.uint64), interior(eo, spec).view(np.uint64))
+    assert g.find_divb() == o.max_divb()
+    g.close()
+    o.close()
+
+
 def test_torus_benchmark_config_at_96x64x96_bitwise(oracle_mod):
     """The cylindrical torus workload (GM = 1 point mass, constant-l
     polytrope, A_phi field loops at min beta 100, 1% seeded pressure noise,
