@@ -905,6 +905,51 @@ __global__ void k_div3_check(unsigned long long seed, long long n, unsigned long
     if (bad) atomicAdd(mismatch, bad);
 }
 
+// dv(x, y) against the IEEE quotient x / y on generated operand pairs: a
+// quarter of the numerators +-0, the denominators' exponents over the whole
+// range with a share of zeros, infinities, NaNs and subnormals
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double special_or_random(unsigned long long z, unsigned long long sel) {
+    const unsigned long long sign = z & 0x8000000000000000ull, man = z & 0x000FFFFFFFFFFFFFull;
+    switch (sel % 16) {
+        case 0: return __longlong_as_double((long long)sign);                                      // +-0
+        case 1: return __longlong_as_double((long long)(sign | 0x7FF0000000000000ull));            // +-inf
+        case 2: return __longlong_as_double((long long)(sign | 0x7FF8000000000000ull | (man >> 1)));  // NaN
+        case 3: return __longlong_as_double((long long)(sign | (man ? man : 1ull)));              // subnormal
+        default: {
+            const unsigned long long e = (z >> 52) & 0x7FFull;  // any exponent, inf/NaN included
+            return __longlong_as_double((long long)(sign | (e << 52) | man));
+        }
+    }
+}
+__global__ void k_dv_check(unsigned long long seed, long long n, unsigned long long *mismatch, double *example) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    unsigned long long bad = 0;
+    for (; i < n; i += stride) {
+        const unsigned long long z1 = mix64(seed + (unsigned long long)i * 0x9E3779B97F4A7C15ull);
+        const unsigned long long z2 = mix64(z1 ^ 0xD1B54A32D192ED03ull);
+        const unsigned long long z3 = mix64(z2 + 0x8CB92BA72F3D8DD7ull);
+        // numerator: +-0 for a quarter, else a special or random value
+        const double x = (z3 & 3) == 0 ? __longlong_as_double((long long)(z1 & 0x8000000000000000ull))
+                                       : special_or_random(z1, (z3 >> 2) % 64);
+        // denominator: mostly normal, a share of the special values
+        const double y = special_or_random(z2, (z3 >> 8) % 64);
+        const double a = x / y;
+        const double b = dv<double>(x, y);
+        const bool same = __double_as_longlong(a) == __double_as_longlong(b) || (isnan(a) && isnan(b));
+        if (!same) {
+            if (bad == 0) { example[0] = x; example[1] = y; }
+            ++bad;
+        }
+    }
+    if (bad) atomicAdd(mismatch, bad);
+}
+
 // FP64 pipe probe: independent DFMA chains, 8 per thread, no memory traffic
 __global__ void k_dfma_probe(double *out, int iters) {
     double a[8];
@@ -2671,6 +2716,21 @@ int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mi
     cudaError_t e = cudaDeviceSynchronize();
     cudaMemcpy(mismatches, m, sizeof(*m), cudaMemcpyDeviceToHost);
     cudaMemcpy(example, ex, sizeof(*ex), cudaMemcpyDeviceToHost);
+    cudaFree(m);
+    cudaFree(ex);
+    return e == cudaSuccess ? CUMC_OK : CUMC_ECUDA;
+}
+
+int cumc_check_dv(unsigned long long seed, long long n, unsigned long long *mismatches, double *example) {
+    unsigned long long *m = nullptr;
+    double *ex = nullptr;
+    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, 2 * sizeof(*ex)) != cudaSuccess) return CUMC_ECUDA;
+    cudaMemset(m, 0, sizeof(*m));
+    cudaMemset(ex, 0, 2 * sizeof(*ex));
+    k_dv_check<<<148 * 16, 256>>>(seed, n, m, ex);
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemcpy(mismatches, m, sizeof(*m), cudaMemcpyDeviceToHost);
+    cudaMemcpy(example, ex, 2 * sizeof(*ex), cudaMemcpyDeviceToHost);
     cudaFree(m);
     cudaFree(ex);
     return e == cudaSuccess ? CUMC_OK : CUMC_ECUDA;

@@ -21,7 +21,7 @@ EXPORTS = [
     "cumc_create", "cumc_destroy", "cumc_set_state", "cumc_get_state", "cumc_get_array",
     "cumc_initial_update", "cumc_finddt", "cumc_rk3_step", "cumc_evolve", "cumc_max_divb",
     "cumc_sync", "cumc_launch_count", "cumc_stream", "cumc_profile_step", "cumc_fp64_peak", "cumc_autotune",
-    "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_fallback_count", "cumc_check_div3",
+    "cumc_set_tuning", "cumc_set_concurrent_sweeps", "cumc_fallback_count", "cumc_check_div3", "cumc_check_dv",
     "cumc_batch_create", "cumc_batch_destroy", "cumc_batch_set_state", "cumc_batch_get_state",
     "cumc_batch_run", "cumc_batch_sync", "cumc_batch_stream", "cumc_batch_launch_count", "cumc_batch_last_error",
     "cumc_batch_set_cluster",
@@ -79,6 +79,7 @@ def load_library(path=None):
     L.cumc_set_concurrent_sweeps.argtypes = [C.c_void_p, C.c_int]
     L.cumc_fallback_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)]
     L.cumc_check_div3.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
+    L.cumc_check_dv.argtypes = [C.c_ulonglong, C.c_longlong, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double)]
     L.cumc_last_error.argtypes = [C.c_void_p]
     L.cumc_last_error.restype = C.c_char_p
     L.cumc_batch_create.argtypes = [C.POINTER(capi.CumcBatchConfig), C.POINTER(C.c_void_p)]
@@ -857,3 +858,14 @@ class SlabRank:
         self._hsend, self._hrecv = {}, {}
         torch.cuda.synchronize(self.device)
         self.solver.close()
+
+
+def check_dv(seed, n):
+    """(mismatches, (x, y) of one differing pair) of the engine's FP64
+    division against the IEEE quotient x / y."""
+    m = C.c_ulonglong()
+    ex = (C.c_double * 2)()
+    rc = load_library().cumc_check_dv(seed, n, C.byref(m), ex)
+    if rc != 0:
+        raise CumcError(rc, "dv check failed to run")
+    return m.value, (ex[0], ex[1])

@@ -314,6 +314,12 @@ INTERFACE
     INTEGER(C_INT), VALUE :: enable
     INTEGER(C_LONG_LONG), INTENT(OUT) :: count_out
   END FUNCTION
+  INTEGER(C_INT) FUNCTION cumc_check_dv(seed, n, mismatches, example) BIND(C, NAME='cumc_check_dv')
+    IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
+    INTEGER(C_LONG_LONG), VALUE :: seed, n
+    INTEGER(C_LONG_LONG) :: mismatches
+    REAL(C_DOUBLE) :: example(2)
+  END FUNCTION
   INTEGER(C_INT) FUNCTION cumc_check_div3(seed, n, mismatches, example) BIND(C, NAME='cumc_check_div3')
     IMPORT :: C_INT, C_LONG_LONG, C_DOUBLE
     INTEGER(C_LONG_LONG), VALUE :: seed, n

@@ -234,6 +234,13 @@ int cumc_fallback_count(cumc_handle *h, int enable, unsigned long long *count_ou
  * normal inputs; *mismatches counts differing bit patterns. */
 int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example);
 
+/* Numerics self-check (no counterpart in the reference): compares the FP64
+ * engine's division (the IEEE quotient with a shortcut for a zero numerator)
+ * with x / y on n generated pairs, zeros, infinities, NaNs and subnormals
+ * among them; *mismatches counts differing results (any NaN equals any NaN),
+ * example[0..1] = one differing pair. */
+int cumc_check_dv(unsigned long long seed, long long n, unsigned long long *mismatches, double *example);
+
 /* Measured FP64 fused-multiply-add throughput of the current device in
  * TFLOP/s (the denominator of the FP64-pipe roofline). */
 int cumc_fp64_peak(double *tflops);

@@ -16,3 +16,13 @@ def test_fma_corrected_div3_equals_ieee_division():
         total += 1 << 30
     assert total == 1 << 32
 
+
+
+def test_zero_numerator_division_equals_ieee_division():
+    """The FP64 division of the flux and update kernels (a zero numerator
+    returns the signed zero without the division's slow path) against x / y:
+    2^28 pairs, a quarter of the numerators +-0, the denominators over every
+    exponent with zeros, infinities, NaNs and subnormals among them."""
+    for seed in (11, 12):
+        bad, ex = engine.check_dv(seed * 0x9E3779B9, 1 << 27)
+        assert bad == 0, "dv differs from x / y for (x, y) = %r" % (ex,)
