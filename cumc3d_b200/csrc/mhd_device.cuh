@@ -32,20 +32,21 @@ template <> __device__ __forceinline__ float dabs<float>(float x) { return fabsf
 // numerator (chosen in inline PTX, so the optimizer cannot put x back) is
 // discarded and the signed zero sign(x) * sign(y) returned; every other case
 // is the ordinary division.  The tests run on the integer pipe, which the
-// FP64-bound kernels leave idle.  FP32 divides directly.
+// FP64-bound kernels leave idle, on the 32-bit words of the operands (one
+// logic op and one compare per test).  FP32 divides directly.
 template <class T> __device__ __forceinline__ T dv(T x, T y) { return x / y; }
 template <> __device__ __forceinline__ double dv<double>(double x, double y) {
-    const unsigned long long xb = (unsigned long long)__double_as_longlong(x);
-    const unsigned long long yb = (unsigned long long)__double_as_longlong(y);
-    const unsigned ye = (unsigned)(yb >> 52) & 0x7FFu;  // biased exponent of y
-    const int z = ((xb << 1) == 0ull) & ((ye - 1u) < 0x7FEu);
-    unsigned long long nb;
-    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\tselp.b64 %0, 0x3FF0000000000000, %1, p;\n\t}"
-        : "=l"(nb)
-        : "l"(xb), "r"(z));
-    const double q = __longlong_as_double((long long)nb) / y;
-    const unsigned long long zb = (xb ^ yb) & 0x8000000000000000ull;
-    return z ? __longlong_as_double((long long)zb) : q;
+    const unsigned xh = (unsigned)__double2hiint(x), xl = (unsigned)__double2loint(x);
+    const unsigned yh = (unsigned)__double2hiint(y);
+    // x == +-0: no bit set but the sign; y normal: biased exponent 1..2046
+    const int z = (((xh & 0x7FFFFFFFu) | xl) == 0u) & (((yh & 0x7FF00000u) - 0x00100000u) < 0x7FE00000u);
+    unsigned nh, nl;
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\tselp.b32 %0, 0x3FF00000, %2, p;\n\tselp.b32 %1, 0, %3, p;\n\t}"
+        : "=r"(nh), "=r"(nl)
+        : "r"(xh), "r"(xl), "r"(z));
+    const double q = __hiloint2double((int)nh, (int)nl) / y;
+    const double zr = __hiloint2double((int)((xh ^ yh) & 0x80000000u), 0);
+    return z ? zr : q;
 }
 
 // Fortran SIGN(1, x)
