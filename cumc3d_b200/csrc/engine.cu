@@ -482,6 +482,8 @@ template <class FT>  // storage type of the hydro face fluxes (double, or float 
 __global__ void __launch_bounds__(128, 4) k_rk(const Dev d, int stage) {
     if (d.S->done) return;
     // flat index over j,k,l = 0..n (x fastest)
+    // (64-bit index arithmetic: the 32-bit form, cheaper in instructions,
+    // changes this kernel's register allocation and measured 10% slower)
     const int ex = d.nx + 1, ey = d.ny + 1, ez = d.nz + 1;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ex * ey * ez) return;

@@ -105,6 +105,18 @@ __device__ __forceinline__ int cidx(const Dev &d, int j, int k, int l) {
     return (j + 2) + d.NX * ((k + 2) + d.NY * (l + 2));
 }
 
+// (a, b, e) of a flat index t = a + ex (b + ey e).  Every flat count of a
+// grid the engine accepts fits 32 bits (its padded cells times 8 stay below
+// 2^31), so the divisions are 32-bit ones, several times cheaper than the
+// 64-bit division routine.
+__device__ __forceinline__ void unflat3(unsigned t, unsigned ex, unsigned ey, int &a, int &b, int &e) {
+    const unsigned r = t / ex;
+    a = (int)(t - r * ex);
+    const unsigned q = r / ey;
+    b = (int)(r - q * ey);
+    e = (int)q;
+}
+
 // host-side launchers of the face-flux kernels (one per precision unit)
 void launch_flux_fp64(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);
 void launch_flux_fp32(const Dev &d, int dir, int rec, int rs, dim3 grid, dim3 block, size_t smem, cudaStream_t s);

@@ -221,15 +221,13 @@ __global__ void __launch_bounds__(256) k_recon(const Dev d) {
     // padding per row: x extent nx+2 (x sweep) or nx, then y, then z
     int c, j, k, l, ns;
     {
-        const int ex = (DIR == 0) ? d.nx + 2 : d.nx;
-        const int ey = (DIR == 1) ? d.ny + 2 : d.ny;
-        const int ez = (DIR == 2) ? d.nz + 2 : d.nz;
-        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (t >= (long long)ex * ey * ez) return;
-        const int a = (int)(t % ex);
-        const long long r = t / ex;
-        const int b = (int)(r % ey);
-        const int e = (int)(r / ey);
+        const unsigned ex = (DIR == 0) ? d.nx + 2 : d.nx;
+        const unsigned ey = (DIR == 1) ? d.ny + 2 : d.ny;
+        const unsigned ez = (DIR == 2) ? d.nz + 2 : d.nz;
+        const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= ex * ey * ez) return;
+        int a, b, e;
+        unflat3(t, ex, ey, a, b, e);
         if (DIR == 0) { c = a; j = c; k = b + 1; l = e + 1; ns = d.nx; }
         else if (DIR == 1) { c = b; k = c; j = a + 1; l = e + 1; ns = d.ny; }
         else { c = e; l = c; j = a + 1; k = b + 1; ns = d.nz; }
@@ -289,15 +287,13 @@ __global__ void __launch_bounds__(128, MINB) k_riemann(const Dev d) {
     if (d.S->done) return;
     int f, j, k, l, ns;
     {
-        const int ex = (DIR == 0) ? d.nx + 1 : d.nx;
-        const int ey = (DIR == 1) ? d.ny + 1 : d.ny;
-        const int ez = (DIR == 2) ? d.nz + 1 : d.nz;
-        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (t >= (long long)ex * ey * ez) return;
-        const int a = (int)(t % ex);
-        const long long r = t / ex;
-        const int b = (int)(r % ey);
-        const int e = (int)(r / ey);
+        const unsigned ex = (DIR == 0) ? d.nx + 1 : d.nx;
+        const unsigned ey = (DIR == 1) ? d.ny + 1 : d.ny;
+        const unsigned ez = (DIR == 2) ? d.nz + 1 : d.nz;
+        const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t >= ex * ey * ez) return;
+        int a, b, e;
+        unflat3(t, ex, ey, a, b, e);
         if (DIR == 0) { f = a; j = f; k = b + 1; l = e + 1; ns = d.nx; }
         else if (DIR == 1) { f = b; k = f; j = a + 1; l = e + 1; ns = d.ny; }
         else { f = e; l = f; j = a + 1; k = b + 1; ns = d.nz; }
@@ -362,26 +358,24 @@ __global__ void __launch_bounds__(128, MINB) k_riemann_pf(const Dev d) {
     __shared__ T qb[2][14][128];
     __shared__ double bb[2][128];
     const int tid = threadIdx.x;
-    const int ex = (DIR == 0) ? d.nx + 1 : d.nx;
-    const int ey = (DIR == 1) ? d.ny + 1 : d.ny;
-    const int ez = (DIR == 2) ? d.nz + 1 : d.nz;
-    const long long total = (long long)ex * ey * ez;
-    const long long stride = (long long)gridDim.x * 128;
+    const unsigned ex = (DIR == 0) ? d.nx + 1 : d.nx;
+    const unsigned ey = (DIR == 1) ? d.ny + 1 : d.ny;
+    const unsigned ez = (DIR == 2) ? d.nz + 1 : d.nz;
+    const unsigned total = ex * ey * ez;
+    const unsigned stride = gridDim.x * 128;
     using F = Frame<DIR>;
     constexpr int tb1 = (DIR == 0) ? 1 : 0;
     constexpr int tb2 = (DIR == 2) ? 1 : 2;
     const T *const *QL = reinterpret_cast<const T *const *>(d.QL);
     const T *const *QR = reinterpret_cast<const T *const *>(d.QR);
-    auto face_index = [&](long long t) {
-        const int a = (int)(t % ex);
-        const long long r = t / ex;
-        const int b = (int)(r % ey);
-        const int e = (int)(r / ey);
+    auto face_index = [&](unsigned t) {
+        int a, b, e;
+        unflat3(t, ex, ey, a, b, e);
         if (DIR == 0) return cidx(d, a, b + 1, e + 1);
         if (DIR == 1) return cidx(d, a + 1, b, e + 1);
         return cidx(d, a + 1, b + 1, e);
     };
-    auto issue = [&](long long t, int buf) {
+    auto issue = [&](unsigned t, int buf) {
         if (t < total) {
             const int ci = face_index(t);
 #pragma unroll
@@ -393,7 +387,7 @@ __global__ void __launch_bounds__(128, MINB) k_riemann_pf(const Dev d) {
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    long long t = (long long)blockIdx.x * 128 + tid;
+    unsigned t = blockIdx.x * 128 + tid;
     issue(t, 0);
     for (int i = 0; t < total; ++i, t += stride) {
         issue(t + stride, (i + 1) & 1);
