@@ -2711,7 +2711,10 @@ int cumc_learn_harvest(cumc_handle *h, int dir, long long stride, float *out, lo
 int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mismatches, double *example) {
     unsigned long long *m = nullptr;
     double *ex = nullptr;
-    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, sizeof(*ex)) != cudaSuccess) return CUMC_ECUDA;
+    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, sizeof(*ex)) != cudaSuccess) {
+        cudaFree(m);  // (freeing a null pointer is a no-op)
+        return CUMC_ECUDA;
+    }
     cudaMemset(m, 0, sizeof(*m));
     cudaMemset(ex, 0, sizeof(*ex));
     k_div3_check<<<148 * 16, 256>>>(seed, n, m, ex);
@@ -2726,7 +2729,10 @@ int cumc_check_div3(unsigned long long seed, long long n, unsigned long long *mi
 int cumc_check_dv(unsigned long long seed, long long n, unsigned long long *mismatches, double *example) {
     unsigned long long *m = nullptr;
     double *ex = nullptr;
-    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, 2 * sizeof(*ex)) != cudaSuccess) return CUMC_ECUDA;
+    if (cudaMalloc(&m, sizeof(*m)) != cudaSuccess || cudaMalloc(&ex, 2 * sizeof(*ex)) != cudaSuccess) {
+        cudaFree(m);
+        return CUMC_ECUDA;
+    }
     cudaMemset(m, 0, sizeof(*m));
     cudaMemset(ex, 0, 2 * sizeof(*ex));
     k_dv_check<<<148 * 16, 256>>>(seed, n, m, ex);
