@@ -786,10 +786,11 @@ def torus_sph(nr=None, ntheta=None, nphi=None, faces=None, r_range=(1.5, 31.5), 
 # ---------------------------------------------------------------------------
 # self-gravitating star on a spherical grid: the setting of the collapsar
 # model's gravity solve (model/collapsar/src/custom.f90:489-620).  The
-# reference reads a progenitor profile from files it does not ship
-# (model/collapsar/src/model.f90:40-90); this stand-in is an analytic,
-# seeded one of the same shape: a centrally condensed star inside a
-# tenuous atmosphere, rotating differentially.
+# model itself, from the progenitor files the reference ships
+# (model/collapsar/profile, read by model.f90:44-105), is collapsar_model
+# below; this analytic, seeded star of the same shape (a centrally
+# condensed star inside a tenuous atmosphere, rotating differentially) is
+# the small, fast setting of the tests.
 # ---------------------------------------------------------------------------
 def star_sph(nr=96, ntheta=48, nphi=48, r_range=(2.0, 40.0), theta_range=(0.1 * math.pi, 0.9 * math.pi), rho_c=1.0,
              r_core=2.0, r_star=20.0, rho_atm=1e-6, p_atm=1e-8, asym=0.05, seed=20261203, recon="weno",
