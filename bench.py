@@ -911,23 +911,30 @@ def bench_config(args, world, rank, local, dist):
         # problem; bit-identical to the 3D engine): one launch instead of ~60
         # graph nodes per step
         bs = engine.BatchSolver([spec])
-        for _ in range(args.warmup):
-            bs.set_state(0, prim, eps)
-            bs.run()
-        bs.set_state(0, prim, eps)
         stb = torch.cuda.ExternalStream(bs.stream())
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stb)
-        _, bsteps, _ = bs.run()
-        e1.record(stb)
-        torch.cuda.synchronize()
-        bms = e0.elapsed_time(e1)
+        pk = {}
+        # one CTA (the batch default for problems of up to 1024 cells), and the
+        # problem shared by an 8-CTA cluster (one cell per thread): a single
+        # problem's time is its steps' latency, which more threads shorten
+        for label, shape in (("one_cta", (8, 1024)), ("cluster_of_8", (8, 128))):
+            bs.set_cluster(*shape)
+            for _ in range(args.warmup):
+                bs.set_state(0, prim, eps)
+                bs.run()
+            bs.set_state(0, prim, eps)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stb)
+            _, bsteps, _ = bs.run()
+            e1.record(stb)
+            torch.cuda.synchronize()
+            bms = e0.elapsed_time(e1)
+            pk[label] = {"zone_updates_per_s": zones * int(bsteps[0]) / (bms * 1e-3), "steps": int(bsteps[0]),
+                         "ms": bms}
         bs.close()
-        extra["persistent_1d_kernel"] = {"zone_updates_per_s": zones * int(bsteps[0]) / (bms * 1e-3),
-                                         "steps": int(bsteps[0]), "ms": bms,
-                                         "note": "cumc_batch_run with this one problem (INITIAL_UPDATE included)"}
+        extra["persistent_1d_kernel"] = dict(pk, note="cumc_batch_run with this one problem (INITIAL_UPDATE "
+                                                      "included); results bit-identical for both shapes")
         if not args.no_cpu:
             cpu = cpu_baseline_of(lambda: models.brio_wu(800, recon=spec["recon"], riemann=spec["riemann"]), 100,
                                   "CPU oracle, Brio-Wu 800 zones, 100 RK3 steps")
