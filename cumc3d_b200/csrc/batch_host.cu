@@ -25,6 +25,7 @@ struct cumc_batch {
     std::string err;
     int sm_count = 148;
     int cluster_size = BATCH_CLUSTER;  // CTAs that share one large problem
+    int coop_min_n = -1;               // set by cumc_batch_set_cluster; -1: chosen per run
     int64_t launches = 0;
 };
 
@@ -187,6 +188,16 @@ int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, 
     if (!b) return bfail(b, CUMC_EINVAL, "null batch");
     b->d.max_steps = max_steps > 0 ? max_steps : 0x7fffffff;
     if (cudaMemsetAsync(b->d.next, 0, sizeof(int), b->stream) != cudaSuccess) return bfail(b, CUMC_ECUDA, "memset failed");
+    // sharing threshold: a batch no larger than the clusters that can be
+    // resident at once (two 256-thread CTAs per SM) leaves SMs idle, so its
+    // problems are shared from 256 cells up (one cell per thread and fewer
+    // steps' worth of latency); a larger one shares only its largest problems
+    if (b->coop_min_n < 0) {
+        const int resident = b->cluster_size > 1 ? 2 * b->sm_count / b->cluster_size : 2 * b->sm_count;
+        b->d.coop_min_n = b->nprob <= resident ? BATCH_COOP_MIN_N_FEW : BATCH_COOP_MIN_N;
+    } else {
+        b->d.coop_min_n = b->coop_min_n;
+    }
     cudaError_t e = b->precision == CUMC_FP32
                         ? launch_batch_fp32(b->d, b->recon, b->riemann, 0, b->cluster_size, b->stream)
                         : launch_batch_fp64(b->d, b->recon, b->riemann, 0, b->cluster_size, b->stream);
@@ -218,7 +229,7 @@ int cumc_batch_set_cluster(cumc_batch *b, int cluster_size, int coop_min_n) {
         coop_min_n < 1)
         return bfail(b, CUMC_EINVAL, "cluster size must be 1, 2, 4, 8 or 16 and coop_min_n >= 1");
     b->cluster_size = cluster_size;
-    b->d.coop_min_n = coop_min_n;
+    b->coop_min_n = coop_min_n;
     return CUMC_OK;
 }
 

@@ -96,6 +96,7 @@ __device__ __forceinline__ void batch_floor(const BatchDev &b, double &e) {
 constexpr int BATCH_THREADS = 256;
 constexpr int BATCH_CLUSTER = 8;          // CTAs that share one large problem
 constexpr int BATCH_COOP_MIN_N = 1024;    // default: problems of at most this many cells run on one CTA
+constexpr int BATCH_COOP_MIN_N_FEW = 256; // the same when every problem can have a cluster of its own
 
 struct BatchShared {
     unsigned long long part_dt;  // this CTA's FINDDT minimum (bit pattern)

@@ -279,7 +279,9 @@ int cumc_batch_run(cumc_batch *b, int max_steps, double *t_out, int *steps_out, 
  * than coop_min_n cells are shared by a thread-block cluster of cluster_size
  * CTAs (1, 2, 4, 8 or 16; 16 is a non-portable size and falls back to one
  * CTA per problem where the device cannot place it), smaller ones run one
- * per CTA.  Defaults 8 and 1024.  Results do not depend on it. */
+ * per CTA.  Defaults: 8, and 1024 for batches larger than the clusters the
+ * device holds at once, 256 for smaller ones (whose problems then get a
+ * cluster each).  Results do not depend on it. */
 int cumc_batch_set_cluster(cumc_batch *b, int cluster_size, int coop_min_n);
 int cumc_batch_sync(cumc_batch *b);
 void *cumc_batch_stream(cumc_batch *b);
